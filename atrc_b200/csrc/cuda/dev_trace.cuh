@@ -1,0 +1,270 @@
+// Two-level BVH traversal (top level over entities, bottom level per leaf
+// geometry) with the reference's ray-primitive tests.
+//
+// Replaces, for a batch of rays, the reference's EntityBVH / NativeAggregate
+// traversal (src/tracer/src/core/aggregate/entity_bvh.cpp:118-172), the
+// transform_wrapper ray transform (src/tracer/src/core/geometry/
+// transform_wrapper.cpp:51-68), the per-mesh BVH
+// (src/tracer/src/core/geometry/triangle_bvh.cpp:363-488) and the
+// Moller-Trumbore test (src/tracer/include/agz/tracer/utility/
+// triangle_aux.h:9-69).  In EXACT mode every float operation of the ray
+// transform and of Moller-Trumbore is evaluated in the reference's order
+// without fused multiply-adds, so hit distances are bit-identical.
+#pragma once
+
+#include <climits>
+
+#include "dev_math.cuh"
+#include "dev_scene.h"
+
+namespace atrc {
+namespace dev {
+
+constexpr int kStackSize = 96;
+constexpr int32_t kSentinel = INT_MIN;  // "return from a bottom-level tree"
+
+struct Hit {
+    float t;
+    float u, v;      // barycentrics (alpha, beta) for triangles
+    int32_t entity;  // -1 when nothing was hit
+    int32_t tri;     // pool triangle index (-1 for analytic shapes)
+};
+
+struct RayState {
+    Vec3 o, d, inv;
+    float tmin, tmax;
+};
+
+__device__ __forceinline__ Vec3 safe_inv(Vec3 d) { return Vec3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z); }
+
+// Slab test of two child boxes.  The far distance is widened by a few ulps
+// so that float rounding cannot cull a box that a primitive test would hit.
+__device__ __forceinline__ void box2(const float4& n0, const float4& n1, const float4& n2, const RayState& r,
+                                     bool* h0, float* t0, bool* h1, float* t1) {
+    const float ox = r.o.x * r.inv.x, oy = r.o.y * r.inv.y, oz = r.o.z * r.inv.z;
+    float a0 = fmaf(n0.x, r.inv.x, -ox), b0 = fmaf(n0.y, r.inv.x, -ox);
+    float a1 = fmaf(n0.z, r.inv.y, -oy), b1 = fmaf(n0.w, r.inv.y, -oy);
+    float a2 = fmaf(n2.x, r.inv.z, -oz), b2 = fmaf(n2.y, r.inv.z, -oz);
+    float lo = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), r.tmin));
+    float hi = fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fminf(fmaxf(a2, b2), r.tmax));
+    *h0 = lo <= hi * 1.0000005f + 1e-30f;
+    *t0 = lo;
+    a0 = fmaf(n1.x, r.inv.x, -ox); b0 = fmaf(n1.y, r.inv.x, -ox);
+    a1 = fmaf(n1.z, r.inv.y, -oy); b1 = fmaf(n1.w, r.inv.y, -oy);
+    a2 = fmaf(n2.z, r.inv.z, -oz); b2 = fmaf(n2.w, r.inv.z, -oz);
+    lo = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), r.tmin));
+    hi = fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fminf(fmaxf(a2, b2), r.tmax));
+    *h1 = lo <= hi * 1.0000005f + 1e-30f;
+    *t1 = lo;
+}
+
+// Moller-Trumbore.  ANY selects has_intersection_with_triangle (alpha <= 1
+// also checked), otherwise closest_intersection_with_triangle.
+template <bool EXACT, bool ANY>
+__device__ __forceinline__ bool mt_test(const RayState& r, const float4& p0, const float4& p1, const float4& p2,
+                                        float tmax, float* t_out, float* u_out, float* v_out) {
+    const Vec3 A(p0.x, p0.y, p0.z), B_A(p1.x, p1.y, p1.z), C_A(p2.x, p2.y, p2.z);
+    if (EXACT) {
+        const Vec3 s1 = cross_rn(r.d, C_A);
+        const float div = dot_rn(s1, B_A);
+        if (div == 0.0f) return false;
+        const float inv_div = __fdiv_rn(1.0f, div);
+        const Vec3 o_A = sub_rn(r.o, A);
+        const float alpha = __fmul_rn(dot_rn(o_A, s1), inv_div);
+        if (alpha < 0 || (ANY && alpha > 1)) return false;
+        const Vec3 s2 = cross_rn(o_A, B_A);
+        const float beta = __fmul_rn(dot_rn(r.d, s2), inv_div);
+        if (beta < 0 || __fadd_rn(alpha, beta) > 1) return false;
+        const float t = __fmul_rn(dot_rn(C_A, s2), inv_div);
+        if (!(r.tmin <= t && t <= tmax)) return false;
+        *t_out = t;
+        *u_out = alpha;
+        *v_out = beta;
+        return true;
+    } else {
+        const Vec3 s1 = cross(r.d, C_A);
+        const float div = dot(s1, B_A);
+        if (div == 0.0f) return false;
+        const float inv_div = 1.0f / div;
+        const Vec3 o_A = r.o - A;
+        const float alpha = dot(o_A, s1) * inv_div;
+        if (alpha < 0 || (ANY && alpha > 1)) return false;
+        const Vec3 s2 = cross(o_A, B_A);
+        const float beta = dot(r.d, s2) * inv_div;
+        if (beta < 0 || alpha + beta > 1) return false;
+        const float t = dot(C_A, s2) * inv_div;
+        if (!(r.tmin <= t && t <= tmax)) return false;
+        *t_out = t;
+        *u_out = alpha;
+        *v_out = beta;
+        return true;
+    }
+}
+
+// Sphere (sphere_aux.h:53-86) in local space.
+template <bool ANY>
+__device__ __forceinline__ bool sphere_test(const RayState& r, float radius, float tmax, float* t_out) {
+    const float A = dot(r.d, r.d), B = 2 * dot(r.d, r.o), C = dot(r.o, r.o) - radius * radius;
+    float delta = B * B - 4 * A * C;
+    if (delta < 0) return false;
+    delta = sqrtf(delta);
+    const float inv2A = 0.5f / A;
+    const float t0 = (-B - delta) * inv2A, t1 = (-B + delta) * inv2A;
+    if (ANY) {
+        if (r.tmin <= t0 && t0 <= tmax) { *t_out = t0; return true; }
+        if (r.tmin <= t1 && t1 <= tmax) { *t_out = t1; return true; }
+        return false;
+    }
+    if (tmax < t0 || t1 < r.tmin) return false;
+    const bool not_t0 = t0 < r.tmin;
+    if (not_t0 && t1 > tmax) return false;
+    *t_out = not_t0 ? t1 : t0;
+    return true;
+}
+
+// Disk (disk.cpp:43-74) in local space.
+__device__ __forceinline__ bool disk_test(const RayState& r, float radius, float tmax, float* t_out) {
+    const float t = -r.o.z / r.d.z;
+    if (isinf(t) || !(r.tmin <= t && t <= tmax)) return false;
+    const float px = r.o.x + t * r.d.x, py = r.o.y + t * r.d.y;
+    if (px * px + py * py > radius * radius) return false;
+    *t_out = t;
+    return true;
+}
+
+__device__ __forceinline__ void load_node(const BvhNode* nodes, int32_t i, float4* n0, float4* n1, float4* n2,
+                                          int2* links) {
+    const float4* p = reinterpret_cast<const float4*>(nodes + i);
+    *n0 = __ldg(p);
+    *n1 = __ldg(p + 1);
+    *n2 = __ldg(p + 2);
+    const float4 n3 = __ldg(p + 3);
+    *links = make_int2(__float_as_int(n3.x), __float_as_int(n3.y));
+}
+
+// Move a world ray into an entity's primitive space (wrapper, then the
+// geometry's own transform), as transform_wrapper / TransformedGeometry do.
+template <bool EXACT>
+__device__ __forceinline__ void to_entity_space(const Entity& e, Vec3 o, Vec3 d, Vec3* lo, Vec3* ld) {
+    if (e.flags & ENT_WRAP) {
+        o = apply_point_rn(e.wrap_inv, o);
+        d = apply_vector_rn(e.wrap_inv, d);
+    }
+    if (e.flags & ENT_LOCAL) {
+        o = apply_point_rn(e.local_inv, o);
+        d = apply_vector_rn(e.local_inv, d);
+    }
+    *lo = o;
+    *ld = d;
+}
+
+// Trace one ray.  Returns true if something was hit (ANY: occluded).
+// `watchdog` is set when the traversal stack would overflow.
+template <bool EXACT, bool ANY>
+__device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog) {
+    if (S.entity_count == 0) return false;
+    int32_t stack[kStackSize];
+    int sp = 0;
+    RayState r;
+    r.o = wo; r.d = wd; r.inv = safe_inv(wd); r.tmin = tmin; r.tmax = tmax;
+    const Vec3 winv = r.inv;
+    float best_t = tmax;
+    int32_t best_e = -1, best_tri = -1;
+    float best_u = 0, best_v = 0;
+    int32_t cur_entity = -1;
+    int32_t link = S.tlas_root;
+    for (;;) {
+        // descend interior nodes
+        while (link >= 0) {
+            float4 n0, n1, n2;
+            int2 lk;
+            load_node(S.nodes, link, &n0, &n1, &n2, &lk);
+            bool h0, h1;
+            float t0, t1;
+            box2(n0, n1, n2, r, &h0, &t0, &h1, &t1);
+            if (h0 && h1) {
+                int32_t nearl = t0 <= t1 ? lk.x : lk.y, farl = t0 <= t1 ? lk.y : lk.x;
+                if (sp >= kStackSize) { *watchdog = 1; goto done; }
+                stack[sp++] = farl;
+                link = nearl;
+            } else if (h0) {
+                link = lk.x;
+            } else if (h1) {
+                link = lk.y;
+            } else {
+                goto pop;
+            }
+        }
+        // leaf
+        {
+            const uint32_t enc = uint32_t(~link);
+            const int32_t first = int32_t(enc >> 4), count = int32_t(enc & 15) + 1;
+            if (cur_entity < 0) {
+                // top-level leaf: one entity per leaf slot
+                for (int32_t k = 0; k < count; ++k) {
+                    const int32_t ei = int32_t(__ldg(S.tlas_order + first + k));
+                    const Entity& e = S.entities[ei];
+                    Vec3 lo, ld;
+                    to_entity_space<EXACT>(e, wo, wd, &lo, &ld);
+                    if (e.kind == LEAF_TRIANGLES) {
+                        if (count != 1) { *watchdog = 2; goto done; }  // builder guarantees 1
+                        if (sp >= kStackSize) { *watchdog = 1; goto done; }
+                        stack[sp++] = kSentinel;
+                        r.o = lo; r.d = ld; r.inv = safe_inv(ld);
+                        cur_entity = ei;
+                        link = e.blas_root;
+                        goto next;
+                    }
+                    RayState lr;
+                    lr.o = lo; lr.d = ld; lr.tmin = tmin; lr.inv = Vec3();
+                    float t;
+                    bool h = e.kind == LEAF_SPHERE ? sphere_test<ANY>(lr, e.radius, best_t, &t)
+                                                   : disk_test(lr, e.radius, best_t, &t);
+                    if (h) {
+                        if (ANY) { hit->entity = ei; hit->t = t; return true; }
+                        if (t < best_t || (t == best_t && ei < best_e)) {
+                            best_t = t; best_e = ei; best_tri = -1; best_u = 0; best_v = 0;
+                            r.tmax = t;
+                        }
+                    }
+                }
+            } else {
+                for (int32_t k = 0; k < count; ++k) {
+                    const int32_t ti = first + k;
+                    const float4* tp = reinterpret_cast<const float4*>(S.tris) + size_t(ti) * 3;
+                    const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+                    float t, u, v;
+                    if (mt_test<EXACT, ANY>(r, p0, p1, p2, best_t, &t, &u, &v)) {
+                        if (ANY) { hit->entity = cur_entity; hit->t = t; return true; }
+                        if (t < best_t || (t == best_t && (cur_entity < best_e || (cur_entity == best_e && ti < best_tri)))) {
+                            best_t = t; best_e = cur_entity; best_tri = ti; best_u = u; best_v = v;
+                            r.tmax = t;
+                        }
+                    }
+                }
+            }
+        }
+    pop:
+        for (;;) {
+            if (sp == 0) goto done;
+            link = stack[--sp];
+            if (link != kSentinel) break;
+            // back to the top level
+            cur_entity = -1;
+            r.o = wo; r.d = wd; r.inv = winv;
+        }
+    next:;
+    }
+done:
+    if (ANY) return false;
+    if (best_e < 0) return false;
+    hit->t = best_t;
+    hit->u = best_u;
+    hit->v = best_v;
+    hit->entity = best_e;
+    hit->tri = best_tri;
+    return true;
+}
+
+}  // namespace dev
+}  // namespace atrc

@@ -1,0 +1,975 @@
+// Wavefront path tracer (`pt_cuda`) and the device half of the C ABI.
+//
+// Replaces PerPixelRenderer::render / render_grid
+// (src/tracer/src/core/renderer/perpixel_renderer.cpp:13-207) driving
+// render::trace_std (src/tracer/src/render/path_tracing.cpp:15-225) with the
+// MIS direct lighting of src/tracer/src/render/direct_illum.cpp:11-278.
+//
+// Structure: a pool of P path slots in HBM (structure of arrays); every
+// iteration runs six kernels over device-side queues, so the host never reads
+// queue sizes inside the loop:
+//   begin     - 1 thread: flip queues, plan how many new camera samples to take
+//   generate  - camera rays for free slots (thin_lens.cpp:74-94)
+//   extend    - closest hit for every queued path
+//   shade     - resolve the previous vertex's MIS-BSDF term, Russian roulette,
+//               medium sampling, emission, next-event estimation (one shadow
+//               ray per light), BSDF sampling
+//   shadow    - any hit for the shadow queue, unoccluded contributions added
+//   finish    - FP64 film splat of completed paths, slots returned
+// The BSDF sample of a vertex serves both as the MIS-BSDF ray of
+// mis_sample_bsdf and as the continuation ray (the reference draws two
+// independent samples from the same distribution; the expectation of both
+// terms is unchanged), which saves one closest-hit ray per vertex.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/atrc_cuda.h"
+#include "../host/scene_build.h"
+#include "dev_math.cuh"
+#include "dev_scene.h"
+#include "dev_shade.cuh"
+#include "dev_trace.cuh"
+
+namespace atrc {
+
+void set_last_error(const std::string& msg);  // capi_host.cpp
+
+namespace {
+
+using namespace dev;
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(x)                                                                                     \
+    do {                                                                                          \
+        cudaError_t err_ = (x);                                                                   \
+        if (err_ != cudaSuccess)                                                                  \
+            throw CudaError(std::string(#x) + ": " + cudaGetErrorString(err_));                   \
+    } while (0)
+
+// ---------------------------------------------------------------- buffers
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { if (p) cudaFree(p); }
+    void alloc(size_t b) {
+        if (p) { cudaFree(p); p = nullptr; }
+        bytes = b;
+        if (b) {
+            cudaError_t e = cudaMalloc(&p, b);
+            if (e != cudaSuccess) {
+                p = nullptr;
+                throw CudaError(std::string("cudaMalloc of ") + std::to_string(b) + " bytes: " + cudaGetErrorString(e));
+            }
+        }
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+template <class T>
+const T* upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
+    if (v.empty()) return nullptr;
+    b.alloc(v.size() * sizeof(T));
+    CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    return b.as<T>();
+}
+
+// ------------------------------------------------------- warp aggregation
+__device__ __forceinline__ int warp_append(int* counter, bool pred) {
+    const unsigned active = __activemask();
+    const unsigned mask = __ballot_sync(active, pred);
+    if (!pred) return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// ------------------------------------------------------------ ray queries
+template <bool EXACT, bool ANY>
+__global__ void k_trace_rays(Scene S, const AtrcRay* __restrict__ rays, size_t n, AtrcHit* __restrict__ hits,
+                             int* watchdog) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const AtrcRay q = rays[i];
+        Hit h;
+        h.entity = -1;
+        int wd = 0;
+        const bool hit = trace_ray<EXACT, ANY>(S, Vec3(q.o[0], q.o[1], q.o[2]), Vec3(q.d[0], q.d[1], q.d[2]), q.t_min,
+                                               q.t_max, &h, &wd);
+        if (wd) atomicMax(watchdog, wd);
+        AtrcHit r;
+        if (ANY) {
+            r.t = hit ? 1.0f : -1.0f;
+            r.entity = hit ? 0 : -1;
+            r.prim = 0;
+            r.u = 0;
+        } else if (hit) {
+            r.t = h.t;
+            r.entity = h.entity;
+            r.prim = h.tri >= 0 ? int32_t(S.tri_orig[h.tri]) : 0;
+            r.u = h.u;
+        } else {
+            r.t = -1;
+            r.entity = -1;
+            r.prim = -1;
+            r.u = 0;
+        }
+        hits[i] = r;
+    }
+}
+
+// ------------------------------------------------------------ wavefront
+enum PathFlags : int {
+    PF_MIS = 1,        // a MIS-BSDF term waits for this ray's hit
+    PF_MIS_DELTA = 2,  // ... from a delta (specular) sample
+    PF_TERMINATE = 4,  // finish after resolving the pending MIS term
+};
+
+struct Counters {
+    int in, out;              // queue buffers read / written this iteration
+    int n_ext, n_next;        // paths to extend / continuations written
+    int n_shadow, n_finish;
+    int n_free, n_new, n_cont, free_base;
+    unsigned long long gen_base, issued, total, completed;
+    unsigned long long rays_closest, rays_shadow, iterations;
+    int watchdog, done;
+};
+
+struct Camera {
+    float pos[3], fx[3], fy[3], fz[3];
+    float film_w, film_h, focal, lens_radius;
+};
+
+struct Params {
+    int W, H;
+    int first_spp;
+    int min_depth, max_depth, specular_depth;
+    float cont_prob, eps;
+    unsigned long long seed;
+    Camera cam;
+    int filter_type;
+    float filter_radius, filter_value, filter_alpha, filter_exp;
+};
+
+struct Pool {
+    float4 *ray_o, *ray_d;        // o.xyz tmin / d.xyz tmax
+    float4* hit;                  // t, u, v, entity(bits)
+    int* hit_tri;
+    float4* coef;                 // coef.xyz, mis_pdf
+    float4* L;                    // radiance.xyz, film x
+    float4* mis_f;                // pending MIS numerator.xyz, film y
+    float4* gb_albedo;            // albedo.xyz, denoise
+    float4* gb_normal;            // normal.xyz
+    uint4* st;                    // pixel, rng lo, rng hi, unused
+    int4* ctr;                    // depth, s_depth, scattering_count, flags | medium << 8
+    int* q[2];                    // extend queues
+    int* q_finish;
+    int* free_list;
+    float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
+    int shadow_cap;
+};
+
+struct Film {
+    double *value, *weight, *value_sq, *albedo, *normal, *denoise;
+};
+
+__global__ void k_init(Pool P, int cap, Counters* c, unsigned long long total) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < cap) P.free_list[i] = i;
+    if (i == 0) {
+        memset(c, 0, sizeof(Counters));
+        c->n_free = cap;
+        c->total = total;
+        c->out = 0;
+    }
+}
+
+__global__ void k_begin(Counters* c) {
+    c->iterations++;
+    c->rays_shadow += c->n_shadow;
+    c->n_free += c->n_finish;
+    c->completed += c->n_finish;
+    const int n_cont = c->n_next;
+    c->in = c->out;
+    c->out = c->in ^ 1;
+    const unsigned long long remaining = c->total - c->issued;
+    const int n_new = int(remaining < (unsigned long long)c->n_free ? remaining : (unsigned long long)c->n_free);
+    c->gen_base = c->issued;
+    c->issued += n_new;
+    c->free_base = c->n_free - n_new;
+    c->n_free = c->free_base;
+    c->n_new = n_new;
+    c->n_cont = n_cont;
+    c->n_ext = n_cont + n_new;
+    c->rays_closest += c->n_ext;
+    c->n_next = 0;
+    c->n_shadow = 0;
+    c->n_finish = 0;
+    if (c->n_ext == 0) c->done = 1;
+}
+
+__device__ __forceinline__ Rng load_rng(const uint4& s) { Rng r; r.state = (uint64_t(s.z) << 32) | s.y; return r; }
+__device__ __forceinline__ void store_rng(uint4& s, const Rng& r) { s.y = uint32_t(r.state); s.z = uint32_t(r.state >> 32); }
+__device__ __forceinline__ Vec3 xyz(const float4& v) { return Vec3(v.x, v.y, v.z); }
+
+__global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
+    const int n = c->n_new, base = c->n_cont, fb = c->free_base, in = c->in;
+    const unsigned long long gen = c->gen_base;
+    const unsigned long long npix = (unsigned long long)p.W * p.H;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = P.free_list[fb + i];
+        const unsigned long long k = gen + i;
+        const unsigned long long pixel = k % npix;
+        const unsigned long long s = (unsigned long long)p.first_spp + k / npix;
+        Rng rng;
+        rng.state = mix64(p.seed ^ mix64(pixel * 0x9E3779B97F4A7C15ULL + s * 0xD1B54A32D192ED03ULL + 1));
+        const int px = int(pixel % p.W), py = int(pixel / p.W);
+        // render_grid (perpixel_renderer.cpp:27-36) + ThinLensCamera::sample_we
+        const float fx = px + rng.u(), fy = py + rng.u();
+        const float film_x = fx / p.W, film_y = fy / p.H;
+        const float au = rng.u(), av = rng.u();
+        const Camera& cam = p.cam;
+        const Vec3 focal((0.5f - film_x) * cam.film_w, (film_y - 0.5f) * cam.film_h, cam.focal);
+        float dx, dy;
+        concentric_disk(au, av, &dx, &dy);
+        const Vec3 lens(cam.lens_radius * dx, cam.lens_radius * dy, 0);
+        const Vec3 FX(cam.fx[0], cam.fx[1], cam.fx[2]), FY(cam.fy[0], cam.fy[1], cam.fy[2]), FZ(cam.fz[0], cam.fz[1], cam.fz[2]);
+        const Vec3 o = Vec3(cam.pos[0], cam.pos[1], cam.pos[2]) + FX * lens.x + FY * lens.y;
+        const Vec3 ld = focal - lens;
+        const Vec3 d = normalize(FX * ld.x + FY * ld.y + FZ * ld.z);
+        P.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+        P.ray_d[slot] = make_float4(d.x, d.y, d.z, INFINITY);
+        P.coef[slot] = make_float4(1, 1, 1, 0);
+        P.L[slot] = make_float4(0, 0, 0, fx);
+        P.mis_f[slot] = make_float4(0, 0, 0, fy);
+        P.gb_albedo[slot] = make_float4(0, 0, 0, 1);
+        P.gb_normal[slot] = make_float4(0, 0, 0, 0);
+        uint4 st;
+        st.x = uint32_t(pixel);
+        st.w = 0;
+        store_rng(st, rng);
+        P.st[slot] = st;
+        P.ctr[slot] = make_int4(1, 1, 0, 0);
+        P.q[in][base + i] = slot;
+    }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(128) k_extend(Scene S, Pool P, Counters* c) {
+    const int n = c->n_ext, in = c->in;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = P.q[in][i];
+        const float4 o = P.ray_o[slot], d = P.ray_d[slot];
+        Hit h;
+        h.entity = -1;
+        h.tri = -1;
+        int wd = 0;
+        const bool hit = trace_ray<EXACT, false>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd);
+        if (wd) atomicMax(&c->watchdog, wd);
+        P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.entity : -1));
+        P.hit_tri[slot] = h.tri;
+    }
+}
+
+__device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d, float tmin, float tmax, Vec3 contrib,
+                                            int slot) {
+    const int k = warp_append(&c->n_shadow, true);
+    if (k >= P.shadow_cap) { atomicMax(&c->watchdog, 4); return; }
+    P.sh_o[k] = make_float4(o.x, o.y, o.z, tmin);
+    P.sh_d[k] = make_float4(d.x, d.y, d.z, tmax);
+    P.sh_c[k] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(slot));
+}
+
+__global__ void __launch_bounds__(128) k_shade(Scene S, Params p, Pool P, Counters* c) {
+    const int n = c->n_ext, in = c->in, out = c->out;
+    const float eps = p.eps;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = P.q[in][i];
+        int4 ct = P.ctr[slot];
+        int depth = ct.x, s_depth = ct.y, scat = ct.z, flags = ct.w & 0xff, ray_med = ct.w >> 8;
+        uint4 st = P.st[slot];
+        Rng rng = load_rng(st);
+        const float4 ro = P.ray_o[slot], rd = P.ray_d[slot];
+        const Vec3 o = xyz(ro), d = xyz(rd);
+        const float4 hv = P.hit[slot];
+        const int ent = __float_as_int(hv.w);
+        float4 coef4 = P.coef[slot];
+        Vec3 coef = xyz(coef4);
+        float4 L4 = P.L[slot];
+        Vec3 L = xyz(L4);
+        float4 mf4 = P.mis_f[slot];
+        int wd = 0;
+        bool finish = false, cont = false;
+        Surface s;
+        bool have_surface = false;
+        if (ent >= 0) {
+            Hit h;
+            h.t = hv.x; h.u = hv.y; h.v = hv.z; h.entity = ent; h.tri = P.hit_tri[slot];
+            s = make_surface(S, h, o, d);
+            have_surface = true;
+        }
+        // (1) pending MIS-BSDF term of the previous vertex (direct_illum.cpp:130-192)
+        if (flags & PF_MIS) {
+            const Vec3 mis_f = xyz(mf4);
+            const float mis_pdf = coef4.w;
+            if (!have_surface) {
+                if (S.env.type != ATRC_ENV_NONE) {
+                    const Vec3 le = env_radiance(S, d);
+                    if (!black(le)) L += mis_f * le / ((flags & PF_MIS_DELTA) ? mis_pdf : mis_pdf + env_pdf(S, d));
+                }
+            } else {
+                const Entity& e = S.entities[ent];
+                if (e.flags & ENT_LIGHT) {
+                    const Vec3 le = area_light_radiance(e, s.geo.z, s.wr);
+                    if (!black(le)) {
+                        const Vec3 tr = medium_tr(S, ray_med, o, s.pos, rng, &wd);
+                        const Vec3 f = tr * le * mis_f;
+                        L += (flags & PF_MIS_DELTA) ? f / mis_pdf : f / (mis_pdf + area_light_pdf(S, e, o, s.pos, s.geo.z));
+                    }
+                }
+            }
+            flags &= ~(PF_MIS | PF_MIS_DELTA);
+        }
+        if ((flags & PF_TERMINATE) || depth > p.max_depth) finish = true;
+        // (2) Russian roulette (path_tracing.cpp:30-35)
+        if (!finish && depth > p.min_depth) {
+            if (rng.u() > p.cont_prob) finish = true;
+            else coef = coef / p.cont_prob;
+        }
+        if (!finish && !have_surface) {
+            if (depth == 1 && S.env.type != ATRC_ENV_NONE) L += coef * env_radiance(S, d);
+            finish = true;
+        }
+        if (!finish) {
+            const Entity& e = S.entities[ent];
+            Vec3 sn;
+            const BSDF b = shade(S, s, &sn);
+            if (depth == 1) {
+                const Vec3 alb = bsdf_albedo(b);
+                P.gb_albedo[slot] = make_float4(alb.x, alb.y, alb.z, (e.flags & ENT_NO_DENOISE) ? 0.0f : 1.0f);
+                P.gb_normal[slot] = make_float4(sn.x, sn.y, sn.z, 0);
+            }
+            bool scattered = false;
+            Vec3 spos, swr;
+            Phase ph;
+            int med = dot(s.wr, s.geo.z) >= 0 ? e.med_out : e.med_in;
+            if (S.has_media) {
+                if (scat < S.media[med].max_scattering_count) {
+                    Vec3 tp;
+                    scattered = medium_sample(S, med, o, s.pos, scat > 0, rng, &tp, &spos, &swr, &ph, &wd);
+                    coef *= tp;
+                } else {
+                    coef *= medium_ab(S, med, o, s.pos, rng, &wd);
+                }
+            }
+            if (scattered) {
+                // medium vertex (path_tracing.cpp:73-104)
+                ++scat;
+                for (int li = 0; li < S.light_count; ++li) {
+                    const int le_i = S.light_entity[li];
+                    if (le_i < 0) continue;  // env NEE from a medium point is 0 (direct_illum.cpp:101-108)
+                    LightSample ls;
+                    const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+                    if (!area_light_sample(S, S.entities[le_i], spos, u0, u1, u2, &ls)) continue;
+                    if (black(ls.rad) || ls.pdf == 0.0f) continue;
+                    const Vec3 to_light = normalize(ls.pos - spos);
+                    const float fph = hg_pdf(ph, to_light, swr);
+                    if (fph == 0.0f) continue;
+                    const Vec3 tr = medium_tr(S, med, spos, ls.pos, rng, &wd);
+                    const Vec3 contrib = coef * tr * ls.rad * fph / (ls.pdf + fph);
+                    const float dis = length(ls.pos - spos);
+                    push_shadow(P, c, ls.pos, normalize(spos - ls.pos), eps, dis - eps, contrib, slot);
+                }
+                const BSDFSample bs = hg_sample(ph, swr, rng.u(), rng.u());
+                if (black(bs.f)) {
+                    finish = true;
+                } else {
+                    const Vec3 dir = normalize(bs.dir);
+                    mf4 = make_float4(coef.x * bs.f.x, coef.y * bs.f.y, coef.z * bs.f.z, mf4.w);
+                    coef4.w = bs.pdf;
+                    flags |= PF_MIS;
+                    ray_med = med;
+                    if (bs.pdf < eps) flags |= PF_TERMINATE;
+                    else coef = coef * bs.f / bs.pdf;
+                    P.ray_o[slot] = make_float4(spos.x, spos.y, spos.z, 0.0f);
+                    P.ray_d[slot] = make_float4(dir.x, dir.y, dir.z, INFINITY);
+                    ++depth;
+                    cont = true;
+                }
+            } else {
+                scat = 0;
+                if (depth == 1 && (e.flags & ENT_LIGHT)) L += coef * area_light_radiance(e, s.geo.z, s.wr);
+                // next-event estimation over every light (path_tracing.cpp:134-146)
+                for (int li = 0; li < S.light_count; ++li) {
+                    const int le_i = S.light_entity[li];
+                    const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+                    if (le_i < 0) {
+                        float lpdf;
+                        const Vec3 dir = env_sample(S, u0, u1, u2, &lpdf);
+                        const Vec3 rad = env_radiance(S, dir);
+                        if (black(rad)) continue;
+                        const Vec3 lpos = env_emit_pos(S, s.pos, dir);
+                        const Vec3 to_light = normalize(lpos - s.pos);
+                        const Vec3 bf = bsdf_eval(b, to_light, s.wr);
+                        if (black(bf)) continue;
+                        const Vec3 contrib = coef * rad * bf * (fabsf(cosv(to_light, s.geo.z)) / (lpdf + bsdf_pdf(b, to_light, s.wr)));
+                        push_shadow(P, c, s.pos, to_light, eps, length(s.pos - lpos) - eps, contrib, slot);
+                    } else {
+                        const Entity& le = S.entities[le_i];
+                        LightSample ls;
+                        if (!area_light_sample(S, le, s.pos, u0, u1, u2, &ls)) continue;
+                        if (black(ls.rad) || ls.pdf == 0.0f) continue;
+                        const float slen = length(ls.pos - s.pos) - eps;
+                        if (slen <= eps) continue;
+                        const Vec3 to_light = normalize(ls.pos - s.pos);
+                        const Vec3 bf = bsdf_eval(b, to_light, s.wr);
+                        if (black(bf)) continue;
+                        Vec3 tr(1.0f);
+                        if (S.has_media) tr = medium_tr(S, medium_of(s, e, to_light), ls.pos, s.pos, rng, &wd);
+                        const Vec3 contrib = coef * tr * ls.rad * bf * (fabsf(cosv(to_light, s.geo.z)) / (ls.pdf + bsdf_pdf(b, to_light, s.wr)));
+                        push_shadow(P, c, s.pos, to_light, eps, slen, contrib, slot);
+                    }
+                }
+                // BSDF sample: MIS-BSDF ray and continuation (path_tracing.cpp:148-169)
+                const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+                const BSDFSample bs = bsdf_sample(b, s.wr, u0, u1, u2);
+                if (black(bs.f)) {
+                    finish = true;
+                } else {
+                    const Vec3 dir = normalize(bs.dir);
+                    const float gcos = fabsf(dot(s.geo.z, dir));
+                    mf4 = make_float4(coef.x * bs.f.x * gcos, coef.y * bs.f.y * gcos, coef.z * bs.f.z * gcos, mf4.w);
+                    coef4.w = bs.pdf;
+                    flags |= PF_MIS | (bs.delta ? PF_MIS_DELTA : 0);
+                    ray_med = medium_of(s, e, dir);
+                    if (bs.pdf < eps) flags |= PF_TERMINATE;
+                    else coef = coef * bs.f * (fabsf(cosv(s.geo.z, bs.dir)) / bs.pdf);
+                    const Vec3 no = eps_offset(s, bs.dir, eps);
+                    P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                    P.ray_d[slot] = make_float4(dir.x, dir.y, dir.z, INFINITY);
+                    if (!(bs.delta && depth >= 2 && s_depth <= p.specular_depth)) ++depth;
+                    else ++s_depth;
+                    cont = true;
+                }
+            }
+        }
+        if (wd) atomicMax(&c->watchdog, wd);
+        store_rng(st, rng);
+        P.st[slot] = st;
+        P.coef[slot] = make_float4(coef.x, coef.y, coef.z, coef4.w);
+        P.L[slot] = make_float4(L.x, L.y, L.z, L4.w);
+        P.mis_f[slot] = mf4;
+        P.ctr[slot] = make_int4(depth, s_depth, scat, (flags & 0xff) | (ray_med << 8));
+        const int qi = warp_append(&c->n_next, cont);
+        if (cont) P.q[out][qi] = slot;
+        const int fi = warp_append(&c->n_finish, !cont);
+        if (!cont) P.q_finish[fi] = slot;
+    }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(128) k_shadow(Scene S, Pool P, Counters* c) {
+    const int n = min(c->n_shadow, P.shadow_cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = P.sh_o[i], d = P.sh_d[i];
+        Hit h;
+        int wd = 0;
+        const bool occluded = trace_ray<EXACT, true>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd);
+        if (wd) atomicMax(&c->watchdog, wd);
+        if (!occluded) {
+            const float4 cc = P.sh_c[i];
+            const int slot = __float_as_int(cc.w);
+            float* l = reinterpret_cast<float*>(P.L + slot);
+            atomicAdd(l, cc.x);
+            atomicAdd(l + 1, cc.y);
+            atomicAdd(l + 2, cc.z);
+        }
+    }
+}
+
+__device__ __forceinline__ float filter_eval(const Params& p, float x, float y) {
+    if (p.filter_type == ATRC_FILTER_BOX) return p.filter_value;
+    const float gx = fmaxf(0.0f, __expf(-p.filter_alpha * x * x) - p.filter_exp);
+    const float gy = fmaxf(0.0f, __expf(-p.filter_alpha * y * y) - p.filter_exp);
+    return gx * gy;
+}
+
+__global__ void k_finish(Params p, Pool P, Film F, Counters* c) {
+    const int n = c->n_finish, fb = c->n_free;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = P.q_finish[i];
+        const float4 L = P.L[slot];
+        const float sx = L.w, sy = P.mis_f[slot].w;
+        if (isfinite(L.x) && isfinite(L.y) && isfinite(L.z)) {
+            const float4 ga = P.gb_albedo[slot], gn = P.gb_normal[slot];
+            // apply_image_filter (framebuffer.h:49-80)
+            const float r = p.filter_radius;
+            const int x0 = max(0, int(ceilf(sx - r - 0.5f))), y0 = max(0, int(ceilf(sy - r - 0.5f)));
+            const int x1 = min(p.W - 1, int(floorf(sx + r - 0.5f))), y1 = min(p.H - 1, int(floorf(sy + r - 0.5f)));
+            float yrel = fabsf(y0 + 0.5f - sy);
+            for (int y = y0; y <= y1; ++y, yrel += 1) {
+                if (yrel > r) continue;
+                float xrel = fabsf(x0 + 0.5f - sx);
+                for (int x = x0; x <= x1; ++x, xrel += 1) {
+                    if (xrel > r) continue;
+                    const double w = filter_eval(p, xrel, yrel);
+                    const size_t px = size_t(y) * p.W + x;
+                    atomicAdd(F.value + 3 * px, w * L.x);
+                    atomicAdd(F.value + 3 * px + 1, w * L.y);
+                    atomicAdd(F.value + 3 * px + 2, w * L.z);
+                    atomicAdd(F.weight + px, w);
+                    if (F.value_sq) {
+                        atomicAdd(F.value_sq + 3 * px, w * double(L.x) * L.x);
+                        atomicAdd(F.value_sq + 3 * px + 1, w * double(L.y) * L.y);
+                        atomicAdd(F.value_sq + 3 * px + 2, w * double(L.z) * L.z);
+                    }
+                    if (F.albedo) {
+                        atomicAdd(F.albedo + 3 * px, w * ga.x);
+                        atomicAdd(F.albedo + 3 * px + 1, w * ga.y);
+                        atomicAdd(F.albedo + 3 * px + 2, w * ga.z);
+                    }
+                    if (F.normal) {
+                        atomicAdd(F.normal + 3 * px, w * gn.x);
+                        atomicAdd(F.normal + 3 * px + 1, w * gn.y);
+                        atomicAdd(F.normal + 3 * px + 2, w * gn.z);
+                    }
+                    if (F.denoise) atomicAdd(F.denoise + px, w * ga.w);
+                }
+            }
+        }
+        P.free_list[fb + i] = slot;
+    }
+}
+
+__global__ void k_add_film(double* dst, const double* src, size_t n) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) dst[i] += src[i];
+}
+
+int grid_for(int sm_count, int blocks_per_sm) { return std::max(1, sm_count * blocks_per_sm); }
+
+}  // namespace
+
+// ==================================================================== scene
+struct DeviceSceneImpl {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    Scene scene{};
+    DevBuf nodes, tris, tri_shade, tri_orig, entities, tlas_order, materials, tex2d, tex3d, texels, media, alias_prob,
+        alias_idx, env_probs, env_alias_prob, env_alias_idx;
+    DevBuf watchdog;
+    // render workspace (kept between calls)
+    DevBuf pool_buf, counters, film_buf;
+    size_t pool_cap = 0;
+    int pool_lights = 0;
+    ~DeviceSceneImpl() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace atrc
+
+struct AtrcScene {
+    atrc::DeviceSceneImpl impl;
+};
+
+namespace atrc {
+namespace {
+
+int fail(int code, const std::string& msg) {
+    set_last_error(msg);
+    return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const CudaError& e) {
+        return fail(ATRC_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(ATRC_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(ATRC_ERR_UNSUPPORTED, e.what());
+    }
+}
+
+void check_device_ready() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        throw CudaError(std::string("no usable CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0"));
+}
+
+// Layout of the path pool inside one allocation.
+struct PoolLayout {
+    size_t off[24];
+    size_t total;
+};
+
+PoolLayout pool_layout(size_t cap, size_t shadow_cap) {
+    PoolLayout L{};
+    size_t o = 0;
+    auto take = [&](int i, size_t bytes) {
+        o = (o + 255) & ~size_t(255);
+        L.off[i] = o;
+        o += bytes;
+    };
+    take(0, cap * 16); take(1, cap * 16); take(2, cap * 16); take(3, cap * 4);
+    take(4, cap * 16); take(5, cap * 16); take(6, cap * 16); take(7, cap * 16); take(8, cap * 16);
+    take(9, cap * 16); take(10, cap * 16);
+    take(11, cap * 4); take(12, cap * 4); take(13, cap * 4); take(14, cap * 4);
+    take(15, shadow_cap * 16); take(16, shadow_cap * 16); take(17, shadow_cap * 16);
+    L.total = (o + 255) & ~size_t(255);
+    return L;
+}
+
+Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
+    char* b = static_cast<char*>(base);
+    Pool P;
+    P.ray_o = reinterpret_cast<float4*>(b + L.off[0]);
+    P.ray_d = reinterpret_cast<float4*>(b + L.off[1]);
+    P.hit = reinterpret_cast<float4*>(b + L.off[2]);
+    P.hit_tri = reinterpret_cast<int*>(b + L.off[3]);
+    P.coef = reinterpret_cast<float4*>(b + L.off[4]);
+    P.L = reinterpret_cast<float4*>(b + L.off[5]);
+    P.mis_f = reinterpret_cast<float4*>(b + L.off[6]);
+    P.gb_albedo = reinterpret_cast<float4*>(b + L.off[7]);
+    P.gb_normal = reinterpret_cast<float4*>(b + L.off[8]);
+    P.st = reinterpret_cast<uint4*>(b + L.off[9]);
+    P.ctr = reinterpret_cast<int4*>(b + L.off[10]);
+    P.q[0] = reinterpret_cast<int*>(b + L.off[11]);
+    P.q[1] = reinterpret_cast<int*>(b + L.off[12]);
+    P.q_finish = reinterpret_cast<int*>(b + L.off[13]);
+    P.free_list = reinterpret_cast<int*>(b + L.off[14]);
+    P.sh_o = reinterpret_cast<float4*>(b + L.off[15]);
+    P.sh_d = reinterpret_cast<float4*>(b + L.off[16]);
+    P.sh_c = reinterpret_cast<float4*>(b + L.off[17]);
+    P.shadow_cap = int(shadow_cap);
+    return P;
+}
+
+Params make_params(const AtrcRenderDesc& d) {
+    Params p{};
+    p.W = d.width;
+    p.H = d.height;
+    p.first_spp = d.first_spp;
+    p.min_depth = d.min_depth;
+    p.max_depth = d.max_depth;
+    p.specular_depth = d.specular_depth;
+    p.cont_prob = d.cont_prob;
+    p.eps = d.eps;
+    p.seed = d.seed;
+    // ThinLensCamera::init_from_params (thin_lens.cpp:34-55)
+    const AtrcCameraDesc& c = d.camera;
+    const Vec3 pos(c.pos[0], c.pos[1], c.pos[2]), dst(c.dst[0], c.dst[1], c.dst[2]), up(c.up[0], c.up[1], c.up[2]);
+    const Vec3 fz = normalize(dst - pos);
+    const Vec3 fx = normalize(cross(up, fz));
+    const Vec3 fy = cross(fz, fx);
+    for (int k = 0; k < 3; ++k) {
+        p.cam.pos[k] = pos[k];
+        p.cam.fx[k] = fx[k];
+        p.cam.fy[k] = fy[k];
+        p.cam.fz[k] = fz[k];
+    }
+    const float aspect = float(d.width) / float(d.height);
+    p.cam.film_h = 2 * c.focal_distance * std::tan(c.fov / 2);
+    p.cam.film_w = aspect * p.cam.film_h;
+    p.cam.focal = c.focal_distance;
+    p.cam.lens_radius = c.lens_radius;
+    // film filters (box_filter.cpp:6-34, gaussian_filter.cpp:6-78)
+    p.filter_type = d.filter_type;
+    if (d.filter_type == ATRC_FILTER_BOX) {
+        p.filter_radius = d.filter_radius - d.eps;
+        p.filter_value = 1 / (4 * p.filter_radius * p.filter_radius);
+    } else {
+        p.filter_radius = d.filter_radius;
+        p.filter_alpha = d.filter_alpha;
+        p.filter_exp = std::exp(-d.filter_alpha * d.filter_radius * d.filter_radius);
+        p.filter_value = 1;
+    }
+    return p;
+}
+
+}  // namespace
+}  // namespace atrc
+
+using namespace atrc;
+
+extern "C" {
+
+int atrc_cuda_device_init(int device, AtrcDeviceInfo* info) {
+    return guarded([&] {
+        check_device_ready();
+        CK(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        if (info) {
+            std::memset(info, 0, sizeof(*info));
+            std::snprintf(info->name, sizeof(info->name), "%s", prop.name);
+            info->sm_count = prop.multiProcessorCount;
+            info->cc_major = prop.major;
+            info->cc_minor = prop.minor;
+            info->global_mem_bytes = prop.totalGlobalMem;
+        }
+        if (prop.major < 10) throw CudaError("pt_cuda is built for sm_100a (Blackwell); device is sm_" +
+                                             std::to_string(prop.major) + std::to_string(prop.minor));
+        return int(ATRC_OK);
+    });
+}
+
+int atrc_cuda_scene_create(const AtrcSceneDesc* desc, AtrcScene** out) {
+    if (!desc || !out) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_scene_create: null argument");
+    *out = nullptr;
+    return guarded([&] {
+        check_device_ready();
+        auto hs = std::make_unique<HostScene>();
+        build_host_scene(*desc, hs.get());
+        auto sc = std::make_unique<AtrcScene>();
+        DeviceSceneImpl& d = sc->impl;
+        CK(cudaGetDevice(&d.device));
+        CK(cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, d.device));
+        CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+        cudaStream_t s = d.stream;
+        Scene S = hs->scene;
+        S.nodes = upload(d.nodes, hs->nodes, s);
+        S.tris = upload(d.tris, hs->tris, s);
+        S.tri_shade = upload(d.tri_shade, hs->tri_shade, s);
+        S.tri_orig = upload(d.tri_orig, hs->tri_orig, s);
+        S.entities = upload(d.entities, hs->entities, s);
+        S.tlas_order = upload(d.tlas_order, hs->tlas_order, s);
+        S.materials = upload(d.materials, hs->materials, s);
+        S.tex2d = upload(d.tex2d, hs->tex2d, s);
+        S.tex3d = upload(d.tex3d, hs->tex3d, s);
+        S.texels = upload(d.texels, hs->texels, s);
+        S.media = upload(d.media, hs->media, s);
+        S.alias_prob = upload(d.alias_prob, hs->alias_prob, s);
+        S.alias_idx = upload(d.alias_idx, hs->alias_idx, s);
+        S.env.probs = upload(d.env_probs, hs->env_probs, s);
+        S.env.alias_prob = upload(d.env_alias_prob, hs->env_alias_prob, s);
+        S.env.alias_idx = upload(d.env_alias_idx, hs->env_alias_idx, s);
+        S.eps = 3e-4f;
+        d.scene = S;
+        d.watchdog.alloc(sizeof(int));
+        CK(cudaStreamSynchronize(s));
+        *out = sc.release();
+        return int(ATRC_OK);
+    });
+}
+
+void atrc_cuda_scene_destroy(AtrcScene* scene) { delete scene; }
+
+int atrc_cuda_trace_rays_device(AtrcScene* scene, const AtrcRay* d_rays, size_t n, AtrcHit* d_hits, int mode,
+                                int exact) {
+    if (!scene || (n && (!d_rays || !d_hits))) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_trace_rays: null argument");
+    if (mode != ATRC_QUERY_CLOSEST && mode != ATRC_QUERY_ANY) return fail(ATRC_ERR_INVALID_ARG, "bad query mode");
+    return guarded([&] {
+        DeviceSceneImpl& d = scene->impl;
+        if (n == 0) return int(ATRC_OK);
+        CK(cudaMemsetAsync(d.watchdog.p, 0, sizeof(int), d.stream));
+        const int grid = grid_for(d.sm_count, 8);
+        int* wd = d.watchdog.as<int>();
+        if (mode == ATRC_QUERY_ANY) {
+            if (exact) k_trace_rays<true, true><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
+            else k_trace_rays<false, true><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
+        } else {
+            if (exact) k_trace_rays<true, false><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
+            else k_trace_rays<false, false><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
+        }
+        CK(cudaGetLastError());
+        int w = 0;
+        CK(cudaMemcpyAsync(&w, wd, sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+        CK(cudaStreamSynchronize(d.stream));
+        if (w) return fail(ATRC_ERR_WATCHDOG, "traversal stack limit reached (code " + std::to_string(w) + ")");
+        return int(ATRC_OK);
+    });
+}
+
+int atrc_cuda_trace_rays(AtrcScene* scene, const AtrcRay* rays, size_t n, AtrcHit* hits, int mode, int exact) {
+    if (!scene || (n && (!rays || !hits))) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_trace_rays: null argument");
+    return guarded([&] {
+        DeviceSceneImpl& d = scene->impl;
+        if (n == 0) return int(ATRC_OK);
+        DevBuf r, h;
+        r.alloc(n * sizeof(AtrcRay));
+        h.alloc(n * sizeof(AtrcHit));
+        CK(cudaMemcpyAsync(r.p, rays, n * sizeof(AtrcRay), cudaMemcpyHostToDevice, d.stream));
+        int rc = atrc_cuda_trace_rays_device(scene, r.as<AtrcRay>(), n, h.as<AtrcHit>(), mode, exact);
+        if (rc != ATRC_OK) return rc;
+        CK(cudaMemcpyAsync(hits, h.p, n * sizeof(AtrcHit), cudaMemcpyDeviceToHost, d.stream));
+        CK(cudaStreamSynchronize(d.stream));
+        return int(ATRC_OK);
+    });
+}
+
+int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* film, volatile const int* cancel,
+                     AtrcProgressFn progress, void* user, AtrcRenderStats* stats) {
+    if (!scene || !desc || !film || !film->value || !film->weight)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: null argument");
+    if (desc->width <= 0 || desc->height <= 0 || desc->spp <= 0 || desc->max_depth < 0)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid film size, spp or depth");
+    if (desc->spp_count < 0 || desc->first_spp < 0)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid sample range");
+    if (desc->filter_type == ATRC_FILTER_BOX ? !(desc->filter_radius - desc->eps > 0) : !(desc->filter_radius > 0 && desc->filter_alpha > 0))
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid film filter");
+    return guarded([&] {
+        const auto t_start = std::chrono::steady_clock::now();
+        DeviceSceneImpl& d = scene->impl;
+        CK(cudaSetDevice(d.device));
+        cudaStream_t s = d.stream;
+        d.scene.eps = desc->eps;
+        const Params p = make_params(*desc);
+        const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
+        const unsigned long long total = (unsigned long long)desc->width * desc->height * spp;
+        // path pool: enough paths to fill the GPU; shadow capacity = pool x lights
+        const int nl = std::max(1, d.scene.light_count);
+        size_t cap = desc->path_pool > 0 ? size_t(desc->path_pool) : size_t(1) << 21;
+        cap = std::min<size_t>(cap, std::max<unsigned long long>(total, 1024ULL));
+        cap = std::min<size_t>(cap, (size_t(1) << 28) / nl);
+        const size_t shadow_cap = cap * nl;
+        const PoolLayout L = pool_layout(cap, shadow_cap);
+        if (d.pool_cap != cap || d.pool_lights != nl) {
+            d.pool_buf.alloc(L.total);
+            d.pool_cap = cap;
+            d.pool_lights = nl;
+        }
+        if (!d.counters.p) d.counters.alloc(sizeof(Counters));
+        Pool P = pool_from(d.pool_buf.p, L, shadow_cap);
+        Counters* c = d.counters.as<Counters>();
+        // film
+        const size_t npix = size_t(desc->width) * desc->height;
+        Film F{};
+        std::vector<std::pair<double*, size_t>> host_targets;
+        DevBuf local_film;
+        if (film->on_device) {
+            F.value = film->value; F.weight = film->weight; F.value_sq = film->value_sq;
+            F.albedo = film->albedo; F.normal = film->normal; F.denoise = film->denoise;
+        } else {
+            size_t doubles = npix * 4 + (film->value_sq ? npix * 3 : 0) + (film->albedo ? npix * 3 : 0) +
+                             (film->normal ? npix * 3 : 0) + (film->denoise ? npix : 0);
+            local_film.alloc(doubles * sizeof(double));
+            CK(cudaMemsetAsync(local_film.p, 0, doubles * sizeof(double), s));
+            double* b = local_film.as<double>();
+            F.value = b; b += npix * 3; host_targets.push_back({film->value, npix * 3});
+            F.weight = b; b += npix; host_targets.push_back({film->weight, npix});
+            if (film->value_sq) { F.value_sq = b; b += npix * 3; host_targets.push_back({film->value_sq, npix * 3}); }
+            if (film->albedo) { F.albedo = b; b += npix * 3; host_targets.push_back({film->albedo, npix * 3}); }
+            if (film->normal) { F.normal = b; b += npix * 3; host_targets.push_back({film->normal, npix * 3}); }
+            if (film->denoise) { F.denoise = b; b += npix; host_targets.push_back({film->denoise, npix}); }
+        }
+        const int gsm = grid_for(d.sm_count, 16);
+        k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
+        CK(cudaGetLastError());
+        uint64_t launches = 1;
+        cudaEvent_t ev0, ev1;
+        CK(cudaEventCreate(&ev0));
+        CK(cudaEventCreate(&ev1));
+        // per-kernel timing events for one checkpoint window
+        const int window = 4;
+        std::vector<cudaEvent_t> kev(window * 6);
+        for (auto& e : kev) CK(cudaEventCreate(&e));
+        double t_ext = 0, t_shade = 0, t_shadow = 0;
+        CK(cudaEventRecord(ev0, s));
+        Counters hc{};
+        Counters* pinned = nullptr;
+        CK(cudaMallocHost(&pinned, sizeof(Counters)));
+        int status = ATRC_OK;
+        const bool exact = false;
+        for (int iter_block = 0;; ++iter_block) {
+            for (int k = 0; k < window; ++k) {
+                k_begin<<<1, 1, 0, s>>>(c);
+                k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
+                CK(cudaEventRecord(kev[k * 6 + 0], s));
+                if (exact) k_extend<true><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                else k_extend<false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                CK(cudaEventRecord(kev[k * 6 + 1], s));
+                k_shade<<<gsm, 128, 0, s>>>(d.scene, p, P, c);
+                CK(cudaEventRecord(kev[k * 6 + 2], s));
+                if (exact) k_shadow<true><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                else k_shadow<false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                CK(cudaEventRecord(kev[k * 6 + 3], s));
+                k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
+                launches += 6;
+            }
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            hc = *pinned;
+            for (int k = 0; k < window; ++k) {
+                float a = 0, b2 = 0, e3 = 0;
+                CK(cudaEventElapsedTime(&a, kev[k * 6 + 0], kev[k * 6 + 1]));
+                CK(cudaEventElapsedTime(&b2, kev[k * 6 + 1], kev[k * 6 + 2]));
+                CK(cudaEventElapsedTime(&e3, kev[k * 6 + 2], kev[k * 6 + 3]));
+                t_ext += a * 1e-3;
+                t_shade += b2 * 1e-3;
+                t_shadow += e3 * 1e-3;
+            }
+            if (hc.watchdog) { status = ATRC_ERR_WATCHDOG; break; }
+            if (hc.done) break;
+            if (progress) progress(100.0 * double(hc.completed) / double(std::max(1ULL, total)), user);
+            if (cancel && *cancel) { status = ATRC_ERR_CANCELLED; break; }
+        }
+        CK(cudaEventRecord(ev1, s));
+        CK(cudaEventSynchronize(ev1));
+        float kms = 0;
+        CK(cudaEventElapsedTime(&kms, ev0, ev1));
+        // bring host films up to date
+        uint64_t d2h = sizeof(Counters);
+        if (!host_targets.empty()) {
+            size_t doubles = 0;
+            for (auto& t : host_targets) doubles += t.second;
+            std::vector<double> tmp(doubles);
+            CK(cudaMemcpyAsync(tmp.data(), local_film.p, doubles * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            d2h += doubles * sizeof(double);
+            size_t off = 0;
+            for (auto& t : host_targets) {
+                for (size_t k = 0; k < t.second; ++k) t.first[k] += tmp[off + k];
+                off += t.second;
+            }
+        }
+        CK(cudaFreeHost(pinned));
+        for (auto& e : kev) cudaEventDestroy(e);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+            stats->kernel_seconds = kms * 1e-3;
+            stats->samples = hc.completed;
+            stats->rays_closest = hc.rays_closest;
+            stats->rays_shadow = hc.rays_shadow;
+            stats->iterations = hc.iterations;
+            stats->kernel_launches = launches;
+            stats->watchdog_flags = uint64_t(hc.watchdog);
+            stats->extend_seconds = t_ext;
+            stats->shade_seconds = t_shade;
+            stats->shadow_seconds = t_shadow;
+            stats->h2d_bytes = 0;
+            stats->d2h_bytes = d2h;
+        }
+        if (progress && status == ATRC_OK) progress(100.0, user);
+        if (status == ATRC_ERR_WATCHDOG)
+            return fail(status, "a device loop reached its iteration cap (code " + std::to_string(hc.watchdog) + ")");
+        if (status == ATRC_ERR_CANCELLED) return fail(status, "render cancelled");
+        return int(ATRC_OK);
+    });
+}
+
+}  // extern "C"

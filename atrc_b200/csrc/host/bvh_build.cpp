@@ -1,0 +1,191 @@
+// Binned SAH build (32 bins per axis, centroid bounds), iterative with an
+// explicit task stack; large ranges are split across threads.
+#include "bvh_build.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <limits>
+#include <mutex>
+#include <stdexcept>
+#include <thread>
+
+namespace atrc {
+
+namespace {
+
+struct Box {
+    float lo[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
+                   std::numeric_limits<float>::max()};
+    float hi[3] = {-std::numeric_limits<float>::max(), -std::numeric_limits<float>::max(),
+                   -std::numeric_limits<float>::max()};
+    void grow(const float* l, const float* h) {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], l[k]);
+            hi[k] = std::max(hi[k], h[k]);
+        }
+    }
+    void grow(const Box& b) { grow(b.lo, b.hi); }
+    float area() const {
+        float d[3];
+        for (int k = 0; k < 3; ++k) d[k] = std::max(0.0f, hi[k] - lo[k]);
+        return 2.0f * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+    }
+    bool valid() const { return lo[0] <= hi[0]; }
+};
+
+constexpr int kBins = 32;
+
+struct Builder {
+    const std::vector<BuildPrim>& prims;
+    std::vector<uint32_t>& idx;
+    std::vector<float> cen;  // 3 per prim
+    int max_leaf;
+    float ct, ci;
+    std::mutex mtx;
+    std::vector<BvhNode>& nodes;
+    std::atomic<int> max_depth{0};
+
+    Builder(const std::vector<BuildPrim>& p, std::vector<uint32_t>& i, std::vector<BvhNode>& n, int ml, float t,
+            float c)
+        : prims(p), idx(i), max_leaf(ml), ct(t), ci(c), nodes(n) {
+        cen.resize(p.size() * 3);
+        for (size_t k = 0; k < p.size(); ++k)
+            for (int a = 0; a < 3; ++a) cen[k * 3 + a] = 0.5f * (p[k].lo[a] + p[k].hi[a]);
+    }
+
+    int alloc_node() {
+        std::lock_guard<std::mutex> lk(mtx);
+        nodes.push_back(BvhNode{});
+        return int(nodes.size() - 1);
+    }
+
+    Box range_box(uint32_t b, uint32_t e) const {
+        Box r;
+        for (uint32_t i = b; i < e; ++i) r.grow(prims[idx[i]].lo, prims[idx[i]].hi);
+        return r;
+    }
+
+    // Split [b, e) and return the split position, or e if a leaf is better.
+    uint32_t split(uint32_t b, uint32_t e, const Box& box) {
+        const uint32_t n = e - b;
+        if (n <= 1) return e;
+        Box cb;
+        for (uint32_t i = b; i < e; ++i) {
+            const float* c = &cen[size_t(idx[i]) * 3];
+            cb.grow(c, c);
+        }
+        float best_cost = std::numeric_limits<float>::max();
+        int best_axis = -1, best_bin = -1;
+        for (int a = 0; a < 3; ++a) {
+            const float ext = cb.hi[a] - cb.lo[a];
+            if (!(ext > 0)) continue;
+            Box bb[kBins];
+            uint32_t cnt[kBins] = {0};
+            const float scale = kBins / ext;
+            for (uint32_t i = b; i < e; ++i) {
+                const uint32_t p = idx[i];
+                int k = int((cen[size_t(p) * 3 + a] - cb.lo[a]) * scale);
+                k = std::min(std::max(k, 0), kBins - 1);
+                cnt[k]++;
+                bb[k].grow(prims[p].lo, prims[p].hi);
+            }
+            float right_area[kBins];
+            uint32_t right_cnt[kBins];
+            Box acc;
+            uint32_t c = 0;
+            for (int k = kBins - 1; k > 0; --k) {
+                acc.grow(bb[k]);
+                c += cnt[k];
+                right_area[k] = acc.valid() ? acc.area() : 0;
+                right_cnt[k] = c;
+            }
+            Box lacc;
+            uint32_t lc = 0;
+            for (int k = 0; k < kBins - 1; ++k) {
+                lacc.grow(bb[k]);
+                lc += cnt[k];
+                if (lc == 0 || right_cnt[k + 1] == 0) continue;
+                const float cost = (lacc.valid() ? lacc.area() : 0) * lc + right_area[k + 1] * right_cnt[k + 1];
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = a;
+                    best_bin = k;
+                }
+            }
+        }
+        const float parent_area = std::max(box.area(), 1e-30f);
+        const float leaf_cost = ci * n;
+        const float split_cost = ct + ci * best_cost / parent_area;
+        if (best_axis < 0) {
+            // all centroids coincide: median split if the range is too large
+            if (n <= uint32_t(max_leaf)) return e;
+            return b + n / 2;
+        }
+        if (n <= uint32_t(max_leaf) && leaf_cost <= split_cost) return e;
+        const float ext = cb.hi[best_axis] - cb.lo[best_axis];
+        const float scale = kBins / ext;
+        auto mid_it = std::partition(idx.begin() + b, idx.begin() + e, [&](uint32_t p) {
+            int k = int((cen[size_t(p) * 3 + best_axis] - cb.lo[best_axis]) * scale);
+            k = std::min(std::max(k, 0), kBins - 1);
+            return k <= best_bin;
+        });
+        uint32_t mid = uint32_t(mid_it - idx.begin());
+        if (mid == b || mid == e) mid = b + n / 2;
+        return mid;
+    }
+
+    // Builds the subtree of [b, e) and returns its link.
+    int32_t build(uint32_t b, uint32_t e, const Box& box, int depth) {
+        int md = max_depth.load();
+        while (depth > md && !max_depth.compare_exchange_weak(md, depth)) {}
+        const uint32_t mid = split(b, e, box);
+        if (mid == e) return leaf_link(b, e - b);
+        const int node = alloc_node();
+        Box lb = range_box(b, mid), rb = range_box(mid, e);
+        int32_t l, r;
+        if (e - b > 200000 && depth < 6) {
+            auto fut = std::async(std::launch::async, [&] { return build(b, mid, lb, depth + 1); });
+            r = build(mid, e, rb, depth + 1);
+            l = fut.get();
+        } else {
+            l = build(b, mid, lb, depth + 1);
+            r = build(mid, e, rb, depth + 1);
+        }
+        std::lock_guard<std::mutex> lk(mtx);
+        BvhNode& nd = nodes[node];
+        nd.c0lo_x = lb.lo[0]; nd.c0hi_x = lb.hi[0]; nd.c0lo_y = lb.lo[1]; nd.c0hi_y = lb.hi[1];
+        nd.c1lo_x = rb.lo[0]; nd.c1hi_x = rb.hi[0]; nd.c1lo_y = rb.lo[1]; nd.c1hi_y = rb.hi[1];
+        nd.c0lo_z = lb.lo[2]; nd.c0hi_z = lb.hi[2]; nd.c1lo_z = rb.lo[2]; nd.c1hi_z = rb.hi[2];
+        nd.link0 = l;
+        nd.link1 = r;
+        return node;
+    }
+};
+
+}  // namespace
+
+BvhResult build_bvh(const std::vector<BuildPrim>& prims, int max_leaf, float traversal_cost, float intersect_cost) {
+    BvhResult res;
+    if (max_leaf < 1 || max_leaf > 16) throw std::runtime_error("max_leaf must be in [1, 16]");
+    if (prims.size() >= (1u << 27)) throw std::runtime_error("too many primitives for one BVH");
+    res.order.resize(prims.size());
+    for (size_t i = 0; i < prims.size(); ++i) res.order[i] = uint32_t(i);
+    if (prims.empty()) {
+        res.root_link = 0;
+        for (int k = 0; k < 3; ++k) { res.bound_lo[k] = 0; res.bound_hi[k] = 0; }
+        return res;
+    }
+    res.nodes.reserve(prims.size() / 2 + 1);
+    Builder b(prims, res.order, res.nodes, max_leaf, traversal_cost, intersect_cost);
+    Box box = b.range_box(0, uint32_t(prims.size()));
+    // reserve the root slot so that an interior root is node 0
+    res.root_link = b.build(0, uint32_t(prims.size()), box, 0);
+    res.max_depth = b.max_depth.load();
+    for (int k = 0; k < 3; ++k) { res.bound_lo[k] = box.lo[k]; res.bound_hi[k] = box.hi[k]; }
+    return res;
+}
+
+}  // namespace atrc

@@ -1,0 +1,287 @@
+// Host file formats: float images (.pfm, Radiance .hdr), meshes (.bm, .obj)
+// and image writers for the output post processors.
+//
+// The reference reads these through agz-utils (img::load_rgb_from_hdr_file,
+// mesh::load_from_file), which is absent from its checkout; the formats are
+// implemented here from their public specifications.  `.bm` follows
+// src/factory/src/utility/bin_mesh.cpp:7-27 (size_t count, then per triangle
+// three {position[3], normal[3], tex_coord[2]} float vertices).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "scene_loader.h"
+
+namespace atrc {
+
+namespace {
+
+bool has_ext(const std::string& fn, const char* ext) {
+    size_t n = std::strlen(ext);
+    if (fn.size() < n) return false;
+    for (size_t i = 0; i < n; ++i)
+        if (std::tolower((unsigned char)fn[fn.size() - n + i]) != ext[i]) return false;
+    return true;
+}
+
+// Portable float map: "PF\n<w> <h>\n<scale>\n" then rows bottom-to-top.
+std::vector<float> load_pfm(const std::string& fn, int* w, int* h) {
+    std::ifstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open image: " + fn);
+    std::string magic;
+    f >> magic;
+    int ch;
+    if (magic == "PF") ch = 3;
+    else if (magic == "Pf") ch = 1;
+    else throw ConfigError("not a PFM file: " + fn);
+    double scale;
+    f >> *w >> *h >> scale;
+    f.get();
+    if (!f || *w <= 0 || *h <= 0) throw ConfigError("bad PFM header: " + fn);
+    const bool little = scale < 0;
+    std::vector<float> raw(size_t(*w) * *h * ch);
+    f.read(reinterpret_cast<char*>(raw.data()), raw.size() * sizeof(float));
+    if (!f) throw ConfigError("truncated PFM: " + fn);
+    if (!little) {
+        for (auto& v : raw) {
+            uint32_t u;
+            std::memcpy(&u, &v, 4);
+            u = __builtin_bswap32(u);
+            std::memcpy(&v, &u, 4);
+        }
+    }
+    std::vector<float> out(size_t(*w) * *h * 3);
+    for (int y = 0; y < *h; ++y) {
+        const int src_row = *h - 1 - y;  // PFM stores the bottom row first
+        for (int x = 0; x < *w; ++x)
+            for (int c = 0; c < 3; ++c)
+                out[(size_t(y) * *w + x) * 3 + c] = raw[(size_t(src_row) * *w + x) * ch + (ch == 3 ? c : 0)];
+    }
+    return out;
+}
+
+// Radiance RGBE (.hdr), flat or new-style run-length encoded scanlines.
+std::vector<float> load_rgbe(const std::string& fn, int* w, int* h) {
+    std::ifstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open image: " + fn);
+    std::string line;
+    std::getline(f, line);
+    if (line.rfind("#?", 0) != 0) throw ConfigError("not a Radiance HDR file: " + fn);
+    while (std::getline(f, line) && !line.empty()) {
+        if (line.rfind("FORMAT=", 0) == 0 && line != "FORMAT=32-bit_rle_rgbe")
+            throw ConfigError("unsupported HDR format: " + line);
+    }
+    std::getline(f, line);
+    char ya[4], xa[4];
+    if (std::sscanf(line.c_str(), "%3s %d %3s %d", ya, h, xa, w) != 4 || std::string(ya) != "-Y" || std::string(xa) != "+X")
+        throw ConfigError("unsupported HDR orientation: " + line);
+    std::vector<float> out(size_t(*w) * *h * 3);
+    std::vector<uint8_t> scan(size_t(*w) * 4);
+    for (int y = 0; y < *h; ++y) {
+        uint8_t hdr[4];
+        f.read(reinterpret_cast<char*>(hdr), 4);
+        if (!f) throw ConfigError("truncated HDR: " + fn);
+        if (*w >= 8 && *w < 32768 && hdr[0] == 2 && hdr[1] == 2 && ((hdr[2] << 8) | hdr[3]) == *w) {
+            for (int c = 0; c < 4; ++c) {
+                int x = 0;
+                while (x < *w) {
+                    int cnt = f.get();
+                    if (cnt == EOF) throw ConfigError("truncated HDR: " + fn);
+                    if (cnt > 128) {
+                        cnt -= 128;
+                        int v = f.get();
+                        for (int k = 0; k < cnt && x < *w; ++k) scan[size_t(x++) * 4 + c] = uint8_t(v);
+                    } else {
+                        for (int k = 0; k < cnt && x < *w; ++k) scan[size_t(x++) * 4 + c] = uint8_t(f.get());
+                    }
+                }
+            }
+        } else {
+            std::memcpy(scan.data(), hdr, 4);
+            f.read(reinterpret_cast<char*>(scan.data() + 4), (size_t(*w) - 1) * 4);
+        }
+        for (int x = 0; x < *w; ++x) {
+            const uint8_t* p = &scan[size_t(x) * 4];
+            float s = p[3] ? std::ldexp(1.0f, int(p[3]) - 136) : 0.0f;
+            for (int c = 0; c < 3; ++c) out[(size_t(y) * *w + x) * 3 + c] = p[c] * s;
+        }
+    }
+    return out;
+}
+
+uint32_t crc32_table[256];
+bool crc_init = false;
+
+uint32_t crc32(const uint8_t* d, size_t n, uint32_t c = 0xFFFFFFFFu) {
+    if (!crc_init) {
+        for (uint32_t i = 0; i < 256; ++i) {
+            uint32_t v = i;
+            for (int k = 0; k < 8; ++k) v = (v & 1) ? 0xEDB88320u ^ (v >> 1) : v >> 1;
+            crc32_table[i] = v;
+        }
+        crc_init = true;
+    }
+    for (size_t i = 0; i < n; ++i) c = crc32_table[(c ^ d[i]) & 0xFF] ^ (c >> 8);
+    return c;
+}
+
+void put_be32(std::vector<uint8_t>& v, uint32_t x) {
+    v.push_back(uint8_t(x >> 24)); v.push_back(uint8_t(x >> 16));
+    v.push_back(uint8_t(x >> 8)); v.push_back(uint8_t(x));
+}
+
+void png_chunk(std::ofstream& f, const char* type, const std::vector<uint8_t>& data) {
+    std::vector<uint8_t> buf;
+    put_be32(buf, uint32_t(data.size()));
+    buf.insert(buf.end(), type, type + 4);
+    buf.insert(buf.end(), data.begin(), data.end());
+    uint32_t c = crc32(buf.data() + 4, buf.size() - 4) ^ 0xFFFFFFFFu;
+    put_be32(buf, c);
+    f.write(reinterpret_cast<const char*>(buf.data()), buf.size());
+}
+
+}  // namespace
+
+std::vector<float> load_rgb_image(const std::string& fn, int* w, int* h) {
+    if (has_ext(fn, ".pfm")) return load_pfm(fn, w, h);
+    if (has_ext(fn, ".hdr")) return load_rgbe(fn, w, h);
+    throw ConfigError("unsupported image format (pt_cuda reads .pfm and .hdr): " + fn);
+}
+
+std::vector<float> load_triangle_mesh(const std::string& fn) {
+    if (has_ext(fn, ".bm")) {
+        std::ifstream f(fn, std::ios::binary);
+        if (!f) throw ConfigError("failed to open file: " + fn);
+        uint64_t count = 0;
+        f.read(reinterpret_cast<char*>(&count), sizeof(count));
+        if (!f) throw ConfigError("failed to load triangle count from " + fn);
+        std::vector<float> v(size_t(count) * 24);
+        f.read(reinterpret_cast<char*>(v.data()), v.size() * sizeof(float));
+        if (!f) throw ConfigError("failed to load triangle data from " + fn);
+        return v;
+    }
+    if (has_ext(fn, ".obj")) {
+        std::ifstream f(fn);
+        if (!f) throw ConfigError("failed to open file: " + fn);
+        std::vector<float> pos, nor, uv, out;
+        std::string line;
+        auto fix = [](int i, size_t n) -> long { return i > 0 ? long(i) - 1 : long(n) + i; };
+        while (std::getline(f, line)) {
+            std::istringstream ss(line);
+            std::string tag;
+            ss >> tag;
+            if (tag == "v") { float x, y, z; ss >> x >> y >> z; pos.insert(pos.end(), {x, y, z}); }
+            else if (tag == "vn") { float x, y, z; ss >> x >> y >> z; nor.insert(nor.end(), {x, y, z}); }
+            else if (tag == "vt") { float x, y; ss >> x >> y; uv.insert(uv.end(), {x, y}); }
+            else if (tag == "f") {
+                struct Idx { long p = -1, t = -1, n = -1; };
+                std::vector<Idx> poly;
+                std::string tok;
+                while (ss >> tok) {
+                    Idx id;
+                    int a = 0, b = 0, c = 0;
+                    if (std::sscanf(tok.c_str(), "%d/%d/%d", &a, &b, &c) == 3) { id.p = fix(a, pos.size() / 3); id.t = fix(b, uv.size() / 2); id.n = fix(c, nor.size() / 3); }
+                    else if (std::sscanf(tok.c_str(), "%d//%d", &a, &c) == 2) { id.p = fix(a, pos.size() / 3); id.n = fix(c, nor.size() / 3); }
+                    else if (std::sscanf(tok.c_str(), "%d/%d", &a, &b) == 2) { id.p = fix(a, pos.size() / 3); id.t = fix(b, uv.size() / 2); }
+                    else if (std::sscanf(tok.c_str(), "%d", &a) == 1) { id.p = fix(a, pos.size() / 3); }
+                    else throw ConfigError("bad OBJ face: " + line);
+                    poly.push_back(id);
+                }
+                for (size_t k = 1; k + 1 < poly.size(); ++k) {
+                    const Idx tri[3] = {poly[0], poly[k], poly[k + 1]};
+                    Vec3 P[3];
+                    for (int i = 0; i < 3; ++i) {
+                        if (tri[i].p < 0 || size_t(tri[i].p) * 3 + 2 >= pos.size() + 0) {
+                            if (tri[i].p < 0 || size_t(tri[i].p) >= pos.size() / 3) throw ConfigError("OBJ index out of range");
+                        }
+                        P[i] = Vec3(pos[tri[i].p * 3], pos[tri[i].p * 3 + 1], pos[tri[i].p * 3 + 2]);
+                    }
+                    Vec3 fn_ = normalize(cross(P[1] - P[0], P[2] - P[0]));
+                    for (int i = 0; i < 3; ++i) {
+                        Vec3 n = fn_;
+                        if (tri[i].n >= 0 && size_t(tri[i].n) < nor.size() / 3)
+                            n = Vec3(nor[tri[i].n * 3], nor[tri[i].n * 3 + 1], nor[tri[i].n * 3 + 2]);
+                        float u = 0, v = 0;
+                        if (tri[i].t >= 0 && size_t(tri[i].t) < uv.size() / 2) { u = uv[tri[i].t * 2]; v = uv[tri[i].t * 2 + 1]; }
+                        out.insert(out.end(), {P[i].x, P[i].y, P[i].z, n.x, n.y, n.z, u, v});
+                    }
+                }
+            }
+        }
+        return out;
+    }
+    throw ConfigError("unsupported mesh format (pt_cuda reads .bm and .obj): " + fn);
+}
+
+void save_pfm(const std::string& fn, const float* rgb, int w, int h) {
+    std::ofstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open output: " + fn);
+    f << "PF\n" << w << " " << h << "\n-1.0\n";
+    for (int y = h - 1; y >= 0; --y) f.write(reinterpret_cast<const char*>(rgb + size_t(y) * w * 3), size_t(w) * 3 * sizeof(float));
+}
+
+void save_png8(const std::string& fn, const float* rgb, int w, int h, float inv_gamma) {
+    // 8-bit RGB PNG with stored (uncompressed) deflate blocks.
+    std::vector<uint8_t> raw;
+    raw.reserve(size_t(h) * (size_t(w) * 3 + 1));
+    for (int y = 0; y < h; ++y) {
+        raw.push_back(0);
+        for (int x = 0; x < w * 3; ++x) {
+            float v = rgb[size_t(y) * w * 3 + x];
+            if (!(v > 0)) v = 0;
+            if (inv_gamma != 1.0f) v = std::pow(v, inv_gamma);
+            v = std::fmin(v, 1.0f);
+            raw.push_back(uint8_t(std::lround(v * 255.0f)));
+        }
+    }
+    std::vector<uint8_t> z = {0x78, 0x01};
+    size_t off = 0;
+    while (off < raw.size() || raw.empty()) {
+        size_t n = std::min<size_t>(65535, raw.size() - off);
+        bool last = off + n >= raw.size();
+        z.push_back(last ? 1 : 0);
+        z.push_back(uint8_t(n)); z.push_back(uint8_t(n >> 8));
+        z.push_back(uint8_t(~n)); z.push_back(uint8_t((~n) >> 8));
+        z.insert(z.end(), raw.begin() + off, raw.begin() + off + n);
+        off += n;
+        if (raw.empty()) break;
+    }
+    uint32_t a = 1, b = 0;
+    for (uint8_t c : raw) { a = (a + c) % 65521; b = (b + a) % 65521; }
+    put_be32(z, (b << 16) | a);
+    std::ofstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open output: " + fn);
+    const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
+    f.write(reinterpret_cast<const char*>(sig), 8);
+    std::vector<uint8_t> ihdr;
+    put_be32(ihdr, uint32_t(w));
+    put_be32(ihdr, uint32_t(h));
+    ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});
+    png_chunk(f, "IHDR", ihdr);
+    png_chunk(f, "IDAT", z);
+    png_chunk(f, "IEND", {});
+}
+
+void save_hdr_rgbe(const std::string& fn, const float* rgb, int w, int h) {
+    std::ofstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open output: " + fn);
+    f << "#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y " << h << " +X " << w << "\n";
+    for (size_t i = 0; i < size_t(w) * h; ++i) {
+        float r = rgb[3 * i], g = rgb[3 * i + 1], b = rgb[3 * i + 2];
+        float m = std::fmax(r, std::fmax(g, b));
+        uint8_t e[4] = {0, 0, 0, 0};
+        if (m > 1e-32f) {
+            int ex;
+            float s = std::frexp(m, &ex) * 256.0f / m;
+            e[0] = uint8_t(std::fmax(r, 0.f) * s); e[1] = uint8_t(std::fmax(g, 0.f) * s);
+            e[2] = uint8_t(std::fmax(b, 0.f) * s); e[3] = uint8_t(ex + 128);
+        }
+        f.write(reinterpret_cast<const char*>(e), 4);
+    }
+}
+
+}  // namespace atrc

@@ -1,0 +1,392 @@
+"""Seeded synthetic scenes in the Atrc JSON format.
+
+The reference publishes no benchmark scenes (its example assets are not part
+of the checkout), so the workloads are generated: a Cornell box, a 2.1M
+triangle instanced scene with Disney materials under an importance-sampled
+procedural sky, and a participating-media scene.  Every generator writes a
+reference-format JSON file plus its assets (``.bm`` meshes in the layout of
+src/factory/src/utility/bin_mesh.cpp, ``.pfm`` float environment maps, ``.bin``
+density grids in the layout of src/factory/src/utility/texture3d_loader.cpp)
+and rounds every float written into JSON to 6 decimals, matching the
+reference's std::to_string round trip of JSON numbers.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = ["cornell_box", "instanced_disney", "media_scene", "write_bm", "write_pfm", "write_grid",
+           "icosphere", "heightfield", "cache_dir", "SCENES"]
+
+
+def r6(x) -> float:
+    return float(f"{float(x):.6f}")
+
+
+def v3(a) -> list:
+    return [r6(a[0]), r6(a[1]), r6(a[2])]
+
+
+def cache_dir() -> Path:
+    d = Path(os.environ.get("ATRC_SCENE_CACHE", "/tmp/atrc_scenes"))
+    d.mkdir(parents=True, exist_ok=True)
+    return d
+
+
+# ------------------------------------------------------------------ writers
+def write_bm(path: Path, pos: np.ndarray, nor: np.ndarray, uv: np.ndarray) -> None:
+    """pos, nor: (T, 3, 3) float32; uv: (T, 3, 2)."""
+    t = pos.shape[0]
+    data = np.concatenate([pos, nor, uv], axis=2).astype(np.float32)  # (T, 3, 8)
+    with open(path, "wb") as f:
+        f.write(np.uint64(t).tobytes())
+        f.write(np.ascontiguousarray(data).tobytes())
+
+
+def write_pfm(path: Path, rgb: np.ndarray) -> None:
+    """rgb: (H, W, 3), row 0 = top (v = 0).  PFM stores the bottom row first."""
+    h, w, _ = rgb.shape
+    with open(path, "wb") as f:
+        f.write(f"PF\n{w} {h}\n-1.0\n".encode())
+        f.write(np.ascontiguousarray(rgb[::-1].astype("<f4")).tobytes())
+
+
+def write_grid(path: Path, grid: np.ndarray) -> None:
+    """grid: (D, H, W) float32, z-major (texture3d_loader.cpp:11-37)."""
+    d, h, w = grid.shape
+    with open(path, "wb") as f:
+        f.write(np.array([w, h, d], dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(grid.astype("<f4")).tobytes())
+
+
+# -------------------------------------------------------------------- noise
+def _hash3(ix, iy, iz, seed):
+    h = (ix.astype(np.int64) * 73856093) ^ (iy.astype(np.int64) * 19349663) ^ (iz.astype(np.int64) * 83492791) ^ (
+        seed * 2654435761)
+    h = (h ^ (h >> 13)) * 1274126177
+    h = h ^ (h >> 16)
+    return (h & 0xFFFFFF).astype(np.float64) / float(0xFFFFFF)
+
+
+def value_noise3(p: np.ndarray, seed: int) -> np.ndarray:
+    """Trilinearly interpolated lattice value noise in [0, 1], smoothstep fade."""
+    fl = np.floor(p)
+    f = p - fl
+    f = f * f * (3 - 2 * f)
+    i = fl.astype(np.int64)
+    out = 0.0
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                w = (f[..., 0] if dx else 1 - f[..., 0]) * (f[..., 1] if dy else 1 - f[..., 1]) * (
+                    f[..., 2] if dz else 1 - f[..., 2])
+                out = out + w * _hash3(i[..., 0] + dx, i[..., 1] + dy, i[..., 2] + dz, seed)
+    return out
+
+
+def fbm3(p: np.ndarray, seed: int, octaves: int = 5, freq: float = 1.0) -> np.ndarray:
+    """Fractional Brownian motion of value noise, in about [-1, 1]."""
+    amp, total, norm = 1.0, 0.0, 0.0
+    for o in range(octaves):
+        total = total + amp * (value_noise3(p * freq * (2 ** o), seed + 17 * o) * 2 - 1)
+        norm += amp
+        amp *= 0.5
+    return total / norm
+
+
+# ------------------------------------------------------------------- meshes
+def _normals_from_faces(v: np.ndarray, f: np.ndarray) -> np.ndarray:
+    fn = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    vn = np.zeros_like(v)
+    for k in range(3):
+        np.add.at(vn, f[:, k], fn)
+    ln = np.linalg.norm(vn, axis=1, keepdims=True)
+    return vn / np.where(ln > 0, ln, 1)
+
+
+def icosphere(level: int, seed: int, amplitude: float = 0.05) -> tuple:
+    """Unit icosphere subdivided `level` times, radially displaced by 5-octave fBm."""
+    t = (1 + 5 ** 0.5) / 2
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(level):
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * (len(v) + 1) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a = uniq // (len(v) + 1)
+        b = uniq % (len(v) + 1)
+        mid = v[a] + v[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = len(v)
+        v = np.concatenate([v, mid])
+        nf = len(f)
+        m01, m12, m20 = inv[:nf] + base, inv[nf:2 * nf] + base, inv[2 * nf:] + base
+        f = np.concatenate([np.stack([f[:, 0], m01, m20], 1), np.stack([f[:, 1], m12, m01], 1),
+                            np.stack([f[:, 2], m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    disp = 1 + amplitude * fbm3(v * 2.0, seed, 5)
+    v = v * disp[:, None]
+    n = _normals_from_faces(v, f)
+    d = v / np.linalg.norm(v, axis=1, keepdims=True)
+    uv = np.stack([0.5 + np.arctan2(d[:, 1], d[:, 0]) / (2 * np.pi), np.arccos(np.clip(d[:, 2], -1, 1)) / np.pi], 1)
+    return v.astype(np.float32), n.astype(np.float32), uv.astype(np.float32), f
+
+
+def heightfield(res: int, seed: int, amplitude: float = 0.15) -> tuple:
+    """res x res vertices on [-1, 1]^2 (z up), heights from 5-octave fBm."""
+    xs = np.linspace(-1, 1, res)
+    X, Y = np.meshgrid(xs, xs, indexing="xy")
+    P = np.stack([X * 2, Y * 2, np.full_like(X, 0.37)], -1)
+    Z = amplitude * fbm3(P, seed, 5)
+    v = np.stack([X, Y, Z], -1).reshape(-1, 3)
+    i = np.arange(res - 1)
+    I, J = np.meshgrid(i, i, indexing="xy")
+    a = (J * res + I).ravel()
+    b, c, d = a + 1, a + res + 1, a + res
+    f = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)])
+    n = _normals_from_faces(v, f)
+    uv = np.stack([(X.ravel() + 1) / 2, (Y.ravel() + 1) / 2], 1)
+    return v.astype(np.float32), n.astype(np.float32), uv.astype(np.float32), f
+
+
+def _mesh_to_bm(path: Path, mesh) -> int:
+    v, n, uv, f = mesh
+    write_bm(path, v[f], n[f], uv[f])
+    return len(f)
+
+
+def _box_mesh(half: tuple) -> tuple:
+    """12-triangle axis-aligned box centred at the origin, outward faces."""
+    hx, hy, hz = half
+    c = np.array([[-hx, -hy, -hz], [hx, -hy, -hz], [hx, hy, -hz], [-hx, hy, -hz],
+                  [-hx, -hy, hz], [hx, -hy, hz], [hx, hy, hz], [-hx, hy, hz]], dtype=np.float32)
+    quads = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (2, 3, 7, 6), (1, 2, 6, 5), (0, 4, 7, 3)]
+    pos, nor, uv = [], [], []
+    for q in quads:
+        a, b, cc, d = (c[k] for k in q)
+        nrm = np.cross(b - a, cc - a)
+        nrm = nrm / np.linalg.norm(nrm)
+        for tri in ((a, b, cc), (a, cc, d)):
+            pos.append(np.stack(tri))
+            nor.append(np.stack([nrm] * 3))
+            uv.append(np.array([[0, 0], [1, 0], [1, 1]], dtype=np.float32))
+    return np.array(pos, np.float32), np.array(nor, np.float32), np.array(uv, np.float32)
+
+
+def _const(v) -> dict:
+    return {"type": "constant", "texel": v3(v) if np.ndim(v) else [r6(v)]}
+
+
+# ----------------------------------------------------------- Cornell (cfg 0)
+def cornell_box(out_dir: Path | None = None, seed: int = 1000, width: int = 256, height: int = 256, spp: int = 64,
+                renderer: str = "pt", max_depth: int = 8, min_depth: int = 2) -> Path:
+    """Plain pt on a seeded Cornell box: 5 quad walls of [-1,1]^3, two 12-triangle
+    boxes rotated by U[0, 30] degrees about y, a 0.5x0.5 quad light at the
+    ceiling with radiance (17, 12, 4), Lambertian albedos U[0.1, 0.8]^3 with a
+    red and a green wall, pinhole camera with 40 degree FOV, box filter."""
+    out = Path(out_dir) if out_dir else cache_dir() / f"cornell_{seed}"
+    out.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    alb = lambda: v3(rng.uniform(0.1, 0.8, 3))  # noqa: E731
+    walls = [  # (A, B, C, D) with normals facing the box interior, albedo
+        ([-1, -1, 1], [1, -1, 1], [1, -1, -1], [-1, -1, -1], alb()),   # floor (normal +y)
+        ([-1, 1, -1], [1, 1, -1], [1, 1, 1], [-1, 1, 1], alb()),       # ceiling (normal -y)
+        ([-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1], alb()),   # back (normal +z)
+        ([-1, -1, 1], [-1, -1, -1], [-1, 1, -1], [-1, 1, 1], [0.63, 0.065, 0.05]),  # left, red (+x)
+        ([1, -1, -1], [1, -1, 1], [1, 1, 1], [1, 1, -1], [0.14, 0.45, 0.091]),     # right, green (-x)
+    ]
+    ents = []
+    for a, b, c, d, al in walls:
+        ents.append({"type": "geometric",
+                     "geometry": {"type": "quad", "A": v3(a), "B": v3(b), "C": v3(c), "D": v3(d), "transform": []},
+                     "material": {"type": "ideal_diffuse", "albedo": _const(al)}})
+    specs = [((0.3, 0.6, 0.3), (-0.4, -0.4, -0.3)), ((0.3, 0.3, 0.3), (0.4, -0.7, 0.3))]
+    for k, (half, pos) in enumerate(specs):
+        p, n, uv = _box_mesh(half)
+        fn = out / f"box{k}.bm"
+        write_bm(fn, p, n, uv)
+        deg = r6(rng.uniform(0, 30))
+        ents.append({"type": "geometric",
+                     "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/" + fn.name,
+                                  "transform": [{"type": "translate", "offset": v3(pos)},
+                                                {"type": "rotate_y", "deg": deg}]},
+                     "material": {"type": "ideal_diffuse", "albedo": _const(rng.uniform(0.1, 0.8, 3))}})
+    ents.append({"type": "geometric",
+                 "geometry": {"type": "quad", "A": [-0.25, 0.999, -0.25], "B": [0.25, 0.999, -0.25],
+                              "C": [0.25, 0.999, 0.25], "D": [-0.25, 0.999, 0.25], "transform": []},
+                 "material": {"type": "ideal_black"}, "emit_radiance": [17, 12, 4]})
+    cfg = {"scene": {"type": "default", "entities": ents, "aggregate": {"type": "bvh"}},
+           "rendering": {"camera": {"type": "thin_lens", "pos": [0, 0, 3.8], "dst": [0, 0, 0], "up": [0, 1, 0],
+                                    "fov": 40},
+                         "width": width, "height": height,
+                         "renderer": {"type": renderer, "spp": spp, "max_depth": max_depth, "min_depth": min_depth},
+                         "reporter": {"type": "noout"},
+                         "film_filter": {"type": "box", "radius": 0.5}}}
+    path = out / "scene.json"
+    path.write_text(json.dumps(cfg, indent=1))
+    return path
+
+
+# ------------------------------------------------------------------ sky map
+def sky_map(width: int = 1024, height: int = 512, sun_dir=(0.3, -0.4, 0.866), sun_radius_deg: float = 0.5,
+            sun_peak: float = 5e4) -> np.ndarray:
+    """Procedural z-up sky: gradient plus a sun lobe (row 0 = zenith, v = theta / pi)."""
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = v * np.pi
+    phi = u * 2 * np.pi
+    T, P = np.meshgrid(theta, phi, indexing="ij")
+    d = np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], -1)
+    z = d[..., 2]
+    top, horizon, ground = np.array([0.25, 0.45, 1.0]), np.array([0.9, 0.85, 0.8]), np.array([0.18, 0.15, 0.12])
+    t = np.clip(z, 0, 1)[..., None]
+    sky = np.where(z[..., None] >= 0, horizon * (1 - t) + top * t, ground + (horizon - ground) * np.exp(8 * z)[..., None])
+    s = np.asarray(sun_dir, np.float64)
+    s /= np.linalg.norm(s)
+    ang = np.arccos(np.clip(d @ s, -1, 1))
+    r = math.radians(sun_radius_deg)
+    sun = sun_peak * np.exp(-(ang / r) ** 2 * 2.0)[..., None] * np.array([1.0, 0.92, 0.82])
+    return (sky + sun).astype(np.float32)
+
+
+def _rand_rotation(rng) -> np.ndarray:
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    a, b, c, d = q
+    return np.array([[a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
+                     [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
+                     [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d]])
+
+
+# --------------------------------------------------- instanced Disney (cfg 1)
+def instanced_disney(out_dir: Path | None = None, seed: int = 1001, width: int = 1920, height: int = 1080,
+                     spp: int = 256, max_depth: int = 16, renderer: str = "pt_cuda", ico_level: int = 7,
+                     hf_res: int = 1024, instances: int = 64) -> Path:
+    """64 instances (transform_wrapper + reference) of 4 seeded meshes -- three
+    level-7 fBm-displaced icospheres (327,680 triangles each) and a 1024x1024
+    heightfield (2,093,058 triangles) -- with uniform random translations in
+    [-20, 20]^3, scales in [0.5, 3] and rotations; Disney materials with
+    roughness U[0.05, 1], metallic Bernoulli(0.3), base colour U[0.05, 0.95]^3;
+    an importance-sampled 1024x512 procedural sky with a 0.5 degree sun of
+    peak 5e4."""
+    tag = f"inst_{seed}_{ico_level}_{hf_res}_{instances}"
+    out = Path(out_dir) if out_dir else cache_dir() / tag
+    out.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    mesh_files = []
+    for k in range(3):
+        fn = out / f"ico{k}.bm"
+        if not fn.exists():
+            _mesh_to_bm(fn, icosphere(ico_level, seed + 11 * k))
+        mesh_files.append(fn.name)
+    fn = out / "heightfield.bm"
+    if not fn.exists():
+        _mesh_to_bm(fn, heightfield(hf_res, seed + 97))
+    mesh_files.append(fn.name)
+    env = out / "sky.pfm"
+    if not env.exists():
+        write_pfm(env, sky_map())
+    meshes = {f"mesh{k}": {"type": "triangle_bvh", "filename": "${scene-directory}/" + m, "transform": []}
+              for k, m in enumerate(mesh_files)}
+    ents = []
+    for i in range(instances):
+        m = int(rng.integers(0, 4))
+        tr = rng.uniform(-20, 20, 3)
+        sc = rng.uniform(0.5, 3)
+        R = _rand_rotation(rng)
+        mat = {"type": "disney",
+               "base_color": _const(rng.uniform(0.05, 0.95, 3)),
+               "metallic": _const(1.0 if rng.random() < 0.3 else 0.0),
+               "roughness": _const(rng.uniform(0.05, 1.0))}
+        ents.append({"type": "geometric",
+                     "geometry": {"type": "transform_wrapper",
+                                  "internal": {"type": "reference", "name": ["meshes", f"mesh{m}"]},
+                                  "transform": [{"type": "translate", "offset": v3(tr)},
+                                                {"type": "mat3", "row_major": [r6(x) for x in R.ravel()]},
+                                                {"type": "scale", "ratio": r6(sc)}]},
+                     "material": mat})
+    cfg = {"scene": {"type": "default", "entities": ents, "aggregate": {"type": "bvh"}, "meshes": meshes,
+                     "env": {"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/sky.pfm"}}},
+           "rendering": {"camera": {"type": "thin_lens", "pos": [0, -48, 18], "dst": [0, 0, 0], "up": [0, 0, 1],
+                                    "fov": 55},
+                         "width": width, "height": height,
+                         "renderer": {"type": renderer, "spp": spp, "max_depth": max_depth},
+                         "reporter": {"type": "noout"}}}
+    path = out / "scene.json"
+    path.write_text(json.dumps(cfg))
+    return path
+
+
+# ----------------------------------------------------------- media (cfg 2)
+def media_scene(out_dir: Path | None = None, seed: int = 1002, width: int = 1024, height: int = 1024, spp: int = 512,
+                max_depth: int = 32, renderer: str = "pt_cuda", grid_res: int = 128, sphere_level: int = 6) -> Path:
+    """A homogeneous box medium (sigma_a 0.05, sigma_s 0.5, g 0.6) and a 128^3
+    fBm density grid scaled to sigma_t in [0, 8] (albedo 0.9, delta tracking)
+    enclosing a displaced sphere, two quad lights and the procedural sky."""
+    out = Path(out_dir) if out_dir else cache_dir() / f"media_{seed}_{grid_res}_{sphere_level}"
+    out.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    env = out / "sky.pfm"
+    if not env.exists():
+        write_pfm(env, sky_map())
+    g = out / "density.bin"
+    if not g.exists():
+        xs = (np.arange(grid_res) + 0.5) / grid_res
+        Z, Y, X = np.meshgrid(xs, xs, xs, indexing="ij")
+        d = fbm3(np.stack([X, Y, Z], -1) * 4, seed, 5)
+        d = (d - d.min()) / (d.max() - d.min()) * 8.0
+        write_grid(g, d.astype(np.float32))
+    sph = out / "sphere.bm"
+    if not sph.exists():
+        _mesh_to_bm(sph, icosphere(sphere_level, seed + 5, 0.05))
+    unit_box = lambda: {"type": "triangle_bvh", "filename": "${scene-directory}/unitbox.bm"}  # noqa: E731
+    p, n, uv = _box_mesh((0.5, 0.5, 0.5))
+    write_bm(out / "unitbox.bm", p + 0.5, n, uv)  # [0,1]^3, outward
+    ents = [
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-6, -6, -1], "B": [6, -6, -1], "C": [6, 6, -1],
+                                           "D": [-6, 6, -1], "transform": []},
+         "material": {"type": "ideal_diffuse", "albedo": _const([0.6, 0.6, 0.6])}},
+        {"type": "geometric", "geometry": {**unit_box(), "transform": [{"type": "translate", "offset": [-2.6, -1, -1]},
+                                                                        {"type": "scale", "ratio": 2}]},
+         "material": {"type": "invisible_surface"},
+         "med_in": {"type": "homogeneous", "sigma_a": [0.05], "sigma_s": [0.5], "g": 0.6}},
+        {"type": "geometric", "geometry": {**unit_box(), "transform": [{"type": "translate", "offset": [0.4, -1.2, -1]},
+                                                                        {"type": "scale", "ratio": 2.4}]},
+         "material": {"type": "invisible_surface"},
+         "med_in": {"type": "heterogeneous",
+                    "transform": [{"type": "translate", "offset": [0.4, -1.2, -1]}, {"type": "scale", "ratio": 2.4}],
+                    "density": {"type": "image3d", "format": "real", "binary_filename": "${scene-directory}/density.bin"},
+                    "albedo": {"type": "constant", "texel": [0.9]},
+                    "g": {"type": "constant", "texel": [0.0]}}},
+        {"type": "geometric", "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/sphere.bm",
+                                           "transform": [{"type": "translate", "offset": [1.6, 0, 0.2]},
+                                                         {"type": "scale", "ratio": 0.6}]},
+         "material": {"type": "disney", "base_color": _const([0.8, 0.3, 0.2]), "metallic": _const(0.0),
+                      "roughness": _const(0.4)}},
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-1, -1, 4], "B": [-1, 1, 4], "C": [1, 1, 4],
+                                           "D": [1, -1, 4], "transform": [{"type": "translate", "offset": [-3, 0, 0]}]},
+         "material": {"type": "ideal_black"}, "emit_radiance": [8, 8, 8]},
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-0.5, -0.5, 3], "B": [-0.5, 0.5, 3], "C": [0.5, 0.5, 3],
+                                           "D": [0.5, -0.5, 3], "transform": [{"type": "translate", "offset": [3, 1, 0]}]},
+         "material": {"type": "ideal_black"}, "emit_radiance": [20, 16, 10]},
+    ]
+    cfg = {"scene": {"type": "default", "entities": ents, "aggregate": {"type": "bvh"},
+                     "env": {"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/sky.pfm"}}},
+           "rendering": {"camera": {"type": "thin_lens", "pos": [0, -9, 3], "dst": [0, 0, 0], "up": [0, 0, 1], "fov": 45},
+                         "width": width, "height": height,
+                         "renderer": {"type": renderer, "spp": spp, "max_depth": max_depth},
+                         "reporter": {"type": "noout"}}}
+    path = out / "scene.json"
+    path.write_text(json.dumps(cfg))
+    return path
+
+
+SCENES = {"cornell": cornell_box, "instanced": instanced_disney, "media": media_scene}

@@ -1,0 +1,399 @@
+/*
+ * atrc_cuda.h — C ABI of the B200 path tracer (`pt_cuda`).
+ *
+ * Two layers live behind this header, both exported from libatrc_cuda.so:
+ *
+ *  1. Scene ingestion (host only, no GPU needed).  The Atrc JSON scene format
+ *     is parsed by a factory that mirrors the reference's creators and is
+ *     flattened into the POD `AtrcSceneDesc` below.  This replaces the
+ *     reference's `CreatingContext::create<Scene>` path
+ *     (src/factory/include/agz/factory/context.h:280-300,
+ *      src/factory/src/creator/scene_creators.cpp:24-65) plus the parsing of
+ *     `rendering` settings (src/factory/src/utility/render_session.cpp:14-66).
+ *
+ *  2. Device execution.  `atrc_cuda_scene_create` uploads a scene and builds the
+ *     device acceleration structure; `atrc_cuda_trace_rays` replaces
+ *     `Scene::closest_intersection / has_intersection`
+ *     (src/tracer/include/agz/tracer/core/scene.h, aggregate.h;
+ *      src/tracer/src/core/scene/scene_default.cpp:136-147) for batches of rays;
+ *     `atrc_cuda_render` replaces `Renderer::render` of the `pt` renderer
+ *     (src/tracer/include/agz/tracer/core/renderer.h:33-35,
+ *      src/tracer/src/core/renderer/pt.cpp:8-48,
+ *      src/tracer/src/core/renderer/perpixel_renderer.cpp:13-207).
+ *
+ * Conventions
+ *  - Every function returns int: 0 on success, a negative AtrcStatus on error.
+ *    The message of the last error on the calling thread is available from
+ *    atrc_last_error().
+ *  - Handles are opaque, owned by the caller, and destroyed explicitly.
+ *  - Calls block the calling thread.  One CUDA stream per device scene is used
+ *    internally.  A scene handle is not re-entrant; distinct handles may be
+ *    used from distinct threads.
+ *  - Vectors are float[3] (x, y, z); colours are float[3] (r, g, b).
+ *  - Affine transforms are row-major 3x4 matrices m[12]: row r = (m[4r+0],
+ *    m[4r+1], m[4r+2], m[4r+3]); p' = M[:, :3] p + M[:, 3].
+ */
+#ifndef ATRC_CUDA_H
+#define ATRC_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATRC_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status */
+
+typedef enum AtrcStatus {
+    ATRC_OK               = 0,
+    ATRC_ERR_INVALID_ARG  = -1,  /* bad pointer, size or enum value          */
+    ATRC_ERR_CONFIG       = -2,  /* malformed JSON / unknown creator / file  */
+    ATRC_ERR_OUT_OF_MEMORY= -3,  /* host or device allocation failed         */
+    ATRC_ERR_CUDA         = -4,  /* CUDA runtime error or no usable device   */
+    ATRC_ERR_CANCELLED    = -5,  /* the cancel flag was raised               */
+    ATRC_ERR_WATCHDOG     = -6,  /* a device loop hit its iteration cap      */
+    ATRC_ERR_UNSUPPORTED  = -7   /* scene feature outside pt_cuda's support  */
+} AtrcStatus;
+
+/* ---------------------------------------------------------- scene format */
+
+typedef struct AtrcTransform {
+    float m[12];    /* local -> world, row-major 3x4                         */
+    float inv[12];  /* world -> local, row-major 3x4 (computed on the host)  */
+} AtrcTransform;
+
+/* Triangle mesh in the reference's `.bm` memory layout: per triangle three
+ * vertices of {position[3], normal[3], tex_coord[2]} floats (96 bytes), in the
+ * file's original order (src/factory/src/utility/bin_mesh.cpp:7-27). */
+typedef struct AtrcMeshDesc {
+    uint64_t     triangle_count;
+    const float* vertices;      /* triangle_count * 24 floats */
+} AtrcMeshDesc;
+
+typedef enum AtrcGeometryType {
+    ATRC_GEOM_TRIANGLE_BVH = 0,  /* mesh, vertices baked by `transform`      */
+    ATRC_GEOM_TRIANGLE     = 1,  /* single triangle, ray moved to local space*/
+    ATRC_GEOM_QUAD         = 2,  /* ABC + ACD, vertices baked by `transform` */
+    ATRC_GEOM_SPHERE       = 3,  /* radius around local origin               */
+    ATRC_GEOM_DISK         = 4   /* radius, local z = normal                 */
+} AtrcGeometryType;
+
+/* A leaf geometry as created by its creator
+ * (src/factory/src/creator/geometry_creators.cpp).  Leaf geometries may be
+ * shared by several entities through the `reference` creator. */
+typedef struct AtrcGeometryDesc {
+    int32_t       type;          /* AtrcGeometryType                         */
+    int32_t       mesh;          /* index into meshes (TRIANGLE_BVH)         */
+    AtrcTransform transform;     /* the geometry's own `transform` list      */
+    float         p[4][3];       /* A, B, C (, D) for TRIANGLE / QUAD        */
+    float         uv[4][2];      /* tA, tB, tC (, tD)                        */
+    float         radius;        /* SPHERE / DISK                            */
+    int32_t       pad_;
+} AtrcGeometryDesc;
+
+/* A `geometric` entity (src/tracer/src/core/entity/geometric.cpp:10-58).
+ * The entity's geometry chain is flattened into: an optional instance
+ * transform (`transform_wrapper`, transform_wrapper.cpp:51-68), an optional
+ * `double_sided` adapter, and a leaf geometry. */
+typedef struct AtrcEntityDesc {
+    int32_t       geometry;      /* leaf geometry index                      */
+    int32_t       has_instance;  /* 1 if wrapped by transform_wrapper        */
+    AtrcTransform instance;      /* transform_wrapper local -> world         */
+    int32_t       double_sided;  /* 1 if wrapped by double_sided             */
+    int32_t       material;      /* material index                           */
+    int32_t       medium_in;     /* medium index (0 = the void medium)       */
+    int32_t       medium_out;
+    float         emit_radiance[3];
+    int32_t       no_denoise;
+    float         power;         /* user light power, <= 0 means automatic   */
+    int32_t       pad_;
+} AtrcEntityDesc;
+
+typedef enum AtrcTextureType {
+    ATRC_TEX_CONSTANT = 0,
+    ATRC_TEX_IMAGE    = 1        /* float RGB texels (`hdr`, `image`)        */
+} AtrcTextureType;
+
+typedef enum AtrcWrapMode {
+    ATRC_WRAP_CLAMP = 0, ATRC_WRAP_REPEAT = 1, ATRC_WRAP_MIRROR = 2
+} AtrcWrapMode;
+
+/* Texture2D (src/tracer/include/agz/tracer/core/texture2d.h:55-174). */
+typedef struct AtrcTexture2DDesc {
+    int32_t      type;           /* AtrcTextureType                          */
+    float        texel[3];       /* CONSTANT                                 */
+    int32_t      width, height;  /* IMAGE                                    */
+    const float* data;           /* IMAGE: height rows of width RGB floats,  */
+                                 /* row 0 is v = 0                           */
+    int32_t      nearest;        /* 1 = nearest, 0 = bilinear                */
+    float        uv_transform[6];/* 2x3 row-major affine applied to uv       */
+    int32_t      wrap_u, wrap_v; /* AtrcWrapMode                             */
+    float        inv_gamma;
+    int32_t      pad_;
+} AtrcTexture2DDesc;
+
+/* Texture3D (src/tracer/include/agz/tracer/core/texture3d.h:30-223). */
+typedef struct AtrcTexture3DDesc {
+    int32_t      type;           /* AtrcTextureType                          */
+    float        texel[3];
+    int32_t      width, height, depth;
+    int32_t      channels;       /* 1 (real/gray8) or 3 (spec/rgb8)          */
+    const float* data;           /* depth x height x width x channels, z-major */
+    int32_t      nearest;
+    float        uvw_transform[12]; /* 3x4 row-major affine on uvw          */
+    int32_t      uvw_perm[3];
+    int32_t      wrap[3];
+    float        inv_gamma;
+    float        max_real;       /* max over texels of the real channel      */
+} AtrcTexture3DDesc;
+
+typedef enum AtrcMaterialType {
+    ATRC_MAT_IDEAL_DIFFUSE     = 0,
+    ATRC_MAT_IDEAL_BLACK       = 1,
+    ATRC_MAT_DISNEY            = 2,
+    ATRC_MAT_INVISIBLE_SURFACE = 3
+} AtrcMaterialType;
+
+/* Disney texture slots, in the order of create_disney
+ * (src/factory/src/creator/material_creators.cpp:56-113). */
+typedef enum AtrcDisneySlot {
+    ATRC_DISNEY_BASE_COLOR = 0, ATRC_DISNEY_METALLIC, ATRC_DISNEY_ROUGHNESS,
+    ATRC_DISNEY_TRANSMISSION, ATRC_DISNEY_TRANSMISSION_ROUGHNESS,
+    ATRC_DISNEY_IOR, ATRC_DISNEY_SPECULAR_SCALE, ATRC_DISNEY_SPECULAR_TINT,
+    ATRC_DISNEY_ANISOTROPIC, ATRC_DISNEY_SHEEN, ATRC_DISNEY_SHEEN_TINT,
+    ATRC_DISNEY_CLEARCOAT, ATRC_DISNEY_CLEARCOAT_GLOSS,
+    ATRC_DISNEY_SLOT_COUNT
+} AtrcDisneySlot;
+
+typedef struct AtrcMaterialDesc {
+    int32_t type;                    /* AtrcMaterialType                      */
+    int32_t tex[ATRC_DISNEY_SLOT_COUNT]; /* texture2d indices; IDEAL_DIFFUSE */
+                                     /* uses tex[0] as albedo                */
+    int32_t normal_map;              /* texture2d index or -1                */
+} AtrcMaterialDesc;
+
+typedef enum AtrcMediumType {
+    ATRC_MED_VOID = 0, ATRC_MED_HOMOGENEOUS = 1, ATRC_MED_HETEROGENEOUS = 2
+} AtrcMediumType;
+
+typedef struct AtrcMediumDesc {
+    int32_t       type;              /* AtrcMediumType                       */
+    float         sigma_a[3];        /* HOMOGENEOUS                          */
+    float         sigma_s[3];
+    float         g;
+    int32_t       max_scattering_count;
+    AtrcTransform transform;         /* HETEROGENEOUS: texture space -> world*/
+    int32_t       density, albedo, g_tex;  /* texture3d indices             */
+    int32_t       white_for_indirect;      /* heterogeneous.cpp:107-110     */
+} AtrcMediumDesc;
+
+typedef enum AtrcEnvType {
+    ATRC_ENV_NONE = 0, ATRC_ENV_IBL = 1, ATRC_ENV_NATIVE_SKY = 2
+} AtrcEnvType;
+
+typedef struct AtrcEnvDesc {
+    int32_t type;                    /* AtrcEnvType                          */
+    int32_t tex;                     /* IBL texture2d index                  */
+    int32_t no_importance_sampling;
+    float   power;
+    float   top[3], bottom[3];       /* NATIVE_SKY                           */
+} AtrcEnvDesc;
+
+typedef enum AtrcAggregateType {
+    ATRC_AGG_NATIVE = 0, ATRC_AGG_BVH = 1
+} AtrcAggregateType;
+
+typedef struct AtrcSceneDesc {
+    uint32_t abi_version;            /* ATRC_ABI_VERSION                     */
+    int32_t  aggregate;              /* AtrcAggregateType (CPU semantics)    */
+    int32_t  aggregate_max_leaf_size;
+    int32_t  pad_;
+    const AtrcMeshDesc*      meshes;     uint32_t mesh_count;
+    const AtrcGeometryDesc*  geometries; uint32_t geometry_count;
+    const AtrcEntityDesc*    entities;   uint32_t entity_count;
+    const AtrcMaterialDesc*  materials;  uint32_t material_count;
+    const AtrcTexture2DDesc* textures2d; uint32_t texture2d_count;
+    const AtrcTexture3DDesc* textures3d; uint32_t texture3d_count;
+    const AtrcMediumDesc*    media;      uint32_t medium_count; /* [0]=void */
+    AtrcEnvDesc env;
+} AtrcSceneDesc;
+
+/* ------------------------------------------------------ render settings */
+
+typedef enum AtrcFilterType { ATRC_FILTER_BOX = 0, ATRC_FILTER_GAUSSIAN = 1 } AtrcFilterType;
+
+typedef struct AtrcCameraDesc {      /* thin_lens (thin_lens.cpp:34-94)      */
+    float pos[3], dst[3], up[3];
+    float fov;                       /* radians, vertical                    */
+    float lens_radius;
+    float focal_distance;
+} AtrcCameraDesc;
+
+typedef struct AtrcRenderDesc {
+    int32_t  width, height;
+    int32_t  spp;
+    int32_t  min_depth, max_depth;   /* pt keys (renderer_creators.cpp:127-146) */
+    float    cont_prob;
+    int32_t  specular_depth;
+    int32_t  use_mis;
+    int32_t  filter_type;            /* AtrcFilterType                       */
+    float    filter_radius;          /* user radius (box: 0.5 by default)    */
+    float    filter_alpha;           /* gaussian                             */
+    float    eps;                    /* scene epsilon (default 3e-4)         */
+    uint64_t seed;                   /* random stream selector               */
+    int32_t  first_spp;              /* render sample indices                */
+    int32_t  spp_count;              /* [first_spp, first_spp + spp_count)   */
+                                     /* of every pixel; 0 means all of spp   */
+    AtrcCameraDesc camera;
+    int32_t  path_pool;              /* wavefront path capacity, 0 = auto    */
+    int32_t  pad_;
+} AtrcRenderDesc;
+
+/* FP64 film accumulators, caller allocated, `width*height` pixels each.
+ * Any pointer except `value` and `weight` may be NULL.  The renderer ADDS
+ * into them (so several calls accumulate); the image is value / weight. */
+typedef struct AtrcFilm {
+    double* value;     /* 3 per pixel: sum of w * L                          */
+    double* weight;    /* 1 per pixel: sum of w                              */
+    double* value_sq;  /* 3 per pixel: sum of w * L^2 (for variance tests)   */
+    double* albedo;    /* 3 per pixel: sum of w * first-hit albedo           */
+    double* normal;    /* 3 per pixel: sum of w * first-hit shading normal   */
+    double* denoise;   /* 1 per pixel: sum of w * denoise flag               */
+    int32_t on_device; /* 1 if the pointers above are device pointers        */
+    int32_t pad_;
+} AtrcFilm;
+
+typedef struct AtrcRenderStats {
+    double   seconds;          /* wall time of the render call               */
+    double   kernel_seconds;   /* device time of the wavefront loop          */
+    uint64_t samples;          /* camera samples completed                   */
+    uint64_t rays_closest;     /* closest-hit rays traced                    */
+    uint64_t rays_shadow;      /* any-hit (shadow) rays traced               */
+    uint64_t iterations;       /* wavefront iterations                       */
+    uint64_t kernel_launches;  /* kernels launched by this call              */
+    uint64_t watchdog_flags;   /* device loops that hit their caps           */
+    double   extend_seconds;   /* device time inside closest-hit kernels     */
+    double   shadow_seconds;   /* device time inside any-hit kernels         */
+    double   shade_seconds;    /* device time inside shading kernels         */
+    uint64_t h2d_bytes, d2h_bytes;
+} AtrcRenderStats;
+
+/* Progress callback, fired on the calling thread between wavefront
+ * iterations with a percentage in [0, 100]. */
+typedef void (*AtrcProgressFn)(double percent, void* user);
+
+/* ------------------------------------------------------------ ray queries */
+
+typedef struct AtrcRay {       /* 32 bytes */
+    float o[3];
+    float t_min;
+    float d[3];                /* not necessarily normalised                 */
+    float t_max;
+} AtrcRay;
+
+typedef struct AtrcHit {       /* 16 bytes */
+    float    t;                /* hit distance; -1 when nothing was hit      */
+    int32_t  entity;           /* entity index or -1                         */
+    int32_t  prim;             /* ORIGINAL triangle index within the mesh,   */
+                               /* 0/1 = quad half ABC/ACD, 0 otherwise       */
+    float    u;                /* barycentric alpha (or 0)                   */
+} AtrcHit;
+
+typedef enum AtrcQueryMode { ATRC_QUERY_CLOSEST = 0, ATRC_QUERY_ANY = 1 } AtrcQueryMode;
+
+/* ------------------------------------------------------------- functions */
+
+typedef struct AtrcConfig AtrcConfig;   /* parsed JSON config (host)        */
+typedef struct AtrcScene  AtrcScene;    /* device scene                     */
+
+typedef struct AtrcDeviceInfo {
+    char    name[128];
+    int32_t sm_count;
+    int32_t cc_major, cc_minor;
+    int32_t pad_;
+    uint64_t global_mem_bytes;
+} AtrcDeviceInfo;
+
+/* Version of the ABI the library was built with. */
+int atrc_abi_version(void);
+
+/* sizeof of the ABI structs as compiled into the library, in this order:
+ * AtrcSceneDesc, AtrcMeshDesc, AtrcGeometryDesc, AtrcEntityDesc,
+ * AtrcTexture2DDesc, AtrcTexture3DDesc, AtrcMaterialDesc, AtrcMediumDesc,
+ * AtrcEnvDesc, AtrcRenderDesc, AtrcFilm, AtrcRenderStats, AtrcRay, AtrcHit,
+ * AtrcDeviceInfo.  Writes min(n, 15) values; returns 15.  Lets bindings in
+ * other languages verify their struct layouts. */
+int atrc_abi_struct_sizes(uint64_t* sizes, int n);
+
+/* Thread-local message of the last failing call ("" if none). */
+const char* atrc_last_error(void);
+
+/* Parse an Atrc JSON configuration ({"scene": ..., "rendering": ...}) from a
+ * file.  `${scene-directory}` maps to the file's directory and
+ * `${working-directory}` to the current directory (src/cli/src/main.cpp:29-41).
+ * Replaces json_to_config + CreatingContext::create<Scene>. */
+int atrc_config_load_file(const char* path, AtrcConfig** out);
+
+/* Same, from a JSON string; `scene_dir` stands for ${scene-directory}. */
+int atrc_config_load_string(const char* json, const char* scene_dir,
+                            AtrcConfig** out);
+
+void atrc_config_destroy(AtrcConfig* cfg);
+
+/* Flattened scene owned by `cfg` (valid until atrc_config_destroy). */
+int atrc_config_scene(const AtrcConfig* cfg, const AtrcSceneDesc** out);
+
+/* Number of `rendering` entries (1 for an object, N for an array). */
+int atrc_config_rendering_count(const AtrcConfig* cfg, int* out);
+
+/* Rendering settings of entry `index`.  `renderer_type` receives the
+ * renderer's `type` string (e.g. "pt" or "pt_cuda"), at most cap bytes. */
+int atrc_config_rendering(const AtrcConfig* cfg, int index,
+                          AtrcRenderDesc* out,
+                          char* renderer_type, size_t cap);
+
+/* Post-processing list of entry `index` as a JSON text (for the CLI). */
+int atrc_config_post_processors(const AtrcConfig* cfg, int index,
+                                char* json_out, size_t cap, size_t* needed);
+
+/* Query device 0..N-1 and make it current for this thread. */
+int atrc_cuda_device_init(int device, AtrcDeviceInfo* info);
+
+/* Upload a scene and build its acceleration structure on the current device.
+ * The description is copied; the caller may free it afterwards. */
+int atrc_cuda_scene_create(const AtrcSceneDesc* desc, AtrcScene** out);
+
+void atrc_cuda_scene_destroy(AtrcScene* scene);
+
+/* Trace `n` rays from host memory into host `hits`.  mode: AtrcQueryMode.
+ * ANY mode writes t = 1 / entity = 0 for an occluded ray and t = -1 otherwise.
+ * `exact` = 1 selects the reference-exact Moller-Trumbore test (same
+ * operation order, no fused multiply-add), 0 the fast test. */
+int atrc_cuda_trace_rays(AtrcScene* scene, const AtrcRay* rays, size_t n,
+                         AtrcHit* hits, int mode, int exact);
+
+/* Same with device pointers (no copies). */
+int atrc_cuda_trace_rays_device(AtrcScene* scene, const AtrcRay* d_rays,
+                                size_t n, AtrcHit* d_hits, int mode, int exact);
+
+/* Render `desc` (a pt_cuda / pt configuration) and ADD the samples into
+ * `film`.  `cancel` (may be NULL) is polled between wavefront iterations;
+ * raising it ends the call with ATRC_ERR_CANCELLED after the samples already
+ * taken are in the film.  `progress` (may be NULL) is called on this thread. */
+int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc,
+                     AtrcFilm* film, volatile const int* cancel,
+                     AtrcProgressFn progress, void* user,
+                     AtrcRenderStats* stats);
+
+/* Average the accumulators into an image: rgb[3*i] = value / weight (0 where
+ * weight == 0); host pointers. */
+int atrc_film_resolve(const AtrcFilm* film, int width, int height, float* rgb);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATRC_CUDA_H */

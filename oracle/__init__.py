@@ -1,0 +1,121 @@
+"""ctypes binding of the CPU oracle (``oracle/build/liboracle.so``).
+
+TEST INFRASTRUCTURE ONLY: tests/, ``__graft_entry__.smoke()`` and the CPU
+baseline of ``bench.py`` use it as the checker / the timed CPU baseline.  The
+product package ``atrc_b200`` never imports it.  Parity status: unpinned (the
+reference has no golden vectors and cannot be built here; see oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from atrc_b200 import _abi as abi
+from atrc_b200 import HIT_DTYPE, RAY_DTYPE
+
+SO = Path(__file__).resolve().parent / "build" / "liboracle.so"
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not SO.exists():
+            from atrc_b200.build import build_oracle
+            build_oracle()
+        lib = C.CDLL(str(SO))
+        lib.oracle_last_error.restype = C.c_char_p
+        lib.oracle_scene_create.argtypes = [C.POINTER(abi.AtrcSceneDesc), C.c_float, C.POINTER(C.c_void_p)]
+        lib.oracle_scene_destroy.argtypes = [C.c_void_p]
+        lib.oracle_scene_destroy.restype = None
+        lib.oracle_trace_rays.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRay), C.c_size_t, C.POINTER(abi.AtrcHit),
+                                          C.c_int, C.c_int]
+        lib.oracle_prim_hit.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRay), C.c_int, C.c_int, C.POINTER(C.c_float)]
+        lib.oracle_render.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRenderDesc), C.POINTER(abi.AtrcFilm), C.c_int]
+        lib.oracle_env_pdf.argtypes = [C.c_void_p, abi.c_float_p, C.c_size_t, abi.c_float_p]
+        lib.oracle_env_sample.argtypes = [C.c_void_p, abi.c_float_p, C.c_size_t, abi.c_float_p, abi.c_float_p]
+        lib.oracle_bsdf_eval.argtypes = [C.c_void_p, C.c_int, abi.c_float_p, abi.c_float_p, C.c_size_t,
+                                         abi.c_float_p, abi.c_float_p]
+        lib.oracle_bsdf_sample.argtypes = [C.c_void_p, C.c_int, abi.c_float_p, abi.c_float_p, C.c_size_t,
+                                           abi.c_float_p, abi.c_float_p, abi.c_float_p, C.POINTER(C.c_int)]
+        _lib = lib
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(f"oracle error {rc}: {load().oracle_last_error().decode()}")
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(abi.c_float_p)
+
+
+class OracleScene:
+    def __init__(self, scene_desc_ptr, eps: float = 3e-4):
+        lib = load()
+        h = C.c_void_p()
+        _check(lib.oracle_scene_create(scene_desc_ptr, eps, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.oracle_scene_destroy(self._h)
+            self._h = None
+
+    def trace_rays(self, rays: np.ndarray, mode: str = "closest", threads: int = 0) -> np.ndarray:
+        r = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        hits = np.empty(len(r), dtype=HIT_DTYPE)
+        _check(load().oracle_trace_rays(self._h, r.ctypes.data_as(C.POINTER(abi.AtrcRay)), len(r),
+                                        hits.ctypes.data_as(C.POINTER(abi.AtrcHit)), 0 if mode == "closest" else 1,
+                                        threads))
+        return hits
+
+    def prim_hit(self, ray: np.ndarray, entity: int, prim: int) -> float:
+        r = np.ascontiguousarray(ray, dtype=RAY_DTYPE).reshape(1)
+        t = C.c_float()
+        _check(load().oracle_prim_hit(self._h, r.ctypes.data_as(C.POINTER(abi.AtrcRay)), entity, prim, C.byref(t)))
+        return t.value
+
+    def render(self, desc: abi.AtrcRenderDesc, film, threads: int = 0) -> None:
+        f = film.as_struct()
+        _check(load().oracle_render(self._h, C.byref(desc), C.byref(f), threads))
+
+    def env_pdf(self, dirs: np.ndarray) -> np.ndarray:
+        d = np.ascontiguousarray(dirs, dtype=np.float32)
+        out = np.empty(len(d), dtype=np.float32)
+        _check(load().oracle_env_pdf(self._h, _fp(d), len(d), _fp(out)))
+        return out
+
+    def env_sample(self, u3: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        u = np.ascontiguousarray(u3, dtype=np.float32)
+        dirs = np.empty((len(u), 3), dtype=np.float32)
+        pdf = np.empty(len(u), dtype=np.float32)
+        _check(load().oracle_env_sample(self._h, _fp(u), len(u), _fp(dirs), _fp(pdf)))
+        return dirs, pdf
+
+    def bsdf_eval(self, material: int, wi: np.ndarray, wo: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        wi = np.ascontiguousarray(wi, dtype=np.float32)
+        wo = np.ascontiguousarray(wo, dtype=np.float32)
+        f = np.empty((len(wi), 3), dtype=np.float32)
+        pdf = np.empty(len(wi), dtype=np.float32)
+        _check(load().oracle_bsdf_eval(self._h, material, _fp(wi), _fp(wo), len(wi), _fp(f), _fp(pdf)))
+        return f, pdf
+
+    def bsdf_sample(self, material: int, wo: np.ndarray, u3: np.ndarray):
+        wo = np.ascontiguousarray(wo, dtype=np.float32)
+        u = np.ascontiguousarray(u3, dtype=np.float32)
+        n = len(wo)
+        wi = np.empty((n, 3), dtype=np.float32)
+        f = np.empty((n, 3), dtype=np.float32)
+        pdf = np.empty(n, dtype=np.float32)
+        delta = np.empty(n, dtype=np.int32)
+        _check(load().oracle_bsdf_sample(self._h, material, _fp(wo), _fp(u), n, _fp(wi), _fp(f), _fp(pdf),
+                                         delta.ctypes.data_as(C.POINTER(C.c_int))))
+        return wi, f, pdf, delta
+
+
+def hardware_threads() -> int:
+    return int(load().oracle_hardware_threads())

@@ -1,0 +1,78 @@
+/*
+ * oracle.h — C ABI of the CPU oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The oracle is a CPU restatement of the
+ * reference's `pt` hot path (AirGuanZ/Atrc, files cited in pt_oracle.cpp).
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load it, and only as the checker / the timed CPU baseline.  The product
+ * (libatrc_cuda.so) never links, loads or calls it.
+ *
+ * Parity status: unpinned.  The reference ships no tests, golden images or
+ * known-answer vectors for this path, and it cannot be compiled here (its
+ * agz-utils submodule is absent), so no reference output exists to pin the
+ * oracle to.  The analytic known-answer tests in tests/ (furnace, slab
+ * transmittance, MT edge cases, pdf normalisation) check it instead.
+ */
+#ifndef ATRC_ORACLE_H
+#define ATRC_ORACLE_H
+
+#include "../include/atrc_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OracleScene OracleScene;
+
+const char* oracle_last_error(void);
+
+/* Build the reference's object graph from a flattened scene: per-mesh
+ * midpoint/median BVH (triangle_bvh.cpp:122-304), entity BVH or native
+ * aggregate (entity_bvh.cpp:46-116, native_aggregate.cpp), lights in the
+ * order of scene_default.cpp:66-82.  `eps` is the scene epsilon. */
+int oracle_scene_create(const AtrcSceneDesc* desc, float eps, OracleScene** out);
+void oracle_scene_destroy(OracleScene* s);
+
+/* Closest / any hit for each ray (Scene::closest_intersection /
+ * has_intersection).  `threads` <= 0 uses all hardware threads. */
+int oracle_trace_rays(OracleScene* s, const AtrcRay* rays, size_t n,
+                      AtrcHit* hits, int mode, int threads);
+
+/* Reference-exact Moller-Trumbore test of one primitive of one entity against
+ * a world ray (ray moved to the entity's local space as transform_wrapper
+ * does).  Writes t (or -1 when the primitive is not hit).  Used to adjudicate
+ * hit mismatches. */
+int oracle_prim_hit(OracleScene* s, const AtrcRay* ray, int entity, int prim,
+                    float* t_out);
+
+/* Render with the reference's `pt` algorithm (perpixel_renderer.cpp:13-53 +
+ * path_tracing.cpp:15-225) and ADD into `film` (host pointers).  Samples
+ * [desc->first_spp, first_spp + spp_count) of every pixel are taken; tile
+ * random streams are seeded from (desc->seed, sample range, tile). */
+int oracle_render(OracleScene* s, const AtrcRenderDesc* desc, AtrcFilm* film,
+                  int threads);
+
+/* Number of hardware threads the oracle would use for threads <= 0. */
+int oracle_hardware_threads(void);
+
+/* Environment-light pdf / radiance probes (ibl.cpp, env_sampler.h), used by
+ * the pdf-normalisation known-answer test. */
+int oracle_env_pdf(OracleScene* s, const float* dirs, size_t n, float* pdf);
+int oracle_env_sample(OracleScene* s, const float* u3, size_t n, float* dirs,
+                      float* pdf);
+
+/* BSDF probes on a synthetic shading point (geometric frame = shading frame =
+ * world axes).  material: index into the scene's materials.  For each i:
+ * eval f(wi, wo) -> f[3], pdf(wi, wo) -> pdf. */
+int oracle_bsdf_eval(OracleScene* s, int material, const float* wi,
+                     const float* wo, size_t n, float* f, float* pdf);
+/* sample(wo, u3) -> wi[3], f[3], pdf, delta */
+int oracle_bsdf_sample(OracleScene* s, int material, const float* wo,
+                       const float* u3, size_t n, float* wi, float* f,
+                       float* pdf, int* is_delta);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

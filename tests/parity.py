@@ -1,0 +1,90 @@
+"""Helpers shared by the parity tests: seeded ray sets, hit comparison with
+mismatch classification, and the per-pixel 3-sigma band test."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from atrc_b200 import RAY_DTYPE
+
+
+def seeded_rays(n: int, lo, hi, cam_pos, seed: int) -> np.ndarray:
+    """Half camera-like rays (from cam_pos towards uniform points of the box),
+    half rays with origins uniform in the box and uniform directions."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    r = np.zeros(n, dtype=RAY_DTYPE)
+    h = n // 2
+    tgt = rng.uniform(lo, hi, (h, 3))
+    o = np.broadcast_to(np.asarray(cam_pos, np.float64), (h, 3))
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r["o"][:h] = o
+    r["d"][:h] = d
+    o2 = rng.uniform(lo, hi, (n - h, 3))
+    d2 = rng.normal(size=(n - h, 3))
+    d2 /= np.linalg.norm(d2, axis=1, keepdims=True)
+    r["o"][h:] = o2
+    r["d"][h:] = d2
+    r["t_min"] = 0
+    r["t_max"] = np.inf
+    return r
+
+
+def ulp_diff(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    ai = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
+    bi = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
+    ai = np.where(ai < 0, -(ai & 0x7FFFFFFF), ai)
+    bi = np.where(bi < 0, -(bi & 0x7FFFFFFF), bi)
+    return np.abs(ai - bi)
+
+
+def classify_closest(rays, gpu, ref, oracle_scene):
+    """Returns counts: exact (same primitive, t within 2 ulp), tie, ref_fn
+    (the reference BVH missed a closer genuine hit), error."""
+    same_prim = (gpu["entity"] == ref["entity"]) & (gpu["prim"] == ref["prim"])
+    both_miss = (gpu["entity"] < 0) & (ref["entity"] < 0)
+    ok_t = ulp_diff(gpu["t"], ref["t"]) <= 2
+    exact = both_miss | (same_prim & ok_t)
+    out = {"exact": int(exact.sum()), "tie": 0, "ref_fn": 0, "error": 0, "max_ulp_same_prim": 0, "errors": []}
+    sp = same_prim & ~both_miss
+    if sp.any():
+        out["max_ulp_same_prim"] = int(ulp_diff(gpu["t"][sp], ref["t"][sp]).max())
+    for i in np.nonzero(~exact)[0]:
+        g, r = gpu[i], ref[i]
+        if g["entity"] >= 0 and r["entity"] >= 0 and ulp_diff(g["t"], r["t"]) <= 2:
+            out["tie"] += 1
+            continue
+        if g["entity"] >= 0 and (r["entity"] < 0 or g["t"] < r["t"]):
+            t = oracle_scene.prim_hit(rays[i], int(g["entity"]), int(g["prim"]))
+            if t >= 0 and ulp_diff(t, g["t"]) <= 2:
+                out["ref_fn"] += 1
+                continue
+        out["error"] += 1
+        if len(out["errors"]) < 10:
+            out["errors"].append((int(i), tuple(g.tolist()), tuple(r.tolist())))
+    return out
+
+
+def band_test(gpu_film, ref_film, filter_value: float, sigmas: float = 3.0):
+    """Per-pixel, per-channel |mu_g - mu_c| <= k sqrt(s_g^2/N_g + s_c^2/N_c).
+    Returns (failing fraction, allowed fraction, details)."""
+    def stats(f):
+        w = f.weight.reshape(-1, 1)
+        mu = f.value.reshape(-1, 3) / np.where(w > 0, w, 1)
+        m2 = f.value_sq.reshape(-1, 3) / np.where(w > 0, w, 1)
+        var = np.maximum(m2 - mu * mu, 0)
+        n = w / filter_value
+        return mu, var, n
+
+    mg, vg, ng = stats(gpu_film)
+    mc, vc, nc = stats(ref_film)
+    se = np.sqrt(vg / np.maximum(ng, 1) + vc / np.maximum(nc, 1))
+    diff = np.abs(mg - mc)
+    fail = diff > sigmas * se + 1e-6 * (np.abs(mg) + np.abs(mc))
+    tests = fail.size
+    p = math.erfc(sigmas / math.sqrt(2))
+    allowed = p + 3.1 * math.sqrt(p * (1 - p) / tests)  # binomial upper 99.9 % bound
+    return float(fail.mean()), allowed, {"max_z": float(np.max(diff / np.maximum(se, 1e-12))),
+                                         "mean_rel": float(np.mean(np.abs(mg - mc)) / max(np.mean(np.abs(mc)), 1e-12))}

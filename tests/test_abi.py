@@ -1,0 +1,57 @@
+"""The C-ABI library loads, exports every declared entry point and agrees
+with its bindings on struct layouts (no GPU calls)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import atrc_b200
+from atrc_b200 import _abi as abi
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_functions():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b(atrc_\w+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for required in ["atrc_cuda_scene_create", "atrc_cuda_render", "atrc_cuda_trace_rays", "atrc_config_load_file",
+                     "atrc_last_error", "atrc_film_resolve", "atrc_cuda_device_init"]:
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = atrc_b200.load_library()
+    missing = [n for n in sorted(declared_functions()) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_struct_layouts_match():
+    lib = atrc_b200.load_library()
+    sizes = (C.c_uint64 * 15)()
+    assert lib.atrc_abi_struct_sizes(sizes, 15) == 15
+    for cls, size in zip(abi.STRUCT_ORDER, sizes):
+        assert C.sizeof(cls) == size, cls.__name__
+    assert C.sizeof(abi.AtrcRay) == 32 and C.sizeof(abi.AtrcHit) == 16
+
+
+def test_abi_version():
+    assert atrc_b200.load_library().atrc_abi_version() == 1
+
+
+def test_errors_are_reported_without_a_gpu():
+    lib = atrc_b200.load_library()
+    h = C.c_void_p()
+    rc = lib.atrc_config_load_string(b"{not json", b".", C.byref(h))
+    assert rc == -2
+    assert b"JSON" in lib.atrc_last_error()
+    rc = lib.atrc_cuda_scene_create(None, C.byref(h))
+    assert rc == -1
+    assert b"null" in lib.atrc_last_error()

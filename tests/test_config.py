@@ -1,0 +1,189 @@
+"""Scene ingestion: the factory mirror of the reference's creators (CPU only)."""
+import ctypes as C
+import json
+
+import numpy as np
+import pytest
+
+from atrc_b200 import AtrcError, Config
+
+
+def base(entities, rendering=None, **scene):
+    r = {"camera": {"type": "thin_lens", "pos": [0, 0, 5], "dst": [0, 0, 0], "up": [0, 1, 0], "fov": 40},
+         "width": 32, "height": 16, "renderer": {"type": "pt", "spp": 4}, "reporter": {"type": "noout"}}
+    if rendering:
+        r.update(rendering)
+    return {"scene": {"type": "default", "entities": entities, **scene}, "rendering": r}
+
+
+QUAD = {"type": "geometric",
+        "geometry": {"type": "quad", "A": [-1, -1, 0], "B": [1, -1, 0], "C": [1, 1, 0], "D": [-1, 1, 0],
+                     "transform": []},
+        "material": {"type": "ideal_diffuse", "albedo": {"type": "constant", "texel": [0.5]}}}
+
+
+def test_pt_defaults_match_reference_creator():
+    # renderer_creators.cpp:127-146
+    cfg = Config.from_string(base([QUAD]))
+    d, kind = cfg.rendering(0)
+    assert kind == "pt"
+    assert (d.spp, d.min_depth, d.max_depth, d.specular_depth, d.use_mis) == (4, 5, 10, 20, 1)
+    assert d.cont_prob == pytest.approx(0.9)
+    assert d.eps == pytest.approx(3e-4)
+    assert d.filter_type == 0 and d.filter_radius == pytest.approx(0.5)
+    assert d.camera.fov == pytest.approx(np.deg2rad(40), rel=1e-6)
+    assert d.camera.focal_distance == 1 and d.camera.lens_radius == 0
+
+
+def test_pt_cuda_accepts_pt_keys():
+    cfg = Config.from_string(base([QUAD], {"renderer": {"type": "pt_cuda", "spp": 8, "min_depth": 2,
+                                                        "max_depth": 7, "cont_prob": 0.5}}))
+    d, kind = cfg.rendering(0)
+    assert kind == "pt_cuda" and (d.spp, d.min_depth, d.max_depth) == (8, 2, 7)
+    assert d.cont_prob == pytest.approx(0.5)
+
+
+def test_floats_round_trip_through_six_decimals():
+    # config_cvt.cpp:43: std::to_string then std::stof
+    q = json.loads(json.dumps(QUAD))
+    q["geometry"]["A"] = [-1.23456789, -1, 0]
+    cfg = Config.from_string(base([q]))
+    g = cfg.scene_desc().contents.geometries[0]
+    assert g.p[0][0] == np.float32(-1.234568)
+
+
+def test_entity_skip_suffix_and_void_medium():
+    skipped = dict(QUAD, type="geometric//")
+    cfg = Config.from_string(base([QUAD, skipped]))
+    s = cfg.scene_desc().contents
+    assert s.entity_count == 1
+    assert s.medium_count >= 1 and s.media[0].type == 0  # the void medium
+    e = s.entities[0]
+    assert e.medium_in == 0 and e.medium_out == 0 and e.power == -1
+
+
+def test_transform_list_applies_last_first():
+    q = json.loads(json.dumps(QUAD))
+    q["geometry"]["transform"] = [{"type": "translate", "offset": [1, 2, 3]}, {"type": "scale", "ratio": 2}]
+    cfg = Config.from_string(base([q]))
+    m = np.array(cfg.scene_desc().contents.geometries[0].transform.m).reshape(3, 4)
+    p = m[:, :3] @ np.array([1.0, 1.0, 1.0]) + m[:, 3]
+    assert np.allclose(p, [3, 4, 5])  # scale first, then translate
+    inv = np.array(cfg.scene_desc().contents.geometries[0].transform.inv).reshape(3, 4)
+    assert np.allclose(inv[:, :3] @ p + inv[:, 3], [1, 1, 1])
+
+
+def test_rotate_and_mat3():
+    q = json.loads(json.dumps(QUAD))
+    q["geometry"]["transform"] = [{"type": "rotate_z", "deg": 90}]
+    c1 = Config.from_string(base([q]))
+    m = np.array(c1.scene_desc().contents.geometries[0].transform.m).reshape(3, 4)
+    assert np.allclose(m[:, :3] @ [1, 0, 0], [0, 1, 0], atol=1e-6)
+    q["geometry"]["transform"] = {"type": "mat3", "row_major": [0, -1, 0, 1, 0, 0, 0, 0, 1]}
+    c2 = Config.from_string(base([q]))
+    m2 = np.array(c2.scene_desc().contents.geometries[0].transform.m).reshape(3, 4)
+    assert np.allclose(m2, m, atol=1e-6)
+
+
+def test_reference_creator_shares_geometry(tmp_path):
+    from atrc_b200.scenes import _box_mesh, write_bm
+    p, n, uv = _box_mesh((1, 1, 1))
+    write_bm(tmp_path / "b.bm", p, n, uv)
+    ents = []
+    for k in range(3):
+        ents.append({"type": "geometric",
+                     "geometry": {"type": "transform_wrapper",
+                                  "internal": {"type": "reference", "name": ["lib", "box"]},
+                                  "transform": [{"type": "translate", "offset": [3 * k, 0, 0]}]},
+                     "material": {"type": "ideal_diffuse", "albedo": {"type": "constant", "texel": [0.5]}}})
+    cfg = Config.from_string(base(ents, lib={"box": {"type": "triangle_bvh", "filename": "${scene-directory}/b.bm",
+                                                     "transform": []}}), tmp_path)
+    s = cfg.scene_desc().contents
+    assert s.entity_count == 3 and s.geometry_count == 1 and s.mesh_count == 1
+    assert s.meshes[0].triangle_count == 12
+    assert all(s.entities[i].geometry == 0 and s.entities[i].has_instance for i in range(3))
+    assert s.entities[2].instance.m[3] == pytest.approx(6.0)
+
+
+def test_bm_mesh_layout(tmp_path):
+    from atrc_b200.scenes import write_bm
+    pos = np.arange(18, dtype=np.float32).reshape(2, 3, 3)
+    nor = np.ones((2, 3, 3), np.float32)
+    uv = np.zeros((2, 3, 2), np.float32)
+    write_bm(tmp_path / "m.bm", pos, nor, uv)
+    q = {"type": "geometric", "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/m.bm",
+                                           "transform": []},
+         "material": {"type": "ideal_black"}}
+    cfg = Config.from_string(base([q]), tmp_path)
+    s = cfg.scene_desc().contents
+    m = s.meshes[0]
+    v = np.ctypeslib.as_array(m.vertices, shape=(int(m.triangle_count) * 24,))
+    assert np.array_equal(v.reshape(2, 3, 8)[..., :3], pos)
+
+
+def test_disney_defaults():
+    q = json.loads(json.dumps(QUAD))
+    q["material"] = {"type": "disney", "base_color": {"type": "constant", "texel": [0.2, 0.4, 0.6]},
+                     "metallic": {"type": "constant", "texel": [0.0]},
+                     "roughness": {"type": "constant", "texel": [0.3]}}
+    cfg = Config.from_string(base([q]))
+    s = cfg.scene_desc().contents
+    m = s.materials[0]
+    assert m.type == 2
+    tex = lambda k: s.textures2d[m.tex[k]].texel[0]  # noqa: E731
+    # material_creators.cpp:56-113 defaults
+    assert tex(3) == 0 and tex(5) == pytest.approx(1.5) and tex(6) == 1 and tex(7) == 0
+    assert tex(12) == 1 and m.tex[4] == m.tex[2]  # transmission_roughness defaults to roughness
+
+
+def test_unknown_types_fail_loudly():
+    q = json.loads(json.dumps(QUAD))
+    q["material"] = {"type": "glass", "ior": {"type": "constant", "texel": [1.5]}}
+    with pytest.raises(AtrcError, match="not supported"):
+        Config.from_string(base([q]))
+    q["material"] = {"type": "no_such_thing"}
+    with pytest.raises(AtrcError):
+        Config.from_string(base([q]))
+    with pytest.raises(AtrcError, match="missing field"):
+        Config.from_string({"scene": {"type": "default"}})
+
+
+def test_rendering_array_and_filters():
+    c = base([QUAD])
+    r0 = c["rendering"]
+    r1 = dict(r0, film_filter={"type": "gaussian", "radius": 1.5, "alpha": 2}, eps=1e-3,
+              camera={"type": "pinhole", "pos": [0, 0, 5], "dst": [0, 0, 0], "up": [0, 1, 0], "width": 2,
+                      "dist": 1})
+    c["rendering"] = [r0, r1]
+    cfg = Config.from_string(c)
+    assert cfg.rendering_count() == 2
+    d1, _ = cfg.rendering(1)
+    assert d1.filter_type == 1 and d1.filter_radius == pytest.approx(1.5) and d1.eps == pytest.approx(1e-3)
+    # pinhole: fov = 2 atan(height / (2 dist)) with height = width / aspect
+    assert d1.camera.fov == pytest.approx(2 * np.arctan((2 / 2.0) / 2), rel=1e-6)
+
+
+def test_env_and_media(tmp_path):
+    from atrc_b200.scenes import write_pfm, write_grid
+    write_pfm(tmp_path / "e.pfm", np.ones((8, 16, 3), np.float32))
+    write_grid(tmp_path / "g.bin", np.arange(8, dtype=np.float32).reshape(2, 2, 2))
+    q = json.loads(json.dumps(QUAD))
+    q["med_in"] = {"type": "heterogeneous", "transform": [],
+                   "density": {"type": "image3d", "format": "real", "binary_filename": "${scene-directory}/g.bin"},
+                   "albedo": {"type": "constant", "texel": [0.9]}, "g": {"type": "constant", "texel": [0.1]}}
+    q["med_out"] = {"type": "homogeneous", "sigma_a": [0.1], "sigma_s": [0.2, 0.3, 0.4], "g": 0.5}
+    c = base([q], env={"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/e.pfm"}})
+    cfg = Config.from_string(c, tmp_path)
+    s = cfg.scene_desc().contents
+    assert s.env.type == 1 and s.textures2d[s.env.tex].width == 16 and s.textures2d[s.env.tex].height == 8
+    e = s.entities[0]
+    assert s.media[e.medium_in].type == 2 and s.media[e.medium_out].type == 1
+    t3 = s.textures3d[s.media[e.medium_in].density]
+    assert (t3.width, t3.height, t3.depth, t3.channels) == (2, 2, 2, 1) and t3.max_real == 7
+    assert list(s.media[e.medium_out].sigma_s) == pytest.approx([0.2, 0.3, 0.4])
+
+
+def test_post_processors_round_trip():
+    c = base([QUAD], {"post_processors": [{"type": "save_to_img", "filename": "out.png", "inv_gamma": 2.2}]})
+    pp = Config.from_string(c).post_processors(0)
+    assert pp[0]["type"] == "save_to_img" and float(pp[0]["inv_gamma"]) == pytest.approx(2.2)
