@@ -83,7 +83,7 @@ class AtrcRenderDesc(C.Structure):
                 ("use_mis", C.c_int32), ("filter_type", C.c_int32), ("filter_radius", C.c_float),
                 ("filter_alpha", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64), ("first_spp", C.c_int32),
                 ("spp_count", C.c_int32), ("camera", AtrcCameraDesc), ("path_pool", C.c_int32),
-                ("pad_", C.c_int32)]
+                ("count_traversal", C.c_int32)]
 
 
 class AtrcFilm(C.Structure):
@@ -96,7 +96,9 @@ class AtrcRenderStats(C.Structure):
                 ("rays_closest", C.c_uint64), ("rays_shadow", C.c_uint64), ("iterations", C.c_uint64),
                 ("kernel_launches", C.c_uint64), ("watchdog_flags", C.c_uint64), ("extend_seconds", C.c_double),
                 ("shadow_seconds", C.c_double), ("shade_seconds", C.c_double), ("h2d_bytes", C.c_uint64),
-                ("d2h_bytes", C.c_uint64)]
+                ("d2h_bytes", C.c_uint64), ("extend_launches", C.c_uint64), ("shadow_launches", C.c_uint64),
+                ("nodes_closest", C.c_uint64), ("tris_closest", C.c_uint64), ("ents_closest", C.c_uint64),
+                ("nodes_shadow", C.c_uint64), ("tris_shadow", C.c_uint64), ("ents_shadow", C.c_uint64)]
 
 
 class AtrcRay(C.Structure):

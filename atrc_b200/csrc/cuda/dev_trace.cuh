@@ -158,10 +158,19 @@ __device__ __forceinline__ void to_entity_space(const Entity& e, Vec3 o, Vec3 d,
     *ld = d;
 }
 
+// Functional work counts of one traversal (for the roofline's algorithmic bytes).
+struct TraceCount {
+    uint32_t nodes;  // 64-byte node fetches
+    uint32_t tris;   // 48-byte triangle fetches + tests
+    uint32_t ents;   // entity (instance) visits
+};
+
 // Trace one ray.  Returns true if something was hit (ANY: occluded).
-// `watchdog` is set when the traversal stack would overflow.
-template <bool EXACT, bool ANY>
-__device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog) {
+// `watchdog` is set when the traversal stack would overflow.  With COUNT the
+// work done is added to *cnt.
+template <bool EXACT, bool ANY, bool COUNT = false>
+__device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog,
+                          TraceCount* cnt = nullptr) {
     if (S.entity_count == 0) return false;
     int32_t stack[kStackSize];
     int sp = 0;
@@ -179,6 +188,7 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
             float4 n0, n1, n2;
             int2 lk;
             load_node(S.nodes, link, &n0, &n1, &n2, &lk);
+            if (COUNT) cnt->nodes++;
             bool h0, h1;
             float t0, t1;
             box2(n0, n1, n2, r, &h0, &t0, &h1, &t1);
@@ -204,6 +214,7 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
                 for (int32_t k = 0; k < count; ++k) {
                     const int32_t ei = int32_t(__ldg(S.tlas_order + first + k));
                     const Entity& e = S.entities[ei];
+                    if (COUNT) cnt->ents++;
                     Vec3 lo, ld;
                     to_entity_space<EXACT>(e, wo, wd, &lo, &ld);
                     if (e.kind == LEAF_TRIANGLES) {
@@ -233,6 +244,7 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
                     const int32_t ti = first + k;
                     const float4* tp = reinterpret_cast<const float4*>(S.tris) + size_t(ti) * 3;
                     const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+                    if (COUNT) cnt->tris++;
                     float t, u, v;
                     if (mt_test<EXACT, ANY>(r, p0, p1, p2, best_t, &t, &u, &v)) {
                         if (ANY) { hit->entity = cur_entity; hit->t = t; return true; }

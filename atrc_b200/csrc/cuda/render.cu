@@ -30,6 +30,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/atrc_cuda.h"
@@ -148,8 +149,18 @@ struct Counters {
     int n_free, n_new, n_cont, free_base;
     unsigned long long gen_base, issued, total, completed;
     unsigned long long rays_closest, rays_shadow, iterations;
+    unsigned long long cnt_closest[3], cnt_shadow[3];  // nodes, tris, entities
     int watchdog, done;
 };
+
+__device__ __forceinline__ void flush_count(unsigned long long* dst, const TraceCount& tc) {
+    unsigned long long v[3] = {tc.nodes, tc.tris, tc.ents};
+    for (int k = 0; k < 3; ++k) {
+        unsigned long long x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(__activemask(), x, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(dst + k, x);
+    }
+}
 
 struct Camera {
     float pos[3], fx[3], fy[3], fz[3];
@@ -270,9 +281,10 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
     }
 }
 
-template <bool EXACT>
+template <bool EXACT, bool COUNT>
 __global__ void __launch_bounds__(128) k_extend(Scene S, Pool P, Counters* c) {
     const int n = c->n_ext, in = c->in;
+    TraceCount tc{0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = P.q[in][i];
         const float4 o = P.ray_o[slot], d = P.ray_d[slot];
@@ -280,11 +292,12 @@ __global__ void __launch_bounds__(128) k_extend(Scene S, Pool P, Counters* c) {
         h.entity = -1;
         h.tri = -1;
         int wd = 0;
-        const bool hit = trace_ray<EXACT, false>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd);
+        const bool hit = trace_ray<EXACT, false, COUNT>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd, &tc);
         if (wd) atomicMax(&c->watchdog, wd);
         P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.entity : -1));
         P.hit_tri[slot] = h.tri;
     }
+    if (COUNT) flush_count(c->cnt_closest, tc);
 }
 
 __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d, float tmin, float tmax, Vec3 contrib,
@@ -483,14 +496,15 @@ __global__ void __launch_bounds__(128) k_shade(Scene S, Params p, Pool P, Counte
     }
 }
 
-template <bool EXACT>
+template <bool EXACT, bool COUNT>
 __global__ void __launch_bounds__(128) k_shadow(Scene S, Pool P, Counters* c) {
     const int n = min(c->n_shadow, P.shadow_cap);
+    TraceCount tc{0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 o = P.sh_o[i], d = P.sh_d[i];
         Hit h;
         int wd = 0;
-        const bool occluded = trace_ray<EXACT, true>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd);
+        const bool occluded = trace_ray<EXACT, true, COUNT>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd, &tc);
         if (wd) atomicMax(&c->watchdog, wd);
         if (!occluded) {
             const float4 cc = P.sh_c[i];
@@ -501,6 +515,7 @@ __global__ void __launch_bounds__(128) k_shadow(Scene S, Pool P, Counters* c) {
             atomicAdd(l + 2, cc.z);
         }
     }
+    if (COUNT) flush_count(c->cnt_shadow, tc);
 }
 
 __device__ __forceinline__ float filter_eval(const Params& p, float x, float y) {
@@ -578,7 +593,34 @@ struct DeviceSceneImpl {
     DevBuf pool_buf, counters, film_buf;
     size_t pool_cap = 0;
     int pool_lights = 0;
+    // per-call resources kept between render calls
+    static constexpr int kWindow = 4;  // wavefront iterations between host checks
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, kev[kWindow * 4] = {};
+    void* pinned_counters = nullptr;
+    void* stage = nullptr;             // pinned host staging for host films
+    size_t stage_bytes = 0;
+    void ensure_render_resources() {
+        if (!ev0) {
+            CK(cudaEventCreate(&ev0));
+            CK(cudaEventCreate(&ev1));
+            for (auto& e : kev) CK(cudaEventCreate(&e));
+        }
+        if (!pinned_counters) CK(cudaMallocHost(&pinned_counters, 512));
+    }
+    void ensure_stage(size_t bytes) {
+        if (stage_bytes >= bytes) return;
+        if (stage) cudaFreeHost(stage);
+        stage = nullptr;
+        stage_bytes = 0;
+        CK(cudaMallocHost(&stage, bytes));
+        stage_bytes = bytes;
+    }
     ~DeviceSceneImpl() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (auto& e : kev) if (e) cudaEventDestroy(e);
+        if (pinned_counters) cudaFreeHost(pinned_counters);
+        if (stage) cudaFreeHost(stage);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -856,14 +898,15 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         const size_t npix = size_t(desc->width) * desc->height;
         Film F{};
         std::vector<std::pair<double*, size_t>> host_targets;
-        DevBuf local_film;
+        DevBuf& local_film = d.film_buf;
+        d.ensure_render_resources();
         if (film->on_device) {
             F.value = film->value; F.weight = film->weight; F.value_sq = film->value_sq;
             F.albedo = film->albedo; F.normal = film->normal; F.denoise = film->denoise;
         } else {
             size_t doubles = npix * 4 + (film->value_sq ? npix * 3 : 0) + (film->albedo ? npix * 3 : 0) +
                              (film->normal ? npix * 3 : 0) + (film->denoise ? npix : 0);
-            local_film.alloc(doubles * sizeof(double));
+            if (local_film.bytes < doubles * sizeof(double)) local_film.alloc(doubles * sizeof(double));
             CK(cudaMemsetAsync(local_film.p, 0, doubles * sizeof(double), s));
             double* b = local_film.as<double>();
             F.value = b; b += npix * 3; host_targets.push_back({film->value, npix * 3});
@@ -876,36 +919,33 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         const int gsm = grid_for(d.sm_count, 16);
         k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
         CK(cudaGetLastError());
-        uint64_t launches = 1;
-        cudaEvent_t ev0, ev1;
-        CK(cudaEventCreate(&ev0));
-        CK(cudaEventCreate(&ev1));
-        // per-kernel timing events for one checkpoint window
-        const int window = 4;
-        std::vector<cudaEvent_t> kev(window * 6);
-        for (auto& e : kev) CK(cudaEventCreate(&e));
+        uint64_t launches = 1, ext_launches = 0;
+        cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
+        cudaEvent_t* kev = d.kev;
+        const int window = DeviceSceneImpl::kWindow;
         double t_ext = 0, t_shade = 0, t_shadow = 0;
         CK(cudaEventRecord(ev0, s));
         Counters hc{};
-        Counters* pinned = nullptr;
-        CK(cudaMallocHost(&pinned, sizeof(Counters)));
+        static_assert(sizeof(Counters) <= 512, "pinned counter buffer too small");
+        Counters* pinned = static_cast<Counters*>(d.pinned_counters);
         int status = ATRC_OK;
-        const bool exact = false;
+        const bool count = desc->count_traversal != 0;
         for (int iter_block = 0;; ++iter_block) {
             for (int k = 0; k < window; ++k) {
                 k_begin<<<1, 1, 0, s>>>(c);
                 k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
-                CK(cudaEventRecord(kev[k * 6 + 0], s));
-                if (exact) k_extend<true><<<gsm, 128, 0, s>>>(d.scene, P, c);
-                else k_extend<false><<<gsm, 128, 0, s>>>(d.scene, P, c);
-                CK(cudaEventRecord(kev[k * 6 + 1], s));
+                CK(cudaEventRecord(kev[k * 4 + 0], s));
+                if (count) k_extend<false, true><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                else k_extend<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                CK(cudaEventRecord(kev[k * 4 + 1], s));
                 k_shade<<<gsm, 128, 0, s>>>(d.scene, p, P, c);
-                CK(cudaEventRecord(kev[k * 6 + 2], s));
-                if (exact) k_shadow<true><<<gsm, 128, 0, s>>>(d.scene, P, c);
-                else k_shadow<false><<<gsm, 128, 0, s>>>(d.scene, P, c);
-                CK(cudaEventRecord(kev[k * 6 + 3], s));
+                CK(cudaEventRecord(kev[k * 4 + 2], s));
+                if (count) k_shadow<false, true><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                else k_shadow<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                CK(cudaEventRecord(kev[k * 4 + 3], s));
                 k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
                 launches += 6;
+                ext_launches += 1;
             }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
@@ -913,9 +953,9 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
             hc = *pinned;
             for (int k = 0; k < window; ++k) {
                 float a = 0, b2 = 0, e3 = 0;
-                CK(cudaEventElapsedTime(&a, kev[k * 6 + 0], kev[k * 6 + 1]));
-                CK(cudaEventElapsedTime(&b2, kev[k * 6 + 1], kev[k * 6 + 2]));
-                CK(cudaEventElapsedTime(&e3, kev[k * 6 + 2], kev[k * 6 + 3]));
+                CK(cudaEventElapsedTime(&a, kev[k * 4 + 0], kev[k * 4 + 1]));
+                CK(cudaEventElapsedTime(&b2, kev[k * 4 + 1], kev[k * 4 + 2]));
+                CK(cudaEventElapsedTime(&e3, kev[k * 4 + 2], kev[k * 4 + 3]));
                 t_ext += a * 1e-3;
                 t_shade += b2 * 1e-3;
                 t_shadow += e3 * 1e-3;
@@ -934,20 +974,27 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         if (!host_targets.empty()) {
             size_t doubles = 0;
             for (auto& t : host_targets) doubles += t.second;
-            std::vector<double> tmp(doubles);
-            CK(cudaMemcpyAsync(tmp.data(), local_film.p, doubles * sizeof(double), cudaMemcpyDeviceToHost, s));
+            d.ensure_stage(doubles * sizeof(double));
+            const double* tmp = static_cast<const double*>(d.stage);
+            CK(cudaMemcpyAsync(d.stage, local_film.p, doubles * sizeof(double), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
             d2h += doubles * sizeof(double);
+            // accumulate into the caller's arrays with a few host threads
             size_t off = 0;
             for (auto& t : host_targets) {
-                for (size_t k = 0; k < t.second; ++k) t.first[k] += tmp[off + k];
-                off += t.second;
+                const size_t n_el = t.second;
+                const unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+                std::vector<std::thread> th;
+                for (unsigned k = 0; k < nt; ++k) {
+                    const size_t b0 = n_el * k / nt, b1 = n_el * (k + 1) / nt;
+                    double* dst = t.first;
+                    const double* src = tmp + off;
+                    th.emplace_back([=] { for (size_t q = b0; q < b1; ++q) dst[q] += src[q]; });
+                }
+                for (auto& x : th) x.join();
+                off += n_el;
             }
         }
-        CK(cudaFreeHost(pinned));
-        for (auto& e : kev) cudaEventDestroy(e);
-        cudaEventDestroy(ev0);
-        cudaEventDestroy(ev1);
         if (stats) {
             std::memset(stats, 0, sizeof(*stats));
             stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
@@ -963,6 +1010,14 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
             stats->shadow_seconds = t_shadow;
             stats->h2d_bytes = 0;
             stats->d2h_bytes = d2h;
+            stats->extend_launches = ext_launches;
+            stats->shadow_launches = ext_launches;
+            stats->nodes_closest = hc.cnt_closest[0];
+            stats->tris_closest = hc.cnt_closest[1];
+            stats->ents_closest = hc.cnt_closest[2];
+            stats->nodes_shadow = hc.cnt_shadow[0];
+            stats->tris_shadow = hc.cnt_shadow[1];
+            stats->ents_shadow = hc.cnt_shadow[2];
         }
         if (progress && status == ATRC_OK) progress(100.0, user);
         if (status == ATRC_ERR_WATCHDOG)

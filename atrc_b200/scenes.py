@@ -315,8 +315,8 @@ def instanced_disney(out_dir: Path | None = None, seed: int = 1001, width: int =
                      "material": mat})
     cfg = {"scene": {"type": "default", "entities": ents, "aggregate": {"type": "bvh"}, "meshes": meshes,
                      "env": {"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/sky.pfm"}}},
-           "rendering": {"camera": {"type": "thin_lens", "pos": [0, -48, 18], "dst": [0, 0, 0], "up": [0, 0, 1],
-                                    "fov": 55},
+           "rendering": {"camera": {"type": "thin_lens", "pos": [0, -27, 5], "dst": [0, 0, 0], "up": [0, 0, 1],
+                                    "fov": 62},
                          "width": width, "height": height,
                          "renderer": {"type": renderer, "spp": spp, "max_depth": max_depth},
                          "reporter": {"type": "noout"}}}
@@ -330,7 +330,10 @@ def media_scene(out_dir: Path | None = None, seed: int = 1002, width: int = 1024
                 max_depth: int = 32, renderer: str = "pt_cuda", grid_res: int = 128, sphere_level: int = 6) -> Path:
     """A homogeneous box medium (sigma_a 0.05, sigma_s 0.5, g 0.6) and a 128^3
     fBm density grid scaled to sigma_t in [0, 8] (albedo 0.9, delta tracking)
-    enclosing a displaced sphere, two quad lights and the procedural sky."""
+    enclosing a displaced sphere, two quad lights and the procedural sky.
+    The medium boxes float 0.02 above the floor: coplanar boundaries would make
+    the medium of the segments below them depend on how ties between equal
+    hit distances are broken, which the reference leaves to traversal order."""
     out = Path(out_dir) if out_dir else cache_dir() / f"media_{seed}_{grid_res}_{sphere_level}"
     out.mkdir(parents=True, exist_ok=True)
     rng = np.random.default_rng(seed)
@@ -354,15 +357,15 @@ def media_scene(out_dir: Path | None = None, seed: int = 1002, width: int = 1024
         {"type": "geometric", "geometry": {"type": "quad", "A": [-6, -6, -1], "B": [6, -6, -1], "C": [6, 6, -1],
                                            "D": [-6, 6, -1], "transform": []},
          "material": {"type": "ideal_diffuse", "albedo": _const([0.6, 0.6, 0.6])}},
-        {"type": "geometric", "geometry": {**unit_box(), "transform": [{"type": "translate", "offset": [-2.6, -1, -1]},
+        {"type": "geometric", "geometry": {**unit_box(), "transform": [{"type": "translate", "offset": [-2.6, -1, -0.98]},
                                                                         {"type": "scale", "ratio": 2}]},
          "material": {"type": "invisible_surface"},
          "med_in": {"type": "homogeneous", "sigma_a": [0.05], "sigma_s": [0.5], "g": 0.6}},
-        {"type": "geometric", "geometry": {**unit_box(), "transform": [{"type": "translate", "offset": [0.4, -1.2, -1]},
+        {"type": "geometric", "geometry": {**unit_box(), "transform": [{"type": "translate", "offset": [0.4, -1.2, -0.98]},
                                                                         {"type": "scale", "ratio": 2.4}]},
          "material": {"type": "invisible_surface"},
          "med_in": {"type": "heterogeneous",
-                    "transform": [{"type": "translate", "offset": [0.4, -1.2, -1]}, {"type": "scale", "ratio": 2.4}],
+                    "transform": [{"type": "translate", "offset": [0.4, -1.2, -0.98]}, {"type": "scale", "ratio": 2.4}],
                     "density": {"type": "image3d", "format": "real", "binary_filename": "${scene-directory}/density.bin"},
                     "albedo": {"type": "constant", "texel": [0.9]},
                     "g": {"type": "constant", "texel": [0.0]}}},

@@ -249,7 +249,8 @@ typedef struct AtrcRenderDesc {
                                      /* of every pixel; 0 means all of spp   */
     AtrcCameraDesc camera;
     int32_t  path_pool;              /* wavefront path capacity, 0 = auto    */
-    int32_t  pad_;
+    int32_t  count_traversal;        /* 1: count BVH work into the stats     */
+                                     /* (slower; for roofline accounting)    */
 } AtrcRenderDesc;
 
 /* FP64 film accumulators, caller allocated, `width*height` pixels each.
@@ -279,6 +280,10 @@ typedef struct AtrcRenderStats {
     double   shadow_seconds;   /* device time inside any-hit kernels         */
     double   shade_seconds;    /* device time inside shading kernels         */
     uint64_t h2d_bytes, d2h_bytes;
+    uint64_t extend_launches;  /* closest-hit kernel launches               */
+    uint64_t shadow_launches;  /* any-hit kernel launches                   */
+    uint64_t nodes_closest, tris_closest, ents_closest;  /* count_traversal  */
+    uint64_t nodes_shadow, tris_shadow, ents_shadow;
 } AtrcRenderStats;
 
 /* Progress callback, fired on the calling thread between wavefront

@@ -34,6 +34,8 @@ def load() -> C.CDLL:
                                           C.c_int, C.c_int]
         lib.oracle_prim_hit.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRay), C.c_int, C.c_int, C.POINTER(C.c_float)]
         lib.oracle_render.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRenderDesc), C.POINTER(abi.AtrcFilm), C.c_int]
+        lib.oracle_render_sample.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRenderDesc), C.POINTER(abi.AtrcFilm),
+                                             C.c_int, C.c_int]
         lib.oracle_env_pdf.argtypes = [C.c_void_p, abi.c_float_p, C.c_size_t, abi.c_float_p]
         lib.oracle_env_sample.argtypes = [C.c_void_p, abi.c_float_p, C.c_size_t, abi.c_float_p, abi.c_float_p]
         lib.oracle_bsdf_eval.argtypes = [C.c_void_p, C.c_int, abi.c_float_p, abi.c_float_p, C.c_size_t,
@@ -82,6 +84,10 @@ class OracleScene:
     def render(self, desc: abi.AtrcRenderDesc, film, threads: int = 0) -> None:
         f = film.as_struct()
         _check(load().oracle_render(self._h, C.byref(desc), C.byref(f), threads))
+
+    def render_sample(self, desc: abi.AtrcRenderDesc, film, threads: int = 0, tile_stride: int = 1) -> None:
+        f = film.as_struct()
+        _check(load().oracle_render_sample(self._h, C.byref(desc), C.byref(f), threads, tile_stride))
 
     def env_pdf(self, dirs: np.ndarray) -> np.ndarray:
         d = np.ascontiguousarray(dirs, dtype=np.float32)

@@ -52,6 +52,12 @@ int oracle_prim_hit(OracleScene* s, const AtrcRay* ray, int entity, int prim,
 int oracle_render(OracleScene* s, const AtrcRenderDesc* desc, AtrcFilm* film,
                   int threads);
 
+/* Same, on a uniform spatial sample: only every `tile_stride`-th 32x32 tile
+ * (in row-major tile order) is rendered.  Used to time a bounded sample of a
+ * large workload. */
+int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* desc, AtrcFilm* film,
+                         int threads, int tile_stride);
+
 /* Number of hardware threads the oracle would use for threads <= 0. */
 int oracle_hardware_threads(void);
 

@@ -2286,7 +2286,12 @@ int oracle_prim_hit(OracleScene* s, const AtrcRay* q, int entity, int prim, floa
 }
 
 int oracle_render(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film, int threads) {
+    return oracle_render_sample(s, d, film, threads, 1);
+}
+
+int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film, int threads, int tile_stride) {
     if (!s || !d || !film || !film->value || !film->weight) { g_err = "null argument"; return ATRC_ERR_INVALID_ARG; }
+    if (tile_stride < 1) { g_err = "tile_stride must be >= 1"; return ATRC_ERR_INVALID_ARG; }
     if (film->on_device) { g_err = "the oracle renders into host memory only"; return ATRC_ERR_INVALID_ARG; }
     g_eps = s->eps = d->eps;
     const int W = d->width, H = d->height;
@@ -2305,7 +2310,9 @@ int oracle_render(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film, int t
     const int grid = 32;  // task_grid_size default (renderer_creators.cpp:128)
     const int tx = (W + grid - 1) / grid, ty = (H + grid - 1) / grid;
     std::mutex mtx;
-    parallel_for(size_t(tx) * ty, threads, [&](size_t tile) {
+    const size_t n_tiles = size_t(tx) * ty;
+    parallel_for((n_tiles + tile_stride - 1) / tile_stride, threads, [&](size_t tile_k) {
+        const size_t tile = tile_k * size_t(tile_stride);
         const int gx = int(tile % tx), gy = int(tile / tx);
         const int x0 = gx * grid, y0 = gy * grid;
         const int x1 = std::min(W, x0 + grid) - 1, y1 = std::min(H, y0 + grid) - 1;

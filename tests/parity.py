@@ -88,3 +88,18 @@ def band_test(gpu_film, ref_film, filter_value: float, sigmas: float = 3.0):
     allowed = p + 3.1 * math.sqrt(p * (1 - p) / tests)  # binomial upper 99.9 % bound
     return float(fail.mean()), allowed, {"max_z": float(np.max(diff / np.maximum(se, 1e-12))),
                                          "mean_rel": float(np.mean(np.abs(mg - mc)) / max(np.mean(np.abs(mc)), 1e-12))}
+
+
+def global_mean_z(gpu_film, ref_film, filter_value: float = 1 / (4 * (0.5 - 3e-4) ** 2)) -> float:
+    """z-score (largest over channels) of the difference between the two
+    whole-image mean radiances; each sample is one draw of the image-wide
+    sample distribution (box filter, one pixel per sample)."""
+    def agg(f):
+        wsum = float(f.weight.sum())
+        mu = f.value.reshape(-1, 3).sum(0) / wsum
+        m2 = f.value_sq.reshape(-1, 3).sum(0) / wsum
+        return mu, np.maximum(m2 - mu * mu, 0), wsum / filter_value
+    mg, vg, ng = agg(gpu_film)
+    mc, vc, nc = agg(ref_film)
+    se = np.sqrt(vg / ng + vc / nc)
+    return float(np.max(np.abs(mg - mc) / np.maximum(se, 1e-30)))
