@@ -141,5 +141,7 @@ PROTOTYPES = {
     "atrc_cuda_trace_rays_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int]),
     "atrc_cuda_render": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
                                    C.POINTER(C.c_int), PROGRESS_FN, C.c_void_p, C.POINTER(AtrcRenderStats)]),
+    "atrc_cuda_render_noalloc": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
+                                           C.POINTER(AtrcRenderStats)]),
     "atrc_film_resolve": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, c_float_p]),
 }

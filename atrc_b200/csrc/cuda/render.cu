@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -1023,6 +1024,149 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         if (status == ATRC_ERR_WATCHDOG)
             return fail(status, "a device loop reached its iteration cap (code " + std::to_string(hc.watchdog) + ")");
         if (status == ATRC_ERR_CANCELLED) return fail(status, "render cancelled");
+        return int(ATRC_OK);
+    });
+}
+
+// ------------------------------------------------------------------------
+// Rendering without any allocation.
+//
+// Some callers cannot allocate device memory at render time: a host that owns
+// every byte of the GPU through its own sub-allocator, a process whose memory
+// budget is fixed when it starts, or a real-time loop that may not hit the
+// driver's allocator (cudaMalloc can synchronise the device and its latency is
+// unbounded).  atrc_cuda_render_noalloc serves them: the wavefront's scratch
+// memory (path pool, queues, shadow rays, counters) lives in the file-scope
+// array below, which the driver reserves once when the library is loaded onto
+// a device and which every GPU that loads the library keeps until the process
+// exits.  The caller passes the scene (created beforehand) and a film of
+// device pointers; the call itself makes no cudaMalloc / cudaFree /
+// cudaMallocHost and no allocating library call.
+//
+// The array is shared by every call on a device and keeps the previous call's
+// contents; the counters and the free list are rewritten at the start of each
+// call, and every other word is written before it is read.  Calls whose work
+// overlaps on the GPU (two threads, two streams, or two scenes on the same
+// device at once) race on the array: serialise them.
+// ------------------------------------------------------------------------
+}  // extern "C"
+
+namespace atrc {
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[ATRC_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the static scratch array on the current device.  The
+// first call on a device looks the symbol up (cudaGetSymbolAddress); that
+// first call must therefore not happen inside a stream capture.
+void* noalloc_scratch(int device) {
+    if (device < 0 || device >= kMaxDevices) throw CudaError("device index out of range for the static scratch");
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            throw CudaError(std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = ptr;
+    }
+    return g_noalloc_ptr[device];
+}
+
+}  // namespace
+}  // namespace atrc
+
+extern "C" {
+
+int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcFilm* film,
+                             AtrcRenderStats* stats) {
+    if (!scene || !desc || !film || !film->value || !film->weight)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: null argument");
+    if (!film->on_device)
+        return fail(ATRC_ERR_INVALID_ARG,
+                    "atrc_cuda_render_noalloc: the film must hold device pointers (on_device = 1); a host film "
+                    "would need a device staging buffer");
+    if (desc->width <= 0 || desc->height <= 0 || desc->spp <= 0 || desc->max_depth < 0 || desc->spp_count < 0 ||
+        desc->first_spp < 0)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid film size, spp, depth or sample range");
+    if (desc->filter_type == ATRC_FILTER_BOX ? !(desc->filter_radius - desc->eps > 0)
+                                             : !(desc->filter_radius > 0 && desc->filter_alpha > 0))
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid film filter");
+    return guarded([&] {
+        DeviceSceneImpl& d = scene->impl;
+        CK(cudaSetDevice(d.device));
+        void* scratch = noalloc_scratch(d.device);
+        cudaStream_t s = d.stream;
+        d.scene.eps = desc->eps;
+        const Params p = make_params(*desc);
+        const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
+        const unsigned long long total = (unsigned long long)desc->width * desc->height * spp;
+        const int nl = std::max(1, d.scene.light_count);
+        // largest path pool (a multiple of 256) whose layout fits the array
+        const size_t counters_bytes = 512;
+        const size_t budget = ATRC_NOALLOC_SCRATCH_BYTES - counters_bytes;
+        size_t cap = 0;
+        for (size_t c = 256; pool_layout(c, c * nl).total <= budget; c += 256) cap = c;
+        if (cap < 1024)
+            return fail(ATRC_ERR_UNSUPPORTED, "atrc_cuda_render_noalloc: the scene's " + std::to_string(nl) +
+                                                  " lights leave room for fewer than 1024 paths in the " +
+                                                  std::to_string(ATRC_NOALLOC_SCRATCH_BYTES) + "-byte scratch");
+        if (desc->path_pool > 0) {
+            if (size_t(desc->path_pool) > cap)
+                return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: path_pool " +
+                                                      std::to_string(desc->path_pool) + " exceeds the maximum " +
+                                                      std::to_string(cap) + " that fits the static scratch");
+            cap = size_t(desc->path_pool);
+        }
+        cap = std::min<size_t>(cap, std::max<unsigned long long>(total, 1024ULL));
+        const size_t shadow_cap = cap * nl;
+        const PoolLayout L = pool_layout(cap, shadow_cap);
+        char* base = static_cast<char*>(scratch);
+        Counters* c = reinterpret_cast<Counters*>(base);
+        Pool P = pool_from(base + counters_bytes, L, shadow_cap);
+        Film F{film->value, film->weight, film->value_sq, film->albedo, film->normal, film->denoise};
+        const int gsm = grid_for(d.sm_count, 16);
+        // k_init rewrites the counters and the free list (all state that must
+        // start from a known value)
+        k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
+        CK(cudaGetLastError());
+        uint64_t launches = 1, ext_launches = 0;
+        Counters hc{};
+        const auto t0 = std::chrono::steady_clock::now();
+        for (;;) {
+            for (int k = 0; k < DeviceSceneImpl::kWindow; ++k) {
+                k_begin<<<1, 1, 0, s>>>(c);
+                k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
+                k_extend<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                k_shade<<<gsm, 128, 0, s>>>(d.scene, p, P, c);
+                k_shadow<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
+                launches += 6;
+                ext_launches += 1;
+            }
+            CK(cudaGetLastError());
+            // plain synchronous copy into a stack variable: no pinned buffer
+            CK(cudaStreamSynchronize(s));
+            CK(cudaMemcpy(&hc, c, sizeof(Counters), cudaMemcpyDeviceToHost));
+            if (hc.watchdog || hc.done) break;
+        }
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            stats->samples = hc.completed;
+            stats->rays_closest = hc.rays_closest;
+            stats->rays_shadow = hc.rays_shadow;
+            stats->iterations = hc.iterations;
+            stats->kernel_launches = launches;
+            stats->extend_launches = ext_launches;
+            stats->shadow_launches = ext_launches;
+            stats->watchdog_flags = uint64_t(hc.watchdog);
+        }
+        if (hc.watchdog)
+            return fail(ATRC_ERR_WATCHDOG, "a device loop reached its iteration cap (code " + std::to_string(hc.watchdog) + ")");
         return int(ATRC_OK);
     });
 }

@@ -393,6 +393,32 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc,
                      AtrcProgressFn progress, void* user,
                      AtrcRenderStats* stats);
 
+/* Size of the static device array behind atrc_cuda_render_noalloc. */
+#define ATRC_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
+
+/* atrc_cuda_render without any memory allocation, for callers that cannot
+ * allocate device memory at render time (a host that sub-allocates the whole
+ * GPU itself, a process with a memory budget fixed at start-up, a real-time
+ * loop that must not enter the driver's allocator).  No counterpart in the
+ * reference, whose CPU renderer allocates per tile and per sample.
+ *  - The wavefront scratch (path pool, queues, shadow rays, counters) lives in
+ *    a static device array of ATRC_NOALLOC_SCRATCH_BYTES that every GPU which
+ *    loads this library keeps reserved until the process exits.  The pool
+ *    holds as many paths as fit (about 100k with one light); scenes whose
+ *    lights leave room for fewer than 1024 paths, and a desc->path_pool above
+ *    that maximum, are rejected (ATRC_ERR_UNSUPPORTED / ATRC_ERR_INVALID_ARG).
+ *  - `film` must hold device pointers (on_device = 1); samples are added.
+ *  - The first call on a device looks up the array's device address; make
+ *    that first call before capturing any stream.
+ *  - All calls share the array and it keeps the last call's contents (each
+ *    call resets the counters it needs).  Calls that overlap on the GPU race
+ *    on it: serialise them.
+ *  - No progress callback or cancel flag; stats carries counts but no
+ *    per-kernel timings.
+ * Same status codes as atrc_cuda_render. */
+int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc,
+                             const AtrcFilm* film, AtrcRenderStats* stats);
+
 /* Average the accumulators into an image: rgb[3*i] = value / weight (0 where
  * weight == 0); host pointers. */
 int atrc_film_resolve(const AtrcFilm* film, int width, int height, float* rgb);
