@@ -1,0 +1,185 @@
+// atrc_cli -- command-line driver for pt_cuda, mirroring the reference's
+// `CLI -d scene.json` / `CLI -s "<json>"` (src/cli/src/main.cpp:14-72,
+// src/cli/src/params.cpp:6-43).  Every `rendering` entry of the configuration
+// is rendered on the GPU through the C ABI and its `save_to_img` post
+// processors run.  `--renderer pt_cuda` renders entries written for the CPU
+// `pt` renderer unchanged.
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../../include/atrc_cuda.h"
+
+namespace {
+
+void usage() {
+    std::printf(
+        "usage: atrc_cli (-d scene.json | -s '<json>') [--renderer pt_cuda] [--device N] [--quiet]\n"
+        "  -d, --scene-filename  scene description file\n"
+        "  -s, --scene           scene description text\n"
+        "  --renderer pt_cuda    render entries whose renderer type is `pt` on the GPU as well\n");
+}
+
+bool check(int rc, const char* what) {
+    if (rc == ATRC_OK) return true;
+    std::fprintf(stderr, "error: %s failed (%d): %s\n", what, rc, atrc_last_error());
+    return false;
+}
+
+std::string replace_all(std::string s, const std::string& a, const std::string& b) {
+    size_t p;
+    while ((p = s.find(a)) != std::string::npos) s.replace(p, a.size(), b);
+    return s;
+}
+
+// minimal reader for the post-processor list the library re-serialises:
+// an array of flat objects whose values are strings
+std::vector<std::vector<std::pair<std::string, std::string>>> parse_post(const std::string& j) {
+    std::vector<std::vector<std::pair<std::string, std::string>>> out;
+    size_t i = 0;
+    auto str = [&](std::string* s) {
+        while (i < j.size() && j[i] != '"') ++i;
+        ++i;
+        s->clear();
+        while (i < j.size() && j[i] != '"') {
+            if (j[i] == '\\' && i + 1 < j.size()) ++i;
+            *s += j[i++];
+        }
+        ++i;
+    };
+    while (i < j.size()) {
+        if (j[i] == '{') {
+            ++i;
+            std::vector<std::pair<std::string, std::string>> obj;
+            while (i < j.size() && j[i] != '}') {
+                if (j[i] == '"') {
+                    std::string k, v;
+                    str(&k);
+                    while (i < j.size() && j[i] != ':') ++i;
+                    ++i;
+                    if (i < j.size() && j[i] == '"') str(&v);
+                    else while (i < j.size() && j[i] != ',' && j[i] != '}') ++i;
+                    obj.push_back({k, v});
+                } else {
+                    ++i;
+                }
+            }
+            out.push_back(obj);
+        }
+        ++i;
+    }
+    return out;
+}
+
+std::string get(const std::vector<std::pair<std::string, std::string>>& o, const std::string& k, const std::string& d = "") {
+    for (auto& kv : o)
+        if (kv.first == k) return kv.second;
+    return d;
+}
+
+void progress(double pct, void*) {
+    std::printf("\r  %.1f%%", pct);
+    std::fflush(stdout);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    std::string file, text, force;
+    int device = 0;
+    bool quiet = false;
+    for (int i = 1; i < argc; ++i) {
+        std::string a = argv[i];
+        if ((a == "-d" || a == "--scene-filename") && i + 1 < argc) file = argv[++i];
+        else if ((a == "-s" || a == "--scene") && i + 1 < argc) text = argv[++i];
+        else if (a == "--renderer" && i + 1 < argc) force = argv[++i];
+        else if (a == "--device" && i + 1 < argc) device = std::atoi(argv[++i]);
+        else if (a == "--quiet") quiet = true;
+        else { usage(); return a == "-h" || a == "--help" ? 0 : 1; }
+    }
+    if (file.empty() && text.empty()) { usage(); return 1; }
+    std::string scene_dir = std::filesystem::current_path().string();
+    AtrcConfig* cfg = nullptr;
+    if (!text.empty()) {
+        if (!check(atrc_config_load_string(text.c_str(), scene_dir.c_str(), &cfg), "loading the scene")) return 1;
+    } else {
+        scene_dir = std::filesystem::absolute(std::filesystem::path(file)).parent_path().string();
+        if (!check(atrc_config_load_file(file.c_str(), &cfg), "loading the scene")) return 1;
+    }
+    AtrcDeviceInfo info;
+    if (!check(atrc_cuda_device_init(device, &info), "initialising the device")) return 1;
+    if (!quiet) std::printf("device %d: %s, %d SMs\n", device, info.name, info.sm_count);
+    const AtrcSceneDesc* sd = nullptr;
+    atrc_config_scene(cfg, &sd);
+    AtrcScene* scene = nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    if (!check(atrc_cuda_scene_create(sd, &scene), "creating the device scene")) return 1;
+    if (!quiet)
+        std::printf("scene: %u entities, built in %.2f s\n", sd->entity_count,
+                    std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    int n = 0;
+    atrc_config_rendering_count(cfg, &n);
+    int rc_all = 0;
+    for (int r = 0; r < n; ++r) {
+        AtrcRenderDesc desc;
+        char type[32];
+        atrc_config_rendering(cfg, r, &desc, type, sizeof(type));
+        if (std::string(type) != "pt_cuda" && force != "pt_cuda") {
+            std::fprintf(stderr, "rendering %d: renderer `%s` runs on the CPU reference; pass --renderer pt_cuda\n", r,
+                         type);
+            rc_all = 1;
+            continue;
+        }
+        const size_t np = size_t(desc.width) * desc.height;
+        std::vector<double> value(np * 3), weight(np);
+        AtrcFilm film{};
+        film.value = value.data();
+        film.weight = weight.data();
+        AtrcRenderStats st;
+        if (!quiet) std::printf("rendering %d: %dx%d, %d spp\n", r, desc.width, desc.height, desc.spp);
+        if (!check(atrc_cuda_render(scene, &desc, &film, nullptr, quiet ? nullptr : progress, nullptr, &st), "rendering")) {
+            rc_all = 1;
+            continue;
+        }
+        if (!quiet)
+            std::printf("\n  %.3f s, %.1f Msamples/s, %.1f Mrays/s\n", st.seconds, st.samples / st.seconds / 1e6,
+                        (st.rays_closest + st.rays_shadow) / st.seconds / 1e6);
+        std::vector<float> rgb(np * 3);
+        atrc_film_resolve(&film, desc.width, desc.height, rgb.data());
+        size_t need = 0;
+        atrc_config_post_processors(cfg, r, nullptr, 0, &need);
+        std::string pj(need, '\0');
+        atrc_config_post_processors(cfg, r, pj.data(), need, nullptr);
+        for (auto& pp : parse_post(pj)) {
+            const std::string t = get(pp, "type");
+            if (t.size() >= 2 && t.compare(t.size() - 2, 2, "//") == 0) continue;
+            if (t == "save_to_img") {
+                // SaveToImageCreator (post_processor_creators.cpp:115-150)
+                std::string fn = replace_all(replace_all(get(pp, "filename"), "${scene-directory}", scene_dir),
+                                             "${working-directory}", std::filesystem::current_path().string());
+                float gamma = 1;
+                if (!get(pp, "gamma").empty()) gamma = std::stof(get(pp, "gamma"));
+                else if (!get(pp, "inv_gamma").empty()) gamma = 1 / std::stof(get(pp, "inv_gamma"));
+                std::filesystem::create_directories(std::filesystem::absolute(fn).parent_path());
+                const std::string ext = get(pp, "ext");
+                if (check(atrc_save_image(fn.c_str(), ext.empty() ? nullptr : ext.c_str(), rgb.data(), desc.width,
+                                          desc.height, gamma),
+                          "saving the image") && !quiet)
+                    std::printf("  saved %s\n", fn.c_str());
+            } else if (!quiet) {
+                std::printf("  post processor `%s` is not part of pt_cuda; skipped\n", t.c_str());
+            }
+        }
+    }
+    atrc_cuda_scene_destroy(scene);
+    atrc_config_destroy(cfg);
+    return rc_all;
+}

@@ -124,6 +124,26 @@ int atrc_config_post_processors(const AtrcConfig* cfg, int index, char* json_out
     return ATRC_OK;
 }
 
+int atrc_save_image(const char* filename, const char* ext, const float* rgb, int width, int height, float gamma) {
+    if (!filename || !rgb || width <= 0 || height <= 0 || !(gamma > 0)) {
+        set_last_error("atrc_save_image: invalid argument");
+        return ATRC_ERR_INVALID_ARG;
+    }
+    return guarded_host([&] {
+        std::string e = ext ? ext : "";
+        const std::string fn = filename;
+        if (e.empty()) {
+            const size_t dot = fn.rfind('.');
+            e = dot == std::string::npos ? "" : fn.substr(dot + 1);
+        }
+        if (e == "png") atrc::save_png8(fn, rgb, width, height, gamma);
+        else if (e == "hdr") atrc::save_hdr_rgbe(fn, rgb, width, height);
+        else if (e == "pfm") atrc::save_pfm(fn, rgb, width, height);
+        else throw atrc::ConfigError("unsupported image extension: " + e + " (png, hdr, pfm)");
+        return int(ATRC_OK);
+    });
+}
+
 int atrc_film_resolve(const AtrcFilm* film, int width, int height, float* rgb) {
     if (!film || !film->value || !film->weight || !rgb || width <= 0 || height <= 0) {
         set_last_error("atrc_film_resolve: invalid argument");

@@ -218,24 +218,27 @@ std::vector<float> load_triangle_mesh(const std::string& fn) {
 }
 
 void save_pfm(const std::string& fn, const float* rgb, int w, int h) {
+    // PFM stores the bottom row first, which is film row 0
     std::ofstream f(fn, std::ios::binary);
     if (!f) throw ConfigError("failed to open output: " + fn);
     f << "PF\n" << w << " " << h << "\n-1.0\n";
-    for (int y = h - 1; y >= 0; --y) f.write(reinterpret_cast<const char*>(rgb + size_t(y) * w * 3), size_t(w) * 3 * sizeof(float));
+    for (int y = 0; y < h; ++y) f.write(reinterpret_cast<const char*>(rgb + size_t(y) * w * 3), size_t(w) * 3 * sizeof(float));
 }
 
-void save_png8(const std::string& fn, const float* rgb, int w, int h, float inv_gamma) {
-    // 8-bit RGB PNG with stored (uncompressed) deflate blocks.
+void save_png8(const std::string& fn, const float* rgb, int w, int h, float gamma) {
+    // 8-bit RGB PNG with stored (uncompressed) deflate blocks.  Texels map as
+    // uint8(clamp(c^gamma, 0, 1) * 255), rows written top to bottom
+    // (save_to_img.cpp:36-49 flips the film vertically).
     std::vector<uint8_t> raw;
     raw.reserve(size_t(h) * (size_t(w) * 3 + 1));
     for (int y = 0; y < h; ++y) {
         raw.push_back(0);
+        const int src = h - 1 - y;
         for (int x = 0; x < w * 3; ++x) {
-            float v = rgb[size_t(y) * w * 3 + x];
-            if (!(v > 0)) v = 0;
-            if (inv_gamma != 1.0f) v = std::pow(v, inv_gamma);
-            v = std::fmin(v, 1.0f);
-            raw.push_back(uint8_t(std::lround(v * 255.0f)));
+            float v = std::pow(rgb[size_t(src) * w * 3 + x], gamma);
+            v = std::fmin(std::fmax(v, 0.0f), 1.0f);
+            if (!(v == v)) v = 0;
+            raw.push_back(uint8_t(v * 255.0f));
         }
     }
     std::vector<uint8_t> z = {0x78, 0x01};
@@ -270,7 +273,8 @@ void save_hdr_rgbe(const std::string& fn, const float* rgb, int w, int h) {
     std::ofstream f(fn, std::ios::binary);
     if (!f) throw ConfigError("failed to open output: " + fn);
     f << "#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y " << h << " +X " << w << "\n";
-    for (size_t i = 0; i < size_t(w) * h; ++i) {
+    for (size_t k = 0; k < size_t(w) * h; ++k) {
+        const size_t i = size_t(h - 1 - k / w) * w + k % w;  // top row first
         float r = rgb[3 * i], g = rgb[3 * i + 1], b = rgb[3 * i + 2];
         float m = std::fmax(r, std::fmax(g, b));
         uint8_t e[4] = {0, 0, 0, 0};

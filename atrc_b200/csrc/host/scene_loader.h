@@ -51,9 +51,9 @@ std::unique_ptr<LoadedConfig> load_config_file(const std::string& path);
 std::vector<float> load_rgb_image(const std::string& filename, int* width, int* height);
 // `.bm` (src/factory/src/utility/bin_mesh.cpp:7-27) or Wavefront OBJ.
 std::vector<float> load_triangle_mesh(const std::string& filename);
-// Write helpers used by the CLI's post processors.
+// Writers used by the CLI's post processors; `rgb` is a film (row 0 = bottom).
 void save_pfm(const std::string& filename, const float* rgb, int w, int h);
-void save_png8(const std::string& filename, const float* rgb, int w, int h, float inv_gamma);
+void save_png8(const std::string& filename, const float* rgb, int w, int h, float gamma);
 void save_hdr_rgbe(const std::string& filename, const float* rgb, int w, int h);
 
 }  // namespace atrc

@@ -45,6 +45,7 @@ def parse():
     p.add_argument("--spp-per-step", type=int, default=16)
     p.add_argument("--scene", default="instanced", choices=["instanced", "cornell", "media"])
     p.add_argument("--path-pool", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed oracle run (profiling)")
     return p.parse_args()
 
 
@@ -206,9 +207,11 @@ def main():
     film = Film(W, H, device=True)
     step_idx = [0]
 
+    from atrc_b200.multigpu import first_spp, reduce_film
+
     def do_step(f, count=False):
         # disjoint sample indices per rank and per step
-        desc.first_spp = (step_idx[0] * world + rank) * spp
+        desc.first_spp = first_spp(step_idx[0], rank, world, spp)
         desc.count_traversal = 1 if count else 0
         step_idx[0] += 1
         return scene.render(desc, f)
@@ -229,8 +232,7 @@ def main():
         for _ in range(args.steps):
             stats.append(do_step(film))
             if dist:
-                dist.reduce(film.value, 0)
-                dist.reduce(film.weight, 0)
+                reduce_film(film, dist, 0)
         ev1.record()
         torch.cuda.synchronize()
     if dist:
@@ -269,7 +271,7 @@ def main():
     shadow_time = sum(st["shadow_seconds"] for st in stats)
     launches = int(sum(st["kernel_launches"] for st in stats))
     if rank == 0:
-        cpu = cpu_baseline(args) if world == 1 else None
+        cpu = cpu_baseline(args) if world == 1 and not args.no_cpu_baseline else None
         clocks = clk.summary()
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,

@@ -419,6 +419,14 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc,
 int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc,
                              const AtrcFilm* film, AtrcRenderStats* stats);
 
+/* Write a resolved film (rgb, row 0 = bottom, as produced by
+ * atrc_film_resolve) the way the `save_to_img` post processor does
+ * (src/tracer/src/core/post_processor/save_to_img.cpp:10-69): flipped
+ * vertically; "png": uint8(clamp(c^gamma, 0, 1) * 255); "hdr": Radiance RGBE;
+ * "pfm": float.  `ext` may be NULL to use the filename's extension. */
+int atrc_save_image(const char* filename, const char* ext, const float* rgb,
+                    int width, int height, float gamma);
+
 /* Average the accumulators into an image: rgb[3*i] = value / weight (0 where
  * weight == 0); host pointers. */
 int atrc_film_resolve(const AtrcFilm* film, int width, int height, float* rgb);

@@ -1,0 +1,139 @@
+"""Known answers and API behaviour of the CUDA path (through the C ABI)."""
+import ctypes as C
+import math
+import threading
+
+import numpy as np
+import pytest
+
+from atrc_b200 import AtrcError, Config, DeviceScene, Film
+from tests import kat_scenes as K
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(cfg_dict, scene_dir="."):
+    cfg = Config.from_string(K.dumps(cfg_dict), scene_dir)
+    desc, _ = cfg.rendering(0)
+    return cfg, desc, DeviceScene(cfg)
+
+
+def test_white_furnace_gpu():
+    cfg, desc, dev = _dev(K.furnace(spp=256, renderer="pt_cuda"))
+    f = Film(desc.width, desc.height, value_sq=True)
+    dev.render(desc, f)
+    mu = f.image().mean()
+    n = float(f.weight.sum()) * 4 * (0.5 - 3e-4) ** 2
+    var = f.value_sq.sum() / f.weight.sum() / 3 - mu * mu
+    assert abs(mu - 1.0) < 4 * math.sqrt(max(var, 1e-12) / n) + 1e-3, mu
+
+
+def test_absorbing_slab_gpu(tmp_path):
+    cfgd, expected = K.slab(tmp_path, renderer="pt_cuda")
+    cfg, desc, dev = _dev(cfgd, tmp_path)
+    f = Film(desc.width, desc.height)
+    dev.render(desc, f)
+    np.testing.assert_allclose(f.image()[4, 4], expected, rtol=2e-3)
+
+
+def test_moller_trumbore_edges_gpu():
+    import oracle
+    cfg, desc, dev = _dev(K.edge_scene())
+    rays, inside = K.edge_rays()
+    for exact in (True, False):
+        h = dev.trace_rays(rays, exact=exact)
+        assert np.array_equal(h["entity"] >= 0, inside)
+        assert np.all(h["t"][inside] == np.float32(2.0))
+    ref = oracle.OracleScene(cfg.scene_desc()).trace_rays(rays)
+    assert np.array_equal(dev.trace_rays(rays, exact=True)["t"], ref["t"])
+
+
+def test_sample_split_is_exact(cornell_path):
+    # sample indices [0, 8) at once == [0, 4) + [4, 8): the multi-GPU sharding
+    cfg = Config.from_file(cornell_path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height = 40, 32
+    dev = DeviceScene(cfg)
+    whole, split = Film(40, 32, value_sq=True), Film(40, 32, value_sq=True)
+    desc.first_spp, desc.spp_count = 0, 8
+    dev.render(desc, whole)
+    for first in (0, 4):
+        desc.first_spp, desc.spp_count = first, 4
+        dev.render(desc, split)
+    for name in ("value", "weight", "value_sq"):
+        np.testing.assert_allclose(getattr(split, name), getattr(whole, name), rtol=1e-9, atol=1e-12)
+
+
+def test_device_film_equals_host_film(cornell_path):
+    cfg = Config.from_file(cornell_path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 32, 24, 8
+    dev = DeviceScene(cfg)
+    a, b = Film(32, 24), Film(32, 24, device=True)
+    dev.render(desc, a)
+    dev.render(desc, b)
+    np.testing.assert_allclose(b.value.cpu().numpy(), a.value, rtol=1e-9, atol=1e-12)
+
+
+def test_cancel_returns_partial_film(cornell_path):
+    cfg = Config.from_file(cornell_path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 256, 256, 4096
+    desc.path_pool = 1 << 16
+    dev = DeviceScene(cfg)
+    f = Film(256, 256)
+    flag = C.c_int(0)
+    seen = []
+
+    def progress(p):
+        seen.append(p)
+        if len(seen) == 3:
+            flag.value = 1
+    with pytest.raises(AtrcError, match="CANCELLED"):
+        dev.render(desc, f, cancel=flag, progress=progress)
+    done = f.weight.sum() * 4 * (0.5 - 3e-4) ** 2
+    assert 0 < done < 256 * 256 * 4096
+
+
+def test_invalid_arguments_are_rejected(cornell_path):
+    cfg = Config.from_file(cornell_path)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    bad = Film(desc.width, desc.height)
+    desc.spp = 0
+    with pytest.raises(AtrcError, match="INVALID_ARG"):
+        dev.render(desc, bad)
+    desc.spp = 4
+    desc.filter_radius = 0.0001
+    with pytest.raises(AtrcError, match="filter"):
+        dev.render(desc, bad)
+    from atrc_b200 import _abi as abi
+    from atrc_b200 import load_library
+    rays = np.zeros(4, dtype=abi.AtrcRay)
+    hits = np.zeros(4, dtype=abi.AtrcHit)
+    rc = load_library().atrc_cuda_trace_rays(dev.handle, rays.ctypes.data_as(C.POINTER(abi.AtrcRay)), 4,
+                                             hits.ctypes.data_as(C.POINTER(abi.AtrcHit)), 7, 1)
+    assert rc == -1
+
+
+def test_empty_scene_and_threads(tmp_path):
+    cfgd = K.furnace(renderer="pt_cuda", spp=4)
+    cfgd["scene"]["entities"] = []
+    cfg, desc, dev = _dev(cfgd)
+    f = Film(desc.width, desc.height)
+    dev.render(desc, f)
+    np.testing.assert_allclose(f.image(), 1.0, rtol=1e-6)  # only the uniform sky
+    # two scenes rendered from two host threads at once
+    cfg2, desc2, dev2 = _dev(K.furnace(renderer="pt_cuda", spp=16))
+    out = {}
+
+    def run(k, d, s):
+        ff = Film(d.width, d.height)
+        s.render(d, ff)
+        out[k] = ff.image().mean()
+    ts = [threading.Thread(target=run, args=(k, desc2, dev2 if k else dev)) for k in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert abs(out[0] - 1) < 1e-5 and abs(out[1] - 1) < 0.05
