@@ -30,7 +30,7 @@ __all__ = ["AtrcError", "load_library", "library_path", "Config", "DeviceScene",
            "ERROR_NAMES"]
 
 ROOT = Path(__file__).resolve().parent
-LIB_PATH = ROOT / "lib" / "libatrc_cuda.so"
+LIB_PATH = Path(os.environ.get("ATRC_LIB", ROOT / "lib" / "libatrc_cuda.so"))
 
 ERROR_NAMES = {0: "ATRC_OK", -1: "ATRC_ERR_INVALID_ARG", -2: "ATRC_ERR_CONFIG", -3: "ATRC_ERR_OUT_OF_MEMORY",
                -4: "ATRC_ERR_CUDA", -5: "ATRC_ERR_CANCELLED", -6: "ATRC_ERR_WATCHDOG", -7: "ATRC_ERR_UNSUPPORTED"}

@@ -21,7 +21,8 @@ namespace atrc {
 namespace dev {
 
 constexpr int kStackSize = 96;
-constexpr int32_t kSentinel = INT_MIN;  // "return from a bottom-level tree"
+constexpr int32_t kSentinel = INT_MIN;      // "return from a bottom-level tree"
+constexpr int32_t kDone = INT_MIN + 1;      // empty stack
 
 struct Hit {
     float t;
@@ -168,6 +169,14 @@ struct TraceCount {
 // Trace one ray.  Returns true if something was hit (ANY: occluded).
 // `watchdog` is set when the traversal stack would overflow.  With COUNT the
 // work done is added to *cnt.
+//
+// Structure (after Aila and Laine, "Understanding the efficiency of ray
+// traversal on GPUs", 2009): a thread that reaches a leaf while descending
+// parks it and keeps descending; the warp switches to leaf processing only
+// once every active lane holds a leaf, so node and leaf code run with most
+// lanes converged.  Top-level leaves (entities) switch the ray into the
+// entity's space and push a sentinel that restores the world ray when the
+// bottom-level tree is exhausted.
 template <bool EXACT, bool ANY, bool COUNT = false>
 __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog,
                           TraceCount* cnt = nullptr) {
@@ -182,8 +191,70 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
     float best_u = 0, best_v = 0;
     int32_t cur_entity = -1;
     int32_t link = S.tlas_root;
+    int32_t held = 0;  // parked leaf (negative) or 0
+    bool overflow = false;
+
+    auto push = [&](int32_t v) {
+        if (sp >= kStackSize) { overflow = true; return; }
+        stack[sp++] = v;
+    };
+    auto pop = [&]() -> int32_t { return sp > 0 ? stack[--sp] : kDone; };
+
+    // Visit leaf `lf`; `next` is what follows it.  Returns the new link.
+    // Sets `found` in ANY mode when something was hit.
+    bool found = false;
+    auto visit_leaf = [&](int32_t lf, int32_t next) -> int32_t {
+        const uint32_t enc = uint32_t(~lf);
+        const int32_t first = int32_t(enc >> 4), count = int32_t(enc & 15) + 1;
+        if (cur_entity < 0) {
+            // top level: one entity per leaf slot (the builder uses leaves of 1)
+            for (int32_t k = 0; k < count; ++k) {
+                const int32_t ei = int32_t(__ldg(S.tlas_order + first + k));
+                const Entity& e = S.entities[ei];
+                if (COUNT) cnt->ents++;
+                Vec3 lo, ld;
+                to_entity_space<EXACT>(e, wo, wd, &lo, &ld);
+                if (e.kind == LEAF_TRIANGLES) {
+                    push(next);
+                    push(kSentinel);
+                    r.o = lo; r.d = ld; r.inv = safe_inv(ld);
+                    cur_entity = ei;
+                    return e.blas_root;
+                }
+                RayState lr;
+                lr.o = lo; lr.d = ld; lr.tmin = tmin; lr.inv = Vec3();
+                float t;
+                const bool h = e.kind == LEAF_SPHERE ? sphere_test<ANY>(lr, e.radius, best_t, &t)
+                                                     : disk_test(lr, e.radius, best_t, &t);
+                if (h) {
+                    if (ANY) { best_e = ei; best_t = t; found = true; return kDone; }
+                    if (t < best_t || (t == best_t && ei < best_e)) {
+                        best_t = t; best_e = ei; best_tri = -1; best_u = 0; best_v = 0;
+                        r.tmax = t;
+                    }
+                }
+            }
+            return next;
+        }
+        for (int32_t k = 0; k < count; ++k) {
+            const int32_t ti = first + k;
+            const float4* tp = reinterpret_cast<const float4*>(S.tris) + size_t(ti) * 3;
+            const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+            if (COUNT) cnt->tris++;
+            float t, u, v;
+            if (mt_test<EXACT, ANY>(r, p0, p1, p2, best_t, &t, &u, &v)) {
+                if (ANY) { best_e = cur_entity; best_t = t; found = true; return kDone; }
+                if (t < best_t || (t == best_t && (cur_entity < best_e || (cur_entity == best_e && ti < best_tri)))) {
+                    best_t = t; best_e = cur_entity; best_tri = ti; best_u = u; best_v = v;
+                    r.tmax = t;
+                }
+            }
+        }
+        return next;
+    };
+
     for (;;) {
-        // descend interior nodes
+        // descend interior nodes, parking the first leaf found
         while (link >= 0) {
             float4 n0, n1, n2;
             int2 lk;
@@ -193,82 +264,49 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
             float t0, t1;
             box2(n0, n1, n2, r, &h0, &t0, &h1, &t1);
             if (h0 && h1) {
-                int32_t nearl = t0 <= t1 ? lk.x : lk.y, farl = t0 <= t1 ? lk.y : lk.x;
-                if (sp >= kStackSize) { *watchdog = 1; goto done; }
-                stack[sp++] = farl;
-                link = nearl;
+                const bool c0_first = t0 <= t1;
+                push(c0_first ? lk.y : lk.x);
+                link = c0_first ? lk.x : lk.y;
             } else if (h0) {
                 link = lk.x;
             } else if (h1) {
                 link = lk.y;
             } else {
-                goto pop;
+                link = pop();
             }
-        }
-        // leaf
-        {
-            const uint32_t enc = uint32_t(~link);
-            const int32_t first = int32_t(enc >> 4), count = int32_t(enc & 15) + 1;
-            if (cur_entity < 0) {
-                // top-level leaf: one entity per leaf slot
-                for (int32_t k = 0; k < count; ++k) {
-                    const int32_t ei = int32_t(__ldg(S.tlas_order + first + k));
-                    const Entity& e = S.entities[ei];
-                    if (COUNT) cnt->ents++;
-                    Vec3 lo, ld;
-                    to_entity_space<EXACT>(e, wo, wd, &lo, &ld);
-                    if (e.kind == LEAF_TRIANGLES) {
-                        if (count != 1) { *watchdog = 2; goto done; }  // builder guarantees 1
-                        if (sp >= kStackSize) { *watchdog = 1; goto done; }
-                        stack[sp++] = kSentinel;
-                        r.o = lo; r.d = ld; r.inv = safe_inv(ld);
-                        cur_entity = ei;
-                        link = e.blas_root;
-                        goto next;
-                    }
-                    RayState lr;
-                    lr.o = lo; lr.d = ld; lr.tmin = tmin; lr.inv = Vec3();
-                    float t;
-                    bool h = e.kind == LEAF_SPHERE ? sphere_test<ANY>(lr, e.radius, best_t, &t)
-                                                   : disk_test(lr, e.radius, best_t, &t);
-                    if (h) {
-                        if (ANY) { hit->entity = ei; hit->t = t; return true; }
-                        if (t < best_t || (t == best_t && ei < best_e)) {
-                            best_t = t; best_e = ei; best_tri = -1; best_u = 0; best_v = 0;
-                            r.tmax = t;
-                        }
-                    }
-                }
-            } else {
-                for (int32_t k = 0; k < count; ++k) {
-                    const int32_t ti = first + k;
-                    const float4* tp = reinterpret_cast<const float4*>(S.tris) + size_t(ti) * 3;
-                    const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
-                    if (COUNT) cnt->tris++;
-                    float t, u, v;
-                    if (mt_test<EXACT, ANY>(r, p0, p1, p2, best_t, &t, &u, &v)) {
-                        if (ANY) { hit->entity = cur_entity; hit->t = t; return true; }
-                        if (t < best_t || (t == best_t && (cur_entity < best_e || (cur_entity == best_e && ti < best_tri)))) {
-                            best_t = t; best_e = cur_entity; best_tri = ti; best_u = u; best_v = v;
-                            r.tmax = t;
-                        }
-                    }
-                }
+            if (link < 0 && link != kSentinel && link != kDone && held == 0) {
+                held = link;
+                link = pop();
             }
+            if (overflow) break;
+            if (!__any_sync(__activemask(), held == 0)) break;
         }
-    pop:
-        for (;;) {
-            if (sp == 0) goto done;
-            link = stack[--sp];
-            if (link != kSentinel) break;
-            // back to the top level
-            cur_entity = -1;
-            r.o = wo; r.d = wd; r.inv = winv;
+        if (overflow) { *watchdog = 1; break; }
+        // leaves: the parked one first, then any leaf / sentinel in `link`
+        if (held != 0) {
+            link = visit_leaf(held, link);
+            held = 0;
+            if (found) break;
         }
-    next:;
+        while (link < 0) {
+            if (link == kDone) break;
+            if (link == kSentinel) {
+                cur_entity = -1;
+                r.o = wo; r.d = wd; r.inv = winv;
+                link = pop();
+                continue;
+            }
+            const int32_t next = pop();
+            link = visit_leaf(link, next);
+            if (found) break;
+        }
+        if (overflow) { *watchdog = 1; break; }
+        if (found || link == kDone) break;
     }
-done:
-    if (ANY) return false;
+    if (ANY) {
+        if (found) { hit->entity = best_e; hit->t = best_t; }
+        return found;
+    }
     if (best_e < 0) return false;
     hit->t = best_t;
     hit->u = best_u;

@@ -41,6 +41,10 @@
 #include "dev_shade.cuh"
 #include "dev_trace.cuh"
 
+#ifndef ATRC_SHADE_MIN_BLOCKS
+#define ATRC_SHADE_MIN_BLOCKS 4  // k_shade blocks per SM the register budget must allow
+#endif
+
 namespace atrc {
 
 void set_last_error(const std::string& msg);  // capi_host.cpp
@@ -310,7 +314,7 @@ __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d
     P.sh_c[k] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(slot));
 }
 
-__global__ void __launch_bounds__(128) k_shade(Scene S, Params p, Pool P, Counters* c) {
+__global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, Params p, Pool P, Counters* c) {
     const int n = c->n_ext, in = c->in, out = c->out;
     const float eps = p.eps;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -918,6 +922,9 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
             if (film->denoise) { F.denoise = b; b += npix; host_targets.push_back({film->denoise, npix}); }
         }
         const int gsm = grid_for(d.sm_count, 16);
+        // one path / ray per thread for the heavy kernels (grids cover the
+        // pool; threads past the device-side count return at once)
+        const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
         k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
         CK(cudaGetLastError());
         uint64_t launches = 1, ext_launches = 0;
@@ -936,13 +943,13 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
                 k_begin<<<1, 1, 0, s>>>(c);
                 k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
                 CK(cudaEventRecord(kev[k * 4 + 0], s));
-                if (count) k_extend<false, true><<<gsm, 128, 0, s>>>(d.scene, P, c);
-                else k_extend<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                if (count) k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c);
+                else k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c);
                 CK(cudaEventRecord(kev[k * 4 + 1], s));
-                k_shade<<<gsm, 128, 0, s>>>(d.scene, p, P, c);
+                k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
                 CK(cudaEventRecord(kev[k * 4 + 2], s));
-                if (count) k_shadow<false, true><<<gsm, 128, 0, s>>>(d.scene, P, c);
-                else k_shadow<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+                else k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 CK(cudaEventRecord(kev[k * 4 + 3], s));
                 k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
                 launches += 6;
@@ -1129,6 +1136,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         Pool P = pool_from(base + counters_bytes, L, shadow_cap);
         Film F{film->value, film->weight, film->value_sq, film->albedo, film->normal, film->denoise};
         const int gsm = grid_for(d.sm_count, 16);
+        const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
         // k_init rewrites the counters and the free list (all state that must
         // start from a known value)
         k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
@@ -1140,9 +1148,9 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
             for (int k = 0; k < DeviceSceneImpl::kWindow; ++k) {
                 k_begin<<<1, 1, 0, s>>>(c);
                 k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
-                k_extend<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
-                k_shade<<<gsm, 128, 0, s>>>(d.scene, p, P, c);
-                k_shadow<false, false><<<gsm, 128, 0, s>>>(d.scene, P, c);
+                k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c);
+                k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
+                k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
                 launches += 6;
                 ext_launches += 1;

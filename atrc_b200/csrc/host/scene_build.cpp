@@ -291,6 +291,11 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs) {
         }
     }
 
+    // leaf links encode (first << 4 | count - 1) in 31 bits; the two most
+    // negative links are reserved as traversal markers
+    if (hs->tri_shade.size() >= (size_t(1) << 27) - 2)
+        throw std::runtime_error("scene has too many triangles for one device scene (limit 134M)");
+
     // ------------------------------------------------------------ entities
     std::vector<bool> leaf_needs_alias(d.geometry_count, false);
     std::vector<Bound> ent_bounds(d.entity_count);
