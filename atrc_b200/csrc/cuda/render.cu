@@ -172,8 +172,22 @@ struct Camera {
     float film_w, film_h, focal, lens_radius;
 };
 
+// The film is cut into tiles of G x G pixels (task_grid_size).  Each tile
+// samples every pixel of its bound grown by the filter's reach
+// (sample_bound_of, framebuffer.h:36-47) and splats only into itself
+// (FilmGrid::apply, render_target.h:383-395), so a pixel near a tile edge is
+// sampled once per tile that reaches it.  The sample grid lays the tiles'
+// sample bounds side by side: column u belongs to tile column gx where
+// tile_cols[gx].w <= u < tile_cols[gx + 1].w, and is pixel
+// tile_cols[gx].z + (u - tile_cols[gx].w); rows likewise.  With the default
+// box filter (radius 0.5 - eps) the sample grid is the film itself.
 struct Params {
     int W, H;
+    int G, TX, TY;          // tile edge, tile columns / rows
+    int SW, SH;             // sample grid size (sum of the tiles' sample bounds)
+    int E0X, E0Y;           // sample-bound extent of the first tile column / row
+    const int4* tile_cols;  // per tile column: x0, x1, first sampled x, first u
+    const int4* tile_rows;  // per tile row:    y0, y1, first sampled y, first v
     int first_spp;
     int min_depth, max_depth, specular_depth;
     float cont_prob, eps;
@@ -244,10 +258,45 @@ __device__ __forceinline__ Rng load_rng(const uint4& s) { Rng r; r.state = (uint
 __device__ __forceinline__ void store_rng(uint4& s, const Rng& r) { s.y = uint32_t(r.state); s.z = uint32_t(r.state >> 32); }
 __device__ __forceinline__ Vec3 xyz(const float4& v) { return Vec3(v.x, v.y, v.z); }
 
+// Tile tables of the sample grid (one thread; TX + TY entries).  The bounds
+// use the reference's float expressions so both agree on every tile.
+__global__ void k_tiles(Params p, int4* cols, int4* rows) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const float r = p.filter_radius;
+    int acc = 0;
+    for (int g = 0; g < p.TX; ++g) {
+        const int a0 = g * p.G, a1 = min(p.W, a0 + p.G) - 1;
+        const int s0 = int(floorf(__fsub_rn(__fadd_rn(float(a0), 0.5f), r)));
+        const int s1 = int(floorf(__fadd_rn(__fadd_rn(float(a1), 0.49999f), r)));
+        cols[g] = make_int4(a0, a1, s0, acc);
+        acc += s1 - s0 + 1;
+    }
+    cols[p.TX] = make_int4(0, 0, 0, acc);
+    acc = 0;
+    for (int g = 0; g < p.TY; ++g) {
+        const int a0 = g * p.G, a1 = min(p.H, a0 + p.G) - 1;
+        const int s0 = int(floorf(__fsub_rn(__fadd_rn(float(a0), 0.5f), r)));
+        const int s1 = int(floorf(__fadd_rn(__fadd_rn(float(a1), 0.49999f), r)));
+        rows[g] = make_int4(a0, a1, s0, acc);
+        acc += s1 - s0 + 1;
+    }
+    rows[p.TY] = make_int4(0, 0, 0, acc);
+}
+
+// sample-grid coordinate -> (tile index along the axis, pixel coordinate)
+__device__ __forceinline__ int tile_of(const int4* t, int n, int e0, int u, int* pix) {
+    int g = min(n - 1, u / e0);
+    while (g > 0 && t[g].w > u) --g;
+    while (g + 1 < n && t[g + 1].w <= u) ++g;
+    const int4 e = t[g];
+    *pix = e.z + (u - e.w);
+    return g;
+}
+
 __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
     const int n = c->n_new, base = c->n_cont, fb = c->free_base, in = c->in;
     const unsigned long long gen = c->gen_base;
-    const unsigned long long npix = (unsigned long long)p.W * p.H;
+    const unsigned long long npix = (unsigned long long)p.SW * p.SH;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = P.free_list[fb + i];
         const unsigned long long k = gen + i;
@@ -255,7 +304,9 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
         const unsigned long long s = (unsigned long long)p.first_spp + k / npix;
         Rng rng;
         rng.state = mix64(p.seed ^ mix64(pixel * 0x9E3779B97F4A7C15ULL + s * 0xD1B54A32D192ED03ULL + 1));
-        const int px = int(pixel % p.W), py = int(pixel / p.W);
+        int px, py;
+        const int gx = tile_of(p.tile_cols, p.TX, p.E0X, int(pixel % p.SW), &px);
+        const int gy = tile_of(p.tile_rows, p.TY, p.E0Y, int(pixel / p.SW), &py);
         // render_grid (perpixel_renderer.cpp:27-36) + ThinLensCamera::sample_we
         const float fx = px + rng.u(), fy = py + rng.u();
         const float film_x = fx / p.W, film_y = fy / p.H;
@@ -278,7 +329,7 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
         P.gb_normal[slot] = make_float4(0, 0, 0, 0);
         uint4 st;
         st.x = uint32_t(pixel);
-        st.w = 0;
+        st.w = uint32_t(gy * p.TX + gx);  // the tile this sample splats into
         store_rng(st, rng);
         P.st[slot] = st;
         P.ctr[slot] = make_int4(1, 1, 0, 0);
@@ -538,10 +589,14 @@ __global__ void k_finish(Params p, Pool P, Film F, Counters* c) {
         const float sx = L.w, sy = P.mis_f[slot].w;
         if (isfinite(L.x) && isfinite(L.y) && isfinite(L.z)) {
             const float4 ga = P.gb_albedo[slot], gn = P.gb_normal[slot];
-            // apply_image_filter (framebuffer.h:49-80)
+            // apply_image_filter (framebuffer.h:49-80) over the sample's tile;
+            // the distances step by one pixel from the tile-clamped start
+            const int tile = int(P.st[slot].w);
+            const int tx0 = (tile % p.TX) * p.G, ty0 = (tile / p.TX) * p.G;
+            const int tx1 = min(p.W, tx0 + p.G) - 1, ty1 = min(p.H, ty0 + p.G) - 1;
             const float r = p.filter_radius;
-            const int x0 = max(0, int(ceilf(sx - r - 0.5f))), y0 = max(0, int(ceilf(sy - r - 0.5f)));
-            const int x1 = min(p.W - 1, int(floorf(sx + r - 0.5f))), y1 = min(p.H - 1, int(floorf(sy + r - 0.5f)));
+            const int x0 = max(tx0, int(ceilf(sx - r - 0.5f))), y0 = max(ty0, int(ceilf(sy - r - 0.5f)));
+            const int x1 = min(tx1, int(floorf(sx + r - 0.5f))), y1 = min(ty1, int(floorf(sy + r - 0.5f)));
             float yrel = fabsf(y0 + 0.5f - sy);
             for (int y = y0; y <= y1; ++y, yrel += 1) {
                 if (yrel > r) continue;
@@ -594,6 +649,7 @@ struct DeviceSceneImpl {
     DevBuf nodes, tris, tri_shade, tri_orig, entities, tlas_order, materials, tex2d, tex3d, texels, media, alias_prob,
         alias_idx, env_probs, env_alias_prob, env_alias_idx;
     DevBuf watchdog;
+    DevBuf tiles;  // tile tables of the film's sample grid
     // render workspace (kept between calls)
     DevBuf pool_buf, counters, film_buf;
     size_t pool_cap = 0;
@@ -751,7 +807,35 @@ Params make_params(const AtrcRenderDesc& d) {
         p.filter_exp = std::exp(-d.filter_alpha * d.filter_radius * d.filter_radius);
         p.filter_value = 1;
     }
+    // sample grid (the same float expressions as k_tiles)
+    p.G = d.task_grid_size > 0 ? d.task_grid_size : 32;
+    p.TX = (d.width + p.G - 1) / p.G;
+    p.TY = (d.height + p.G - 1) / p.G;
+    const float r = p.filter_radius;
+    auto extent = [&](int n, int* first) {
+        int acc = 0;
+        for (int g = 0; g * p.G < n; ++g) {
+            const int a0 = g * p.G, a1 = std::min(n, a0 + p.G) - 1;
+            const int s0 = int(std::floor(float(a0) + 0.5f - r)), s1 = int(std::floor(float(a1) + 0.49999f + r));
+            if (g == 0) *first = s1 - s0 + 1;
+            acc += s1 - s0 + 1;
+        }
+        return acc;
+    };
+    p.SW = extent(d.width, &p.E0X);
+    p.SH = extent(d.height, &p.E0Y);
     return p;
+}
+
+size_t tile_table_bytes(const Params& p) { return size_t(p.TX + p.TY + 2) * sizeof(int4); }
+
+// Point the params at a tile table and fill it on the stream.
+void setup_tiles(Params* p, void* table, cudaStream_t s) {
+    int4* cols = static_cast<int4*>(table);
+    int4* rows = cols + p->TX + 1;
+    p->tile_cols = cols;
+    p->tile_rows = rows;
+    k_tiles<<<1, 32, 0, s>>>(*p, cols, rows);
 }
 
 }  // namespace
@@ -881,9 +965,11 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         CK(cudaSetDevice(d.device));
         cudaStream_t s = d.stream;
         d.scene.eps = desc->eps;
-        const Params p = make_params(*desc);
+        Params p = make_params(*desc);
+        if (d.tiles.bytes < tile_table_bytes(p)) d.tiles.alloc(tile_table_bytes(p));
+        setup_tiles(&p, d.tiles.p, s);
         const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
-        const unsigned long long total = (unsigned long long)desc->width * desc->height * spp;
+        const unsigned long long total = (unsigned long long)p.SW * p.SH * spp;
         // path pool: enough paths to fill the GPU; shadow capacity = pool x lights
         const int nl = std::max(1, d.scene.light_count);
         size_t cap = desc->path_pool > 0 ? size_t(desc->path_pool) : size_t(1) << 21;
@@ -927,7 +1013,7 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
         k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
         CK(cudaGetLastError());
-        uint64_t launches = 1, ext_launches = 0;
+        uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
         cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
         cudaEvent_t* kev = d.kev;
         const int window = DeviceSceneImpl::kWindow;
@@ -1108,13 +1194,16 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         void* scratch = noalloc_scratch(d.device);
         cudaStream_t s = d.stream;
         d.scene.eps = desc->eps;
-        const Params p = make_params(*desc);
+        Params p = make_params(*desc);
         const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
-        const unsigned long long total = (unsigned long long)desc->width * desc->height * spp;
+        const unsigned long long total = (unsigned long long)p.SW * p.SH * spp;
         const int nl = std::max(1, d.scene.light_count);
-        // largest path pool (a multiple of 256) whose layout fits the array
+        // the array holds the counters, the tile tables, then the path pool
         const size_t counters_bytes = 512;
-        const size_t budget = ATRC_NOALLOC_SCRATCH_BYTES - counters_bytes;
+        const size_t tiles_bytes = (tile_table_bytes(p) + 255) & ~size_t(255);
+        if (counters_bytes + tiles_bytes >= ATRC_NOALLOC_SCRATCH_BYTES / 2)
+            return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: film too large for the static scratch");
+        const size_t budget = ATRC_NOALLOC_SCRATCH_BYTES - counters_bytes - tiles_bytes;
         size_t cap = 0;
         for (size_t c = 256; pool_layout(c, c * nl).total <= budget; c += 256) cap = c;
         if (cap < 1024)
@@ -1133,7 +1222,8 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         const PoolLayout L = pool_layout(cap, shadow_cap);
         char* base = static_cast<char*>(scratch);
         Counters* c = reinterpret_cast<Counters*>(base);
-        Pool P = pool_from(base + counters_bytes, L, shadow_cap);
+        setup_tiles(&p, base + counters_bytes, s);
+        Pool P = pool_from(base + counters_bytes + tiles_bytes, L, shadow_cap);
         Film F{film->value, film->weight, film->value_sq, film->albedo, film->normal, film->denoise};
         const int gsm = grid_for(d.sm_count, 16);
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
@@ -1141,7 +1231,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         // start from a known value)
         k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
         CK(cudaGetLastError());
-        uint64_t launches = 1, ext_launches = 0;
+        uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
         Counters hc{};
         const auto t0 = std::chrono::steady_clock::now();
         for (;;) {

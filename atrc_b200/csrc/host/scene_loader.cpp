@@ -606,6 +606,8 @@ public:
         d.cont_prob = rp.child_real_or("cont_prob", 0.9f);
         d.use_mis = rp.child_int_or("use_mis", 1) != 0;
         d.specular_depth = rp.child_int_or("specular_depth", 20);
+        d.task_grid_size = rp.child_int_or("task_grid_size", 32);
+        if (d.task_grid_size <= 0) throw ConfigError("invalid task_grid_size value");
         // pt_cuda-only keys (defaults keep `pt` configs valid)
         d.seed = uint64_t(rp.child_int_or("seed", 42));
         d.path_pool = rp.child_int_or("path_pool", 0);

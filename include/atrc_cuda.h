@@ -251,6 +251,12 @@ typedef struct AtrcRenderDesc {
     int32_t  path_pool;              /* wavefront path capacity, 0 = auto    */
     int32_t  count_traversal;        /* 1: count BVH work into the stats     */
                                      /* (slower; for roofline accounting)    */
+    int32_t  task_grid_size;         /* pt key (default 32): the film filter */
+                                     /* splats per tile of this edge, and    */
+                                     /* pixels near a tile edge are sampled  */
+                                     /* once per tile (render_target.h:      */
+                                     /* 355-395); 0 means 32                 */
+    int32_t  reserved_;
 } AtrcRenderDesc;
 
 /* FP64 film accumulators, caller allocated, `width*height` pixels each.

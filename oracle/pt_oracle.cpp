@@ -2307,7 +2307,7 @@ int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film
     const float film_w = aspect * film_h;
     Filter filter;
     filter.init(*d, s->eps);
-    const int grid = 32;  // task_grid_size default (renderer_creators.cpp:128)
+    const int grid = d->task_grid_size > 0 ? d->task_grid_size : 32;  // renderer_creators.cpp:128
     const int tx = (W + grid - 1) / grid, ty = (H + grid - 1) / grid;
     std::mutex mtx;
     const size_t n_tiles = size_t(tx) * ty;

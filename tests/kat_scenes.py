@@ -84,3 +84,77 @@ def material_probe(material: dict) -> dict:
 
 def dumps(cfg: dict) -> str:
     return json.dumps(cfg)
+
+
+def feature_scene(tmp: Path, renderer="pt", spp=256, width=48, height=36, gaussian=False) -> dict:
+    """Every pt feature the benchmark workloads leave out, in one small scene:
+    sphere / disk / single triangle / double-sided geometry, nested instances,
+    image textures with repeat wrap and uv transforms, a normal map, Disney
+    transmission, clearcoat, sheen and anisotropy, sphere and disk area lights,
+    the native sky, a thin-lens camera with depth of field and (optionally)
+    the Gaussian film filter."""
+    from atrc_b200.scenes import _box_mesh, write_bm, write_pfm
+    rng = np.random.default_rng(77)
+    write_pfm(tmp / "checker.pfm", np.kron(rng.uniform(0.1, 0.9, (4, 4, 3)), np.ones((8, 8, 1))).astype(np.float32))
+    nm = np.zeros((16, 16, 3), np.float32)
+    yy, xx = np.mgrid[0:16, 0:16] / 16.0
+    nm[..., 0] = 0.5 + 0.3 * np.sin(6 * xx)
+    nm[..., 1] = 0.5 + 0.3 * np.cos(6 * yy)
+    nm[..., 2] = 0.9
+    write_pfm(tmp / "normal.pfm", nm)
+    p, n, uv = _box_mesh((0.4, 0.4, 0.4))
+    write_bm(tmp / "box.bm", p, n, uv)
+
+    def const(v):
+        return {"type": "constant", "texel": list(np.atleast_1d(v).astype(float))}
+
+    checker = {"type": "hdr", "filename": "${scene-directory}/checker.pfm", "wrap_u": "repeat", "wrap_v": "mirror",
+               "transform": [{"type": "scale", "ratio": 3}, {"type": "rotate", "deg": 20}]}
+    ents = [
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-4, -4, -1], "B": [4, -4, -1], "C": [4, 4, -1],
+                                           "D": [-4, 4, -1], "tA": [0, 0], "tB": [1, 0], "tC": [1, 1], "tD": [0, 1],
+                                           "transform": []},
+         "material": {"type": "ideal_diffuse", "albedo": checker,
+                      "normal_map": {"type": "hdr", "filename": "${scene-directory}/normal.pfm", "wrap_u": "repeat",
+                                     "wrap_v": "repeat"}}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.7,
+                                           "transform": [{"type": "translate", "offset": [-1.2, 0.3, -0.3]}]},
+         "material": {"type": "disney", "base_color": const([0.8, 0.8, 0.9]), "metallic": const(0),
+                      "roughness": const(0.3), "transmission": const(0.8), "ior": const(1.45)}},
+        {"type": "geometric", "geometry": {"type": "double_sided",
+                                           "internal": {"type": "disk", "radius": 0.6,
+                                                        "transform": [{"type": "translate", "offset": [1.2, 0.6, 0]},
+                                                                      {"type": "rotate_x", "deg": 70}]}},
+         "material": {"type": "disney", "base_color": const([0.7, 0.3, 0.2]), "metallic": const(0.3),
+                      "roughness": const(0.5), "clearcoat": const(0.8), "sheen": const(0.6),
+                      "sheen_tint": const(0.5), "anisotropic": const(0.6), "specular_tint": const(0.4)}},
+        {"type": "geometric", "geometry": {"type": "triangle", "A": [-0.5, 0, 0], "B": [0.5, 0, 0], "C": [0, 0, 0.9],
+                                           "tA": [0, 0], "tB": [1, 0], "tC": [0.5, 1],
+                                           "transform": [{"type": "translate", "offset": [0.2, 1.2, -1]},
+                                                         {"type": "rotate_z", "deg": 15}]},
+         "material": {"type": "ideal_diffuse", "albedo": checker}},
+        {"type": "geometric", "geometry": {"type": "transform_wrapper", "transform": [{"type": "translate", "offset": [0, -0.6, -0.55]}],
+                                           "internal": {"type": "transform_wrapper",
+                                                        "transform": [{"type": "rotate", "axis": [1, 1, 0], "deg": 30}],
+                                                        "internal": {"type": "triangle_bvh",
+                                                                     "filename": "${scene-directory}/box.bm",
+                                                                     "transform": []}}},
+         "material": {"type": "ideal_diffuse", "albedo": const([0.3, 0.6, 0.4])}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.25,
+                                           "transform": [{"type": "translate", "offset": [0.5, -0.3, 1.6]}]},
+         "material": {"type": "ideal_black"}, "emit_radiance": [6, 5, 4]},
+        {"type": "geometric", "geometry": {"type": "disk", "radius": 0.4,
+                                           "transform": [{"type": "translate", "offset": [-1.5, -0.5, 2.0]},
+                                                         {"type": "rotate_x", "deg": 180}]},
+         "material": {"type": "ideal_black"}, "emit_radiance": [3, 4, 6]},
+    ]
+    cfg = {"scene": {"type": "default", "entities": ents,
+                     "env": {"type": "native_sky", "top": [0.4, 0.5, 0.8], "bottom": [0.1, 0.08, 0.05]}},
+           "rendering": {"camera": {"type": "thin_lens", "pos": [0, -5, 1.2], "dst": [0, 0, -0.2], "up": [0, 0, 1],
+                                    "fov": 50, "lens_radius": 0.05, "focal_distance": 5},
+                         "width": width, "height": height,
+                         "renderer": {"type": renderer, "spp": spp, "max_depth": 12, "min_depth": 3},
+                         "reporter": {"type": "noout"}}}
+    if gaussian:
+        cfg["rendering"]["film_filter"] = {"type": "gaussian", "radius": 1.5, "alpha": 2}
+    return cfg

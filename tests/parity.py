@@ -103,3 +103,52 @@ def global_mean_z(gpu_film, ref_film, filter_value: float = 1 / (4 * (0.5 - 3e-4
     mc, vc, nc = agg(ref_film)
     se = np.sqrt(vg / ng + vc / nc)
     return float(np.max(np.abs(mg - mc) / np.maximum(se, 1e-30)))
+
+
+def filter_weight_moments(n: int, radius: float, alpha: float, grid: int = 32, m: int = 4096):
+    """1D moments of the Gaussian filter's splat weight along one film axis,
+    under the reference's tiled splat (render_target.h:355-395,
+    framebuffer.h:36-80): each tile of `grid` pixels samples its bound grown
+    by the radius and splats only into itself, stepping the distance by one
+    pixel from the tile-clamped first pixel.  Jitter is integrated with the
+    midpoint rule over `m` points.  Returns per pixel (sum E[g], sum E[g^2],
+    sum E[g]^2) over the sample pixels that reach it; the 2D weight of one
+    sample per sample pixel is g(x) g(y), so E[w] = spp m1x m1y and
+    Var[w] = spp (s2x s2y - qx qy)."""
+    r = np.float32(radius)
+    er = math.exp(-alpha * float(r) * float(r))
+    m1, s2, q = np.zeros(n), np.zeros(n), np.zeros(n)
+    jit = (np.arange(m) + 0.5) / m
+    for a0 in range(0, n, grid):
+        a1 = min(n, a0 + grid) - 1
+        s0 = int(np.floor(np.float32(a0) + np.float32(0.5) - r))
+        s1 = int(np.floor(np.float32(a1) + np.float32(0.49999) + r))
+        for X in range(s0, s1 + 1):
+            sx = (np.float32(X) + jit.astype(np.float32)).astype(np.float32)
+            xmin = np.maximum(a0, np.ceil(sx - r - np.float32(0.5)).astype(np.int64))
+            xmax = np.minimum(a1, np.floor(sx + r - np.float32(0.5)).astype(np.int64))
+            xr = np.abs((xmin + np.float32(0.5)).astype(np.float32) - sx)
+            for k in range(int(xmax.max() - xmin.min()) + 1):
+                x = xmin + k
+                live = (x <= xmax) & (xr <= r)
+                g = np.where(live, np.maximum(0.0, np.exp(-alpha * xr.astype(np.float64) ** 2) - er), 0.0)
+                for px in np.unique(x[live]):
+                    sel = x == px
+                    gsel = np.where(sel, g, 0.0)
+                    e1 = gsel.sum() / m
+                    m1[px] += e1
+                    s2[px] += (gsel ** 2).sum() / m
+                    q[px] += e1 * e1
+                xr = xr + np.float32(1)
+    return m1, s2, q
+
+
+def filter_weight_z(weight: np.ndarray, width: int, height: int, spp: int, radius: float, alpha: float,
+                    grid: int = 32) -> np.ndarray:
+    """Per-pixel z-scores of a film's Gaussian-filter weights against their
+    expectation under the reference's tiled splat."""
+    mx, sx, qx = filter_weight_moments(width, radius, alpha, grid)
+    my, sy, qy = filter_weight_moments(height, radius, alpha, grid)
+    mean = spp * np.outer(my, mx)
+    var = spp * (np.outer(sy, sx) - np.outer(qy, qx))
+    return (np.asarray(weight).reshape(height, width) - mean) / np.sqrt(np.maximum(var, 1e-300))

@@ -129,3 +129,66 @@ def test_media_image_within_3_sigma(scene_dir):
     r = 0.5 - desc.eps
     frac, allowed, info = band_test(fg, fc, 1 / (4 * r * r))
     assert frac <= allowed, (frac, allowed, info)
+
+
+def test_feature_scene_within_3_sigma(tmp_path):
+    from tests import kat_scenes as K
+    cfg = Config.from_string(K.dumps(K.feature_scene(tmp_path, spp=512)), tmp_path)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    fg = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    fc = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    dev.render(desc, fg)
+    ora.render(desc, fc)
+    r = 0.5 - desc.eps
+    frac, allowed, info = band_test(fg, fc, 1 / (4 * r * r))
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fg, fc) < 4.0
+    # first-hit normals (normal map, frames of every shape) agree
+    gn = fg.normal.reshape(-1, 3) / fg.weight.reshape(-1, 1)
+    cn = fc.normal.reshape(-1, 3) / fc.weight.reshape(-1, 1)
+    assert np.mean(np.abs(gn - cn)) < 0.02
+
+
+def test_gaussian_filter_matches(tmp_path):
+    from tests import kat_scenes as K
+    cfg = Config.from_string(K.dumps(K.feature_scene(tmp_path, spp=128, gaussian=True)), tmp_path)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    fg, fc = Film(desc.width, desc.height, value_sq=True), Film(desc.width, desc.height, value_sq=True)
+    dev.render(desc, fg)
+    ora.render(desc, fc)
+    # the splat footprint: per-tile sampling of the grown bound, per-tile
+    # clamps and one-pixel distance steps, as z-scores against the analytic
+    # expectation of the weights (the oracle is pinned to it on the CPU)
+    from tests.parity import filter_weight_z
+    for f in (fg, fc):
+        z = filter_weight_z(f.weight, desc.width, desc.height, desc.spp, desc.filter_radius, desc.filter_alpha)
+        assert np.mean(np.abs(z)) < 0.9 and np.mean(np.abs(z) > 4) < 0.002, (np.mean(np.abs(z)), np.abs(z).max())
+    # conservative per-pixel z (sample count from the filter's peak weight)
+    wmax = (1 - np.exp(-2 * 1.5 ** 2)) ** 2
+    def st(f):
+        w = f.weight.reshape(-1, 1)
+        mu = f.value.reshape(-1, 3) / w
+        var = np.maximum(f.value_sq.reshape(-1, 3) / w - mu * mu, 0)
+        return mu, var, w / wmax
+    mg, vg, ng = st(fg)
+    mc, vc, nc = st(fc)
+    z = np.abs(mg - mc) / np.sqrt(vg / ng + vc / nc + 1e-12)
+    assert np.mean(z > 4) < 0.01
+
+
+def test_closest_hits_bit_exact_1e7_full_workload():
+    # the full 3.08M-triangle instanced workload and 10^7 seeded rays
+    from atrc_b200.scenes import instanced_disney
+    cfg, desc, dev, ora = _scene(instanced_disney())
+    rays = seeded_rays(10_000_000, [-22.0] * 3, [22.0] * 3, list(desc.camera.pos), seed=13)
+    g = dev.trace_rays(rays, "closest", exact=True)
+    r = ora.trace_rays(rays, "closest")
+    c = classify_closest(rays, g, r, ora)
+    assert c["error"] == 0, c["errors"]
+    assert c["max_ulp_same_prim"] == 0
+    assert c["exact"] + c["tie"] + c["ref_fn"] == len(rays)
+    assert c["exact"] >= len(rays) * 0.9999, c

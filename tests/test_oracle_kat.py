@@ -110,3 +110,19 @@ def test_disney_reports_mixture_pdf_but_never_samples_diffuse():
     assert ratio < 0.7, ratio
     # the continuation estimate f cos / pdf is biased accordingly
     assert np.mean(s_f[ok, 0] * s_wi[ok, 2] / s_pdf[ok]) > 0
+
+
+def test_gaussian_splat_follows_the_tiled_reference(tmp_path):
+    # render_target.h:355-395: a tile samples its bound grown by the filter
+    # radius and splats only into itself; framebuffer.h:49-80 steps the
+    # distance by one pixel from the clamped first pixel.  The weights of the
+    # film follow that model, and not the model of one film-wide tile.
+    from tests.parity import filter_weight_z
+    cfg, desc, ora = _oracle(K.feature_scene(tmp_path, spp=64, gaussian=True), tmp_path)
+    f = Film(desc.width, desc.height)
+    ora.render(desc, f)
+    args = (desc.width, desc.height, desc.spp, desc.filter_radius, desc.filter_alpha)
+    z = filter_weight_z(f.weight, *args)
+    assert np.mean(np.abs(z)) < 0.9 and np.abs(z).max() < 5.5
+    z_untiled = filter_weight_z(f.weight, *args, grid=1 << 20)
+    assert np.abs(z_untiled).max() > 20
