@@ -21,6 +21,22 @@ namespace atrc {
 namespace dev {
 
 constexpr int kStackSize = 96;
+// Optional traversal short stack (ATRC_STACK_RING > 0): the top entries of
+// each thread's stack live in shared memory (a ring, entry i in slot
+// i % kStackRing, slots strided by the block size so a warp's accesses hit
+// 32 banks); deeper entries spill to local memory.  Off by default: on the
+// instanced 3.08M-triangle workload a 16-entry ring ran 3.7 % slower than the
+// plain local-memory stack (597 vs 620 Msamples/s), whose top entries stay
+// in L1 anyway, while the ring's shared memory shrinks L1 for BVH nodes.
+// Every kernel that traces launches blocks of at most kTraceBlock threads
+// (__launch_bounds__ enforces it).
+#ifndef ATRC_STACK_RING
+#define ATRC_STACK_RING 0
+#endif
+constexpr int kStackRing = ATRC_STACK_RING;
+constexpr int kTraceBlock = 128;
+static_assert(kStackRing == 0 || (kStackRing & (kStackRing - 1)) == 0, "ring size must be a power of two");
+static_assert(kStackRing < kStackSize, "ring must be smaller than the stack");
 constexpr int32_t kSentinel = INT_MIN;      // "return from a bottom-level tree"
 constexpr int32_t kDone = INT_MIN + 1;      // empty stack
 
@@ -181,7 +197,13 @@ template <bool EXACT, bool ANY, bool COUNT = false>
 __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog,
                           TraceCount* cnt = nullptr) {
     if (S.entity_count == 0) return false;
+#if ATRC_STACK_RING > 0
+    __shared__ int32_t s_ring[kStackRing * kTraceBlock];
+    int32_t* const ring = s_ring + threadIdx.x;
+    int32_t spill[kStackSize - kStackRing];
+#else
     int32_t stack[kStackSize];
+#endif
     int sp = 0;
     RayState r;
     r.o = wo; r.d = wd; r.inv = safe_inv(wd); r.tmin = tmin; r.tmax = tmax;
@@ -194,11 +216,31 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
     int32_t held = 0;  // parked leaf (negative) or 0
     bool overflow = false;
 
+#if ATRC_STACK_RING > 0
+    // entry i sits in ring slot i % R; pushing entry sp evicts entry sp - R
+    // to the spill array, popping entry sp refills its slot with sp - R
+    auto push = [&](int32_t v) {
+        if (sp >= kStackSize) { overflow = true; return; }
+        int32_t& slot = ring[(sp & (kStackRing - 1)) * kTraceBlock];
+        if (sp >= kStackRing) spill[sp - kStackRing] = slot;
+        slot = v;
+        ++sp;
+    };
+    auto pop = [&]() -> int32_t {
+        if (sp <= 0) return kDone;
+        --sp;
+        int32_t& slot = ring[(sp & (kStackRing - 1)) * kTraceBlock];
+        const int32_t v = slot;
+        if (sp >= kStackRing) slot = spill[sp - kStackRing];
+        return v;
+    };
+#else
     auto push = [&](int32_t v) {
         if (sp >= kStackSize) { overflow = true; return; }
         stack[sp++] = v;
     };
     auto pop = [&]() -> int32_t { return sp > 0 ? stack[--sp] : kDone; };
+#endif
 
     // Visit leaf `lf`; `next` is what follows it.  Returns the new link.
     // Sets `found` in ANY mode when something was hit.

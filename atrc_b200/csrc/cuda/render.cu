@@ -44,6 +44,9 @@
 #ifndef ATRC_SHADE_MIN_BLOCKS
 #define ATRC_SHADE_MIN_BLOCKS 4  // k_shade blocks per SM the register budget must allow
 #endif
+#ifndef ATRC_TRACE_MIN_BLOCKS
+#define ATRC_TRACE_MIN_BLOCKS 8  // the same for the traversal kernels
+#endif
 
 namespace atrc {
 
@@ -109,7 +112,7 @@ __device__ __forceinline__ int warp_append(int* counter, bool pred) {
 
 // ------------------------------------------------------------ ray queries
 template <bool EXACT, bool ANY>
-__global__ void k_trace_rays(Scene S, const AtrcRay* __restrict__ rays, size_t n, AtrcHit* __restrict__ hits,
+__global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_trace_rays(Scene S, const AtrcRay* __restrict__ rays, size_t n, AtrcHit* __restrict__ hits,
                              int* watchdog) {
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         const AtrcRay q = rays[i];
@@ -338,7 +341,7 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
 }
 
 template <bool EXACT, bool COUNT>
-__global__ void __launch_bounds__(128) k_extend(Scene S, Pool P, Counters* c) {
+__global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(Scene S, Pool P, Counters* c) {
     const int n = c->n_ext, in = c->in;
     TraceCount tc{0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -553,7 +556,7 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
 }
 
 template <bool EXACT, bool COUNT>
-__global__ void __launch_bounds__(128) k_shadow(Scene S, Pool P, Counters* c) {
+__global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_shadow(Scene S, Pool P, Counters* c) {
     const int n = min(c->n_shadow, P.shadow_cap);
     TraceCount tc{0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

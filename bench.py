@@ -290,7 +290,8 @@ def main():
                          "traffic": None, "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray,
                          "tris_per_ray": tris_per_ray, "entities_per_ray": ents_per_ray,
                          "avg_launch_ms": ext_time / max(ext_launches, 1) * 1e3},
-            "kernel_time_share": {"extend": ext_time, "shade": shade_time, "shadow": shadow_time},
+            "kernel_time_share": {"extend": ext_time / elapsed, "shade": shade_time / elapsed,
+                                  "shadow": shadow_time / elapsed},
             "rays": {"closest_per_sample": rays_closest / max(samples / world, 1),
                      "shadow_per_sample": sum(st["rays_shadow"] for st in stats) / max(samples / world, 1),
                      "Mrays_per_s": (rays_closest + sum(st["rays_shadow"] for st in stats)) * world / elapsed / 1e6},
