@@ -121,6 +121,7 @@ struct Scene {
     int32_t tlas_root;
     int32_t entity_count;
     const Material* materials;
+    int32_t material_count;
     const Texture2D* tex2d;
     const Texture3D* tex3d;
     const float* texels;

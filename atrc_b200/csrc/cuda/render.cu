@@ -192,6 +192,7 @@ struct Params {
     const int4* tile_cols;  // per tile column: x0, x1, first sampled x, first u
     const int4* tile_rows;  // per tile row:    y0, y1, first sampled y, first v
     int first_spp;
+    int sort_mode, nkeys;   // shade-queue sort (AtrcSortMode, resolved) and key count
     int min_depth, max_depth, specular_depth;
     float cont_prob, eps;
     unsigned long long seed;
@@ -212,6 +213,10 @@ struct Pool {
     uint4* st;                    // pixel, rng lo, rng hi, unused
     int4* ctr;                    // depth, s_depth, scattering_count, flags | medium << 8
     int* q[2];                    // extend queues
+    int* q_sorted;                // the extend queue sorted by material key
+    int* keys;                    // material key per extend-queue entry
+    int* key_count;               // per key: entries this iteration
+    int* key_cursor;              // per key: next write position in q_sorted
     int* q_finish;
     int* free_list;
     float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
@@ -222,9 +227,10 @@ struct Film {
     double *value, *weight, *value_sq, *albedo, *normal, *denoise;
 };
 
-__global__ void k_init(Pool P, int cap, Counters* c, unsigned long long total) {
+__global__ void k_init(Pool P, int cap, int nkeys, Counters* c, unsigned long long total) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < cap) P.free_list[i] = i;
+    if (i < nkeys) P.key_count[i] = 0;
     if (i == 0) {
         memset(c, 0, sizeof(Counters));
         c->n_free = cap;
@@ -340,8 +346,66 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
     }
 }
 
+// Material key of a hit record: 0 for a miss, nkeys - 1 for a path inside a
+// medium (its next step is medium sampling), else 1 + the material type or
+// index of the hit entity.  Counted per warp (one atomic per distinct key).
+__device__ __forceinline__ void count_key(const Scene& S, Pool& P, int sort_mode, int nkeys, int i, int slot,
+                                          bool hit, int entity) {
+    int key;
+    const int med = reinterpret_cast<const int*>(P.ctr + slot)[3] >> 8;
+    if (med != 0) key = nkeys - 1;
+    else if (!hit) key = 0;
+    else {
+        const int m = S.entities[entity].material;
+        key = 1 + (sort_mode == ATRC_SORT_TYPE ? S.materials[m].type : m);
+    }
+    P.keys[i] = key;
+    const unsigned same = __match_any_sync(__activemask(), key);
+    if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(P.key_count + key, __popc(same));
+}
+
+// Exclusive scan of the key counts into write cursors (one block of 1024);
+// clears the counts for the next iteration.
+__global__ void __launch_bounds__(1024) k_sort_scan(Pool P, int nkeys) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x, per = (nkeys + 1023) / 1024;
+    const int b0 = min(nkeys, t * per), b1 = min(nkeys, b0 + per);
+    int sum = 0;
+    for (int k = b0; k < b1; ++k) sum += P.key_count[k];
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int v = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int acc = part[t] - sum;
+    for (int k = b0; k < b1; ++k) {
+        const int cnt = P.key_count[k];
+        P.key_cursor[k] = acc;
+        acc += cnt;
+        P.key_count[k] = 0;
+    }
+}
+
+// Scatter the extend queue into key order (order within a key is arbitrary).
+__global__ void k_sort_scatter(Pool P, Counters* c) {
+    const int n = c->n_ext, in = c->in;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int key = P.keys[i];
+        const unsigned same = __match_any_sync(__activemask(), key);
+        const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(P.key_cursor + key, __popc(same));
+        base = __shfl_sync(same, base, leader);
+        P.q_sorted[base + __popc(same & ((1u << lane) - 1u))] = P.q[in][i];
+    }
+}
+
 template <bool EXACT, bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(Scene S, Pool P, Counters* c) {
+__global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(Scene S, Pool P, Counters* c,
+                                                                              int sort_mode, int nkeys) {
     const int n = c->n_ext, in = c->in;
     TraceCount tc{0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -355,6 +419,7 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(S
         if (wd) atomicMax(&c->watchdog, wd);
         P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.entity : -1));
         P.hit_tri[slot] = h.tri;
+        if (sort_mode != ATRC_SORT_NONE) count_key(S, P, sort_mode, nkeys, i, slot, hit, h.entity);
     }
     if (COUNT) flush_count(c->cnt_closest, tc);
 }
@@ -371,8 +436,9 @@ __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d
 __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, Params p, Pool P, Counters* c) {
     const int n = c->n_ext, in = c->in, out = c->out;
     const float eps = p.eps;
+    const int* queue = p.sort_mode != ATRC_SORT_NONE ? P.q_sorted : P.q[in];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = P.q[in][i];
+        const int slot = queue[i];
         int4 ct = P.ctr[slot];
         int depth = ct.x, s_depth = ct.y, scat = ct.z, flags = ct.w & 0xff, ray_med = ct.w >> 8;
         uint4 st = P.st[slot];
@@ -635,11 +701,43 @@ __global__ void k_finish(Params p, Pool P, Film F, Counters* c) {
     }
 }
 
-__global__ void k_add_film(double* dst, const double* src, size_t n) {
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) dst[i] += src[i];
-}
-
 int grid_for(int sm_count, int blocks_per_sm) { return std::max(1, sm_count * blocks_per_sm); }
+
+// Stream capture scope: ends the capture (and drops the partial graph) if
+// anything throws before end() is called, so the stream never stays in
+// capture mode.
+struct CaptureGuard {
+    cudaStream_t s;
+    bool open = true;
+    explicit CaptureGuard(cudaStream_t st) : s(st) { CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)); }
+    cudaGraph_t end() {
+        cudaGraph_t g = nullptr;
+        open = false;
+        CK(cudaStreamEndCapture(s, &g));
+        return g;
+    }
+    ~CaptureGuard() {
+        if (!open) return;
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+    }
+};
+
+// Reuse an executable graph when the new graph has the same topology (only
+// kernel parameters differ); otherwise instantiate afresh.
+cudaGraphExec_t instantiate_or_update(cudaGraphExec_t exec, cudaGraph_t g) {
+    if (exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(exec, g, &info) == cudaSuccess) return exec;
+        cudaGetLastError();
+        cudaGraphExecDestroy(exec);
+    }
+    cudaGraphExec_t out = nullptr;
+    CK(cudaGraphInstantiate(&out, g, 0));
+    return out;
+}
 
 }  // namespace
 
@@ -661,8 +759,14 @@ struct DeviceSceneImpl {
     static constexpr int kWindow = 4;  // wavefront iterations between host checks
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, kev[kWindow * 4] = {};
     void* pinned_counters = nullptr;
+    cudaGraphExec_t window_exec = nullptr;  // the captured bounce-loop window
     void* stage = nullptr;             // pinned host staging for host films
     size_t stage_bytes = 0;
+    int tuned_sort = ATRC_SORT_NONE;  // ATRC_SORT_AUTO resolves to this
+    void resolve_sort(Params* p, int requested) const {
+        p->sort_mode = requested == ATRC_SORT_AUTO ? tuned_sort : requested;
+        p->nkeys = std::max(scene.material_count, 4) + 2;
+    }
     void ensure_render_resources() {
         if (!ev0) {
             CK(cudaEventCreate(&ev0));
@@ -683,6 +787,7 @@ struct DeviceSceneImpl {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (auto& e : kev) if (e) cudaEventDestroy(e);
+        if (window_exec) cudaGraphExecDestroy(window_exec);
         if (pinned_counters) cudaFreeHost(pinned_counters);
         if (stage) cudaFreeHost(stage);
         if (stream) cudaStreamDestroy(stream);
@@ -729,7 +834,7 @@ struct PoolLayout {
     size_t total;
 };
 
-PoolLayout pool_layout(size_t cap, size_t shadow_cap) {
+PoolLayout pool_layout(size_t cap, size_t shadow_cap, int nkeys) {
     PoolLayout L{};
     size_t o = 0;
     auto take = [&](int i, size_t bytes) {
@@ -742,6 +847,7 @@ PoolLayout pool_layout(size_t cap, size_t shadow_cap) {
     take(9, cap * 16); take(10, cap * 16);
     take(11, cap * 4); take(12, cap * 4); take(13, cap * 4); take(14, cap * 4);
     take(15, shadow_cap * 16); take(16, shadow_cap * 16); take(17, shadow_cap * 16);
+    take(18, cap * 4); take(19, cap * 4); take(20, size_t(nkeys) * 4); take(21, size_t(nkeys) * 4);
     L.total = (o + 255) & ~size_t(255);
     return L;
 }
@@ -767,6 +873,10 @@ Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
     P.sh_o = reinterpret_cast<float4*>(b + L.off[15]);
     P.sh_d = reinterpret_cast<float4*>(b + L.off[16]);
     P.sh_c = reinterpret_cast<float4*>(b + L.off[17]);
+    P.q_sorted = reinterpret_cast<int*>(b + L.off[18]);
+    P.keys = reinterpret_cast<int*>(b + L.off[19]);
+    P.key_count = reinterpret_cast<int*>(b + L.off[20]);
+    P.key_cursor = reinterpret_cast<int*>(b + L.off[21]);
     P.shadow_cap = int(shadow_cap);
     return P;
 }
@@ -856,7 +966,7 @@ int atrc_cuda_device_init(int device, AtrcDeviceInfo* info) {
         CK(cudaGetDeviceProperties(&prop, device));
         if (info) {
             std::memset(info, 0, sizeof(*info));
-            std::snprintf(info->name, sizeof(info->name), "%s", prop.name);
+            std::strncpy(info->name, prop.name, sizeof(info->name) - 1);
             info->sm_count = prop.multiProcessorCount;
             info->cc_major = prop.major;
             info->cc_minor = prop.minor;
@@ -889,6 +999,7 @@ int atrc_cuda_scene_create(const AtrcSceneDesc* desc, AtrcScene** out) {
         S.entities = upload(d.entities, hs->entities, s);
         S.tlas_order = upload(d.tlas_order, hs->tlas_order, s);
         S.materials = upload(d.materials, hs->materials, s);
+        S.material_count = int32_t(hs->materials.size());
         S.tex2d = upload(d.tex2d, hs->tex2d, s);
         S.tex3d = upload(d.tex3d, hs->tex3d, s);
         S.texels = upload(d.texels, hs->texels, s);
@@ -960,6 +1071,8 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid film size, spp or depth");
     if (desc->spp_count < 0 || desc->first_spp < 0)
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid sample range");
+    if (desc->sort_mode < ATRC_SORT_AUTO || desc->sort_mode > ATRC_SORT_MATERIAL)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid sort_mode");
     if (desc->filter_type == ATRC_FILTER_BOX ? !(desc->filter_radius - desc->eps > 0) : !(desc->filter_radius > 0 && desc->filter_alpha > 0))
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid film filter");
     return guarded([&] {
@@ -969,6 +1082,7 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         cudaStream_t s = d.stream;
         d.scene.eps = desc->eps;
         Params p = make_params(*desc);
+        d.resolve_sort(&p, desc->sort_mode);
         if (d.tiles.bytes < tile_table_bytes(p)) d.tiles.alloc(tile_table_bytes(p));
         setup_tiles(&p, d.tiles.p, s);
         const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
@@ -979,8 +1093,8 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         cap = std::min<size_t>(cap, std::max<unsigned long long>(total, 1024ULL));
         cap = std::min<size_t>(cap, (size_t(1) << 28) / nl);
         const size_t shadow_cap = cap * nl;
-        const PoolLayout L = pool_layout(cap, shadow_cap);
-        if (d.pool_cap != cap || d.pool_lights != nl) {
+        const PoolLayout L = pool_layout(cap, shadow_cap, p.nkeys);
+        if (d.pool_buf.bytes < L.total || d.pool_cap != cap || d.pool_lights != nl) {
             d.pool_buf.alloc(L.total);
             d.pool_cap = cap;
             d.pool_lights = nl;
@@ -1014,7 +1128,7 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         // one path / ray per thread for the heavy kernels (grids cover the
         // pool; threads past the device-side count return at once)
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
-        k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
+        k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
         CK(cudaGetLastError());
         uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
         cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
@@ -1027,25 +1141,43 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         Counters* pinned = static_cast<Counters*>(d.pinned_counters);
         int status = ATRC_OK;
         const bool count = desc->count_traversal != 0;
-        for (int iter_block = 0;; ++iter_block) {
+        // The bounce loop runs in windows of `window` iterations.  One window
+        // (6 kernels per iteration, the timing events and the counter
+        // read-back) is captured once per call as a CUDA graph and relaunched
+        // until the device-side counters say the work is done: the kernels
+        // take their sizes from the counters, so every window is the same
+        // graph.  The executable graph is kept with the scene and updated in
+        // place when the next call's parameters differ.
+        {
+            CaptureGuard cap(s);
             for (int k = 0; k < window; ++k) {
                 k_begin<<<1, 1, 0, s>>>(c);
                 k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
-                CK(cudaEventRecord(kev[k * 4 + 0], s));
-                if (count) k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c);
-                else k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c);
-                CK(cudaEventRecord(kev[k * 4 + 1], s));
+                CK(cudaEventRecordWithFlags(kev[k * 4 + 0], s, cudaEventRecordExternal));
+                if (count) k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                else k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                if (p.sort_mode != ATRC_SORT_NONE) {
+                    k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
+                    k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
+                }
+                CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
                 k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
-                CK(cudaEventRecord(kev[k * 4 + 2], s));
+                CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
                 if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 else k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
-                CK(cudaEventRecord(kev[k * 4 + 3], s));
+                CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
                 k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
-                launches += 6;
-                ext_launches += 1;
             }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+            cudaGraph_t g = cap.end();
+            d.window_exec = instantiate_or_update(d.window_exec, g);
+            cudaGraphDestroy(g);
+        }
+        for (int iter_block = 0;; ++iter_block) {
+            CK(cudaGraphLaunch(d.window_exec, s));
+            launches += (p.sort_mode != ATRC_SORT_NONE ? 8 : 6) * window;
+            ext_launches += window;
             CK(cudaStreamSynchronize(s));
             hc = *pinned;
             for (int k = 0; k < window; ++k) {
@@ -1188,6 +1320,8 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
     if (desc->width <= 0 || desc->height <= 0 || desc->spp <= 0 || desc->max_depth < 0 || desc->spp_count < 0 ||
         desc->first_spp < 0)
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid film size, spp, depth or sample range");
+    if (desc->sort_mode < ATRC_SORT_AUTO || desc->sort_mode > ATRC_SORT_MATERIAL)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid sort_mode");
     if (desc->filter_type == ATRC_FILTER_BOX ? !(desc->filter_radius - desc->eps > 0)
                                              : !(desc->filter_radius > 0 && desc->filter_alpha > 0))
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid film filter");
@@ -1198,6 +1332,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         cudaStream_t s = d.stream;
         d.scene.eps = desc->eps;
         Params p = make_params(*desc);
+        d.resolve_sort(&p, desc->sort_mode);
         const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
         const unsigned long long total = (unsigned long long)p.SW * p.SH * spp;
         const int nl = std::max(1, d.scene.light_count);
@@ -1208,7 +1343,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
             return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: film too large for the static scratch");
         const size_t budget = ATRC_NOALLOC_SCRATCH_BYTES - counters_bytes - tiles_bytes;
         size_t cap = 0;
-        for (size_t c = 256; pool_layout(c, c * nl).total <= budget; c += 256) cap = c;
+        for (size_t c = 256; pool_layout(c, c * nl, p.nkeys).total <= budget; c += 256) cap = c;
         if (cap < 1024)
             return fail(ATRC_ERR_UNSUPPORTED, "atrc_cuda_render_noalloc: the scene's " + std::to_string(nl) +
                                                   " lights leave room for fewer than 1024 paths in the " +
@@ -1222,7 +1357,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         }
         cap = std::min<size_t>(cap, std::max<unsigned long long>(total, 1024ULL));
         const size_t shadow_cap = cap * nl;
-        const PoolLayout L = pool_layout(cap, shadow_cap);
+        const PoolLayout L = pool_layout(cap, shadow_cap, p.nkeys);
         char* base = static_cast<char*>(scratch);
         Counters* c = reinterpret_cast<Counters*>(base);
         setup_tiles(&p, base + counters_bytes, s);
@@ -1232,7 +1367,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
         // k_init rewrites the counters and the free list (all state that must
         // start from a known value)
-        k_init<<<int((cap + 255) / 256), 256, 0, s>>>(P, int(cap), c, total);
+        k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
         CK(cudaGetLastError());
         uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
         Counters hc{};
@@ -1241,7 +1376,12 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
             for (int k = 0; k < DeviceSceneImpl::kWindow; ++k) {
                 k_begin<<<1, 1, 0, s>>>(c);
                 k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
-                k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c);
+                k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                if (p.sort_mode != ATRC_SORT_NONE) {
+                    k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
+                    k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
+                    launches += 2;
+                }
                 k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
                 k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);

@@ -611,6 +611,9 @@ public:
         // pt_cuda-only keys (defaults keep `pt` configs valid)
         d.seed = uint64_t(rp.child_int_or("seed", 42));
         d.path_pool = rp.child_int_or("path_pool", 0);
+        d.sort_mode = rp.child_int_or("sort_mode", ATRC_SORT_AUTO);
+        if (d.sort_mode < ATRC_SORT_AUTO || d.sort_mode > ATRC_SORT_MATERIAL)
+            throw ConfigError("invalid sort_mode value (-1 auto, 0 none, 1 material type, 2 material)");
         d.first_spp = 0;
         d.spp_count = 0;
         if (auto n = r.find_child("post_processors")) node_to_json(*n, e.post_processors_json);

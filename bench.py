@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--spp-per-step", type=int, default=16)
     p.add_argument("--scene", default="instanced", choices=["instanced", "cornell", "media"])
     p.add_argument("--path-pool", type=int, default=0)
+    p.add_argument("--sort-mode", type=int, default=-1, choices=[-1, 0, 1, 2],
+                   help="shade-queue sort: -1 auto, 0 none, 1 material type, 2 material")
     p.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed oracle run (profiling)")
     return p.parse_args()
 
@@ -201,6 +203,7 @@ def main():
     scene = DeviceScene(cfg, device=local)
     build_s = time.perf_counter() - t0
     desc.path_pool = args.path_pool
+    desc.sort_mode = args.sort_mode
     spp = args.spp_per_step
     desc.spp_count = spp
     W, H = desc.width, desc.height

@@ -256,8 +256,16 @@ typedef struct AtrcRenderDesc {
                                      /* pixels near a tile edge are sampled  */
                                      /* once per tile (render_target.h:      */
                                      /* 355-395); 0 means 32                 */
-    int32_t  reserved_;
+    int32_t  sort_mode;              /* order of the shade queue: ATRC_SORT_* */
 } AtrcRenderDesc;
+
+/* Sorting of hit records before shading (a counting sort by key). */
+typedef enum AtrcSortMode {
+    ATRC_SORT_AUTO     = -1,  /* the scene's tuned choice, else ATRC_SORT_NONE */
+    ATRC_SORT_NONE     = 0,   /* shade in extend-queue order                   */
+    ATRC_SORT_TYPE     = 1,   /* by material type (miss / each type / medium)  */
+    ATRC_SORT_MATERIAL = 2    /* by material index (miss / each / medium)      */
+} AtrcSortMode;
 
 /* FP64 film accumulators, caller allocated, `width*height` pixels each.
  * Any pointer except `value` and `weight` may be NULL.  The renderer ADDS

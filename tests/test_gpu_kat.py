@@ -137,3 +137,42 @@ def test_empty_scene_and_threads(tmp_path):
     for t in ts:
         t.join()
     assert abs(out[0] - 1) < 1e-5 and abs(out[1] - 1) < 0.05
+
+
+@pytest.mark.parametrize("scene", ["cornell", "media"])
+def test_shade_queue_sort_changes_nothing(scene, cornell_path, scene_dir):
+    # sorting hit records by material key only reorders the shade queue: every
+    # path keeps its own random stream, so the films agree up to the order in
+    # which the FP32 shadow-ray results of several lights add into one path
+    from atrc_b200 import scenes
+    path = cornell_path if scene == "cornell" else scenes.media_scene(scene_dir)
+    cfg = Config.from_file(path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 64, 48, 8
+    dev = DeviceScene(cfg)
+    films = []
+    for mode in (0, 1, 2):
+        desc.sort_mode = mode
+        f = Film(desc.width, desc.height, value_sq=True)
+        dev.render(desc, f)
+        films.append(f)
+    for f in films[1:]:
+        np.testing.assert_allclose(f.value, films[0].value, rtol=2e-6, atol=1e-9)
+        np.testing.assert_allclose(f.weight, films[0].weight, rtol=1e-12)
+    desc.sort_mode = 5
+    with pytest.raises(AtrcError, match="sort_mode"):
+        dev.render(desc, Film(desc.width, desc.height))
+
+
+def test_render_stats_are_filled(cornell_path):
+    # per-kernel device times come from events recorded inside the captured
+    # bounce-loop graph
+    cfg = Config.from_file(cornell_path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 64, 64, 16
+    dev = DeviceScene(cfg)
+    st = dev.render(desc, Film(64, 64))
+    assert st["samples"] == 64 * 64 * 16
+    assert st["extend_seconds"] > 0 and st["shade_seconds"] > 0 and st["shadow_seconds"] > 0
+    assert st["extend_seconds"] + st["shade_seconds"] + st["shadow_seconds"] <= st["kernel_seconds"] * 1.01
+    assert st["rays_closest"] >= st["samples"] and st["kernel_launches"] > 6
