@@ -64,8 +64,10 @@ def load_library() -> C.CDLL:
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    sizes = (C.c_uint64 * 15)()
-    lib.atrc_abi_struct_sizes(sizes, 15)
+    n = len(abi.STRUCT_ORDER)
+    sizes = (C.c_uint64 * n)()
+    if lib.atrc_abi_struct_sizes(sizes, n) != n:
+        raise RuntimeError("ABI mismatch: the library describes a different set of structs")
     for cls, sz in zip(abi.STRUCT_ORDER, sizes):
         if C.sizeof(cls) != sz:
             raise RuntimeError(f"ABI mismatch for {cls.__name__}: python {C.sizeof(cls)} vs library {sz}")
@@ -237,6 +239,26 @@ class DeviceScene:
         _check(load_library().atrc_cuda_trace_rays_device(self._h, C.c_void_p(d_rays_ptr), n,
                                                          C.c_void_p(d_hits_ptr), 0 if mode == "closest" else 1,
                                                          1 if exact else 0))
+
+    def autotune(self, desc: AtrcRenderDesc, trial_spp: int = 0) -> dict:
+        """Search the launch configuration for this scene and view
+        (atrc_cuda_autotune); later renders with path_pool 0 and sort_mode -1
+        use it."""
+        t = abi.AtrcTuning()
+        _check(load_library().atrc_cuda_autotune(self._h, C.byref(desc), trial_spp, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in abi.AtrcTuning._fields_}
+
+    def tuning(self) -> dict:
+        t = abi.AtrcTuning()
+        _check(load_library().atrc_cuda_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in abi.AtrcTuning._fields_}
+
+    def set_tuning(self, **kw) -> None:
+        t = abi.AtrcTuning()
+        _check(load_library().atrc_cuda_get_tuning(self._h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _check(load_library().atrc_cuda_set_tuning(self._h, C.byref(t)))
 
     def render(self, desc: AtrcRenderDesc, film: Film, cancel: Optional[C.c_int] = None,
                progress: Optional[Callable[[float], None]] = None) -> dict:

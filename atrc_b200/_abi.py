@@ -114,9 +114,15 @@ class AtrcDeviceInfo(C.Structure):
                 ("cc_minor", C.c_int32), ("pad_", C.c_int32), ("global_mem_bytes", C.c_uint64)]
 
 
+class AtrcTuning(C.Structure):
+    _fields_ = [("path_pool", C.c_int32), ("sort_mode", C.c_int32), ("gen_blocks_per_sm", C.c_int32),
+                ("gen_threads", C.c_int32), ("finish_threads", C.c_int32), ("trials", C.c_int32),
+                ("ms_per_msample", C.c_double), ("default_ms_per_msample", C.c_double)]
+
+
 STRUCT_ORDER = [AtrcSceneDesc, AtrcMeshDesc, AtrcGeometryDesc, AtrcEntityDesc, AtrcTexture2DDesc,
                 AtrcTexture3DDesc, AtrcMaterialDesc, AtrcMediumDesc, AtrcEnvDesc, AtrcRenderDesc, AtrcFilm,
-                AtrcRenderStats, AtrcRay, AtrcHit, AtrcDeviceInfo]
+                AtrcRenderStats, AtrcRay, AtrcHit, AtrcDeviceInfo, AtrcTuning]
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_double, C.c_void_p)
 
@@ -144,4 +150,7 @@ PROTOTYPES = {
     "atrc_cuda_render_noalloc": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
                                            C.POINTER(AtrcRenderStats)]),
     "atrc_film_resolve": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, c_float_p]),
+    "atrc_cuda_autotune": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32, C.POINTER(AtrcTuning)]),
+    "atrc_cuda_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(AtrcTuning)]),
+    "atrc_cuda_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(AtrcTuning)]),
 }

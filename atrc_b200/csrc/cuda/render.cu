@@ -762,7 +762,17 @@ struct DeviceSceneImpl {
     cudaGraphExec_t window_exec = nullptr;  // the captured bounce-loop window
     void* stage = nullptr;             // pinned host staging for host films
     size_t stage_bytes = 0;
-    int tuned_sort = ATRC_SORT_NONE;  // ATRC_SORT_AUTO resolves to this
+    // launch configuration (atrc_cuda_autotune chooses it; these are the
+    // defaults): ATRC_SORT_AUTO resolves to tuned_sort, path_pool 0 to
+    // tuned_pool; k_generate / k_finish use the grid and block shapes
+    int tuned_sort = ATRC_SORT_NONE;
+    int tuned_pool = 1 << 21;
+    int tuned_gen_blocks = 16;    // k_generate / k_finish blocks per SM
+    int tuned_gen_threads = 256;  // k_generate block
+    int tuned_fin_threads = 128;  // k_finish block
+    int tuned_trials = 0;
+    double tuned_ms = 0, default_ms = 0;
+    DevBuf tune_film;
     void resolve_sort(Params* p, int requested) const {
         p->sort_mode = requested == ATRC_SORT_AUTO ? tuned_sort : requested;
         p->nkeys = std::max(scene.material_count, 4) + 2;
@@ -1063,8 +1073,7 @@ int atrc_cuda_trace_rays(AtrcScene* scene, const AtrcRay* rays, size_t n, AtrcHi
     });
 }
 
-int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* film, volatile const int* cancel,
-                     AtrcProgressFn progress, void* user, AtrcRenderStats* stats) {
+static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcFilm* film) {
     if (!scene || !desc || !film || !film->value || !film->weight)
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: null argument");
     if (desc->width <= 0 || desc->height <= 0 || desc->spp <= 0 || desc->max_depth < 0)
@@ -1075,183 +1084,309 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid sort_mode");
     if (desc->filter_type == ATRC_FILTER_BOX ? !(desc->filter_radius - desc->eps > 0) : !(desc->filter_radius > 0 && desc->filter_alpha > 0))
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid film filter");
+    return ATRC_OK;
+}
+
+// The wavefront render behind atrc_cuda_render (arguments already checked;
+// CUDA failures throw).  Launch shapes, path pool and sort mode left to
+// the library (path_pool 0, sort_mode AUTO) come from the scene's tuning.
+static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcFilm* film, volatile const int* cancel,
+                       AtrcProgressFn progress, void* user, AtrcRenderStats* stats) {
+    const auto t_start = std::chrono::steady_clock::now();
+    DeviceSceneImpl& d = scene->impl;
+    CK(cudaSetDevice(d.device));
+    cudaStream_t s = d.stream;
+    d.scene.eps = desc->eps;
+    Params p = make_params(*desc);
+    d.resolve_sort(&p, desc->sort_mode);
+    if (d.tiles.bytes < tile_table_bytes(p)) d.tiles.alloc(tile_table_bytes(p));
+    setup_tiles(&p, d.tiles.p, s);
+    const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
+    const unsigned long long total = (unsigned long long)p.SW * p.SH * spp;
+    // path pool: enough paths to fill the GPU; shadow capacity = pool x lights
+    const int nl = std::max(1, d.scene.light_count);
+    size_t cap = desc->path_pool > 0 ? size_t(desc->path_pool) : size_t(d.tuned_pool);
+    cap = std::min<size_t>(cap, std::max<unsigned long long>(total, 1024ULL));
+    cap = std::min<size_t>(cap, (size_t(1) << 28) / nl);
+    const size_t shadow_cap = cap * nl;
+    const PoolLayout L = pool_layout(cap, shadow_cap, p.nkeys);
+    if (d.pool_buf.bytes < L.total || d.pool_cap != cap || d.pool_lights != nl) {
+        d.pool_buf.alloc(L.total);
+        d.pool_cap = cap;
+        d.pool_lights = nl;
+    }
+    if (!d.counters.p) d.counters.alloc(sizeof(Counters));
+    Pool P = pool_from(d.pool_buf.p, L, shadow_cap);
+    Counters* c = d.counters.as<Counters>();
+    // film
+    const size_t npix = size_t(desc->width) * desc->height;
+    Film F{};
+    std::vector<std::pair<double*, size_t>> host_targets;
+    DevBuf& local_film = d.film_buf;
+    d.ensure_render_resources();
+    if (film->on_device) {
+        F.value = film->value; F.weight = film->weight; F.value_sq = film->value_sq;
+        F.albedo = film->albedo; F.normal = film->normal; F.denoise = film->denoise;
+    } else {
+        size_t doubles = npix * 4 + (film->value_sq ? npix * 3 : 0) + (film->albedo ? npix * 3 : 0) +
+                         (film->normal ? npix * 3 : 0) + (film->denoise ? npix : 0);
+        if (local_film.bytes < doubles * sizeof(double)) local_film.alloc(doubles * sizeof(double));
+        CK(cudaMemsetAsync(local_film.p, 0, doubles * sizeof(double), s));
+        double* b = local_film.as<double>();
+        F.value = b; b += npix * 3; host_targets.push_back({film->value, npix * 3});
+        F.weight = b; b += npix; host_targets.push_back({film->weight, npix});
+        if (film->value_sq) { F.value_sq = b; b += npix * 3; host_targets.push_back({film->value_sq, npix * 3}); }
+        if (film->albedo) { F.albedo = b; b += npix * 3; host_targets.push_back({film->albedo, npix * 3}); }
+        if (film->normal) { F.normal = b; b += npix * 3; host_targets.push_back({film->normal, npix * 3}); }
+        if (film->denoise) { F.denoise = b; b += npix; host_targets.push_back({film->denoise, npix}); }
+    }
+    const int gsm = grid_for(d.sm_count, d.tuned_gen_blocks);
+    // one path / ray per thread for the heavy kernels (grids cover the
+    // pool; threads past the device-side count return at once)
+    const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
+    k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
+    CK(cudaGetLastError());
+    uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
+    cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
+    cudaEvent_t* kev = d.kev;
+    const int window = DeviceSceneImpl::kWindow;
+    double t_ext = 0, t_shade = 0, t_shadow = 0;
+    CK(cudaEventRecord(ev0, s));
+    Counters hc{};
+    static_assert(sizeof(Counters) <= 512, "pinned counter buffer too small");
+    Counters* pinned = static_cast<Counters*>(d.pinned_counters);
+    int status = ATRC_OK;
+    const bool count = desc->count_traversal != 0;
+    // The bounce loop runs in windows of `window` iterations.  One window
+    // (6 kernels per iteration, the timing events and the counter
+    // read-back) is captured once per call as a CUDA graph and relaunched
+    // until the device-side counters say the work is done: the kernels
+    // take their sizes from the counters, so every window is the same
+    // graph.  The executable graph is kept with the scene and updated in
+    // place when the next call's parameters differ.
+    {
+        CaptureGuard cap(s);
+        for (int k = 0; k < window; ++k) {
+            k_begin<<<1, 1, 0, s>>>(c);
+            k_generate<<<gsm, d.tuned_gen_threads, 0, s>>>(d.scene, p, P, c);
+            CK(cudaEventRecordWithFlags(kev[k * 4 + 0], s, cudaEventRecordExternal));
+            if (count) k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+            else k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+            if (p.sort_mode != ATRC_SORT_NONE) {
+                k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
+                k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
+            }
+            CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
+            k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
+            CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
+            if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+            else k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+            CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
+            k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, F, c);
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+        cudaGraph_t g = cap.end();
+        d.window_exec = instantiate_or_update(d.window_exec, g);
+        cudaGraphDestroy(g);
+    }
+    for (int iter_block = 0;; ++iter_block) {
+        CK(cudaGraphLaunch(d.window_exec, s));
+        launches += (p.sort_mode != ATRC_SORT_NONE ? 8 : 6) * window;
+        ext_launches += window;
+        CK(cudaStreamSynchronize(s));
+        hc = *pinned;
+        for (int k = 0; k < window; ++k) {
+            float a = 0, b2 = 0, e3 = 0;
+            CK(cudaEventElapsedTime(&a, kev[k * 4 + 0], kev[k * 4 + 1]));
+            CK(cudaEventElapsedTime(&b2, kev[k * 4 + 1], kev[k * 4 + 2]));
+            CK(cudaEventElapsedTime(&e3, kev[k * 4 + 2], kev[k * 4 + 3]));
+            t_ext += a * 1e-3;
+            t_shade += b2 * 1e-3;
+            t_shadow += e3 * 1e-3;
+        }
+        if (hc.watchdog) { status = ATRC_ERR_WATCHDOG; break; }
+        if (hc.done) break;
+        if (progress) progress(100.0 * double(hc.completed) / double(std::max(1ULL, total)), user);
+        if (cancel && *cancel) { status = ATRC_ERR_CANCELLED; break; }
+    }
+    CK(cudaEventRecord(ev1, s));
+    CK(cudaEventSynchronize(ev1));
+    float kms = 0;
+    CK(cudaEventElapsedTime(&kms, ev0, ev1));
+    // bring host films up to date
+    uint64_t d2h = sizeof(Counters);
+    if (!host_targets.empty()) {
+        size_t doubles = 0;
+        for (auto& t : host_targets) doubles += t.second;
+        d.ensure_stage(doubles * sizeof(double));
+        const double* tmp = static_cast<const double*>(d.stage);
+        CK(cudaMemcpyAsync(d.stage, local_film.p, doubles * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        d2h += doubles * sizeof(double);
+        // accumulate into the caller's arrays with a few host threads
+        size_t off = 0;
+        for (auto& t : host_targets) {
+            const size_t n_el = t.second;
+            const unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+            std::vector<std::thread> th;
+            for (unsigned k = 0; k < nt; ++k) {
+                const size_t b0 = n_el * k / nt, b1 = n_el * (k + 1) / nt;
+                double* dst = t.first;
+                const double* src = tmp + off;
+                th.emplace_back([=] { for (size_t q = b0; q < b1; ++q) dst[q] += src[q]; });
+            }
+            for (auto& x : th) x.join();
+            off += n_el;
+        }
+    }
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+        stats->kernel_seconds = kms * 1e-3;
+        stats->samples = hc.completed;
+        stats->rays_closest = hc.rays_closest;
+        stats->rays_shadow = hc.rays_shadow;
+        stats->iterations = hc.iterations;
+        stats->kernel_launches = launches;
+        stats->watchdog_flags = uint64_t(hc.watchdog);
+        stats->extend_seconds = t_ext;
+        stats->shade_seconds = t_shade;
+        stats->shadow_seconds = t_shadow;
+        stats->h2d_bytes = 0;
+        stats->d2h_bytes = d2h;
+        stats->extend_launches = ext_launches;
+        stats->shadow_launches = ext_launches;
+        stats->nodes_closest = hc.cnt_closest[0];
+        stats->tris_closest = hc.cnt_closest[1];
+        stats->ents_closest = hc.cnt_closest[2];
+        stats->nodes_shadow = hc.cnt_shadow[0];
+        stats->tris_shadow = hc.cnt_shadow[1];
+        stats->ents_shadow = hc.cnt_shadow[2];
+    }
+    if (progress && status == ATRC_OK) progress(100.0, user);
+    if (status == ATRC_ERR_WATCHDOG)
+        return fail(status, "a device loop reached its iteration cap (code " + std::to_string(hc.watchdog) + ")");
+    if (status == ATRC_ERR_CANCELLED) return fail(status, "render cancelled");
+    return int(ATRC_OK);
+}
+
+int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* film, volatile const int* cancel,
+                     AtrcProgressFn progress, void* user, AtrcRenderStats* stats) {
+    const int rc = check_render_args(scene, desc, film);
+    if (rc != ATRC_OK) return rc;
+    return guarded([&] { return render_impl(scene, desc, film, cancel, progress, user, stats); });
+}
+
+static void tuning_out(const DeviceSceneImpl& d, AtrcTuning* out) {
+    out->path_pool = d.tuned_pool;
+    out->sort_mode = d.tuned_sort;
+    out->gen_blocks_per_sm = d.tuned_gen_blocks;
+    out->gen_threads = d.tuned_gen_threads;
+    out->finish_threads = d.tuned_fin_threads;
+    out->trials = d.tuned_trials;
+    out->ms_per_msample = d.tuned_ms;
+    out->default_ms_per_msample = d.default_ms;
+}
+
+int atrc_cuda_get_tuning(AtrcScene* scene, AtrcTuning* out) {
+    if (!scene || !out) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_get_tuning: null argument");
+    tuning_out(scene->impl, out);
+    return ATRC_OK;
+}
+
+static bool tuning_valid(const AtrcTuning& t) {
+    auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
+    return t.path_pool >= 1024 && t.path_pool <= (1 << 26) && t.sort_mode >= ATRC_SORT_NONE &&
+           t.sort_mode <= ATRC_SORT_MATERIAL && t.gen_blocks_per_sm >= 1 && t.gen_blocks_per_sm <= 64 &&
+           pow2_in(t.gen_threads, 32, 1024) && pow2_in(t.finish_threads, 32, 1024);
+}
+
+int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
+    if (!scene || !in) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_set_tuning: null argument");
+    if (!tuning_valid(*in)) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_set_tuning: value out of range");
+    DeviceSceneImpl& d = scene->impl;
+    d.tuned_pool = in->path_pool;
+    d.tuned_sort = in->sort_mode;
+    d.tuned_gen_blocks = in->gen_blocks_per_sm;
+    d.tuned_gen_threads = in->gen_threads;
+    d.tuned_fin_threads = in->finish_threads;
+    return ATRC_OK;
+}
+
+int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t trial_spp, AtrcTuning* out) {
+    const AtrcFilm probe{reinterpret_cast<double*>(1), reinterpret_cast<double*>(1), nullptr, nullptr, nullptr,
+                         nullptr, 1, 0};
+    const int rc = check_render_args(scene, desc, &probe);
+    if (rc != ATRC_OK) return rc;
     return guarded([&] {
-        const auto t_start = std::chrono::steady_clock::now();
         DeviceSceneImpl& d = scene->impl;
         CK(cudaSetDevice(d.device));
-        cudaStream_t s = d.stream;
-        d.scene.eps = desc->eps;
-        Params p = make_params(*desc);
-        d.resolve_sort(&p, desc->sort_mode);
-        if (d.tiles.bytes < tile_table_bytes(p)) d.tiles.alloc(tile_table_bytes(p));
-        setup_tiles(&p, d.tiles.p, s);
-        const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
-        const unsigned long long total = (unsigned long long)p.SW * p.SH * spp;
-        // path pool: enough paths to fill the GPU; shadow capacity = pool x lights
-        const int nl = std::max(1, d.scene.light_count);
-        size_t cap = desc->path_pool > 0 ? size_t(desc->path_pool) : size_t(1) << 21;
-        cap = std::min<size_t>(cap, std::max<unsigned long long>(total, 1024ULL));
-        cap = std::min<size_t>(cap, (size_t(1) << 28) / nl);
-        const size_t shadow_cap = cap * nl;
-        const PoolLayout L = pool_layout(cap, shadow_cap, p.nkeys);
-        if (d.pool_buf.bytes < L.total || d.pool_cap != cap || d.pool_lights != nl) {
-            d.pool_buf.alloc(L.total);
-            d.pool_cap = cap;
-            d.pool_lights = nl;
-        }
-        if (!d.counters.p) d.counters.alloc(sizeof(Counters));
-        Pool P = pool_from(d.pool_buf.p, L, shadow_cap);
-        Counters* c = d.counters.as<Counters>();
-        // film
         const size_t npix = size_t(desc->width) * desc->height;
-        Film F{};
-        std::vector<std::pair<double*, size_t>> host_targets;
-        DevBuf& local_film = d.film_buf;
-        d.ensure_render_resources();
-        if (film->on_device) {
-            F.value = film->value; F.weight = film->weight; F.value_sq = film->value_sq;
-            F.albedo = film->albedo; F.normal = film->normal; F.denoise = film->denoise;
-        } else {
-            size_t doubles = npix * 4 + (film->value_sq ? npix * 3 : 0) + (film->albedo ? npix * 3 : 0) +
-                             (film->normal ? npix * 3 : 0) + (film->denoise ? npix : 0);
-            if (local_film.bytes < doubles * sizeof(double)) local_film.alloc(doubles * sizeof(double));
-            CK(cudaMemsetAsync(local_film.p, 0, doubles * sizeof(double), s));
-            double* b = local_film.as<double>();
-            F.value = b; b += npix * 3; host_targets.push_back({film->value, npix * 3});
-            F.weight = b; b += npix; host_targets.push_back({film->weight, npix});
-            if (film->value_sq) { F.value_sq = b; b += npix * 3; host_targets.push_back({film->value_sq, npix * 3}); }
-            if (film->albedo) { F.albedo = b; b += npix * 3; host_targets.push_back({film->albedo, npix * 3}); }
-            if (film->normal) { F.normal = b; b += npix * 3; host_targets.push_back({film->normal, npix * 3}); }
-            if (film->denoise) { F.denoise = b; b += npix; host_targets.push_back({film->denoise, npix}); }
-        }
-        const int gsm = grid_for(d.sm_count, 16);
-        // one path / ray per thread for the heavy kernels (grids cover the
-        // pool; threads past the device-side count return at once)
-        const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
-        k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
-        CK(cudaGetLastError());
-        uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
-        cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
-        cudaEvent_t* kev = d.kev;
-        const int window = DeviceSceneImpl::kWindow;
-        double t_ext = 0, t_shade = 0, t_shadow = 0;
-        CK(cudaEventRecord(ev0, s));
-        Counters hc{};
-        static_assert(sizeof(Counters) <= 512, "pinned counter buffer too small");
-        Counters* pinned = static_cast<Counters*>(d.pinned_counters);
-        int status = ATRC_OK;
-        const bool count = desc->count_traversal != 0;
-        // The bounce loop runs in windows of `window` iterations.  One window
-        // (6 kernels per iteration, the timing events and the counter
-        // read-back) is captured once per call as a CUDA graph and relaunched
-        // until the device-side counters say the work is done: the kernels
-        // take their sizes from the counters, so every window is the same
-        // graph.  The executable graph is kept with the scene and updated in
-        // place when the next call's parameters differ.
-        {
-            CaptureGuard cap(s);
-            for (int k = 0; k < window; ++k) {
-                k_begin<<<1, 1, 0, s>>>(c);
-                k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
-                CK(cudaEventRecordWithFlags(kev[k * 4 + 0], s, cudaEventRecordExternal));
-                if (count) k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
-                else k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
-                if (p.sort_mode != ATRC_SORT_NONE) {
-                    k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
-                    k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
-                }
-                CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
-                k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
-                CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
-                if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
-                else k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
-                CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
-                k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
+        if (d.tune_film.bytes < npix * 4 * sizeof(double)) d.tune_film.alloc(npix * 4 * sizeof(double));
+        AtrcFilm film{};
+        film.value = d.tune_film.as<double>();
+        film.weight = film.value + npix * 3;
+        film.on_device = 1;
+        AtrcRenderDesc t = *desc;
+        if (trial_spp <= 0) trial_spp = int32_t(std::max<size_t>(1, ((size_t(1) << 22) + npix - 1) / npix));
+        t.spp_count = std::min(trial_spp, desc->spp);
+        t.first_spp = 0;
+        t.count_traversal = 0;
+        // pools whose workspace stays under a quarter of the free memory
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        const int nl = std::max(1, d.scene.light_count);
+        const int nkeys = std::max(d.scene.material_count, 4) + 2;
+        // (the workspace held now is freed before a larger one is allocated)
+        auto pool_fits = [&](int pool) {
+            return pool_layout(size_t(pool), size_t(pool) * nl, nkeys).total < (free_b + d.pool_buf.bytes) / 4;
+        };
+        AtrcTuning cur{};
+        tuning_out(d, &cur);
+        int trials = 0;
+        auto measure = [&](const AtrcTuning& c) {
+            atrc_cuda_set_tuning(scene, &c);
+            t.sort_mode = ATRC_SORT_AUTO;
+            t.path_pool = 0;
+            double best = 1e30;
+            for (int rep = 0; rep < 2; ++rep) {
+                CK(cudaMemsetAsync(d.tune_film.p, 0, npix * 4 * sizeof(double), d.stream));
+                AtrcRenderStats st{};
+                const int r = render_impl(scene, &t, &film, nullptr, nullptr, nullptr, &st);
+                if (r != ATRC_OK) throw CudaError(std::string("autotune trial failed: ") + atrc_last_error());
+                best = std::min(best, st.kernel_seconds * 1e3 / (double(st.samples) / 1e6));
+                ++trials;
             }
-            CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-            cudaGraph_t g = cap.end();
-            d.window_exec = instantiate_or_update(d.window_exec, g);
-            cudaGraphDestroy(g);
+            return best;
+        };
+        // defaults first (one warm-up trial compiles nothing but pages in)
+        AtrcTuning base{1 << 21, ATRC_SORT_NONE, 16, 256, 128, 0, 0, 0};
+        if (!pool_fits(base.path_pool)) base.path_pool = 1 << 19;
+        measure(base);
+        const double base_ms = measure(base);
+        AtrcTuning best = base;
+        double best_ms = base_ms;
+        auto consider = [&](AtrcTuning c) {
+            if (!tuning_valid(c) || !pool_fits(c.path_pool)) return;
+            const double ms = measure(c);
+            if (ms < best_ms * 0.99) { best_ms = ms; best = c; }
+        };
+        for (int m : {ATRC_SORT_TYPE, ATRC_SORT_MATERIAL}) { AtrcTuning c = best; c.sort_mode = m; consider(c); }
+        const AtrcTuning after_sort = best;
+        for (int pool : {1 << 19, 1 << 20, 1 << 22}) { AtrcTuning c = after_sort; c.path_pool = pool; consider(c); }
+        const AtrcTuning after_pool = best;
+        const int shapes[][3] = {{8, 256, 128}, {32, 256, 128}, {16, 128, 256}, {16, 512, 128}};
+        for (const auto& sh : shapes) {
+            AtrcTuning c = after_pool;
+            c.gen_blocks_per_sm = sh[0]; c.gen_threads = sh[1]; c.finish_threads = sh[2];
+            consider(c);
         }
-        for (int iter_block = 0;; ++iter_block) {
-            CK(cudaGraphLaunch(d.window_exec, s));
-            launches += (p.sort_mode != ATRC_SORT_NONE ? 8 : 6) * window;
-            ext_launches += window;
-            CK(cudaStreamSynchronize(s));
-            hc = *pinned;
-            for (int k = 0; k < window; ++k) {
-                float a = 0, b2 = 0, e3 = 0;
-                CK(cudaEventElapsedTime(&a, kev[k * 4 + 0], kev[k * 4 + 1]));
-                CK(cudaEventElapsedTime(&b2, kev[k * 4 + 1], kev[k * 4 + 2]));
-                CK(cudaEventElapsedTime(&e3, kev[k * 4 + 2], kev[k * 4 + 3]));
-                t_ext += a * 1e-3;
-                t_shade += b2 * 1e-3;
-                t_shadow += e3 * 1e-3;
-            }
-            if (hc.watchdog) { status = ATRC_ERR_WATCHDOG; break; }
-            if (hc.done) break;
-            if (progress) progress(100.0 * double(hc.completed) / double(std::max(1ULL, total)), user);
-            if (cancel && *cancel) { status = ATRC_ERR_CANCELLED; break; }
-        }
-        CK(cudaEventRecord(ev1, s));
-        CK(cudaEventSynchronize(ev1));
-        float kms = 0;
-        CK(cudaEventElapsedTime(&kms, ev0, ev1));
-        // bring host films up to date
-        uint64_t d2h = sizeof(Counters);
-        if (!host_targets.empty()) {
-            size_t doubles = 0;
-            for (auto& t : host_targets) doubles += t.second;
-            d.ensure_stage(doubles * sizeof(double));
-            const double* tmp = static_cast<const double*>(d.stage);
-            CK(cudaMemcpyAsync(d.stage, local_film.p, doubles * sizeof(double), cudaMemcpyDeviceToHost, s));
-            CK(cudaStreamSynchronize(s));
-            d2h += doubles * sizeof(double);
-            // accumulate into the caller's arrays with a few host threads
-            size_t off = 0;
-            for (auto& t : host_targets) {
-                const size_t n_el = t.second;
-                const unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
-                std::vector<std::thread> th;
-                for (unsigned k = 0; k < nt; ++k) {
-                    const size_t b0 = n_el * k / nt, b1 = n_el * (k + 1) / nt;
-                    double* dst = t.first;
-                    const double* src = tmp + off;
-                    th.emplace_back([=] { for (size_t q = b0; q < b1; ++q) dst[q] += src[q]; });
-                }
-                for (auto& x : th) x.join();
-                off += n_el;
-            }
-        }
-        if (stats) {
-            std::memset(stats, 0, sizeof(*stats));
-            stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-            stats->kernel_seconds = kms * 1e-3;
-            stats->samples = hc.completed;
-            stats->rays_closest = hc.rays_closest;
-            stats->rays_shadow = hc.rays_shadow;
-            stats->iterations = hc.iterations;
-            stats->kernel_launches = launches;
-            stats->watchdog_flags = uint64_t(hc.watchdog);
-            stats->extend_seconds = t_ext;
-            stats->shade_seconds = t_shade;
-            stats->shadow_seconds = t_shadow;
-            stats->h2d_bytes = 0;
-            stats->d2h_bytes = d2h;
-            stats->extend_launches = ext_launches;
-            stats->shadow_launches = ext_launches;
-            stats->nodes_closest = hc.cnt_closest[0];
-            stats->tris_closest = hc.cnt_closest[1];
-            stats->ents_closest = hc.cnt_closest[2];
-            stats->nodes_shadow = hc.cnt_shadow[0];
-            stats->tris_shadow = hc.cnt_shadow[1];
-            stats->ents_shadow = hc.cnt_shadow[2];
-        }
-        if (progress && status == ATRC_OK) progress(100.0, user);
-        if (status == ATRC_ERR_WATCHDOG)
-            return fail(status, "a device loop reached its iteration cap (code " + std::to_string(hc.watchdog) + ")");
-        if (status == ATRC_ERR_CANCELLED) return fail(status, "render cancelled");
+        atrc_cuda_set_tuning(scene, &best);
+        d.tuned_trials = trials;
+        d.tuned_ms = best_ms;
+        d.default_ms = base_ms;
+        if (out) tuning_out(d, out);
         return int(ATRC_OK);
     });
 }

@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--sort-mode", type=int, default=-1, choices=[-1, 0, 1, 2],
                    help="shade-queue sort: -1 auto, 0 none, 1 material type, 2 material")
     p.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed oracle run (profiling)")
+    p.add_argument("--no-autotune", action="store_true", help="render with the built-in launch configuration")
     return p.parse_args()
 
 
@@ -204,6 +205,10 @@ def main():
     build_s = time.perf_counter() - t0
     desc.path_pool = args.path_pool
     desc.sort_mode = args.sort_mode
+    # launch configuration for this scene and view (untimed, like the build)
+    t0 = time.perf_counter()
+    tuning = scene.autotune(desc, trial_spp=2) if not args.no_autotune else scene.tuning()
+    tune_s = time.perf_counter() - t0
     spp = args.spp_per_step
     desc.spp_count = spp
     W, H = desc.width, desc.height
@@ -285,7 +290,9 @@ def main():
                        "global_batch": W * H * spp * world,
                        "parallelism": f"sample-split dp{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (BVH + triangles + shading data > 126 MB)",
-                       "scene_build_s": round(build_s, 3)},
+                       "scene_build_s": round(build_s, 3), "autotune_s": round(tune_s, 3),
+                       "tuning": {k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
+                                                         "finish_threads", "trials")}},
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,

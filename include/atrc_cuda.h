@@ -407,6 +407,32 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc,
                      AtrcProgressFn progress, void* user,
                      AtrcRenderStats* stats);
 
+/* Launch configuration of the wavefront for one scene: the values that
+ * renders with `path_pool` 0 and `sort_mode` ATRC_SORT_AUTO use. */
+typedef struct AtrcTuning {
+    int32_t path_pool;          /* paths in flight (queue capacity)              */
+    int32_t sort_mode;          /* AtrcSortMode, never ATRC_SORT_AUTO            */
+    int32_t gen_blocks_per_sm;  /* grid of the generate / finish kernels per SM  */
+    int32_t gen_threads;        /* block size of the camera-ray generator        */
+    int32_t finish_threads;     /* block size of the film splat                  */
+    int32_t trials;             /* trial renders measured by the last autotune   */
+    double  ms_per_msample;     /* device ms per million samples, chosen config  */
+    double  default_ms_per_msample; /* the same for the built-in defaults        */
+} AtrcTuning;
+
+/* Project autotuner (the reference has no counterpart: it renders with a
+ * fixed thread pool and 32x32 tiles, renderer_creators.cpp:127-128).  Renders
+ * short trials of `desc` (each `trial_spp` samples per pixel, or enough for
+ * about 4M samples when trial_spp <= 0) into scratch memory, searching sort
+ * granularity, then path-pool size, then the generate / finish launch shapes
+ * (coordinate descent, best of two timings each), and stores the fastest
+ * configuration in the scene.  The caller's films are untouched. */
+int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc,
+                       int32_t trial_spp, AtrcTuning* out);
+/* Read or replace a scene's launch configuration (e.g. a cached tuning). */
+int atrc_cuda_get_tuning(AtrcScene* scene, AtrcTuning* out);
+int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in);
+
 /* Size of the static device array behind atrc_cuda_render_noalloc. */
 #define ATRC_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
 

@@ -35,8 +35,9 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layouts_match():
     lib = atrc_b200.load_library()
-    sizes = (C.c_uint64 * 15)()
-    assert lib.atrc_abi_struct_sizes(sizes, 15) == 15
+    n = len(abi.STRUCT_ORDER)
+    sizes = (C.c_uint64 * n)()
+    assert lib.atrc_abi_struct_sizes(sizes, n) == n == 16
     for cls, size in zip(abi.STRUCT_ORDER, sizes):
         assert C.sizeof(cls) == size, cls.__name__
     assert C.sizeof(abi.AtrcRay) == 32 and C.sizeof(abi.AtrcHit) == 16

@@ -176,3 +176,28 @@ def test_render_stats_are_filled(cornell_path):
     assert st["extend_seconds"] > 0 and st["shade_seconds"] > 0 and st["shadow_seconds"] > 0
     assert st["extend_seconds"] + st["shade_seconds"] + st["shadow_seconds"] <= st["kernel_seconds"] * 1.01
     assert st["rays_closest"] >= st["samples"] and st["kernel_launches"] > 6
+
+
+def test_autotune_picks_a_valid_configuration(cornell_path):
+    cfg = Config.from_file(cornell_path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 128, 96, 8
+    dev = DeviceScene(cfg)
+    ref = Film(128, 96)
+    desc.sort_mode, desc.path_pool = 0, 1 << 16
+    dev.render(desc, ref)
+    t = dev.autotune(desc, trial_spp=2)
+    assert t["trials"] >= 4 and t["sort_mode"] in (0, 1, 2)
+    assert t["path_pool"] >= 1024 and t["ms_per_msample"] > 0
+    assert t["ms_per_msample"] <= t["default_ms_per_msample"] * 1.0001
+    assert dev.tuning() == t
+    # renders that leave the choice to the library use it; the image does
+    # not depend on the launch configuration (one light: bit-exact paths)
+    desc.sort_mode, desc.path_pool = -1, 0
+    f = Film(128, 96)
+    dev.render(desc, f)
+    np.testing.assert_allclose(f.value, ref.value, rtol=1e-9, atol=1e-12)
+    with pytest.raises(AtrcError, match="out of range"):
+        dev.set_tuning(gen_threads=100)
+    dev.set_tuning(sort_mode=2, path_pool=4096)
+    assert dev.tuning()["sort_mode"] == 2 and dev.tuning()["path_pool"] == 4096
