@@ -83,7 +83,8 @@ class AtrcRenderDesc(C.Structure):
                 ("use_mis", C.c_int32), ("filter_type", C.c_int32), ("filter_radius", C.c_float),
                 ("filter_alpha", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64), ("first_spp", C.c_int32),
                 ("spp_count", C.c_int32), ("camera", AtrcCameraDesc), ("path_pool", C.c_int32),
-                ("count_traversal", C.c_int32), ("task_grid_size", C.c_int32), ("sort_mode", C.c_int32)]
+                ("count_traversal", C.c_int32), ("task_grid_size", C.c_int32), ("sort_mode", C.c_int32),
+                ("disney_fixed", C.c_int32), ("reserved_", C.c_int32)]
 
 
 class AtrcFilm(C.Structure):

@@ -134,6 +134,7 @@ struct Scene {
     int32_t light_entity[kMaxLights]; // -1 for the environment light
     Env env;
     float eps;
+    int32_t disney_fixed;           // sample the Disney diffuse lobe (render option)
     float scene_lo[3], scene_hi[3];
 };
 

@@ -214,6 +214,7 @@ struct BSDF {
     float trans_ax, trans_ay, ax, ay, cc_rough;
     float w_diffuse, w_specular, w_clearcoat, w_transmission;
     float eps;
+    bool disney_fixed;  // sample the diffuse lobe instead of falling through
 };
 
 __device__ __forceinline__ float one_minus_5(float x) { const float t = 1 - x, t2 = t * t; return t2 * t2 * t; }
@@ -533,8 +534,15 @@ __device__ BSDFSample bsdf_sample(const BSDF& b, Vec3 wo, float u0, float u1, fl
             goto done;
         }
     } else {
-        // the diffuse choice is always overwritten (disney.cpp:578-589)
+        // the diffuse choice is always overwritten (disney.cpp:578-589),
+        // unless the fixed sampling mode is on
         float sel = u0;
+        if (b.disney_fixed && sel < b.w_diffuse) {
+            float pdf;
+            lwi = zweighted_on_hemisphere(u1, u2, &pdf);
+            ok = lwi.z > 0;
+            goto done;
+        }
         if (!(sel < b.w_diffuse)) sel -= b.w_diffuse;
         if (sel < b.w_transmission) goto sample_trans;
         sel -= b.w_transmission;
@@ -593,6 +601,7 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
     b.type = m.type;
     b.geo = s.geo;
     b.eps = S.eps;
+    b.disney_fixed = S.disney_fixed != 0;
     b.albedo = Vec3();
     Coord shd = s.user;
     if (m.normal_map >= 0 && (m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_DISNEY)) {

@@ -1097,6 +1097,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
     CK(cudaSetDevice(d.device));
     cudaStream_t s = d.stream;
     d.scene.eps = desc->eps;
+    d.scene.disney_fixed = desc->disney_fixed;
     Params p = make_params(*desc);
     d.resolve_sort(&p, desc->sort_mode);
     if (d.tiles.bytes < tile_table_bytes(p)) d.tiles.alloc(tile_table_bytes(p));
@@ -1466,6 +1467,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         void* scratch = noalloc_scratch(d.device);
         cudaStream_t s = d.stream;
         d.scene.eps = desc->eps;
+    d.scene.disney_fixed = desc->disney_fixed;
         Params p = make_params(*desc);
         d.resolve_sort(&p, desc->sort_mode);
         const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;

@@ -257,6 +257,14 @@ typedef struct AtrcRenderDesc {
                                      /* once per tile (render_target.h:      */
                                      /* 355-395); 0 means 32                 */
     int32_t  sort_mode;              /* order of the shade queue: ATRC_SORT_* */
+    int32_t  disney_fixed;           /* 0: Disney sampling as the reference  */
+                                     /* (its diffuse-lobe choice falls       */
+                                     /* through, disney.cpp:578-589, so the  */
+                                     /* samples do not follow the reported   */
+                                     /* pdf); 1: the diffuse lobe is sampled */
+                                     /* (sampling matches the pdf; needed by */
+                                     /* guided rendering and error studies)  */
+    int32_t  reserved_;
 } AtrcRenderDesc;
 
 /* Sorting of hit records before shading (a counting sort by key). */

@@ -41,7 +41,7 @@ def load() -> C.CDLL:
         lib.oracle_bsdf_eval.argtypes = [C.c_void_p, C.c_int, abi.c_float_p, abi.c_float_p, C.c_size_t,
                                          abi.c_float_p, abi.c_float_p]
         lib.oracle_bsdf_sample.argtypes = [C.c_void_p, C.c_int, abi.c_float_p, abi.c_float_p, C.c_size_t,
-                                           abi.c_float_p, abi.c_float_p, abi.c_float_p, C.POINTER(C.c_int)]
+                                           abi.c_float_p, abi.c_float_p, abi.c_float_p, C.POINTER(C.c_int), C.c_int]
         _lib = lib
     return _lib
 
@@ -110,7 +110,7 @@ class OracleScene:
         _check(load().oracle_bsdf_eval(self._h, material, _fp(wi), _fp(wo), len(wi), _fp(f), _fp(pdf)))
         return f, pdf
 
-    def bsdf_sample(self, material: int, wo: np.ndarray, u3: np.ndarray):
+    def bsdf_sample(self, material: int, wo: np.ndarray, u3: np.ndarray, disney_fixed: bool = False):
         wo = np.ascontiguousarray(wo, dtype=np.float32)
         u = np.ascontiguousarray(u3, dtype=np.float32)
         n = len(wo)
@@ -119,7 +119,7 @@ class OracleScene:
         pdf = np.empty(n, dtype=np.float32)
         delta = np.empty(n, dtype=np.int32)
         _check(load().oracle_bsdf_sample(self._h, material, _fp(wo), _fp(u), n, _fp(wi), _fp(f), _fp(pdf),
-                                         delta.ctypes.data_as(C.POINTER(C.c_int))))
+                                         delta.ctypes.data_as(C.POINTER(C.c_int)), int(disney_fixed)))
         return wi, f, pdf, delta
 
 

@@ -72,10 +72,11 @@ int oracle_env_sample(OracleScene* s, const float* u3, size_t n, float* dirs,
  * eval f(wi, wo) -> f[3], pdf(wi, wo) -> pdf. */
 int oracle_bsdf_eval(OracleScene* s, int material, const float* wi,
                      const float* wo, size_t n, float* f, float* pdf);
-/* sample(wo, u3) -> wi[3], f[3], pdf, delta */
+/* sample(wo, u3) -> wi[3], f[3], pdf, delta; disney_fixed selects the
+ * fixed Disney sampling mode of pt_cuda (0 = the reference's sampler) */
 int oracle_bsdf_sample(OracleScene* s, int material, const float* wo,
                        const float* u3, size_t n, float* wi, float* f,
-                       float* pdf, int* is_delta);
+                       float* pdf, int* is_delta, int disney_fixed);
 
 #ifdef __cplusplus
 }

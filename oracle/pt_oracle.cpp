@@ -376,6 +376,7 @@ struct GeoInct : SurfacePoint {
 };
 
 float g_eps = 3e-4f;  // common.cpp:7 (EPS(), set_eps)
+int g_disney_fixed = 0;  // render option of pt_cuda (not in the reference): sample the Disney diffuse lobe
 
 // triangle_aux.h:9-30
 bool has_tri(const Ray& r, V3 A, V3 B_A, V3 C_A) {
@@ -1468,11 +1469,17 @@ struct BSDF {
                 // choice is always overwritten by a later branch
                 float sel = sam[0];
                 float unused_pdf;
-                if (sel < w_diffuse) lwi = zweighted_on_hemisphere(sam[1], sam[2], &unused_pdf);
-                else sel -= w_diffuse;
-                if (sel < w_transmission) lwi = sample_transmission(lwo, sam[1], sam[2]);
-                else if (sel -= w_transmission, sel < w_specular) lwi = sample_specular(lwo, sam[1], sam[2]);
-                else lwi = sample_clearcoat(lwo, sam[1], sam[2]);
+                if (g_disney_fixed && sel < w_diffuse) {
+                    // fixed sampling mode (not the reference): the diffuse lobe
+                    lwi = zweighted_on_hemisphere(sam[1], sam[2], &unused_pdf);
+                    if (lwi.z <= 0) lwi = V3();
+                } else {
+                    if (sel < w_diffuse) lwi = zweighted_on_hemisphere(sam[1], sam[2], &unused_pdf);
+                    else sel -= w_diffuse;
+                    if (sel < w_transmission) lwi = sample_transmission(lwo, sam[1], sam[2]);
+                    else if (sel -= w_transmission, sel < w_specular) lwi = sample_specular(lwo, sam[1], sam[2]);
+                    else lwi = sample_clearcoat(lwo, sam[1], sam[2]);
+                }
             }
             if (lwi.black()) { r = BSDFSample(); return r; }
             V3 wi = shd.local_to_global(lwi);
@@ -2294,6 +2301,7 @@ int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film
     if (tile_stride < 1) { g_err = "tile_stride must be >= 1"; return ATRC_ERR_INVALID_ARG; }
     if (film->on_device) { g_err = "the oracle renders into host memory only"; return ATRC_ERR_INVALID_ARG; }
     g_eps = s->eps = d->eps;
+    g_disney_fixed = d->disney_fixed;
     const int W = d->width, H = d->height;
     const int spp = d->spp_count > 0 ? d->spp_count : d->spp;
     // camera (thin_lens.cpp:34-94); look-at frame: z = forward, x = up x z
@@ -2426,8 +2434,9 @@ int oracle_bsdf_eval(OracleScene* s, int material, const float* wi, const float*
 }
 
 int oracle_bsdf_sample(OracleScene* s, int material, const float* wo, const float* u3, size_t n, float* wi, float* f,
-                       float* pdf, int* is_delta) {
+                       float* pdf, int* is_delta, int disney_fixed) {
     if (!s || material < 0 || size_t(material) >= s->materials.size()) return ATRC_ERR_INVALID_ARG;
+    g_disney_fixed = disney_fixed;
     BSDF b = probe_bsdf(s, material);
     for (size_t i = 0; i < n; ++i) {
         BSDFSample r = b.sample(V3(wo + 3 * i), u3 + 3 * i);

@@ -131,10 +131,12 @@ def test_media_image_within_3_sigma(scene_dir):
     assert frac <= allowed, (frac, allowed, info)
 
 
-def test_feature_scene_within_3_sigma(tmp_path):
+@pytest.mark.parametrize("disney_fixed", [0, 1])
+def test_feature_scene_within_3_sigma(tmp_path, disney_fixed):
     from tests import kat_scenes as K
     cfg = Config.from_string(K.dumps(K.feature_scene(tmp_path, spp=512)), tmp_path)
     desc, _ = cfg.rendering(0)
+    desc.disney_fixed = disney_fixed
     dev = DeviceScene(cfg)
     ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
     fg = Film(desc.width, desc.height, value_sq=True, gbuffer=True)

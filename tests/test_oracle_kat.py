@@ -126,3 +126,24 @@ def test_gaussian_splat_follows_the_tiled_reference(tmp_path):
     assert np.mean(np.abs(z)) < 0.9 and np.abs(z).max() < 5.5
     z_untiled = filter_weight_z(f.weight, *args, grid=1 << 20)
     assert np.abs(z_untiled).max() > 20
+
+
+def test_fixed_disney_sampling_follows_its_pdf():
+    # with the diffuse lobe sampled, E[1/pdf] over the samples is the area of
+    # the hemisphere, and E[f cos / pdf] is the directional albedo (<= 1)
+    mat = {"type": "disney", "base_color": {"type": "constant", "texel": [0.9]},
+           "metallic": {"type": "constant", "texel": [0.0]}, "roughness": {"type": "constant", "texel": [0.2]}}
+    cfg, desc, ora = _oracle(K.material_probe(mat))
+    n = 400_000
+    wo = np.tile(np.float32([0.0, 0.0, 1.0]), (n, 1))
+    s_wi, s_f, s_pdf, _ = ora.bsdf_sample(0, wo, np.random.default_rng(4).random((n, 3)), disney_fixed=True)
+    ok = s_pdf > 0
+    assert abs(np.mean(np.where(ok, 1 / np.where(ok, s_pdf, 1), 0)) / (2 * math.pi) - 1) < 0.03
+    e_f, e_pdf = ora.bsdf_eval(0, s_wi[ok], wo[ok])
+    np.testing.assert_allclose(s_pdf[ok], e_pdf, rtol=1e-4)
+    # the directional albedo from importance samples matches a uniform-hemisphere estimate
+    est = np.sum(s_f[ok, 0] * s_wi[ok, 2] / s_pdf[ok]) / n
+    wi = _hemi(n, 9)
+    f_u, _ = ora.bsdf_eval(0, wi, wo)
+    ref = np.mean(f_u[:, 0] * wi[:, 2]) * 2 * math.pi
+    assert abs(est - ref) < 0.02 * ref, (est, ref)
