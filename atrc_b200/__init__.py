@@ -209,6 +209,7 @@ class DeviceScene:
         h = C.c_void_p()
         _check(lib.atrc_cuda_scene_create(desc, C.byref(h)))
         self._h = h
+        self.device = device
 
     def close(self) -> None:
         if getattr(self, "_h", None) and _lib is not None:
@@ -259,6 +260,15 @@ class DeviceScene:
         for k, v in kw.items():
             setattr(t, k, v)
         _check(load_library().atrc_cuda_set_tuning(self._h, C.byref(t)))
+
+    def render_guided(self, guide, desc: AtrcRenderDesc, film: Film, record: bool = False) -> dict:
+        """Render with the learned guide sampling surface vertices
+        (atrc_cuda_render_guided); record=True also keeps training records."""
+        st = AtrcRenderStats()
+        f = film.as_struct()
+        _check(load_library().atrc_cuda_render_guided(self._h, guide.handle, C.byref(desc), 1 if record else 0,
+                                                     C.byref(f), C.byref(st)))
+        return {k: getattr(st, k) for k, _ in AtrcRenderStats._fields_}
 
     def render(self, desc: AtrcRenderDesc, film: Film, cancel: Optional[C.c_int] = None,
                progress: Optional[Callable[[float], None]] = None) -> dict:

@@ -121,6 +121,20 @@ class AtrcTuning(C.Structure):
                 ("ms_per_msample", C.c_double), ("default_ms_per_msample", C.c_double)]
 
 
+class AtrcGuideDesc(C.Structure):
+    _fields_ = [("log2_table", C.c_int32), ("base_resolution", C.c_int32), ("max_resolution", C.c_int32),
+                ("batch", C.c_int32), ("record_capacity", C.c_int32), ("learning_rate", C.c_float),
+                ("seed", C.c_uint64)]
+
+
+class AtrcGuideInfo(C.Structure):
+    _fields_ = [("weights", C.c_uint64), ("table_floats", C.c_uint64), ("levels", C.c_int32), ("inputs", C.c_int32),
+                ("hidden", C.c_int32), ("outputs", C.c_int32), ("lobes", C.c_int32), ("steps", C.c_int32),
+                ("log2_table", C.c_int32), ("pad_", C.c_int32), ("grid_lo", C.c_float * 3),
+                ("grid_inv_extent", C.c_float * 3), ("grid_res", C.c_int32 * 16),
+                ("max_select", C.c_float), ("pad2_", C.c_float)]
+
+
 STRUCT_ORDER = [AtrcSceneDesc, AtrcMeshDesc, AtrcGeometryDesc, AtrcEntityDesc, AtrcTexture2DDesc,
                 AtrcTexture3DDesc, AtrcMaterialDesc, AtrcMediumDesc, AtrcEnvDesc, AtrcRenderDesc, AtrcFilm,
                 AtrcRenderStats, AtrcRay, AtrcHit, AtrcDeviceInfo, AtrcTuning]
@@ -153,5 +167,18 @@ PROTOTYPES = {
     "atrc_film_resolve": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, c_float_p]),
     "atrc_cuda_autotune": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32, C.POINTER(AtrcTuning)]),
     "atrc_cuda_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(AtrcTuning)]),
+    "atrc_guide_default_desc": (C.c_int, [C.POINTER(AtrcGuideDesc)]),
+    "atrc_guide_create": (C.c_int, [C.c_int, c_float_p, c_float_p, C.POINTER(AtrcGuideDesc), C.POINTER(C.c_void_p)]),
+    "atrc_guide_destroy": (None, [C.c_void_p]),
+    "atrc_guide_info": (C.c_int, [C.c_void_p, C.POINTER(AtrcGuideInfo)]),
+    "atrc_guide_params": (C.c_int, [C.c_void_p, c_float_p, c_float_p, C.c_int]),
+    "atrc_guide_eval": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, c_float_p]),
+    "atrc_guide_train": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
+    "atrc_guide_pdf": (C.c_int, [C.c_void_p, c_float_p, c_float_p, C.c_size_t, c_float_p, c_float_p]),
+    "atrc_guide_train_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.c_int, C.POINTER(C.c_float)]),
+    "atrc_guide_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "atrc_cuda_scene_bounds": (C.c_int, [C.c_void_p, c_float_p, c_float_p]),
+    "atrc_cuda_render_guided": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32,
+                                          C.POINTER(AtrcFilm), C.POINTER(AtrcRenderStats)]),
     "atrc_cuda_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(AtrcTuning)]),
 }

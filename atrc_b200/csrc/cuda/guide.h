@@ -1,0 +1,53 @@
+// Internal interface between the wavefront (render.cu) and the learned guide
+// (guide.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dev_guide.cuh"
+
+namespace atrc {
+
+// One training record: a guided surface vertex and what the rest of its path
+// brought back (96 bytes).
+struct GuideRecord {
+    float pos[3], nrm[3], wo[3], rough;  // the guide's query
+    float wi[3], pdf_bsdf;               // sampled direction, BSDF pdf of it
+    float coef[3], target;               // path throughput arriving at the vertex; training weight
+    float l_arrive[3];                   // path radiance when the next vertex was reached
+    int32_t prev;                        // previous record of the same path (-1: none)
+    float pad[2];
+};
+static_assert(sizeof(GuideRecord) == 96, "record layout");
+
+// What the wavefront kernels need from a guide during one render call.
+struct GuideFrame {
+    // inference inputs / outputs, indexed by shade-queue position
+    dev::GuideQuery* queries;
+    float* mixes;             // decoded GuideMix, kGuideOut floats per entry
+    // recording (null when the call does not record)
+    GuideRecord* records;
+    int* record_count;
+    int record_cap;
+    int* record_last;         // per path slot: last record of the path
+    dev::HashGrid grid;
+};
+
+struct GuideImpl;
+}  // namespace atrc
+
+struct AtrcGuide;
+
+namespace atrc {
+GuideImpl* guide_impl(AtrcGuide* g);
+
+// Size the per-slot buffers for a pool of `cap` paths; returns the frame.
+GuideFrame guide_frame(GuideImpl* g, size_t cap, bool record, cudaStream_t s);
+// Enqueue the network on the queries whose count is *n_dev.
+void guide_infer(GuideImpl* g, const int* n_dev, cudaStream_t s);
+// Device of the guide (for checks).
+int guide_device(const GuideImpl* g);
+
+}  // namespace atrc

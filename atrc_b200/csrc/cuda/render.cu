@@ -40,6 +40,8 @@
 #include "dev_scene.h"
 #include "dev_shade.cuh"
 #include "dev_trace.cuh"
+#include "cuda_util.h"
+#include "guide.h"
 
 #ifndef ATRC_SHADE_MIN_BLOCKS
 #define ATRC_SHADE_MIN_BLOCKS 4  // k_shade blocks per SM the register budget must allow
@@ -49,53 +51,9 @@
 #endif
 
 namespace atrc {
-
-void set_last_error(const std::string& msg);  // capi_host.cpp
-
 namespace {
 
 using namespace dev;
-
-struct CudaError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-
-#define CK(x)                                                                                     \
-    do {                                                                                          \
-        cudaError_t err_ = (x);                                                                   \
-        if (err_ != cudaSuccess)                                                                  \
-            throw CudaError(std::string(#x) + ": " + cudaGetErrorString(err_));                   \
-    } while (0)
-
-// ---------------------------------------------------------------- buffers
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { if (p) cudaFree(p); }
-    void alloc(size_t b) {
-        if (p) { cudaFree(p); p = nullptr; }
-        bytes = b;
-        if (b) {
-            cudaError_t e = cudaMalloc(&p, b);
-            if (e != cudaSuccess) {
-                p = nullptr;
-                throw CudaError(std::string("cudaMalloc of ") + std::to_string(b) + " bytes: " + cudaGetErrorString(e));
-            }
-        }
-    }
-    template <class T> T* as() const { return static_cast<T*>(p); }
-};
-
-template <class T>
-const T* upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
-    if (v.empty()) return nullptr;
-    b.alloc(v.size() * sizeof(T));
-    CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-    return b.as<T>();
-}
 
 // ------------------------------------------------------- warp aggregation
 __device__ __forceinline__ int warp_append(int* counter, bool pred) {
@@ -145,9 +103,10 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_trace_ra
 
 // ------------------------------------------------------------ wavefront
 enum PathFlags : int {
-    PF_MIS = 1,        // a MIS-BSDF term waits for this ray's hit
-    PF_MIS_DELTA = 2,  // ... from a delta (specular) sample
-    PF_TERMINATE = 4,  // finish after resolving the pending MIS term
+    PF_MIS = 1,          // a MIS-BSDF term waits for this ray's hit
+    PF_MIS_DELTA = 2,    // ... from a delta (specular) sample
+    PF_TERMINATE = 4,    // finish after resolving the pending MIS term
+    PF_REC_PENDING = 8,  // the path's last guide record waits for its arrival radiance
 };
 
 struct Counters {
@@ -199,6 +158,8 @@ struct Params {
     Camera cam;
     int filter_type;
     float filter_radius, filter_value, filter_alpha, filter_exp;
+    int guide_on;           // sample surface vertices with the learned guide
+    GuideFrame gf;          // guide buffers of this call (zero when guide_on == 0)
 };
 
 struct Pool {
@@ -433,6 +394,41 @@ __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d
     P.sh_c[k] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(slot));
 }
 
+// Guide queries of the shade queue (same order as k_shade): surface hits
+// with a Lambert or Disney material and consistent frames; slot -1 marks an
+// entry the guide does not serve.
+__global__ void k_guide_features(Scene S, Params p, Pool P, Counters* c) {
+    const int n = c->n_ext, in = c->in;
+    const int* queue = p.sort_mode != ATRC_SORT_NONE ? P.q_sorted : P.q[in];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = queue[i];
+        GuideQuery q;
+        q.slot = -1;
+        q.pad = 0;
+        const float4 hv = P.hit[slot];
+        const int ent = __float_as_int(hv.w);
+        const int flags = P.ctr[slot].w & 0xff;
+        if (ent >= 0 && !(flags & PF_TERMINATE)) {
+            const float4 ro = P.ray_o[slot], rd = P.ray_d[slot];
+            Hit h;
+            h.t = hv.x; h.u = hv.y; h.v = hv.z; h.entity = ent; h.tri = P.hit_tri[slot];
+            const Surface s = make_surface(S, h, xyz(ro), xyz(rd));
+            Vec3 sn;
+            const BSDF b = shade(S, s, &sn);
+            if ((b.type == ATRC_MAT_IDEAL_DIFFUSE || b.type == ATRC_MAT_DISNEY) && !fringes(b, s.wr)) {
+                q.pos[0] = s.pos.x; q.pos[1] = s.pos.y; q.pos[2] = s.pos.z;
+                q.nrm[0] = sn.x; q.nrm[1] = sn.y; q.nrm[2] = sn.z;
+                q.wo[0] = s.wr.x; q.wo[1] = s.wr.y; q.wo[2] = s.wr.z;
+                q.rough = b.type == ATRC_MAT_DISNEY ? b.roughness : 1.0f;
+                q.slot = slot;
+            }
+        }
+        if (q.slot < 0) { q.pos[0] = q.pos[1] = q.pos[2] = 0; q.nrm[0] = q.nrm[1] = q.nrm[2] = 0;
+                          q.wo[0] = q.wo[1] = q.wo[2] = 0; q.rough = 0; }
+        p.gf.queries[i] = q;
+    }
+}
+
 __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, Params p, Pool P, Counters* c) {
     const int n = c->n_ext, in = c->in, out = c->out;
     const float eps = p.eps;
@@ -454,6 +450,13 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
         float4 mf4 = P.mis_f[slot];
         int wd = 0;
         bool finish = false, cont = false;
+        if (flags & PF_REC_PENDING) {
+            // radiance gathered up to this vertex: the previous record's
+            // incident radiance is what the path brings back from here on
+            GuideRecord* r = p.gf.records + p.gf.record_last[slot];
+            r->l_arrive[0] = L.x; r->l_arrive[1] = L.y; r->l_arrive[2] = L.z;
+            flags &= ~PF_REC_PENDING;
+        }
         Surface s;
         bool have_surface = false;
         if (ent >= 0) {
@@ -552,6 +555,26 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                 }
             } else {
                 scat = 0;
+                // learned guide of this vertex (one-sample MIS with the BSDF)
+                GuideMix mix;
+                bool guided = false;
+                if (p.guide_on) {
+                    const float* gm = p.gf.mixes + size_t(i) * kGuideOut;
+                    guided = gm[kGuideUsed - 1] >= 0.0f && (b.type == ATRC_MAT_IDEAL_DIFFUSE || b.type == ATRC_MAT_DISNEY) &&
+                             !fringes(b, s.wr);
+                    if (guided) {
+                        for (int k = 0; k < kGuideLobes; ++k) {
+                            mix.mu[k][0] = gm[5 * k]; mix.mu[k][1] = gm[5 * k + 1]; mix.mu[k][2] = gm[5 * k + 2];
+                            mix.kappa[k] = gm[5 * k + 3];
+                            mix.w[k] = gm[5 * k + 4];
+                        }
+                        mix.c = gm[kGuideUsed - 1];
+                    }
+                }
+                // pdf of the BSDF-side strategy (BSDF or guide) for a direction
+                auto side_pdf = [&](Vec3 dir, float pb) {
+                    return guided ? mix.c * guide_pdf(mix, dir) + (1.0f - mix.c) * pb : pb;
+                };
                 if (depth == 1 && (e.flags & ENT_LIGHT)) L += coef * area_light_radiance(e, s.geo.z, s.wr);
                 // next-event estimation over every light (path_tracing.cpp:134-146)
                 for (int li = 0; li < S.light_count; ++li) {
@@ -566,7 +589,8 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                         const Vec3 to_light = normalize(lpos - s.pos);
                         const Vec3 bf = bsdf_eval(b, to_light, s.wr);
                         if (black(bf)) continue;
-                        const Vec3 contrib = coef * rad * bf * (fabsf(cosv(to_light, s.geo.z)) / (lpdf + bsdf_pdf(b, to_light, s.wr)));
+                        const Vec3 contrib = coef * rad * bf *
+                                             (fabsf(cosv(to_light, s.geo.z)) / (lpdf + side_pdf(to_light, bsdf_pdf(b, to_light, s.wr))));
                         push_shadow(P, c, s.pos, to_light, eps, length(s.pos - lpos) - eps, contrib, slot);
                     } else {
                         const Entity& le = S.entities[le_i];
@@ -580,16 +604,55 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                         if (black(bf)) continue;
                         Vec3 tr(1.0f);
                         if (S.has_media) tr = medium_tr(S, medium_of(s, e, to_light), ls.pos, s.pos, rng, &wd);
-                        const Vec3 contrib = coef * tr * ls.rad * bf * (fabsf(cosv(to_light, s.geo.z)) / (ls.pdf + bsdf_pdf(b, to_light, s.wr)));
+                        const Vec3 contrib = coef * tr * ls.rad * bf *
+                                             (fabsf(cosv(to_light, s.geo.z)) / (ls.pdf + side_pdf(to_light, bsdf_pdf(b, to_light, s.wr))));
                         push_shadow(P, c, s.pos, to_light, eps, slen, contrib, slot);
                     }
                 }
                 // BSDF sample: MIS-BSDF ray and continuation (path_tracing.cpp:148-169)
-                const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
-                const BSDFSample bs = bsdf_sample(b, s.wr, u0, u1, u2);
-                if (black(bs.f)) {
+                BSDFSample bs;
+                float pdf_bsdf = 0.0f;
+                if (guided) {
+                    // one-sample MIS: the guide with probability c, else the BSDF
+                    if (rng.u() < mix.c) {
+                        const float g0 = rng.u(), g1 = rng.u(), g2 = rng.u();
+                        bs.dir = guide_sample(mix, g0, g1, g2);
+                        bs.f = bsdf_eval(b, bs.dir, s.wr);
+                        pdf_bsdf = bsdf_pdf(b, bs.dir, s.wr);
+                    } else {
+                        const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+                        bs = bsdf_sample(b, s.wr, u0, u1, u2);
+                        pdf_bsdf = bs.pdf;
+                    }
+                    bs.delta = false;
+                    bs.pdf = side_pdf(bs.dir, pdf_bsdf);
+                } else {
+                    const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+                    bs = bsdf_sample(b, s.wr, u0, u1, u2);
+                }
+                if (black(bs.f) || (guided && !(bs.pdf > 0.0f))) {
                     finish = true;
                 } else {
+                    if (guided && p.gf.records) {
+                        // training record of this vertex; its targets are set when the path ends
+                        const int r = atomicAdd(p.gf.record_count, 1);
+                        if (r < p.gf.record_cap) {
+                            const GuideQuery& gq = p.gf.queries[i];
+                            GuideRecord R;
+                            for (int k = 0; k < 3; ++k) { R.pos[k] = gq.pos[k]; R.nrm[k] = gq.nrm[k]; R.wo[k] = gq.wo[k]; }
+                            R.rough = gq.rough;
+                            R.wi[0] = bs.dir.x; R.wi[1] = bs.dir.y; R.wi[2] = bs.dir.z;
+                            R.pdf_bsdf = pdf_bsdf;
+                            R.coef[0] = coef.x; R.coef[1] = coef.y; R.coef[2] = coef.z;
+                            R.target = 0.0f;
+                            R.l_arrive[0] = R.l_arrive[1] = R.l_arrive[2] = 0.0f;
+                            R.prev = p.gf.record_last[slot];
+                            R.pad[0] = R.pad[1] = 0.0f;
+                            p.gf.records[r] = R;
+                            p.gf.record_last[slot] = r;
+                            flags |= PF_REC_PENDING;
+                        }
+                    }
                     const Vec3 dir = normalize(bs.dir);
                     const float gcos = fabsf(dot(s.geo.z, dir));
                     mf4 = make_float4(coef.x * bs.f.x * gcos, coef.y * bs.f.y * gcos, coef.z * bs.f.z * gcos, mf4.w);
@@ -656,6 +719,24 @@ __global__ void k_finish(Params p, Pool P, Film F, Counters* c) {
         const int slot = P.q_finish[i];
         const float4 L = P.L[slot];
         const float sx = L.w, sy = P.mis_f[slot].w;
+        if (p.gf.records) {
+            // targets of the path's guide records: luminance of the radiance
+            // gathered after each vertex over the throughput arriving at it,
+            // i.e. f cos L_i / pdf of the sampled direction
+            int r = p.gf.record_last[slot];
+            for (int k = 0; r >= 0 && k < 256; ++k) {
+                GuideRecord& R = p.gf.records[r];
+                float t = 0.0f;
+                for (int ch = 0; ch < 3; ++ch) {
+                    const float lc = (ch == 0 ? L.x : ch == 1 ? L.y : L.z) - R.l_arrive[ch];
+                    const float w = ch == 0 ? 0.2126f : ch == 1 ? 0.7152f : 0.0722f;
+                    if (R.coef[ch] > 0.0f) t += w * fmaxf(lc, 0.0f) / R.coef[ch];
+                }
+                R.target = isfinite(t) ? t : 0.0f;
+                r = R.prev;
+            }
+            p.gf.record_last[slot] = -1;
+        }
         if (isfinite(L.x) && isfinite(L.y) && isfinite(L.z)) {
             const float4 ga = P.gb_albedo[slot], gn = P.gb_normal[slot];
             // apply_image_filter (framebuffer.h:49-80) over the sample's tile;
@@ -1091,7 +1172,8 @@ static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const
 // CUDA failures throw).  Launch shapes, path pool and sort mode left to
 // the library (path_pool 0, sort_mode AUTO) come from the scene's tuning.
 static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcFilm* film, volatile const int* cancel,
-                       AtrcProgressFn progress, void* user, AtrcRenderStats* stats) {
+                       AtrcProgressFn progress, void* user, AtrcRenderStats* stats, GuideImpl* guide = nullptr,
+                       bool record = false) {
     const auto t_start = std::chrono::steady_clock::now();
     DeviceSceneImpl& d = scene->impl;
     CK(cudaSetDevice(d.device));
@@ -1117,6 +1199,11 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
         d.pool_lights = nl;
     }
     if (!d.counters.p) d.counters.alloc(sizeof(Counters));
+    if (guide) {
+        if (guide_device(guide) != d.device) throw std::runtime_error("the guide lives on another device than the scene");
+        p.guide_on = 1;
+        p.gf = guide_frame(guide, cap, record, s);
+    }
     Pool P = pool_from(d.pool_buf.p, L, shadow_cap);
     Counters* c = d.counters.as<Counters>();
     // film
@@ -1178,6 +1265,10 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
                 k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
             }
             CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
+            if (guide) {
+                k_guide_features<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
+                guide_infer(guide, &c->n_ext, s);
+            }
             k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
             if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
@@ -1193,7 +1284,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
     }
     for (int iter_block = 0;; ++iter_block) {
         CK(cudaGraphLaunch(d.window_exec, s));
-        launches += (p.sort_mode != ATRC_SORT_NONE ? 8 : 6) * window;
+        launches += (6 + (p.sort_mode != ATRC_SORT_NONE ? 2 : 0) + (guide ? 2 : 0)) * window;
         ext_launches += window;
         CK(cudaStreamSynchronize(s));
         hc = *pinned;
@@ -1277,6 +1368,25 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
     const int rc = check_render_args(scene, desc, film);
     if (rc != ATRC_OK) return rc;
     return guarded([&] { return render_impl(scene, desc, film, cancel, progress, user, stats); });
+}
+
+int atrc_cuda_scene_bounds(AtrcScene* scene, float lo[3], float hi[3]) {
+    if (!scene || !lo || !hi) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_scene_bounds: null argument");
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = scene->impl.scene.scene_lo[a];
+        hi[a] = scene->impl.scene.scene_hi[a];
+    }
+    return ATRC_OK;
+}
+
+int atrc_cuda_render_guided(AtrcScene* scene, AtrcGuide* guide, const AtrcRenderDesc* desc, int32_t record,
+                            AtrcFilm* film, AtrcRenderStats* stats) {
+    if (!guide) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_guided: null guide");
+    const int rc = check_render_args(scene, desc, film);
+    if (rc != ATRC_OK) return rc;
+    return guarded([&] {
+        return render_impl(scene, desc, film, nullptr, nullptr, nullptr, stats, guide_impl(guide), record != 0);
+    });
 }
 
 static void tuning_out(const DeviceSceneImpl& d, AtrcTuning* out) {

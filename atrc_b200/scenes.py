@@ -19,7 +19,7 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["cornell_box", "instanced_disney", "media_scene", "write_bm", "write_pfm", "write_grid",
+__all__ = ["cornell_box", "instanced_disney", "media_scene", "indoor_room", "write_bm", "write_pfm", "write_grid",
            "icosphere", "heightfield", "cache_dir", "SCENES"]
 
 
@@ -392,4 +392,94 @@ def media_scene(out_dir: Path | None = None, seed: int = 1002, width: int = 1024
     return path
 
 
-SCENES = {"cornell": cornell_box, "instanced": instanced_disney, "media": media_scene}
+# ------------------------------------------------------- indoor room (cfg 3)
+def _wall_grid(origin, u_vec, v_vec, nu: int, nv: int, normal, hole=None) -> tuple:
+    """nu x nv cells of two triangles spanning origin + [0,1] u_vec + [0,1] v_vec,
+    shading normal `normal`; cells whose centre lies in hole = (u0, u1, v0, v1)
+    (fractions of the wall) are left out.  Returns (pos, nor, uv) per triangle."""
+    o, U, V = (np.asarray(x, np.float64) for x in (origin, u_vec, v_vec))
+    iu, iv = np.meshgrid(np.arange(nu), np.arange(nv), indexing="xy")
+    iu, iv = iu.ravel(), iv.ravel()
+    if hole is not None:
+        cu, cv = (iu + 0.5) / nu, (iv + 0.5) / nv
+        keep = ~((cu > hole[0]) & (cu < hole[1]) & (cv > hole[2]) & (cv < hole[3]))
+        iu, iv = iu[keep], iv[keep]
+    u0, u1, v0, v1 = iu / nu, (iu + 1) / nu, iv / nv, (iv + 1) / nv
+    p = lambda a, b: o + a[:, None] * U + b[:, None] * V  # noqa: E731
+    a, b, c, d = p(u0, v0), p(u1, v0), p(u1, v1), p(u0, v1)
+    pos = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)]).astype(np.float32)
+    n = len(iu)
+    nor = np.broadcast_to(np.asarray(normal, np.float32), (2 * n, 3, 3)).copy()
+    uvs = np.stack([np.stack([u0, v0], 1), np.stack([u1, v0], 1), np.stack([u1, v1], 1)], 1)
+    uvs2 = np.stack([np.stack([u0, v0], 1), np.stack([u1, v1], 1), np.stack([u0, v1], 1)], 1)
+    return pos, nor, np.concatenate([uvs, uvs2]).astype(np.float32)
+
+
+def indoor_room(out_dir: Path | None = None, seed: int = 1003, width: int = 1280, height: int = 720, spp: int = 64,
+                max_depth: int = 16, renderer: str = "pt_cuda", cell: float = 0.1, objects: int = 10,
+                object_level: int = 5) -> Path:
+    """A closed 20 x 12 x 8 room (x in [-10, 10], y in [-6, 6], z in [0, 8])
+    lit only through a 1 x 1 window in the y = -6 wall (x in [-0.5, 0.5],
+    z in [4, 5]) by the instanced workload's sky, whose 0.5 degree sun shines
+    through the window onto the floor.  The walls are 0.1 m grids (198,200
+    triangles) and ten fBm-displaced level-5 icospheres (20,480 triangles each)
+    stand on the floor: 403,000 triangles.  Every surface is Disney with
+    roughness U[0.02, 0.6], base colour U[0.1, 0.9]^3 and metallic
+    Bernoulli(0.2); 1280x720, max depth 16."""
+    tag = f"room_{seed}_{cell}_{objects}_{object_level}"
+    out = Path(out_dir) if out_dir else cache_dir() / tag
+    out.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    X0, X1, Y0, Y1, Z0, Z1 = -10.0, 10.0, -6.0, 6.0, 0.0, 8.0
+    nx, ny, nz = int(round((X1 - X0) / cell)), int(round((Y1 - Y0) / cell)), int(round((Z1 - Z0) / cell))
+    # window: x in [-0.5, 0.5], z in [4, 5] of the y = Y0 wall (fractions of that wall)
+    hole = ((-0.5 - X0) / (X1 - X0), (0.5 - X0) / (X1 - X0), (4.0 - Z0) / (Z1 - Z0), (5.0 - Z0) / (Z1 - Z0))
+    walls = {  # name: (origin, u, v, nu, nv, inward normal, hole)
+        "floor": ((X0, Y0, Z0), (X1 - X0, 0, 0), (0, Y1 - Y0, 0), nx, ny, (0, 0, 1), None),
+        "ceiling": ((X0, Y0, Z1), (0, Y1 - Y0, 0), (X1 - X0, 0, 0), ny, nx, (0, 0, -1), None),
+        "wall_south": ((X0, Y0, Z0), (X1 - X0, 0, 0), (0, 0, Z1 - Z0), nx, nz, (0, 1, 0), hole),
+        "wall_north": ((X0, Y1, Z0), (0, 0, Z1 - Z0), (X1 - X0, 0, 0), nz, nx, (0, -1, 0), None),
+        "wall_west": ((X0, Y0, Z0), (0, 0, Z1 - Z0), (0, Y1 - Y0, 0), nz, ny, (1, 0, 0), None),
+        "wall_east": ((X1, Y0, Z0), (0, Y1 - Y0, 0), (0, 0, Z1 - Z0), ny, nz, (-1, 0, 0), None),
+    }
+    if hole is not None and (nx * hole[0]) % 1 or (nz * hole[2]) % 1:
+        raise ValueError("the window must align with the wall grid")
+
+    def disney():
+        return {"type": "disney", "base_color": _const(rng.uniform(0.1, 0.9, 3)),
+                "metallic": _const(1.0 if rng.random() < 0.2 else 0.0),
+                "roughness": _const(rng.uniform(0.02, 0.6))}
+    ents = []
+    for name, (o, u, v, nu, nv, nrm, hl) in walls.items():
+        fn = out / f"{name}.bm"
+        if not fn.exists():
+            write_bm(fn, *_wall_grid(o, u, v, nu, nv, nrm, hl))
+        ents.append({"type": "geometric", "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/" + fn.name,
+                                                      "transform": []}, "material": disney()})
+    for k in range(objects):
+        fn = out / f"object{k}.bm"
+        if not fn.exists():
+            _mesh_to_bm(fn, icosphere(object_level, seed + 31 * k, amplitude=0.08))
+        r = rng.uniform(0.5, 1.2)
+        c = (rng.uniform(X0 + 1.5, X1 - 1.5), rng.uniform(Y0 + 1.5, Y1 - 1.5), r * 1.01)
+        ents.append({"type": "geometric", "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/" + fn.name,
+                                                      "transform": [{"type": "translate", "offset": v3(c)},
+                                                                    {"type": "scale", "ratio": r6(r)}]},
+                     "material": disney()})
+    env = out / "sky.pfm"
+    if not env.exists():
+        s = np.array([0.25, -0.8, 0.55])
+        write_pfm(env, sky_map(sun_dir=tuple(s / np.linalg.norm(s))))
+    cfg = {"scene": {"type": "default", "entities": ents, "aggregate": {"type": "bvh"},
+                     "env": {"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/sky.pfm"}}},
+           "rendering": {"camera": {"type": "thin_lens", "pos": [7, 4.5, 2.5], "dst": [-2, -2, 1.5], "up": [0, 0, 1],
+                                    "fov": 70},
+                         "width": width, "height": height,
+                         "renderer": {"type": renderer, "spp": spp, "max_depth": max_depth, "disney_fixed": 1},
+                         "reporter": {"type": "noout"}}}
+    path = out / "scene.json"
+    path.write_text(json.dumps(cfg))
+    return path
+
+
+SCENES = {"cornell": cornell_box, "instanced": instanced_disney, "media": media_scene, "room": indoor_room}

@@ -479,6 +479,77 @@ int atrc_save_image(const char* filename, const char* ext, const float* rgb,
  * weight == 0); host pointers. */
 int atrc_film_resolve(const AtrcFilm* film, int width, int height, float* rgb);
 
+/* ------------------------------------------------------------------------
+ * Learned path guiding (no counterpart in the reference, whose `pt` samples
+ * the BSDF only, path_tracing.cpp:150-169).  A guide is a small network --
+ * a 16-level hash grid over the scene bound (2 features per level), one-blob
+ * encodings of the shading normal and outgoing direction, and roughness
+ * (112 inputs), three hidden layers of 64 (ReLU, BF16 weights, FP32
+ * accumulation on the tensor cores) and 48 outputs -- that gives each
+ * surface vertex a mixture of 8 von Mises-Fisher lobes and a probability of
+ * sampling it instead of the BSDF (one-sample MIS, so the render stays
+ * unbiased; pair it with disney_fixed = 1 so that BSDF samples follow the
+ * pdf they report).  It is trained online with Adam on records of the
+ * vertices a recording render sampled and the radiance their paths brought
+ * back (loss -w log(c q + (1 - c) p_bsdf), w = f cos L_i / pdf).
+ * ------------------------------------------------------------------------ */
+typedef struct AtrcGuide AtrcGuide;
+
+typedef struct AtrcGuideDesc {
+    int32_t  log2_table;       /* hash entries per level = 2^log2_table (19) */
+    int32_t  base_resolution;  /* cells per axis of the coarsest level (4)   */
+    int32_t  max_resolution;   /* ... of the finest level (128)              */
+    int32_t  batch;            /* records per training step (2^18)           */
+    int32_t  record_capacity;  /* records kept by a recording render (2^20)  */
+    float    learning_rate;    /* Adam step size (1e-2)                      */
+    uint64_t seed;             /* parameter initialisation                   */
+} AtrcGuideDesc;
+
+typedef struct AtrcGuideInfo {
+    uint64_t weights;          /* MLP weights (packed [out][in] per layer)   */
+    uint64_t table_floats;     /* hash-table floats (levels x 2^log2 x 2)    */
+    int32_t  levels, inputs, hidden, outputs, lobes, steps, log2_table, pad_;
+    float    grid_lo[3], grid_inv_extent[3];  /* position -> [0,1]^3          */
+    int32_t  grid_res[16];     /* cells per axis of each hash level          */
+    float    max_select;       /* c = max_select * sigmoid(o[40])            */
+    float    pad2_;
+} AtrcGuideInfo;
+
+int  atrc_guide_default_desc(AtrcGuideDesc* desc);
+/* A guide for positions in [lo, hi] (e.g. atrc_cuda_scene_bounds). */
+int  atrc_guide_create(int device, const float lo[3], const float hi[3],
+                       const AtrcGuideDesc* desc, AtrcGuide** out);
+void atrc_guide_destroy(AtrcGuide* guide);
+int  atrc_guide_info(AtrcGuide* guide, AtrcGuideInfo* info);
+/* Read (set = 0) or replace (set = 1) the FP32 master parameters; either
+ * pointer may be NULL.  Sizes as in AtrcGuideInfo. */
+int  atrc_guide_params(AtrcGuide* guide, float* weights, float* table, int set);
+/* Raw network outputs (n x 48) for host queries (n x 10: position, shading
+ * normal, outgoing direction, roughness), on the tensor cores. */
+int  atrc_guide_eval(AtrcGuide* guide, const float* queries, size_t n, float* raw);
+/* Mixture pdf of directions dirs (n x 3) at queries (n x 10) and the
+ * selection probability c, as the renderer computes them on the GPU. */
+int  atrc_guide_pdf(AtrcGuide* guide, const float* queries, const float* dirs,
+                    size_t n, float* pdf, float* select);
+/* `steps` Adam steps over the records of the last recording render
+ * (batches of desc.batch, in order); last_loss may be NULL. */
+int  atrc_guide_train(AtrcGuide* guide, int steps, float* last_loss);
+/* The same on host records (n x 24 floats: position, normal, outgoing
+ * direction, roughness, sampled direction, its BSDF pdf, throughput (3),
+ * weight, and 6 unused). */
+int  atrc_guide_train_records(AtrcGuide* guide, const float* records, size_t n,
+                              int steps, float* last_loss);
+/* Copy out the records of the last recording render (24 floats each). */
+int  atrc_guide_records(AtrcGuide* guide, float* records, size_t cap, size_t* count);
+
+/* Scene bound (for atrc_guide_create). */
+int  atrc_cuda_scene_bounds(AtrcScene* scene, float lo[3], float hi[3]);
+/* atrc_cuda_render with the guide sampling surface vertices; record = 1
+ * also keeps training records (replacing the previous ones). */
+int  atrc_cuda_render_guided(AtrcScene* scene, AtrcGuide* guide,
+                             const AtrcRenderDesc* desc, int32_t record,
+                             AtrcFilm* film, AtrcRenderStats* stats);
+
 #ifdef __cplusplus
 }
 #endif
