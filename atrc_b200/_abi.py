@@ -124,7 +124,7 @@ class AtrcTuning(C.Structure):
 class AtrcGuideDesc(C.Structure):
     _fields_ = [("log2_table", C.c_int32), ("base_resolution", C.c_int32), ("max_resolution", C.c_int32),
                 ("batch", C.c_int32), ("record_capacity", C.c_int32), ("learning_rate", C.c_float),
-                ("seed", C.c_uint64)]
+                ("max_depth", C.c_int32), ("pad_", C.c_int32), ("seed", C.c_uint64)]
 
 
 class AtrcGuideInfo(C.Structure):

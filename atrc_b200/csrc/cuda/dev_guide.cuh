@@ -19,7 +19,7 @@
 //   [96]       roughness (0 for non-Disney materials).
 // Output (kGuideOut = 48 raw values, 41 used): per lobe k the unnormalised
 // mean direction o[5k..5k+2], log kappa o[5k+3] and mixture logit o[5k+4];
-// o[40] is the selection logit.
+// o[40] is the selection logit (c = 0.9 sigmoid(o[40] - 2)).
 #pragma once
 
 #include <cstdint>
@@ -36,7 +36,8 @@ constexpr int kGuideOut = 48;
 constexpr int kGuideUsed = 5 * kGuideLobes + 1;
 constexpr int kHashLevels = 16;
 constexpr int kHashFeatures = 2;
-constexpr float kGuideMaxSelect = 0.9f;   // c = kGuideMaxSelect * sigmoid(o[40])
+constexpr float kGuideMaxSelect = 0.9f;   // c = kGuideMaxSelect * sigmoid(o[40] + kSelectOffset)
+constexpr float kSelectOffset = -2.0f;    // an untrained guide (o ~ 0) is picked with c ~ 0.11
 constexpr float kLogKappaMin = -6.9f;     // kappa in [1e-3, 1e4]
 constexpr float kLogKappaMax = 9.2f;
 
@@ -140,7 +141,7 @@ __device__ __forceinline__ void guide_decode(const float* o, GuideMix* m) {
         sum += m->w[k];
     }
     for (int k = 0; k < kGuideLobes; ++k) m->w[k] /= sum;
-    m->c = kGuideMaxSelect * sigmoidf_(o[5 * kGuideLobes]);
+    m->c = kGuideMaxSelect * sigmoidf_(o[5 * kGuideLobes] + kSelectOffset);
 }
 
 __device__ __forceinline__ float guide_pdf(const GuideMix& m, Vec3 d) {

@@ -9,9 +9,11 @@
 // features) is kept as FP32 master and FP16 copy.
 //
 // Kernels:
-//  - k_guide_infer: one CTA of 128 threads per 128 queries (persistent over
-//    tiles); thread t owns query t and TMEM lane t.  The four layers run as
-//    four MMA groups on the same 64 TMEM columns.
+//  - k_guide_encode (and the wavefront's feature kernel) encode queries into
+//    128-row input tiles in global memory, in the operand layout;
+//  - k_guide_mlp: one CTA of 128 threads per tile (persistent over tiles)
+//    copies a tile to shared memory; thread t owns row t and TMEM lane t.
+//    The four layers run as four MMA groups on the same 64 TMEM columns.
 //  - k_guide_train: forward as above, keeping activations and their
 //    transposes in shared memory, then the loss gradient of every record
 //    (thread-local), the backward pass (dA = dZ W on the tensor core) and the
@@ -36,6 +38,7 @@
 #include "../../../include/atrc_cuda.h"
 #include "cuda_util.h"
 #include "dev_guide.cuh"
+#include "dev_guide_enc.cuh"
 #include "dev_tc.cuh"
 #include "guide.h"
 
@@ -51,8 +54,7 @@ constexpr int kOffW2 = kOffW1 + kGuideHidden * kGuideIn;
 constexpr int kOffW3 = kOffW2 + kGuideHidden * kGuideHidden;
 constexpr int kOffW4 = kOffW3 + kGuideHidden * kGuideHidden;
 constexpr int kWeights = kOffW4 + kGuideOut * kGuideHidden;  // 18,432
-constexpr int kTile = 128;
-constexpr int kHashIn = kHashLevels * kHashFeatures;         // 32 inputs from the grid
+constexpr int kTile = kGuideTile;
 
 struct NetView {
     const __nv_bfloat16* w;   // BF16 weights
@@ -60,77 +62,6 @@ struct NetView {
     const float* table_f;     // FP32 table (training)
     HashGrid grid;
 };
-
-// ---------------------------------------------------------------- inputs
-template <class T>
-__device__ __forceinline__ float2 table_pair(const T* t, size_t i);
-template <>
-__device__ __forceinline__ float2 table_pair<float>(const float* t, size_t i) {
-    return *reinterpret_cast<const float2*>(t + 2 * i);
-}
-template <>
-__device__ __forceinline__ float2 table_pair<__half>(const __half* t, size_t i) {
-    return __half22float2(*reinterpret_cast<const __half2*>(t + 2 * i));
-}
-
-// Hash features of one level.
-template <class T>
-__device__ __forceinline__ float2 hash_level(const HashGrid& g, const T* table, int level, const float p01[3]) {
-    HashCell c;
-    hash_cell(g, level, p01, &c);
-    const size_t base = size_t(level) << g.log2_table;
-    float2 acc = make_float2(0, 0);
-    for (int k = 0; k < 8; ++k) {
-        const float2 v = table_pair(table, base + c.slot[k]);
-        acc.x += c.w[k] * v.x;
-        acc.y += c.w[k] * v.y;
-    }
-    return acc;
-}
-
-__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
-    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-    return *reinterpret_cast<const uint32_t*>(&h);
-}
-
-// Write 8 consecutive values of row `row` (k0 a multiple of 8) of a K-major
-// operand with K columns.
-__device__ __forceinline__ void store_row8(uint8_t* buf, int K, int row, int k0, const float* v) {
-    uint4 q;
-    q.x = pack_bf16x2(v[0], v[1]);
-    q.y = pack_bf16x2(v[2], v[3]);
-    q.z = pack_bf16x2(v[4], v[5]);
-    q.w = pack_bf16x2(v[6], v[7]);
-    *reinterpret_cast<uint4*>(buf + tc::kmajor_offset(K, row, k0)) = q;
-}
-__device__ __forceinline__ void store_one(uint8_t* buf, int K, int row, int k, float v) {
-    *reinterpret_cast<__nv_bfloat16*>(buf + tc::kmajor_offset(K, row, k)) = __float2bfloat16_rn(v);
-}
-
-// The 112 input features of query q as row `row` of X (K = 112) and, when
-// xt != null, as column `row` of X^T (112 rows, K = 128).
-template <class T>
-__device__ void write_inputs(const HashGrid& g, const T* table, const GuideQuery& q, int row, uint8_t* x,
-                             uint8_t* xt) {
-    float p01[3];
-    normalise_pos(g, q.pos, p01);
-    float v[16];
-    for (int l = 0; l < kHashLevels; l += 4) {
-        for (int j = 0; j < 4; ++j) {
-            const float2 f = hash_level(g, table, l + j, p01);
-            v[2 * j] = f.x;
-            v[2 * j + 1] = f.y;
-        }
-        store_row8(x, kGuideIn, row, 2 * l, v);
-        if (xt) for (int j = 0; j < 8; ++j) store_one(xt, kTile, 2 * l + j, row, v[j]);
-    }
-    float d[80];
-    guide_dense_features(q, d);
-    for (int k = 0; k < 80; k += 8) {
-        store_row8(x, kGuideIn, row, kHashIn + k, d + k);
-        if (xt) for (int j = 0; j < 8; ++j) store_one(xt, kTile, kHashIn + k + j, row, d[k + j]);
-    }
-}
 
 // Copy W (rows x cols, row-major, BF16 in global) into a K-major operand in
 // shared memory: as is (operand rows = out, K = in) or transposed (rows = in,
@@ -152,7 +83,7 @@ __device__ __forceinline__ void tmem_row(uint32_t tbase, int col0, int n, float*
 }
 
 // ------------------------------------------------------------ inference
-// shared memory of k_guide_infer (bytes)
+// shared memory of k_guide_mlp (bytes)
 constexpr int kInfX = 0;                              // X 128 x 112, later H2 128 x 64
 constexpr int kInfH = kInfX + kTile * kGuideIn * 2;   // H1 / H3 128 x 64
 constexpr int kInfW1 = kInfH + kTile * kGuideHidden * 2;
@@ -162,6 +93,7 @@ constexpr int kInfW4 = kInfW3 + kGuideHidden * kGuideHidden * 2;
 constexpr int kInfBar = kInfW4 + kGuideOut * kGuideHidden * 2;
 constexpr int kInfSmem = kInfBar + 64;
 constexpr uint32_t kInfTmemCols = 64;
+static_assert(kInfX == 0 && kGuideTileBytes == kInfH, "an encoded tile fills X");
 
 // One MMA group: thread 0 issues, all wait.  Returns false (uniformly) when
 // the wait gave up.
@@ -181,9 +113,35 @@ __device__ __forceinline__ bool run_mma(uint64_t* bar, uint32_t* phase, int* err
     return __syncthreads_and(ok) != 0;
 }
 
-__global__ void __launch_bounds__(kTile, 1) k_guide_infer(NetView net, const GuideQuery* __restrict__ queries,
-                                                         const int* __restrict__ n_dev, float* __restrict__ mixes,
-                                                         int* err) {
+// ReLU of this thread's 64 accumulator columns into row t of dst (K = 64),
+// 16 columns at a time.
+__device__ __forceinline__ void relu_row(uint32_t tmem, uint8_t* dst, int t) {
+    const int lane0 = (threadIdx.x >> 5) * 32;
+    for (int c = 0; c < kGuideHidden; c += 16) {
+        float v[16];
+        tc::tmem_ld16(tc::tmem_at(tmem, lane0, c), v);
+        for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j], 0.0f);
+        store_row8(dst, kGuideHidden, t, c, v);
+        store_row8(dst, kGuideHidden, t, c + 8, v + 8);
+    }
+}
+
+// Encode queries into 128-row input tiles (one thread per query).
+template <class T>
+__global__ void k_guide_encode(HashGrid grid, const T* __restrict__ table, const GuideQuery* __restrict__ q, int n,
+                               uint8_t* __restrict__ xtiles) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        write_inputs<T>(grid, table, q[i], i % kTile, xtiles + size_t(i / kTile) * kGuideTileBytes, nullptr);
+}
+
+// The MLP over encoded tiles: *n_dev rows.  DECODE writes the decoded
+// mixture (GuideMix order, kGuideOut floats per row), else the raw outputs.
+// One CTA of 128 threads per tile (persistent over tiles); thread t owns row
+// t and TMEM lane t; the four layers run on the same 64 TMEM columns.
+template <bool DECODE>
+__global__ void __launch_bounds__(kTile, 2) k_guide_mlp(NetView net, const uint8_t* __restrict__ xtiles,
+                                                       const int* __restrict__ n_dev, float* __restrict__ out,
+                                                       int* err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* X = smem + kInfX;
     uint8_t* H = smem + kInfH;
@@ -206,113 +164,37 @@ __global__ void __launch_bounds__(kTile, 1) k_guide_infer(NetView net, const Gui
     uint32_t phase = 0;
     const int t = threadIdx.x;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int i = tile * kTile + t;
-        GuideQuery q;
-        if (i < n) q = queries[i];
-        else { memset(&q, 0, sizeof(q)); q.slot = -1; }
-        write_inputs<__half>(net.grid, net.table_h, q, t, X, nullptr);
-        float v[kGuideHidden];
+        // the tile's encoded inputs (rows past n hold stale values; every
+        // output row depends on its own input row only, and is not written)
+        const uint4* src = reinterpret_cast<const uint4*>(xtiles + size_t(tile) * kGuideTileBytes);
+        for (int k = t; k < kGuideTileBytes / 16; k += kTile) reinterpret_cast<uint4*>(X)[k] = __ldg(src + k);
         if (!run_mma(bar, &phase, err, tmem, sX, tc::smem_addr(smem + kInfW1), kGuideIn, kGuideHidden, false)) break;
-        tmem_row(tmem, 0, kGuideHidden, v);
-        for (int k = 0; k < kGuideHidden; k += 8) {
-            float r[8];
-            for (int j = 0; j < 8; ++j) r[j] = fmaxf(v[k + j], 0.0f);
-            store_row8(H, kGuideHidden, t, k, r);
-        }
+        relu_row(tmem, H, t);
         if (!run_mma(bar, &phase, err, tmem, sH, tc::smem_addr(smem + kInfW2), kGuideHidden, kGuideHidden, false)) break;
-        tmem_row(tmem, 0, kGuideHidden, v);
-        for (int k = 0; k < kGuideHidden; k += 8) {
-            float r[8];
-            for (int j = 0; j < 8; ++j) r[j] = fmaxf(v[k + j], 0.0f);
-            store_row8(X, kGuideHidden, t, k, r);
-        }
+        relu_row(tmem, X, t);
         if (!run_mma(bar, &phase, err, tmem, sX, tc::smem_addr(smem + kInfW3), kGuideHidden, kGuideHidden, false)) break;
-        tmem_row(tmem, 0, kGuideHidden, v);
-        for (int k = 0; k < kGuideHidden; k += 8) {
-            float r[8];
-            for (int j = 0; j < 8; ++j) r[j] = fmaxf(v[k + j], 0.0f);
-            store_row8(H, kGuideHidden, t, k, r);
-        }
+        relu_row(tmem, H, t);
         if (!run_mma(bar, &phase, err, tmem, sH, tc::smem_addr(smem + kInfW4), kGuideHidden, kGuideOut, false)) break;
+        float v[kGuideOut];
         tmem_row(tmem, 0, kGuideOut, v);
+        const int i = tile * kTile + t;
         if (i < n) {
-            float* out = mixes + size_t(i) * kGuideOut;
-            if (q.slot < 0) {
-                out[kGuideUsed - 1] = -1.0f;  // c < 0: no guide for this entry
-            } else {
+            float* o = out + size_t(i) * kGuideOut;
+            if (DECODE) {
                 GuideMix m;
                 guide_decode(v, &m);
                 for (int k = 0; k < kGuideLobes; ++k) {
-                    out[5 * k] = m.mu[k][0];
-                    out[5 * k + 1] = m.mu[k][1];
-                    out[5 * k + 2] = m.mu[k][2];
-                    out[5 * k + 3] = m.kappa[k];
-                    out[5 * k + 4] = m.w[k];
+                    o[5 * k] = m.mu[k][0];
+                    o[5 * k + 1] = m.mu[k][1];
+                    o[5 * k + 2] = m.mu[k][2];
+                    o[5 * k + 3] = m.kappa[k];
+                    o[5 * k + 4] = m.w[k];
                 }
-                out[kGuideUsed - 1] = m.c;
+                o[kGuideUsed - 1] = m.c;
+            } else {
+                for (int k = 0; k < kGuideOut; ++k) o[k] = v[k];
             }
         }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x < 32) tc::tmem_dealloc(tmem, kInfTmemCols);
-}
-
-// Raw outputs for host tests (no decoding): same network, outputs written
-// as is.  Reuses the inference kernel's structure.
-__global__ void __launch_bounds__(kTile, 1) k_guide_raw(NetView net, const GuideQuery* __restrict__ queries, int n,
-                                                       float* __restrict__ raw, int* err) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* X = smem + kInfX;
-    uint8_t* H = smem + kInfH;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kInfBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kInfBar + 8);
-    const int ntiles = (n + kTile - 1) / kTile;
-    if (int(blockIdx.x) >= ntiles) return;
-    load_weights(smem + kInfW1, net.w + kOffW1, kGuideHidden, kGuideIn, false, kGuideHidden);
-    load_weights(smem + kInfW2, net.w + kOffW2, kGuideHidden, kGuideHidden, false, kGuideHidden);
-    load_weights(smem + kInfW3, net.w + kOffW3, kGuideHidden, kGuideHidden, false, kGuideHidden);
-    load_weights(smem + kInfW4, net.w + kOffW4, kGuideOut, kGuideHidden, false, kGuideOut);
-    if (threadIdx.x == 0) tc::mbar_init(bar, 1);
-    if (threadIdx.x < 32) tc::tmem_alloc(tslot, kInfTmemCols);
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *tslot;
-    const uint32_t sX = tc::smem_addr(X), sH = tc::smem_addr(H);
-    uint32_t phase = 0;
-    const int t = threadIdx.x;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int i = tile * kTile + t;
-        GuideQuery q;
-        if (i < n) q = queries[i];
-        else { memset(&q, 0, sizeof(q)); q.slot = -1; }
-        write_inputs<float>(net.grid, net.table_f, q, t, X, nullptr);
-        float v[kGuideHidden];
-        if (!run_mma(bar, &phase, err, tmem, sX, tc::smem_addr(smem + kInfW1), kGuideIn, kGuideHidden, false)) break;
-        tmem_row(tmem, 0, kGuideHidden, v);
-        for (int k = 0; k < kGuideHidden; k += 8) {
-            float r[8];
-            for (int j = 0; j < 8; ++j) r[j] = fmaxf(v[k + j], 0.0f);
-            store_row8(H, kGuideHidden, t, k, r);
-        }
-        if (!run_mma(bar, &phase, err, tmem, sH, tc::smem_addr(smem + kInfW2), kGuideHidden, kGuideHidden, false)) break;
-        tmem_row(tmem, 0, kGuideHidden, v);
-        for (int k = 0; k < kGuideHidden; k += 8) {
-            float r[8];
-            for (int j = 0; j < 8; ++j) r[j] = fmaxf(v[k + j], 0.0f);
-            store_row8(X, kGuideHidden, t, k, r);
-        }
-        if (!run_mma(bar, &phase, err, tmem, sX, tc::smem_addr(smem + kInfW3), kGuideHidden, kGuideHidden, false)) break;
-        tmem_row(tmem, 0, kGuideHidden, v);
-        for (int k = 0; k < kGuideHidden; k += 8) {
-            float r[8];
-            for (int j = 0; j < 8; ++j) r[j] = fmaxf(v[k + j], 0.0f);
-            store_row8(H, kGuideHidden, t, k, r);
-        }
-        if (!run_mma(bar, &phase, err, tmem, sH, tc::smem_addr(smem + kInfW4), kGuideHidden, kGuideOut, false)) break;
-        tmem_row(tmem, 0, kGuideOut, v);
-        if (i < n) for (int k = 0; k < kGuideOut; ++k) raw[size_t(i) * kGuideOut + k] = v[k];
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -641,7 +523,7 @@ struct GuideImpl {
     size_t table_n = 0;  // floats in the table
     DevBuf w_f, w_g, w_m, w_v, w_bf;          // weights: master, grad, Adam m / v, BF16 copy
     DevBuf t_f, t_g, t_m, t_v, t_h;           // table: master, grad, m, v, FP16 copy
-    DevBuf records, rec_count, rec_last, queries, mixes, scratch, err;
+    DevBuf records, rec_count, rec_last, queries, mixes, gidx, xtiles, scratch, err;
     size_t slots = 0;
     int steps = 0;
     NetView view() const {
@@ -662,11 +544,17 @@ GuideFrame guide_frame(GuideImpl* g, size_t cap, bool record, cudaStream_t s) {
         g->queries.alloc(cap * sizeof(GuideQuery));
         g->mixes.alloc(cap * kGuideOut * sizeof(float));
         g->rec_last.alloc(cap * sizeof(int));
+        g->gidx.alloc(cap * sizeof(int));
+        g->xtiles.alloc((cap + kTile - 1) / kTile * kGuideTileBytes);
         g->slots = cap;
     }
     GuideFrame f{};
     f.queries = g->queries.as<GuideQuery>();
     f.mixes = g->mixes.as<float>();
+    f.gidx = g->gidx.as<int>();
+    f.max_depth = g->desc.max_depth;
+    f.xtiles = g->xtiles.as<uint8_t>();
+    f.table_h = g->t_h.as<__half>();
     f.grid = g->grid;
     if (record) {
         CK(cudaMemsetAsync(g->rec_count.p, 0, sizeof(int), s));
@@ -680,8 +568,8 @@ GuideFrame guide_frame(GuideImpl* g, size_t cap, bool record, cudaStream_t s) {
 }
 
 void guide_infer(GuideImpl* g, const int* n_dev, cudaStream_t s) {
-    k_guide_infer<<<g->sm_count * 2, kTile, kInfSmem, s>>>(g->view(), g->queries.as<GuideQuery>(), n_dev,
-                                                          g->mixes.as<float>(), g->err.as<int>());
+    k_guide_mlp<true><<<g->sm_count * 2, kTile, kInfSmem, s>>>(g->view(), g->xtiles.as<uint8_t>(), n_dev,
+                                                              g->mixes.as<float>(), g->err.as<int>());
 }
 
 int guide_device(const GuideImpl* g) { return g->device; }
@@ -731,8 +619,8 @@ void check_err(GuideImpl& g, const char* what) {
 
 // dynamic shared memory above 48 KB (set on the current device)
 void set_smem_limits() {
-    CK(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfSmem));
-    CK(cudaFuncSetAttribute(k_guide_raw, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfSmem));
+    CK(cudaFuncSetAttribute(k_guide_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfSmem));
+    CK(cudaFuncSetAttribute(k_guide_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfSmem));
     CK(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrSmem));
 }
 
@@ -747,7 +635,11 @@ int atrc_guide_default_desc(AtrcGuideDesc* d) {
     // guiding needs a smooth field: finer levels memorise single records
     // (the training loss falls below the achievable optimum)
     d->base_resolution = 4;
-    d->max_resolution = 128;
+    d->max_resolution = 64;
+    // vertices past depth 3 carry little of the image's variance on the
+    // indoor workload but cost inference (best time to relMSE 1e-3 of
+    // depths 2, 3, 4 and all)
+    d->max_depth = 3;
     d->learning_rate = 1e-2f;
     d->batch = 1 << 18;
     d->record_capacity = 1 << 20;
@@ -761,7 +653,7 @@ int atrc_guide_create(int device, const float scene_lo[3], const float scene_hi[
     *out = nullptr;
     if (desc->log2_table < 8 || desc->log2_table > 22 || desc->base_resolution < 2 ||
         desc->max_resolution < desc->base_resolution || desc->batch < kTile || desc->record_capacity < kTile ||
-        !(desc->learning_rate > 0))
+        !(desc->learning_rate > 0) || desc->max_depth < 0)
         return gfail(ATRC_ERR_INVALID_ARG, "atrc_guide_create: parameter out of range");
     return gguarded([&] {
         auto g = std::make_unique<AtrcGuide>();
@@ -891,13 +783,20 @@ int atrc_guide_eval(AtrcGuide* g, const float* queries, size_t n, float* raw) {
             q[i].slot = 0;
             q[i].pad = 0;
         }
-        DevBuf dq, dr;
+        DevBuf dq, dr, dx, dn;
+        const size_t tiles = (n + kTile - 1) / kTile;
         dq.alloc(n * sizeof(GuideQuery));
         dr.alloc(n * kGuideOut * 4);
+        dx.alloc(tiles * kGuideTileBytes);
+        dn.alloc(sizeof(int));
+        const int ni = int(n);
         CK(cudaMemcpyAsync(dq.p, q.data(), n * sizeof(GuideQuery), cudaMemcpyHostToDevice, s));
-        const int tiles = int((n + kTile - 1) / kTile);
-        k_guide_raw<<<std::min(tiles, G.sm_count * 2), kTile, kInfSmem, s>>>(G.view(), dq.as<GuideQuery>(), int(n),
-                                                                           dr.as<float>(), G.err.as<int>());
+        CK(cudaMemcpyAsync(dn.p, &ni, sizeof(int), cudaMemcpyHostToDevice, s));
+        // the FP32 master table, so that the check needs no FP16 rounding
+        k_guide_encode<float><<<G.sm_count * 4, 128, 0, s>>>(G.grid, G.t_f.as<float>(), dq.as<GuideQuery>(), ni,
+                                                            dx.as<uint8_t>());
+        k_guide_mlp<false><<<G.sm_count * 2, kTile, kInfSmem, s>>>(G.view(), dx.as<uint8_t>(), dn.as<int>(),
+                                                                  dr.as<float>(), G.err.as<int>());
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(raw, dr.p, n * kGuideOut * 4, cudaMemcpyDeviceToHost, s));
         check_err(G, "atrc_guide_eval");
@@ -925,7 +824,8 @@ int atrc_guide_pdf(AtrcGuide* g, const float* queries, const float* dirs, size_t
             q[i].slot = 0;
             q[i].pad = 0;
         }
-        DevBuf dq, dm, dd, dout, dn;
+        DevBuf dq, dm, dd, dout, dn, dx;
+        dx.alloc((n + kTile - 1) / kTile * kGuideTileBytes);
         dq.alloc(n * sizeof(GuideQuery));
         dm.alloc(n * kGuideOut * 4);
         dd.alloc(n * 3 * 4);
@@ -935,8 +835,10 @@ int atrc_guide_pdf(AtrcGuide* g, const float* queries, const float* dirs, size_t
         CK(cudaMemcpyAsync(dq.p, q.data(), n * sizeof(GuideQuery), cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(dd.p, dirs, n * 3 * 4, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(dn.p, &ni, sizeof(int), cudaMemcpyHostToDevice, s));
-        k_guide_infer<<<G.sm_count * 2, kTile, kInfSmem, s>>>(G.view(), dq.as<GuideQuery>(), dn.as<int>(),
-                                                              dm.as<float>(), G.err.as<int>());
+        k_guide_encode<__half><<<G.sm_count * 4, 128, 0, s>>>(G.grid, G.t_h.as<__half>(), dq.as<GuideQuery>(), ni,
+                                                             dx.as<uint8_t>());
+        k_guide_mlp<true><<<G.sm_count * 2, kTile, kInfSmem, s>>>(G.view(), dx.as<uint8_t>(), dn.as<int>(),
+                                                                 dm.as<float>(), G.err.as<int>());
         k_mix_pdf<<<G.sm_count * 4, 128, 0, s>>>(dm.as<float>(), dd.as<float>(), ni, dout.as<float>(),
                                                 dout.as<float>() + n);
         CK(cudaGetLastError());

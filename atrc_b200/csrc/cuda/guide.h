@@ -2,6 +2,7 @@
 // (guide.cu).  Not part of the C ABI.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -25,8 +26,12 @@ static_assert(sizeof(GuideRecord) == 96, "record layout");
 // What the wavefront kernels need from a guide during one render call.
 struct GuideFrame {
     // inference inputs / outputs, indexed by shade-queue position
-    dev::GuideQuery* queries;
-    float* mixes;             // decoded GuideMix, kGuideOut floats per entry
+    dev::GuideQuery* queries; // compact list of this iteration's queries
+    float* mixes;             // decoded GuideMix, kGuideOut floats per query
+    int* gidx;                // per shade-queue entry: its query, or -1
+    int max_depth;            // guide vertices up to this depth (0: all)
+    uint8_t* xtiles;          // encoded inputs of the queries, 128-row tiles
+    const __half* table_h;    // FP16 hash table
     // recording (null when the call does not record)
     GuideRecord* records;
     int* record_count;

@@ -41,6 +41,7 @@
 #include "dev_shade.cuh"
 #include "dev_trace.cuh"
 #include "cuda_util.h"
+#include "dev_guide_enc.cuh"
 #include "guide.h"
 
 #ifndef ATRC_SHADE_MIN_BLOCKS
@@ -113,6 +114,7 @@ struct Counters {
     int in, out;              // queue buffers read / written this iteration
     int n_ext, n_next;        // paths to extend / continuations written
     int n_shadow, n_finish;
+    int n_guide;              // guide queries this iteration
     int n_free, n_new, n_cont, free_base;
     unsigned long long gen_base, issued, total, completed;
     unsigned long long rays_closest, rays_shadow, iterations;
@@ -221,6 +223,7 @@ __global__ void k_begin(Counters* c) {
     c->n_next = 0;
     c->n_shadow = 0;
     c->n_finish = 0;
+    c->n_guide = 0;
     if (c->n_ext == 0) c->done = 1;
 }
 
@@ -395,8 +398,9 @@ __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d
 }
 
 // Guide queries of the shade queue (same order as k_shade): surface hits
-// with a Lambert or Disney material and consistent frames; slot -1 marks an
-// entry the guide does not serve.
+// with a Lambert or Disney material, consistent frames and a depth the guide
+// serves are appended to a compact query list; gidx[i] is the query of
+// shade-queue entry i, or -1.
 __global__ void k_guide_features(Scene S, Params p, Pool P, Counters* c) {
     const int n = c->n_ext, in = c->in;
     const int* queue = p.sort_mode != ATRC_SORT_NONE ? P.q_sorted : P.q[in];
@@ -407,8 +411,9 @@ __global__ void k_guide_features(Scene S, Params p, Pool P, Counters* c) {
         q.pad = 0;
         const float4 hv = P.hit[slot];
         const int ent = __float_as_int(hv.w);
-        const int flags = P.ctr[slot].w & 0xff;
-        if (ent >= 0 && !(flags & PF_TERMINATE)) {
+        const int4 ct = P.ctr[slot];
+        const int flags = ct.w & 0xff;
+        if (ent >= 0 && !(flags & PF_TERMINATE) && (p.gf.max_depth <= 0 || ct.x <= p.gf.max_depth)) {
             const float4 ro = P.ray_o[slot], rd = P.ray_d[slot];
             Hit h;
             h.t = hv.x; h.u = hv.y; h.v = hv.z; h.entity = ent; h.tri = P.hit_tri[slot];
@@ -423,9 +428,13 @@ __global__ void k_guide_features(Scene S, Params p, Pool P, Counters* c) {
                 q.slot = slot;
             }
         }
-        if (q.slot < 0) { q.pos[0] = q.pos[1] = q.pos[2] = 0; q.nrm[0] = q.nrm[1] = q.nrm[2] = 0;
-                          q.wo[0] = q.wo[1] = q.wo[2] = 0; q.rough = 0; }
-        p.gf.queries[i] = q;
+        const int k = warp_append(&c->n_guide, q.slot >= 0);
+        if (q.slot >= 0) {
+            p.gf.queries[k] = q;
+            write_inputs<__half>(p.gf.grid, p.gf.table_h, q, k % kGuideTile,
+                                 p.gf.xtiles + size_t(k / kGuideTile) * kGuideTileBytes, nullptr);
+        }
+        p.gf.gidx[i] = q.slot >= 0 ? k : -1;
     }
 }
 
@@ -558,10 +567,10 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                 // learned guide of this vertex (one-sample MIS with the BSDF)
                 GuideMix mix;
                 bool guided = false;
-                if (p.guide_on) {
-                    const float* gm = p.gf.mixes + size_t(i) * kGuideOut;
-                    guided = gm[kGuideUsed - 1] >= 0.0f && (b.type == ATRC_MAT_IDEAL_DIFFUSE || b.type == ATRC_MAT_DISNEY) &&
-                             !fringes(b, s.wr);
+                const int gq_i = p.guide_on ? p.gf.gidx[i] : -1;
+                if (gq_i >= 0) {
+                    const float* gm = p.gf.mixes + size_t(gq_i) * kGuideOut;
+                    guided = (b.type == ATRC_MAT_IDEAL_DIFFUSE || b.type == ATRC_MAT_DISNEY) && !fringes(b, s.wr);
                     if (guided) {
                         for (int k = 0; k < kGuideLobes; ++k) {
                             mix.mu[k][0] = gm[5 * k]; mix.mu[k][1] = gm[5 * k + 1]; mix.mu[k][2] = gm[5 * k + 2];
@@ -637,7 +646,7 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                         // training record of this vertex; its targets are set when the path ends
                         const int r = atomicAdd(p.gf.record_count, 1);
                         if (r < p.gf.record_cap) {
-                            const GuideQuery& gq = p.gf.queries[i];
+                            const GuideQuery& gq = p.gf.queries[gq_i];
                             GuideRecord R;
                             for (int k = 0; k < 3; ++k) { R.pos[k] = gq.pos[k]; R.nrm[k] = gq.nrm[k]; R.wo[k] = gq.wo[k]; }
                             R.rough = gq.rough;
@@ -1267,7 +1276,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
             CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
             if (guide) {
                 k_guide_features<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
-                guide_infer(guide, &c->n_ext, s);
+                guide_infer(guide, &c->n_guide, s);
             }
             k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));

@@ -49,7 +49,10 @@ class Guide:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            load_library().atrc_guide_destroy(self._h)
+            try:
+                load_library().atrc_guide_destroy(self._h)
+            except Exception:  # interpreter shutdown: the library is gone already
+                pass
             self._h = None
 
     def __del__(self):
@@ -118,14 +121,37 @@ class Guide:
         return out
 
 
-def rel_mse(image, reference) -> float:
-    """Mean over pixels and channels of (I - R)^2 / (R^2 + 1e-2) (torch or numpy)."""
+def rel_mse(image, reference, ref_var=None) -> float:
+    """Mean over pixels and channels of (I - R)^2 / (R^2 + 1e-2) (torch or
+    numpy).  With `ref_var`, the variance of the reference's per-pixel mean,
+    the reference's own noise is taken out: E[(I - R)^2] = (E I - mu)^2 +
+    Var I + Var R, so subtracting Var R estimates the error against the
+    converged image."""
     d = image - reference
-    return float(((d * d) / (reference * reference + 1e-2)).mean())
+    e = d * d
+    if ref_var is not None:
+        e = e - ref_var
+    return float((e / (reference * reference + 1e-2)).mean())
+
+
+def time_to(curve, target: float) -> Optional[float]:
+    """First time a (time, spp, relMSE) curve reaches `target`,
+    interpolated log-log between checkpoints."""
+    prev = None
+    for t, _, e in curve:
+        if e <= target:
+            if prev is None or prev[1] <= 0 or e <= 0:
+                return t
+            t0, e0 = prev
+            a = (np.log(target) - np.log(e0)) / (np.log(e) - np.log(e0))
+            return float(np.exp(np.log(t0) + a * (np.log(t) - np.log(t0))))
+        prev = (t, e)
+    return None
 
 
 def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, train_fraction: float = 0.25,
-                  train_steps: int = 4, spp_per_pass: int = 1, reference=None, checkpoints=(), first_spp: int = 0):
+                  train_steps: int = 4, spp_per_pass: int = 1, reference=None, checkpoints=(), first_spp: int = 0,
+                  ref_var=None, stop_at: Optional[float] = None):
     """Render passes of `spp_per_pass` samples per pixel into one device film
     until `seconds` of render time have passed.  With a guide, the passes of
     the first `train_fraction` of the budget record training data and run
@@ -145,7 +171,8 @@ def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, tr
     passes = 0
     curve = []
     pending = sorted(checkpoints)
-    while elapsed < seconds:
+    stopped = False
+    while elapsed < seconds and not stopped:
         desc.first_spp = first_spp + passes * spp_per_pass
         training = guide is not None and elapsed < train_fraction * seconds
         t0 = time.perf_counter()
@@ -165,12 +192,14 @@ def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, tr
             pending.pop(0)
             img = (film.value.view(desc.height, desc.width, 3) /
                    film.weight.view(desc.height, desc.width, 1).clamp_min(1e-30))
-            curve.append((elapsed, passes * spp_per_pass, rel_mse(img.float(), reference)))
+            curve.append((elapsed, passes * spp_per_pass, rel_mse(img.float(), reference, ref_var)))
+            if stop_at is not None and curve[-1][2] <= stop_at:
+                stopped = True
     torch.cuda.synchronize()
     final = None
     if reference is not None:
         img = film.value.view(desc.height, desc.width, 3) / film.weight.view(desc.height, desc.width, 1).clamp_min(1e-30)
-        final = rel_mse(img.float(), reference)
+        final = rel_mse(img.float(), reference, ref_var)
         curve.append((elapsed, passes * spp_per_pass, final))
     return {"film": film, "seconds": elapsed, "render_s": t_render, "train_s": t_train, "spp": passes * spp_per_pass,
             "curve": curve, "rel_mse": final}

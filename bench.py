@@ -49,6 +49,11 @@ def parse():
                    help="shade-queue sort: -1 auto, 0 none, 1 material type, 2 material")
     p.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed oracle run (profiling)")
     p.add_argument("--no-autotune", action="store_true", help="render with the built-in launch configuration")
+    p.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain time-to-relMSE comparison")
+    p.add_argument("--guided-ref-spp", type=int, default=1024)
+    p.add_argument("--guided-max-s", type=float, default=30.0)
+    p.add_argument("--guided-max-depth", type=int, default=-1, help="guide vertices up to this depth (-1: library default)")
+    p.add_argument("--guided-train-steps", type=int, default=4)
     return p.parse_args()
 
 
@@ -179,6 +184,57 @@ def cpu_baseline(args) -> dict:
             "sample": f"{passes} whole-film 1 spp passes ({samples} camera samples), {total:.1f} s"}
 
 
+def guided_comparison(args) -> dict:
+    """Time to relMSE 1e-3 of guided and of plain pt_cuda on the indoor room
+    (1280x720, depth 16, fixed Disney sampling), equal-time protocol: plain
+    renders until it reaches the target; the guided render gets the same
+    budget and trains during its first 25 %.  relMSE is measured against a
+    plain reference of --guided-ref-spp samples per pixel with the
+    reference's own per-pixel variance subtracted (an unbiased estimate of
+    the error against the converged image)."""
+    from atrc_b200 import Config, DeviceScene, Film, scenes
+    from atrc_b200.guide import Guide, render_budget, time_to
+    target = 1e-3
+    cfg = Config.from_file(scenes.indoor_room())
+    desc, _ = cfg.rendering(0)
+    W, H = desc.width, desc.height
+    dev = DeviceScene(cfg)
+    dev.autotune(desc, trial_spp=1)
+    ref = Film(W, H, value_sq=True, device=True)
+    desc.seed, desc.first_spp, desc.spp_count = 777, 0, args.guided_ref_spp
+    t0 = time.perf_counter()
+    dev.render(desc, ref)
+    t_ref = time.perf_counter() - t0
+    w = ref.weight.view(H, W, 1)
+    R = ref.value.view(H, W, 3) / w
+    fv = 1.0 / (4 * (0.5 - desc.eps) ** 2)       # box-filter weight of one sample
+    n = (w / fv).clamp_min(2.0)
+    ref_var = ((ref.value_sq.view(H, W, 3) / w - R * R).clamp_min(0) / (n - 1)).float()
+    R = R.float()
+    desc.seed = 42
+    plain = render_budget(dev, desc, args.guided_max_s, reference=R, ref_var=ref_var,
+                          checkpoints=list(np.arange(0.25, args.guided_max_s, 0.25)), stop_at=0.7 * target)
+    t_plain = time_to(plain["curve"], target)
+    budget = t_plain if t_plain else args.guided_max_s
+    guide = Guide.for_scene(dev, **({"max_depth": args.guided_max_depth} if args.guided_max_depth >= 0 else {}))
+    desc.seed = 4242
+    guided = render_budget(dev, desc, budget, guide=guide, reference=R, ref_var=ref_var,
+                           checkpoints=list(np.arange(0.1, budget, 0.1)), train_fraction=0.25,
+                           train_steps=args.guided_train_steps)
+    t_guided = time_to(guided["curve"], target)
+    thin = lambda c: [[round(t, 3), s, float(f"{e:.4g}")] for t, s, e in c[::max(1, len(c) // 12)]]  # noqa: E731
+    return {"workload": "indoor_room_1280x720_depth16", "target_rel_mse": target,
+            "reference": {"spp": args.guided_ref_spp, "seconds": round(t_ref, 2),
+                          "Msamples_per_s": W * H * args.guided_ref_spp / t_ref / 1e6,
+                          "noise": "per-pixel variance of the reference mean subtracted"},
+            "plain": {"time_to_target_s": t_plain, "spp": plain["spp"], "seconds": round(plain["seconds"], 3),
+                      "curve": thin(plain["curve"])},
+            "guided": {"time_to_target_s": t_guided, "budget_s": round(budget, 3), "spp": guided["spp"],
+                       "render_s": round(guided["render_s"], 3), "train_s": round(guided["train_s"], 3),
+                       "rel_mse_at_budget": guided["rel_mse"], "curve": thin(guided["curve"])},
+            "time_ratio_guided_over_plain": (t_guided / t_plain) if (t_guided and t_plain) else None}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -280,6 +336,7 @@ def main():
     launches = int(sum(st["kernel_launches"] for st in stats))
     if rank == 0:
         cpu = cpu_baseline(args) if world == 1 and not args.no_cpu_baseline else None
+        guided = guided_comparison(args) if world == 1 and not args.no_guided else None
         clocks = clk.summary()
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -308,6 +365,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "guided": guided,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -498,10 +498,13 @@ typedef struct AtrcGuide AtrcGuide;
 typedef struct AtrcGuideDesc {
     int32_t  log2_table;       /* hash entries per level = 2^log2_table (19) */
     int32_t  base_resolution;  /* cells per axis of the coarsest level (4)   */
-    int32_t  max_resolution;   /* ... of the finest level (128)              */
+    int32_t  max_resolution;   /* ... of the finest level (64)               */
     int32_t  batch;            /* records per training step (2^18)           */
     int32_t  record_capacity;  /* records kept by a recording render (2^20)  */
     float    learning_rate;    /* Adam step size (1e-2)                      */
+    int32_t  max_depth;        /* guide vertices up to this path depth (3;   */
+                               /* 0: every depth)                            */
+    int32_t  pad_;
     uint64_t seed;             /* parameter initialisation                   */
 } AtrcGuideDesc;
 
@@ -511,7 +514,7 @@ typedef struct AtrcGuideInfo {
     int32_t  levels, inputs, hidden, outputs, lobes, steps, log2_table, pad_;
     float    grid_lo[3], grid_inv_extent[3];  /* position -> [0,1]^3          */
     int32_t  grid_res[16];     /* cells per axis of each hash level          */
-    float    max_select;       /* c = max_select * sigmoid(o[40])            */
+    float    max_select;       /* c = max_select * sigmoid(o[40] - 2)        */
     float    pad2_;
 } AtrcGuideInfo;
 

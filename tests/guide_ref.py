@@ -10,6 +10,7 @@ import numpy as np
 LEVELS = 16
 IN, HID, OUT, LOBES = 112, 64, 48, 8
 MAX_SELECT = 0.9
+SELECT_OFFSET = -2.0
 LOG_KAPPA = (-6.9, 9.2)
 
 
@@ -94,7 +95,7 @@ def decode(raw: np.ndarray):
     logit = o[:, 4:40:5]
     w = np.exp(logit - logit.max(1, keepdims=True))
     w /= w.sum(1, keepdims=True)
-    c = MAX_SELECT / (1 + np.exp(-o[:, 40]))
+    c = MAX_SELECT / (1 + np.exp(-(o[:, 40] + SELECT_OFFSET)))
     return mu, kappa, w, c
 
 
