@@ -261,6 +261,19 @@ class DeviceScene:
             setattr(t, k, v)
         _check(load_library().atrc_cuda_set_tuning(self._h, C.byref(t)))
 
+    def render_batch(self, descs, films, guide=None) -> tuple[dict, np.ndarray]:
+        """Render several views in one wavefront (atrc_cuda_render_batch);
+        films must be device films.  Returns the stats and each view's
+        completion time in seconds from the start of the call."""
+        n = len(descs)
+        arr = (AtrcRenderDesc * n)(*descs)
+        farr = (AtrcFilm * n)(*[f.as_struct() for f in films])
+        secs = (C.c_double * n)()
+        st = AtrcRenderStats()
+        _check(load_library().atrc_cuda_render_batch(self._h, guide.handle if guide is not None else None, arr, n, farr,
+                                                    secs, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in AtrcRenderStats._fields_}, np.array(secs[:])
+
     def render_guided(self, guide, desc: AtrcRenderDesc, film: Film, record: bool = False) -> dict:
         """Render with the learned guide sampling surface vertices
         (atrc_cuda_render_guided); record=True also keeps training records."""

@@ -178,6 +178,8 @@ PROTOTYPES = {
     "atrc_guide_train_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.c_int, C.POINTER(C.c_float)]),
     "atrc_guide_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "atrc_cuda_scene_bounds": (C.c_int, [C.c_void_p, c_float_p, c_float_p]),
+    "atrc_cuda_render_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32,
+                                         C.POINTER(AtrcFilm), C.POINTER(C.c_double), C.POINTER(AtrcRenderStats)]),
     "atrc_cuda_render_guided": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32,
                                           C.POINTER(AtrcFilm), C.POINTER(AtrcRenderStats)]),
     "atrc_cuda_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(AtrcTuning)]),

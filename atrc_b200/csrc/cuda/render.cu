@@ -136,6 +136,14 @@ struct Camera {
     float film_w, film_h, focal, lens_radius;
 };
 
+struct Film {
+    double *value, *weight, *value_sq, *albedo, *normal, *denoise;
+};
+
+// One camera view of a render.  A render is a batch of views (one for
+// atrc_cuda_render) whose samples share one path pool: global sample index k
+// belongs to the view with start <= k < start + count.
+//
 // The film is cut into tiles of G x G pixels (task_grid_size).  Each tile
 // samples every pixel of its bound grown by the filter's reach
 // (sample_bound_of, framebuffer.h:36-47) and splats only into itself
@@ -145,21 +153,32 @@ struct Camera {
 // tile_cols[gx].w <= u < tile_cols[gx + 1].w, and is pixel
 // tile_cols[gx].z + (u - tile_cols[gx].w); rows likewise.  With the default
 // box filter (radius 0.5 - eps) the sample grid is the film itself.
-struct Params {
+struct View {
     int W, H;
     int G, TX, TY;          // tile edge, tile columns / rows
     int SW, SH;             // sample grid size (sum of the tiles' sample bounds)
     int E0X, E0Y;           // sample-bound extent of the first tile column / row
-    const int4* tile_cols;  // per tile column: x0, x1, first sampled x, first u
-    const int4* tile_rows;  // per tile row:    y0, y1, first sampled y, first v
+    int4* tile_cols;        // per tile column: x0, x1, first sampled x, first u
+    int4* tile_rows;        // per tile row:    y0, y1, first sampled y, first v
     int first_spp;
-    int sort_mode, nkeys;   // shade-queue sort (AtrcSortMode, resolved) and key count
-    int min_depth, max_depth, specular_depth;
-    float cont_prob, eps;
     unsigned long long seed;
+    unsigned long long start, count;  // global sample indices of this view
     Camera cam;
     int filter_type;
     float filter_radius, filter_value, filter_alpha, filter_exp;
+    Film film;
+};
+constexpr int kTileBits = 22;  // path state packs (view << kTileBits) | tile
+constexpr int kMaxViews = 1024;
+
+// Settings shared by every view of a render.
+struct Params {
+    int nviews;
+    const View* views;                 // device array
+    unsigned long long* view_done;     // per view: finished samples (batch renders; else null)
+    int sort_mode, nkeys;   // shade-queue sort (AtrcSortMode, resolved) and key count
+    int min_depth, max_depth, specular_depth;
+    float cont_prob, eps;
     int guide_on;           // sample surface vertices with the learned guide
     GuideFrame gf;          // guide buffers of this call (zero when guide_on == 0)
 };
@@ -184,10 +203,6 @@ struct Pool {
     int* free_list;
     float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
     int shadow_cap;
-};
-
-struct Film {
-    double *value, *weight, *value_sq, *albedo, *normal, *denoise;
 };
 
 __global__ void k_init(Pool P, int cap, int nkeys, Counters* c, unsigned long long total) {
@@ -231,29 +246,42 @@ __device__ __forceinline__ Rng load_rng(const uint4& s) { Rng r; r.state = (uint
 __device__ __forceinline__ void store_rng(uint4& s, const Rng& r) { s.y = uint32_t(r.state); s.z = uint32_t(r.state >> 32); }
 __device__ __forceinline__ Vec3 xyz(const float4& v) { return Vec3(v.x, v.y, v.z); }
 
-// Tile tables of the sample grid (one thread; TX + TY entries).  The bounds
-// use the reference's float expressions so both agree on every tile.
-__global__ void k_tiles(Params p, int4* cols, int4* rows) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    const float r = p.filter_radius;
+// Tile tables of each view's sample grid (block = view, one thread; TX + TY
+// entries).  The bounds use the reference's float expressions so both agree
+// on every tile.
+__global__ void k_tiles(Params p) {
+    if (threadIdx.x != 0 || int(blockIdx.x) >= p.nviews) return;
+    const View& v = p.views[blockIdx.x];
+    const float r = v.filter_radius;
     int acc = 0;
-    for (int g = 0; g < p.TX; ++g) {
-        const int a0 = g * p.G, a1 = min(p.W, a0 + p.G) - 1;
+    for (int g = 0; g < v.TX; ++g) {
+        const int a0 = g * v.G, a1 = min(v.W, a0 + v.G) - 1;
         const int s0 = int(floorf(__fsub_rn(__fadd_rn(float(a0), 0.5f), r)));
         const int s1 = int(floorf(__fadd_rn(__fadd_rn(float(a1), 0.49999f), r)));
-        cols[g] = make_int4(a0, a1, s0, acc);
+        v.tile_cols[g] = make_int4(a0, a1, s0, acc);
         acc += s1 - s0 + 1;
     }
-    cols[p.TX] = make_int4(0, 0, 0, acc);
+    v.tile_cols[v.TX] = make_int4(0, 0, 0, acc);
     acc = 0;
-    for (int g = 0; g < p.TY; ++g) {
-        const int a0 = g * p.G, a1 = min(p.H, a0 + p.G) - 1;
+    for (int g = 0; g < v.TY; ++g) {
+        const int a0 = g * v.G, a1 = min(v.H, a0 + v.G) - 1;
         const int s0 = int(floorf(__fsub_rn(__fadd_rn(float(a0), 0.5f), r)));
         const int s1 = int(floorf(__fadd_rn(__fadd_rn(float(a1), 0.49999f), r)));
-        rows[g] = make_int4(a0, a1, s0, acc);
+        v.tile_rows[g] = make_int4(a0, a1, s0, acc);
         acc += s1 - s0 + 1;
     }
-    rows[p.TY] = make_int4(0, 0, 0, acc);
+    v.tile_rows[v.TY] = make_int4(0, 0, 0, acc);
+}
+
+// View of global sample index k (views are ordered by start).
+__device__ __forceinline__ int view_of(const Params& p, unsigned long long k) {
+    int lo = 0, hi = p.nviews - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.views[mid].start <= k) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 // sample-grid coordinate -> (tile index along the axis, pixel coordinate)
@@ -269,22 +297,25 @@ __device__ __forceinline__ int tile_of(const int4* t, int n, int e0, int u, int*
 __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
     const int n = c->n_new, base = c->n_cont, fb = c->free_base, in = c->in;
     const unsigned long long gen = c->gen_base;
-    const unsigned long long npix = (unsigned long long)p.SW * p.SH;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = P.free_list[fb + i];
         const unsigned long long k = gen + i;
-        const unsigned long long pixel = k % npix;
-        const unsigned long long s = (unsigned long long)p.first_spp + k / npix;
+        const int vi = view_of(p, k);
+        const View& v = p.views[vi];
+        const unsigned long long local = k - v.start;
+        const unsigned long long npix = (unsigned long long)v.SW * v.SH;
+        const unsigned long long pixel = local % npix;
+        const unsigned long long s = (unsigned long long)v.first_spp + local / npix;
         Rng rng;
-        rng.state = mix64(p.seed ^ mix64(pixel * 0x9E3779B97F4A7C15ULL + s * 0xD1B54A32D192ED03ULL + 1));
+        rng.state = mix64(v.seed ^ mix64(pixel * 0x9E3779B97F4A7C15ULL + s * 0xD1B54A32D192ED03ULL + 1));
         int px, py;
-        const int gx = tile_of(p.tile_cols, p.TX, p.E0X, int(pixel % p.SW), &px);
-        const int gy = tile_of(p.tile_rows, p.TY, p.E0Y, int(pixel / p.SW), &py);
+        const int gx = tile_of(v.tile_cols, v.TX, v.E0X, int(pixel % v.SW), &px);
+        const int gy = tile_of(v.tile_rows, v.TY, v.E0Y, int(pixel / v.SW), &py);
         // render_grid (perpixel_renderer.cpp:27-36) + ThinLensCamera::sample_we
         const float fx = px + rng.u(), fy = py + rng.u();
-        const float film_x = fx / p.W, film_y = fy / p.H;
+        const float film_x = fx / v.W, film_y = fy / v.H;
         const float au = rng.u(), av = rng.u();
-        const Camera& cam = p.cam;
+        const Camera& cam = v.cam;
         const Vec3 focal((0.5f - film_x) * cam.film_w, (film_y - 0.5f) * cam.film_h, cam.focal);
         float dx, dy;
         concentric_disk(au, av, &dx, &dy);
@@ -302,7 +333,8 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
         P.gb_normal[slot] = make_float4(0, 0, 0, 0);
         uint4 st;
         st.x = uint32_t(pixel);
-        st.w = uint32_t(gy * p.TX + gx);  // the tile this sample splats into
+        // the view and tile this sample splats into
+        st.w = (uint32_t(vi) << kTileBits) | uint32_t(gy * v.TX + gx);
         store_rng(st, rng);
         P.st[slot] = st;
         P.ctr[slot] = make_int4(1, 1, 0, 0);
@@ -715,19 +747,24 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_shadow(S
     if (COUNT) flush_count(c->cnt_shadow, tc);
 }
 
-__device__ __forceinline__ float filter_eval(const Params& p, float x, float y) {
+__device__ __forceinline__ float filter_eval(const View& p, float x, float y) {
     if (p.filter_type == ATRC_FILTER_BOX) return p.filter_value;
     const float gx = fmaxf(0.0f, __expf(-p.filter_alpha * x * x) - p.filter_exp);
     const float gy = fmaxf(0.0f, __expf(-p.filter_alpha * y * y) - p.filter_exp);
     return gx * gy;
 }
 
-__global__ void k_finish(Params p, Pool P, Film F, Counters* c) {
+__global__ void k_finish(Params p, Pool P, Counters* c) {
     const int n = c->n_finish, fb = c->n_free;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = P.q_finish[i];
         const float4 L = P.L[slot];
         const float sx = L.w, sy = P.mis_f[slot].w;
+        const uint32_t vt = P.st[slot].w;
+        const int vi = int(vt >> kTileBits), tile = int(vt & ((1u << kTileBits) - 1u));
+        const View& v = p.views[vi];
+        const Film& F = v.film;
+        if (p.view_done) atomicAdd(p.view_done + vi, 1ull);
         if (p.gf.records) {
             // targets of the path's guide records: luminance of the radiance
             // gathered after each vertex over the throughput arriving at it,
@@ -750,10 +787,9 @@ __global__ void k_finish(Params p, Pool P, Film F, Counters* c) {
             const float4 ga = P.gb_albedo[slot], gn = P.gb_normal[slot];
             // apply_image_filter (framebuffer.h:49-80) over the sample's tile;
             // the distances step by one pixel from the tile-clamped start
-            const int tile = int(P.st[slot].w);
-            const int tx0 = (tile % p.TX) * p.G, ty0 = (tile / p.TX) * p.G;
-            const int tx1 = min(p.W, tx0 + p.G) - 1, ty1 = min(p.H, ty0 + p.G) - 1;
-            const float r = p.filter_radius;
+            const int tx0 = (tile % v.TX) * v.G, ty0 = (tile / v.TX) * v.G;
+            const int tx1 = min(v.W, tx0 + v.G) - 1, ty1 = min(v.H, ty0 + v.G) - 1;
+            const float r = v.filter_radius;
             const int x0 = max(tx0, int(ceilf(sx - r - 0.5f))), y0 = max(ty0, int(ceilf(sy - r - 0.5f)));
             const int x1 = min(tx1, int(floorf(sx + r - 0.5f))), y1 = min(ty1, int(floorf(sy + r - 0.5f)));
             float yrel = fabsf(y0 + 0.5f - sy);
@@ -762,8 +798,8 @@ __global__ void k_finish(Params p, Pool P, Film F, Counters* c) {
                 float xrel = fabsf(x0 + 0.5f - sx);
                 for (int x = x0; x <= x1; ++x, xrel += 1) {
                     if (xrel > r) continue;
-                    const double w = filter_eval(p, xrel, yrel);
-                    const size_t px = size_t(y) * p.W + x;
+                    const double w = filter_eval(v, xrel, yrel);
+                    const size_t px = size_t(y) * v.W + x;
                     atomicAdd(F.value + 3 * px, w * L.x);
                     atomicAdd(F.value + 3 * px + 1, w * L.y);
                     atomicAdd(F.value + 3 * px + 2, w * L.z);
@@ -849,6 +885,17 @@ struct DeviceSceneImpl {
     static constexpr int kWindow = 4;  // wavefront iterations between host checks
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, kev[kWindow * 4] = {};
     void* pinned_counters = nullptr;
+    DevBuf views_buf;                   // view table (+ per-view completion counters)
+    void* view_stage = nullptr;         // pinned copy of the completion counters
+    size_t view_stage_bytes = 0;
+    void ensure_view_stage(size_t bytes) {
+        if (view_stage_bytes >= bytes) return;
+        if (view_stage) cudaFreeHost(view_stage);
+        view_stage = nullptr;
+        view_stage_bytes = 0;
+        CK(cudaMallocHost(&view_stage, bytes));
+        view_stage_bytes = bytes;
+    }
     cudaGraphExec_t window_exec = nullptr;  // the captured bounce-loop window
     void* stage = nullptr;             // pinned host staging for host films
     size_t stage_bytes = 0;
@@ -888,6 +935,7 @@ struct DeviceSceneImpl {
         if (ev1) cudaEventDestroy(ev1);
         for (auto& e : kev) if (e) cudaEventDestroy(e);
         if (window_exec) cudaGraphExecDestroy(window_exec);
+        if (view_stage) cudaFreeHost(view_stage);
         if (pinned_counters) cudaFreeHost(pinned_counters);
         if (stage) cudaFreeHost(stage);
         if (stream) cudaStreamDestroy(stream);
@@ -981,16 +1029,24 @@ Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
     return P;
 }
 
+// Settings shared by the views of a render (taken from the first view).
 Params make_params(const AtrcRenderDesc& d) {
     Params p{};
-    p.W = d.width;
-    p.H = d.height;
-    p.first_spp = d.first_spp;
     p.min_depth = d.min_depth;
     p.max_depth = d.max_depth;
     p.specular_depth = d.specular_depth;
     p.cont_prob = d.cont_prob;
     p.eps = d.eps;
+    return p;
+}
+
+// One view: camera, film geometry, tiles and filter (count and start, tile
+// tables and film are filled in by the caller).
+View make_view(const AtrcRenderDesc& d) {
+    View p{};
+    p.W = d.width;
+    p.H = d.height;
+    p.first_spp = d.first_spp;
     p.seed = d.seed;
     // ThinLensCamera::init_from_params (thin_lens.cpp:34-55)
     const AtrcCameraDesc& c = d.camera;
@@ -1040,15 +1096,12 @@ Params make_params(const AtrcRenderDesc& d) {
     return p;
 }
 
-size_t tile_table_bytes(const Params& p) { return size_t(p.TX + p.TY + 2) * sizeof(int4); }
+size_t tile_table_bytes(const View& p) { return size_t(p.TX + p.TY + 2) * sizeof(int4); }
 
-// Point the params at a tile table and fill it on the stream.
-void setup_tiles(Params* p, void* table, cudaStream_t s) {
-    int4* cols = static_cast<int4*>(table);
-    int4* rows = cols + p->TX + 1;
-    p->tile_cols = cols;
-    p->tile_rows = rows;
-    k_tiles<<<1, 32, 0, s>>>(*p, cols, rows);
+// Point a view at its tile table (filled on the device by k_tiles).
+void set_tiles(View* v, void* table) {
+    v->tile_cols = static_cast<int4*>(table);
+    v->tile_rows = v->tile_cols + v->TX + 1;
 }
 
 }  // namespace
@@ -1180,10 +1233,17 @@ static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const
 // The wavefront render behind atrc_cuda_render (arguments already checked;
 // CUDA failures throw).  Launch shapes, path pool and sort mode left to
 // the library (path_pool 0, sort_mode AUTO) come from the scene's tuning.
-static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcFilm* film, volatile const int* cancel,
-                       AtrcProgressFn progress, void* user, AtrcRenderStats* stats, GuideImpl* guide = nullptr,
-                       bool record = false) {
+// `nviews` views share one path pool (a batch); descs[0] gives the settings
+// they share.  A single view may use a host film (staged on the device);
+// batches need device films.  view_seconds (optional, nviews entries)
+// receives the time from the start of the call at which each view's last
+// sample was splatted, observed at window granularity.
+static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const AtrcFilm* films, int nviews,
+                       volatile const int* cancel, AtrcProgressFn progress, void* user, AtrcRenderStats* stats,
+                       GuideImpl* guide = nullptr, bool record = false, double* view_seconds = nullptr) {
     const auto t_start = std::chrono::steady_clock::now();
+    const AtrcRenderDesc* desc = descs;
+    const AtrcFilm* film = films;
     DeviceSceneImpl& d = scene->impl;
     CK(cudaSetDevice(d.device));
     cudaStream_t s = d.stream;
@@ -1191,10 +1251,28 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
     d.scene.disney_fixed = desc->disney_fixed;
     Params p = make_params(*desc);
     d.resolve_sort(&p, desc->sort_mode);
-    if (d.tiles.bytes < tile_table_bytes(p)) d.tiles.alloc(tile_table_bytes(p));
-    setup_tiles(&p, d.tiles.p, s);
-    const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
-    const unsigned long long total = (unsigned long long)p.SW * p.SH * spp;
+    // views, their tile tables and sample ranges
+    std::vector<View> views(nviews);
+    size_t table_bytes = 0;
+    unsigned long long total = 0;
+    for (int v = 0; v < nviews; ++v) {
+        views[v] = make_view(descs[v]);
+        if (size_t(views[v].TX) * views[v].TY >= (size_t(1) << kTileBits))
+            throw std::runtime_error("film too large: more than 2^22 filter tiles");
+        table_bytes += (tile_table_bytes(views[v]) + 255) & ~size_t(255);
+        const int spp_v = descs[v].spp_count > 0 ? descs[v].spp_count : descs[v].spp;
+        views[v].start = total;
+        views[v].count = (unsigned long long)views[v].SW * views[v].SH * spp_v;
+        total += views[v].count;
+    }
+    if (d.tiles.bytes < table_bytes) d.tiles.alloc(table_bytes);
+    {
+        char* tb = d.tiles.as<char>();
+        for (int v = 0; v < nviews; ++v) {
+            set_tiles(&views[v], tb);
+            tb += (tile_table_bytes(views[v]) + 255) & ~size_t(255);
+        }
+    }
     // path pool: enough paths to fill the GPU; shadow capacity = pool x lights
     const int nl = std::max(1, d.scene.light_count);
     size_t cap = desc->path_pool > 0 ? size_t(desc->path_pool) : size_t(d.tuned_pool);
@@ -1215,12 +1293,16 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
     }
     Pool P = pool_from(d.pool_buf.p, L, shadow_cap);
     Counters* c = d.counters.as<Counters>();
-    // film
+    // films
     const size_t npix = size_t(desc->width) * desc->height;
-    Film F{};
     std::vector<std::pair<double*, size_t>> host_targets;
     DevBuf& local_film = d.film_buf;
     d.ensure_render_resources();
+    for (int v = 1; v < nviews; ++v) {
+        const AtrcFilm& f = films[v];
+        views[v].film = Film{f.value, f.weight, f.value_sq, f.albedo, f.normal, f.denoise};
+    }
+    Film& F = views[0].film;
     if (film->on_device) {
         F.value = film->value; F.weight = film->weight; F.value_sq = film->value_sq;
         F.albedo = film->albedo; F.normal = film->normal; F.denoise = film->denoise;
@@ -1237,6 +1319,19 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
         if (film->normal) { F.normal = b; b += npix * 3; host_targets.push_back({film->normal, npix * 3}); }
         if (film->denoise) { F.denoise = b; b += npix; host_targets.push_back({film->denoise, npix}); }
     }
+    // view table on the device (+ per-view completion counters of batches)
+    const size_t vbytes = nviews * sizeof(View), dbytes = nviews > 1 ? nviews * sizeof(unsigned long long) : 0;
+    if (d.views_buf.bytes < vbytes + dbytes) d.views_buf.alloc(vbytes + dbytes);
+    CK(cudaMemcpyAsync(d.views_buf.p, views.data(), vbytes, cudaMemcpyHostToDevice, s));
+    p.nviews = nviews;
+    p.views = d.views_buf.as<View>();
+    p.view_done = nullptr;
+    if (dbytes) {
+        p.view_done = reinterpret_cast<unsigned long long*>(d.views_buf.as<char>() + vbytes);
+        CK(cudaMemsetAsync(p.view_done, 0, dbytes, s));
+        d.ensure_view_stage(dbytes);
+    }
+    k_tiles<<<nviews, 32, 0, s>>>(p);
     const int gsm = grid_for(d.sm_count, d.tuned_gen_blocks);
     // one path / ray per thread for the heavy kernels (grids cover the
     // pool; threads past the device-side count return at once)
@@ -1244,6 +1339,8 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
     k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
     CK(cudaGetLastError());
     uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
+    std::vector<char> view_finished(nviews, 0);
+    int views_left = nviews;
     cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
     cudaEvent_t* kev = d.kev;
     const int window = DeviceSceneImpl::kWindow;
@@ -1283,10 +1380,11 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
             if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
             else k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
             CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
-            k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, F, c);
+            k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, c);
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+        if (dbytes) CK(cudaMemcpyAsync(d.view_stage, p.view_done, dbytes, cudaMemcpyDeviceToHost, s));
         cudaGraph_t g = cap.end();
         d.window_exec = instantiate_or_update(d.window_exec, g);
         cudaGraphDestroy(g);
@@ -1297,6 +1395,18 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcF
         ext_launches += window;
         CK(cudaStreamSynchronize(s));
         hc = *pinned;
+        if (view_seconds && views_left) {
+            const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+            const unsigned long long* done = static_cast<const unsigned long long*>(d.view_stage);
+            for (int v = 0; v < nviews; ++v) {
+                const bool fin = nviews == 1 ? hc.done != 0 || hc.completed >= total : done[v] >= views[v].count;
+                if (!view_finished[v] && fin) {
+                    view_finished[v] = 1;
+                    view_seconds[v] = now;
+                    --views_left;
+                }
+            }
+        }
         for (int k = 0; k < window; ++k) {
             float a = 0, b2 = 0, e3 = 0;
             CK(cudaEventElapsedTime(&a, kev[k * 4 + 0], kev[k * 4 + 1]));
@@ -1376,7 +1486,7 @@ int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* fil
                      AtrcProgressFn progress, void* user, AtrcRenderStats* stats) {
     const int rc = check_render_args(scene, desc, film);
     if (rc != ATRC_OK) return rc;
-    return guarded([&] { return render_impl(scene, desc, film, cancel, progress, user, stats); });
+    return guarded([&] { return render_impl(scene, desc, film, 1, cancel, progress, user, stats); });
 }
 
 int atrc_cuda_scene_bounds(AtrcScene* scene, float lo[3], float hi[3]) {
@@ -1394,7 +1504,30 @@ int atrc_cuda_render_guided(AtrcScene* scene, AtrcGuide* guide, const AtrcRender
     const int rc = check_render_args(scene, desc, film);
     if (rc != ATRC_OK) return rc;
     return guarded([&] {
-        return render_impl(scene, desc, film, nullptr, nullptr, nullptr, stats, guide_impl(guide), record != 0);
+        return render_impl(scene, desc, film, 1, nullptr, nullptr, nullptr, stats, guide_impl(guide), record != 0);
+    });
+}
+
+int atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide, const AtrcRenderDesc* views, int32_t n,
+                           const AtrcFilm* films, double* view_seconds, AtrcRenderStats* stats) {
+    if (!scene || !views || !films || n < 1) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_batch: null argument");
+    if (n > kMaxViews) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_batch: more than 1024 views");
+    const AtrcRenderDesc& a = views[0];
+    for (int v = 0; v < n; ++v) {
+        const int rc = check_render_args(scene, views + v, films + v);
+        if (rc != ATRC_OK) return rc;
+        if (!films[v].on_device)
+            return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_batch: every film must hold device pointers");
+        const AtrcRenderDesc& b = views[v];
+        if (b.min_depth != a.min_depth || b.max_depth != a.max_depth || b.cont_prob != a.cont_prob ||
+            b.specular_depth != a.specular_depth || b.eps != a.eps || b.sort_mode != a.sort_mode ||
+            b.disney_fixed != a.disney_fixed || b.path_pool != a.path_pool || b.count_traversal != a.count_traversal)
+            return fail(ATRC_ERR_INVALID_ARG,
+                        "atrc_cuda_render_batch: views must share depth, roulette, eps, sort, Disney and pool settings");
+    }
+    return guarded([&] {
+        return render_impl(scene, views, films, n, nullptr, nullptr, nullptr, stats, guide ? guide_impl(guide) : nullptr,
+                           false, view_seconds);
     });
 }
 
@@ -1473,7 +1606,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
             for (int rep = 0; rep < 2; ++rep) {
                 CK(cudaMemsetAsync(d.tune_film.p, 0, npix * 4 * sizeof(double), d.stream));
                 AtrcRenderStats st{};
-                const int r = render_impl(scene, &t, &film, nullptr, nullptr, nullptr, &st);
+                const int r = render_impl(scene, &t, &film, 1, nullptr, nullptr, nullptr, &st);
                 if (r != ATRC_OK) throw CudaError(std::string("autotune trial failed: ") + atrc_last_error());
                 best = std::min(best, st.kernel_seconds * 1e3 / (double(st.samples) / 1e6));
                 ++trials;
@@ -1586,15 +1719,19 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         void* scratch = noalloc_scratch(d.device);
         cudaStream_t s = d.stream;
         d.scene.eps = desc->eps;
-    d.scene.disney_fixed = desc->disney_fixed;
+        d.scene.disney_fixed = desc->disney_fixed;
         Params p = make_params(*desc);
         d.resolve_sort(&p, desc->sort_mode);
+        View view = make_view(*desc);
         const int spp = desc->spp_count > 0 ? desc->spp_count : desc->spp;
-        const unsigned long long total = (unsigned long long)p.SW * p.SH * spp;
+        view.start = 0;
+        view.count = (unsigned long long)view.SW * view.SH * spp;
+        const unsigned long long total = view.count;
         const int nl = std::max(1, d.scene.light_count);
-        // the array holds the counters, the tile tables, then the path pool
+        // the array holds the counters, the view, the tile tables, then the path pool
         const size_t counters_bytes = 512;
-        const size_t tiles_bytes = (tile_table_bytes(p) + 255) & ~size_t(255);
+        const size_t view_bytes = (sizeof(View) + 255) & ~size_t(255);
+        const size_t tiles_bytes = view_bytes + ((tile_table_bytes(view) + 255) & ~size_t(255));
         if (counters_bytes + tiles_bytes >= ATRC_NOALLOC_SCRATCH_BYTES / 2)
             return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: film too large for the static scratch");
         const size_t budget = ATRC_NOALLOC_SCRATCH_BYTES - counters_bytes - tiles_bytes;
@@ -1616,9 +1753,15 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         const PoolLayout L = pool_layout(cap, shadow_cap, p.nkeys);
         char* base = static_cast<char*>(scratch);
         Counters* c = reinterpret_cast<Counters*>(base);
-        setup_tiles(&p, base + counters_bytes, s);
+        set_tiles(&view, base + counters_bytes + view_bytes);
+        view.film = Film{film->value, film->weight, film->value_sq, film->albedo, film->normal, film->denoise};
+        View* dview = reinterpret_cast<View*>(base + counters_bytes);
+        CK(cudaMemcpyAsync(dview, &view, sizeof(View), cudaMemcpyHostToDevice, s));
+        p.nviews = 1;
+        p.views = dview;
+        p.view_done = nullptr;
+        k_tiles<<<1, 32, 0, s>>>(p);
         Pool P = pool_from(base + counters_bytes + tiles_bytes, L, shadow_cap);
-        Film F{film->value, film->weight, film->value_sq, film->albedo, film->normal, film->denoise};
         const int gsm = grid_for(d.sm_count, 16);
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
         // k_init rewrites the counters and the free list (all state that must
@@ -1640,7 +1783,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
                 }
                 k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
                 k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
-                k_finish<<<gsm, 128, 0, s>>>(p, P, F, c);
+                k_finish<<<gsm, 128, 0, s>>>(p, P, c);
                 launches += 6;
                 ext_launches += 1;
             }

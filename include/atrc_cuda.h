@@ -545,6 +545,18 @@ int  atrc_guide_train_records(AtrcGuide* guide, const float* records, size_t n,
 /* Copy out the records of the last recording render (24 floats each). */
 int  atrc_guide_records(AtrcGuide* guide, float* records, size_t cap, size_t* count);
 
+/* Batched multi-view render (no counterpart in the reference, which renders
+ * one camera per `rendering` entry): n views (camera, size, spp, seed,
+ * filter may differ; depth, roulette, eps, sort, Disney and pool settings
+ * must be equal) share one wavefront path pool, so small views fill the GPU
+ * together.  Films must hold device pointers.  `guide` may be NULL (plain)
+ * or a trained guide (sampling only).  view_seconds (may be NULL) receives
+ * per view the time from the start of the call at which its last sample was
+ * splatted.  At most 1024 views. */
+int  atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide,
+                            const AtrcRenderDesc* views, int32_t n,
+                            const AtrcFilm* films, double* view_seconds,
+                            AtrcRenderStats* stats);
 /* Scene bound (for atrc_guide_create). */
 int  atrc_cuda_scene_bounds(AtrcScene* scene, float lo[3], float hi[3]);
 /* atrc_cuda_render with the guide sampling surface vertices; record = 1
