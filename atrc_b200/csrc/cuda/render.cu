@@ -764,7 +764,10 @@ __global__ void k_finish(Params p, Pool P, Counters* c) {
         const int vi = int(vt >> kTileBits), tile = int(vt & ((1u << kTileBits) - 1u));
         const View& v = p.views[vi];
         const Film& F = v.film;
-        if (p.view_done) atomicAdd(p.view_done + vi, 1ull);
+        if (p.view_done) {  // one atomic per view present in the warp
+            const unsigned same = __match_any_sync(__activemask(), vi);
+            if (int(threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(p.view_done + vi, (unsigned long long)__popc(same));
+        }
         if (p.gf.records) {
             // targets of the path's guide records: luminance of the radiance
             // gathered after each vertex over the throughput arriving at it,

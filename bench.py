@@ -54,6 +54,10 @@ def parse():
     p.add_argument("--guided-max-s", type=float, default=30.0)
     p.add_argument("--guided-max-depth", type=int, default=-1, help="guide vertices up to this depth (-1: library default)")
     p.add_argument("--guided-train-steps", type=int, default=4)
+    p.add_argument("--no-batch", action="store_true", help="skip the batched multi-view comparison")
+    p.add_argument("--batch-views", type=int, default=64)
+    p.add_argument("--batch-spp-scale", type=float, default=1.0 / 64,
+                   help="scale of the [16, 1024] spp budgets (1/64 keeps the default run within minutes)")
     return p.parse_args()
 
 
@@ -235,6 +239,86 @@ def guided_comparison(args) -> dict:
             "time_ratio_guided_over_plain": (t_guided / t_plain) if (t_guided and t_plain) else None}
 
 
+def batch_views(cfg, n: int, seed: int, spp_scale: float):
+    """Seeded camera poses in the indoor room with resolutions drawn from
+    {128^2, 256^2, 512^2, 1024^2, 1920x1080} and spp drawn log-uniformly from
+    [16, 1024] (times spp_scale, at least 1)."""
+    rng = np.random.default_rng(seed)
+    sizes = [(128, 128), (256, 256), (512, 512), (1024, 1024), (1920, 1080)]
+    views = []
+    for _ in range(n):
+        d, _ = cfg.rendering(0)
+        d.width, d.height = sizes[int(rng.integers(0, len(sizes)))]
+        d.spp = max(1, int(round(np.exp(rng.uniform(np.log(16), np.log(1024))) * spp_scale)))
+        while True:  # a camera that looks at least 2 m away and not straight up or down
+            pos = rng.uniform([-8, -4, 1], [8, 4, 6])
+            dst = rng.uniform([-9, -5, 0.2], [9, 5, 7])
+            fwd = dst - pos
+            if np.linalg.norm(fwd) > 2 and abs(fwd[2]) < 0.9 * np.linalg.norm(fwd):
+                break
+        for k in range(3):
+            d.camera.pos[k], d.camera.dst[k] = float(pos[k]), float(dst[k])
+        d.camera.up[0], d.camera.up[1], d.camera.up[2] = 0.0, 0.0, 1.0
+        d.camera.fov = float(np.radians(rng.uniform(55, 80)))
+        d.seed = int(rng.integers(1, 2**31))
+        views.append(d)
+    return views
+
+
+def batch_comparison(args) -> dict:
+    """64 views of the indoor room in one batched launch with the
+    guided tracer (guide trained briefly first, then only sampled) against the
+    same views rendered one by one.  Aggregate Msamples/s and per-view
+    completion times."""
+    from atrc_b200 import Config, DeviceScene, Film, scenes
+    from atrc_b200.guide import Guide
+    cfg = Config.from_file(scenes.indoor_room())
+    dev = DeviceScene(cfg)
+    d0, _ = cfg.rendering(0)
+    tuning = dev.autotune(d0, trial_spp=1)
+    guide = Guide.for_scene(dev)
+    d0.spp_count = 1
+    for k in range(16):                       # a short training phase
+        d0.first_spp = k
+        f = Film(d0.width, d0.height, device=True)
+        dev.render_guided(guide, d0, f, record=True)
+        guide.train(steps=4)
+    q = lambda a: {"median_s": float(np.median(a)), "p90_s": float(np.quantile(a, 0.9)), "max_s": float(np.max(a))}  # noqa: E731
+
+    def compare(views):
+        samples = sum(v.width * v.height * v.spp for v in views)
+        films = [Film(v.width, v.height, device=True) for v in views]
+        dev.render_batch(views[:2], films[:2], guide=guide)       # warm-up (graph, buffers)
+        for f in films[:2]:
+            f.clear()
+        t0 = time.perf_counter()
+        st, secs = dev.render_batch(views, films, guide=guide)
+        t_batch = time.perf_counter() - t0
+        one_secs = []
+        t0 = time.perf_counter()
+        for v, f in zip(views, films):
+            f.clear()
+            dev.render_guided(guide, v, f)
+            one_secs.append(time.perf_counter() - t0)
+        t_one = one_secs[-1]
+        return {"views": len(views), "samples": samples,
+                "resolutions": sorted({f"{v.width}x{v.height}" for v in views}),
+                "spp_range": [min(v.spp for v in views), max(v.spp for v in views)],
+                "batched": {"seconds": t_batch, "Msamples_per_s": samples / t_batch / 1e6, "completion": q(secs)},
+                "one_by_one": {"seconds": t_one, "Msamples_per_s": samples / t_one / 1e6, "completion": q(one_secs)},
+                "speedup": t_one / t_batch}
+    full = compare(batch_views(cfg, args.batch_views, 1004, args.batch_spp_scale))
+    # the regime batching is for: many small views that cannot fill the GPU alone
+    small = batch_views(cfg, args.batch_views, 1005, 1.0 / 64)
+    for v in small:
+        v.width = v.height = 128 if v.width < 1024 else 256
+    small_r = compare(small)
+    return {"workload": f"indoor_room_{args.batch_views}_views", "spp_scale": args.batch_spp_scale,
+            "tuning": {k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
+                                              "finish_threads")},
+            **full, "small_views": small_r}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -337,6 +421,7 @@ def main():
     if rank == 0:
         cpu = cpu_baseline(args) if world == 1 and not args.no_cpu_baseline else None
         guided = guided_comparison(args) if world == 1 and not args.no_guided else None
+        batch = batch_comparison(args) if world == 1 and not args.no_batch else None
         clocks = clk.summary()
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -366,6 +451,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "guided": guided,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     if dist:
