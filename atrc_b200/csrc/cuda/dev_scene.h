@@ -112,7 +112,7 @@ struct Env {
 };
 
 struct Scene {
-    const BvhNode* nodes;           // all BVH nodes (TLAS + every BLAS)
+    const Bvh4Node* nodes;          // all 4-wide BVH nodes (every BLAS + the TLAS)
     const float* tris;              // 12 floats per triangle: A,_, B-A,_, C-A,_
     const TriShade* tri_shade;
     const uint32_t* tri_orig;       // original index per pool triangle

@@ -39,6 +39,7 @@ static_assert(kStackRing == 0 || (kStackRing & (kStackRing - 1)) == 0, "ring siz
 static_assert(kStackRing < kStackSize, "ring must be smaller than the stack");
 constexpr int32_t kSentinel = INT_MIN;      // "return from a bottom-level tree"
 constexpr int32_t kDone = INT_MIN + 1;      // empty stack
+constexpr int kMaxTraversalSteps = 1 << 20; // node + leaf visits per ray before the watchdog trips
 
 struct Hit {
     float t;
@@ -53,27 +54,6 @@ struct RayState {
 };
 
 __device__ __forceinline__ Vec3 safe_inv(Vec3 d) { return Vec3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z); }
-
-// Slab test of two child boxes.  The far distance is widened by a few ulps
-// so that float rounding cannot cull a box that a primitive test would hit.
-__device__ __forceinline__ void box2(const float4& n0, const float4& n1, const float4& n2, const RayState& r,
-                                     bool* h0, float* t0, bool* h1, float* t1) {
-    const float ox = r.o.x * r.inv.x, oy = r.o.y * r.inv.y, oz = r.o.z * r.inv.z;
-    float a0 = fmaf(n0.x, r.inv.x, -ox), b0 = fmaf(n0.y, r.inv.x, -ox);
-    float a1 = fmaf(n0.z, r.inv.y, -oy), b1 = fmaf(n0.w, r.inv.y, -oy);
-    float a2 = fmaf(n2.x, r.inv.z, -oz), b2 = fmaf(n2.y, r.inv.z, -oz);
-    float lo = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), r.tmin));
-    float hi = fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fminf(fmaxf(a2, b2), r.tmax));
-    *h0 = lo <= hi * 1.0000005f + 1e-30f;
-    *t0 = lo;
-    a0 = fmaf(n1.x, r.inv.x, -ox); b0 = fmaf(n1.y, r.inv.x, -ox);
-    a1 = fmaf(n1.z, r.inv.y, -oy); b1 = fmaf(n1.w, r.inv.y, -oy);
-    a2 = fmaf(n2.z, r.inv.z, -oz); b2 = fmaf(n2.w, r.inv.z, -oz);
-    lo = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), r.tmin));
-    hi = fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fminf(fmaxf(a2, b2), r.tmax));
-    *h1 = lo <= hi * 1.0000005f + 1e-30f;
-    *t1 = lo;
-}
 
 // Moller-Trumbore.  ANY selects has_intersection_with_triangle (alpha <= 1
 // also checked), otherwise closest_intersection_with_triangle.
@@ -149,14 +129,42 @@ __device__ __forceinline__ bool disk_test(const RayState& r, float radius, float
     return true;
 }
 
-__device__ __forceinline__ void load_node(const BvhNode* nodes, int32_t i, float4* n0, float4* n1, float4* n2,
-                                          int2* links) {
-    const float4* p = reinterpret_cast<const float4*>(nodes + i);
-    *n0 = __ldg(p);
-    *n1 = __ldg(p + 1);
-    *n2 = __ldg(p + 2);
-    const float4 n3 = __ldg(p + 3);
-    *links = make_int2(__float_as_int(n3.x), __float_as_int(n3.y));
+// Slab test of the four children of a wide node (seven 128-bit loads):
+// t[k] = entry distance of child k, +inf when it is missed or the slot is
+// empty.  Boxes are widened by 1.0000005 as in the binary test, so a box
+// that touches the ray in exact arithmetic is never culled.
+__device__ __forceinline__ void box4(const Bvh4Node* node, const RayState& r, float* t, int32_t* l) {
+    const float4* p = reinterpret_cast<const float4*>(node);
+    const float4 lx = __ldg(p), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3);
+    const float4 lz = __ldg(p + 4), hz = __ldg(p + 5);
+    const int4 lk = __ldg(reinterpret_cast<const int4*>(p + 6));
+    const float ox = r.o.x * r.inv.x, oy = r.o.y * r.inv.y, oz = r.o.z * r.inv.z;
+    const float alx[4] = {lx.x, lx.y, lx.z, lx.w}, ahx[4] = {hx.x, hx.y, hx.z, hx.w};
+    const float aly[4] = {ly.x, ly.y, ly.z, ly.w}, ahy[4] = {hy.x, hy.y, hy.z, hy.w};
+    const float alz[4] = {lz.x, lz.y, lz.z, lz.w}, ahz[4] = {hz.x, hz.y, hz.z, hz.w};
+    const int32_t al[4] = {lk.x, lk.y, lk.z, lk.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float a0 = fmaf(alx[k], r.inv.x, -ox), b0 = fmaf(ahx[k], r.inv.x, -ox);
+        const float a1 = fmaf(aly[k], r.inv.y, -oy), b1 = fmaf(ahy[k], r.inv.y, -oy);
+        const float a2 = fmaf(alz[k], r.inv.z, -oz), b2 = fmaf(ahz[k], r.inv.z, -oz);
+        const float lo = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), r.tmin));
+        const float hi = fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fminf(fmaxf(a2, b2), r.tmax));
+        const bool hit = al[k] != kEmptyLink && lo <= hi * 1.0000005f + 1e-30f;
+        t[k] = hit ? lo : INFINITY;
+        l[k] = al[k];
+    }
+}
+
+// Sort four (distance, link) pairs by distance (five compare-exchanges).
+__device__ __forceinline__ void sort4(float* t, int32_t* l) {
+    auto cx = [&](int a, int b) {
+        if (t[b] < t[a]) {
+            const float tt = t[a]; t[a] = t[b]; t[b] = tt;
+            const int32_t ll = l[a]; l[a] = l[b]; l[b] = ll;
+        }
+    };
+    cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
 }
 
 // Move a world ray into an entity's primitive space (wrapper, then the
@@ -295,26 +303,25 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
         return next;
     };
 
+    int steps = 0;
     for (;;) {
         // descend interior nodes, parking the first leaf found
         while (link >= 0) {
-            float4 n0, n1, n2;
-            int2 lk;
-            load_node(S.nodes, link, &n0, &n1, &n2, &lk);
+            if (++steps > kMaxTraversalSteps) { overflow = true; break; }
             if (COUNT) cnt->nodes++;
-            bool h0, h1;
-            float t0, t1;
-            box2(n0, n1, n2, r, &h0, &t0, &h1, &t1);
-            if (h0 && h1) {
-                const bool c0_first = t0 <= t1;
-                push(c0_first ? lk.y : lk.x);
-                link = c0_first ? lk.x : lk.y;
-            } else if (h0) {
-                link = lk.x;
-            } else if (h1) {
-                link = lk.y;
-            } else {
+            // four children: entry distances (+inf when missed or empty),
+            // sorted near to far; the far ones go on the stack
+            float tc[4];
+            int32_t lc[4];
+            box4(S.nodes + link, r, tc, lc);
+            sort4(tc, lc);
+            if (tc[0] == INFINITY) {
                 link = pop();
+            } else {
+                if (tc[3] != INFINITY) push(lc[3]);
+                if (tc[2] != INFINITY) push(lc[2]);
+                if (tc[1] != INFINITY) push(lc[1]);
+                link = lc[0];
             }
             if (link < 0 && link != kSentinel && link != kDone && held == 0) {
                 held = link;
@@ -332,6 +339,7 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
         }
         while (link < 0) {
             if (link == kDone) break;
+            if (++steps > kMaxTraversalSteps) { overflow = true; break; }
             if (link == kSentinel) {
                 cur_entity = -1;
                 r.o = wo; r.d = wd; r.inv = winv;

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <future>
@@ -186,6 +187,111 @@ BvhResult build_bvh(const std::vector<BuildPrim>& prims, int max_leaf, float tra
     res.max_depth = b.max_depth.load();
     for (int k = 0; k < 3; ++k) { res.bound_lo[k] = box.lo[k]; res.bound_hi[k] = box.hi[k]; }
     return res;
+}
+
+int32_t collapse_bvh4(const BvhResult& b, std::vector<Bvh4Node>* out) {
+    if (b.root_link < 0) return b.root_link;  // a single leaf
+    struct Child {
+        int32_t link;  // binary-tree link (node index or leaf)
+        float lo[3], hi[3];
+        float area() const {
+            const float dx = std::max(0.0f, hi[0] - lo[0]), dy = std::max(0.0f, hi[1] - lo[1]),
+                        dz = std::max(0.0f, hi[2] - lo[2]);
+            return dx * dy + dy * dz + dz * dx;
+        }
+    };
+    auto children_of = [&](int32_t n, Child* c) {
+        const BvhNode& nd = b.nodes[size_t(n)];
+        c[0] = Child{nd.link0, {nd.c0lo_x, nd.c0lo_y, nd.c0lo_z}, {nd.c0hi_x, nd.c0hi_y, nd.c0hi_z}};
+        c[1] = Child{nd.link1, {nd.c1lo_x, nd.c1lo_y, nd.c1lo_z}, {nd.c1hi_x, nd.c1hi_y, nd.c1hi_z}};
+    };
+    // iterative depth-first build: (binary node, wide parent and slot to patch)
+    struct Pending {
+        int32_t bin;
+        size_t parent;
+        int slot;
+    };
+    std::vector<Pending> stack;
+    out->reserve(out->size() + b.nodes.size() / 2 + 1);
+    const size_t root = out->size();
+    stack.push_back({0, SIZE_MAX, 0});
+    while (!stack.empty()) {
+        const Pending pd = stack.back();
+        stack.pop_back();
+        Child kids[4];
+        int n = 2;
+        children_of(pd.bin, kids);
+        while (n < 4) {  // open the widest interior child
+            int best = -1;
+            float best_a = -1.0f;
+            for (int k = 0; k < n; ++k)
+                if (kids[k].link >= 0 && kids[k].area() > best_a) { best_a = kids[k].area(); best = k; }
+            if (best < 0) break;
+            Child two[2];
+            children_of(kids[best].link, two);
+            kids[best] = two[0];
+            kids[n++] = two[1];
+        }
+        const size_t me = out->size();
+        out->push_back(Bvh4Node{});
+        if (pd.parent != SIZE_MAX) (*out)[pd.parent].link[pd.slot] = int32_t(me);
+        Bvh4Node& w = (*out)[me];
+        for (int k = 0; k < 4; ++k) {
+            if (k < n) {
+                w.lo_x[k] = kids[k].lo[0]; w.hi_x[k] = kids[k].hi[0];
+                w.lo_y[k] = kids[k].lo[1]; w.hi_y[k] = kids[k].hi[1];
+                w.lo_z[k] = kids[k].lo[2]; w.hi_z[k] = kids[k].hi[2];
+                w.link[k] = kids[k].link;  // leaves keep their encoding; interior links patched below
+            } else {
+                w.lo_x[k] = w.lo_y[k] = w.lo_z[k] = 1.0f;
+                w.hi_x[k] = w.hi_y[k] = w.hi_z[k] = -1.0f;
+                w.link[k] = kEmptyLink;
+            }
+            w.pad[k] = 0;
+        }
+        for (int k = n - 1; k >= 0; --k)
+            if (kids[k].link >= 0) stack.push_back({kids[k].link, me, k});
+    }
+    return int32_t(root);
+}
+
+void validate_bvh4(const std::vector<Bvh4Node>& nodes, int32_t root, uint32_t prim_first, uint32_t prim_count) {
+    std::vector<uint8_t> covered(prim_count, 0);
+    std::vector<uint8_t> seen;
+    std::vector<int32_t> stack{root};
+    size_t visits = 0;
+    auto leaf = [&](int32_t link) {
+        const uint32_t enc = uint32_t(~link);
+        const uint32_t first = enc >> 4, count = (enc & 15) + 1;
+        if (first < prim_first || first - prim_first + count > prim_count)
+            throw std::runtime_error("BVH leaf outside its primitive range");
+        for (uint32_t k = 0; k < count; ++k) {
+            if (covered[first - prim_first + k]) throw std::runtime_error("BVH primitive in two leaves");
+            covered[first - prim_first + k] = 1;
+        }
+    };
+    while (!stack.empty()) {
+        const int32_t l = stack.back();
+        stack.pop_back();
+        if (l == kEmptyLink) continue;
+        if (l < 0) {
+            leaf(l);
+            continue;
+        }
+        if (size_t(l) >= nodes.size()) throw std::runtime_error("BVH node link out of range");
+        if (seen.size() < nodes.size()) seen.resize(nodes.size(), 0);
+        if (seen[size_t(l)]) throw std::runtime_error("BVH node reached twice");
+        seen[size_t(l)] = 1;
+        if (++visits > nodes.size()) throw std::runtime_error("BVH has a cycle");
+        bool any = false;
+        for (int k = 0; k < 4; ++k) {
+            if (nodes[size_t(l)].link[k] != kEmptyLink) any = true;
+            stack.push_back(nodes[size_t(l)].link[k]);
+        }
+        if (!any) throw std::runtime_error("BVH node without children");
+    }
+    for (uint32_t k = 0; k < prim_count; ++k)
+        if (!covered[k]) throw std::runtime_error("BVH primitive in no leaf");
 }
 
 }  // namespace atrc

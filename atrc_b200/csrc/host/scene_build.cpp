@@ -264,19 +264,17 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs) {
         // bottom-level BVH over this leaf's triangles
         BvhResult bvh = build_bvh(prims, 4);
         hs->max_blas_depth = std::max(hs->max_blas_depth, bvh.max_depth);
-        const int32_t node_off = int32_t(hs->nodes.size());
         const int32_t tri_off = int32_t(hs->tri_shade.size());
-        auto fix = [&](int32_t link) -> int32_t {
-            if (link >= 0) return link + node_off;
+        auto fix_leaf = [&](int32_t link) -> int32_t {
+            if (link >= 0 || link == kEmptyLink) return link;
             uint32_t enc = uint32_t(~link);
             return leaf_link((enc >> 4) + uint32_t(tri_off), (enc & 15) + 1);
         };
-        for (BvhNode nd : bvh.nodes) {
-            nd.link0 = fix(nd.link0);
-            nd.link1 = fix(nd.link1);
-            hs->nodes.push_back(nd);
-        }
-        L.root = fix(bvh.root_link);
+        const size_t first_node = hs->nodes.size();
+        L.root = fix_leaf(collapse_bvh4(bvh, &hs->nodes));
+        for (size_t k = first_node; k < hs->nodes.size(); ++k)
+            for (int32_t& l : hs->nodes[k].link) l = fix_leaf(l);
+        validate_bvh4(hs->nodes, L.root, uint32_t(tri_off), uint32_t(prims.size()));
         L.tri_first = tri_off;
         L.tri_count = int32_t(prims.size());
         if (g.type == ATRC_GEOM_TRIANGLE_BVH) {
@@ -375,14 +373,8 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs) {
         }
         BvhResult tl = build_bvh(eprims, 1);  // one entity per top-level leaf
         hs->tlas_depth = tl.max_depth;
-        const int32_t node_off = int32_t(hs->nodes.size());
-        auto fix = [&](int32_t link) -> int32_t { return link >= 0 ? link + node_off : link; };
-        for (BvhNode nd : tl.nodes) {
-            nd.link0 = fix(nd.link0);
-            nd.link1 = fix(nd.link1);
-            hs->nodes.push_back(nd);
-        }
-        hs->scene.tlas_root = fix(tl.root_link);
+        hs->scene.tlas_root = collapse_bvh4(tl, &hs->nodes);
+        validate_bvh4(hs->nodes, hs->scene.tlas_root, 0, uint32_t(d.entity_count));
         hs->tlas_order = tl.order;
     } else {
         hs->scene.tlas_root = 0;

@@ -13,7 +13,7 @@
 namespace atrc {
 
 struct HostScene {
-    std::vector<BvhNode> nodes;
+    std::vector<Bvh4Node> nodes;  // every 4-wide node (each BLAS, then the TLAS)
     std::vector<float> tris;          // 12 per triangle
     std::vector<dev::TriShade> tri_shade;
     std::vector<uint32_t> tri_orig;

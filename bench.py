@@ -411,7 +411,7 @@ def main():
     nodes_per_ray = cstats["nodes_closest"] / crays
     tris_per_ray = cstats["tris_closest"] / crays
     ents_per_ray = cstats["ents_closest"] / crays
-    bytes_per_ray = nodes_per_ray * 64 + tris_per_ray * 48 + ents_per_ray * 64 + 56
+    bytes_per_ray = nodes_per_ray * 112 + tris_per_ray * 48 + ents_per_ray * 64 + 56
     achieved = bytes_per_ray * rays_closest / max(ext_time, 1e-9) / 1e9
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
