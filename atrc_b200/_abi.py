@@ -165,6 +165,12 @@ PROTOTYPES = {
     "atrc_cuda_render_noalloc": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
                                            C.POINTER(AtrcRenderStats)]),
     "atrc_film_resolve": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, c_float_p]),
+    "atrc_save_png_bytes": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int]),
+    "atrc_cuda_film_resolve": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "atrc_cuda_post_apply": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int32, C.c_float]),
+    "atrc_cuda_encode_ldr": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    "atrc_cuda_post_process": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p,
+                                         C.c_size_t]),
     "atrc_cuda_autotune": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32, C.POINTER(AtrcTuning)]),
     "atrc_cuda_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(AtrcTuning)]),
     "atrc_guide_default_desc": (C.c_int, [C.POINTER(AtrcGuideDesc)]),

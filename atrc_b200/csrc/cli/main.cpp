@@ -34,57 +34,6 @@ bool check(int rc, const char* what) {
     return false;
 }
 
-std::string replace_all(std::string s, const std::string& a, const std::string& b) {
-    size_t p;
-    while ((p = s.find(a)) != std::string::npos) s.replace(p, a.size(), b);
-    return s;
-}
-
-// minimal reader for the post-processor list the library re-serialises:
-// an array of flat objects whose values are strings
-std::vector<std::vector<std::pair<std::string, std::string>>> parse_post(const std::string& j) {
-    std::vector<std::vector<std::pair<std::string, std::string>>> out;
-    size_t i = 0;
-    auto str = [&](std::string* s) {
-        while (i < j.size() && j[i] != '"') ++i;
-        ++i;
-        s->clear();
-        while (i < j.size() && j[i] != '"') {
-            if (j[i] == '\\' && i + 1 < j.size()) ++i;
-            *s += j[i++];
-        }
-        ++i;
-    };
-    while (i < j.size()) {
-        if (j[i] == '{') {
-            ++i;
-            std::vector<std::pair<std::string, std::string>> obj;
-            while (i < j.size() && j[i] != '}') {
-                if (j[i] == '"') {
-                    std::string k, v;
-                    str(&k);
-                    while (i < j.size() && j[i] != ':') ++i;
-                    ++i;
-                    if (i < j.size() && j[i] == '"') str(&v);
-                    else while (i < j.size() && j[i] != ',' && j[i] != '}') ++i;
-                    obj.push_back({k, v});
-                } else {
-                    ++i;
-                }
-            }
-            out.push_back(obj);
-        }
-        ++i;
-    }
-    return out;
-}
-
-std::string get(const std::vector<std::pair<std::string, std::string>>& o, const std::string& k, const std::string& d = "") {
-    for (auto& kv : o)
-        if (kv.first == k) return kv.second;
-    return d;
-}
-
 void progress(double pct, void*) {
     std::printf("\r  %.1f%%", pct);
     std::fflush(stdout);
@@ -152,32 +101,18 @@ int main(int argc, char** argv) {
         if (!quiet)
             std::printf("\n  %.3f s, %.1f Msamples/s, %.1f Mrays/s\n", st.seconds, st.samples / st.seconds / 1e6,
                         (st.rays_closest + st.rays_shadow) / st.seconds / 1e6);
-        std::vector<float> rgb(np * 3);
-        atrc_film_resolve(&film, desc.width, desc.height, rgb.data());
+        // the rendering's post processors, on the device, in order
         size_t need = 0;
         atrc_config_post_processors(cfg, r, nullptr, 0, &need);
         std::string pj(need, '\0');
         atrc_config_post_processors(cfg, r, pj.data(), need, nullptr);
-        for (auto& pp : parse_post(pj)) {
-            const std::string t = get(pp, "type");
-            if (t.size() >= 2 && t.compare(t.size() - 2, 2, "//") == 0) continue;
-            if (t == "save_to_img") {
-                // SaveToImageCreator (post_processor_creators.cpp:115-150)
-                std::string fn = replace_all(replace_all(get(pp, "filename"), "${scene-directory}", scene_dir),
-                                             "${working-directory}", std::filesystem::current_path().string());
-                float gamma = 1;
-                if (!get(pp, "gamma").empty()) gamma = std::stof(get(pp, "gamma"));
-                else if (!get(pp, "inv_gamma").empty()) gamma = 1 / std::stof(get(pp, "inv_gamma"));
-                std::filesystem::create_directories(std::filesystem::absolute(fn).parent_path());
-                const std::string ext = get(pp, "ext");
-                if (check(atrc_save_image(fn.c_str(), ext.empty() ? nullptr : ext.c_str(), rgb.data(), desc.width,
-                                          desc.height, gamma),
-                          "saving the image") && !quiet)
-                    std::printf("  saved %s\n", fn.c_str());
-            } else if (!quiet) {
-                std::printf("  post processor `%s` is not part of pt_cuda; skipped\n", t.c_str());
-            }
-        }
+        std::vector<char> log(4096, 0);
+        if (!check(atrc_cuda_post_process(&film, desc.width, desc.height, pj.c_str(), scene_dir.c_str(), log.data(),
+                                          log.size()),
+                   "post processing"))
+            rc_all = 1;
+        else if (!quiet)
+            std::printf("%s", log.data());
     }
     atrc_cuda_scene_destroy(scene);
     atrc_config_destroy(cfg);

@@ -144,6 +144,17 @@ int atrc_save_image(const char* filename, const char* ext, const float* rgb, int
     });
 }
 
+int atrc_save_png_bytes(const char* filename, const uint8_t* rgb8, int width, int height) {
+    if (!filename || !rgb8 || width <= 0 || height <= 0) {
+        set_last_error("atrc_save_png_bytes: invalid argument");
+        return ATRC_ERR_INVALID_ARG;
+    }
+    return guarded_host([&] {
+        atrc::write_png_bytes(filename, rgb8, width, height);
+        return int(ATRC_OK);
+    });
+}
+
 int atrc_film_resolve(const AtrcFilm* film, int width, int height, float* rgb) {
     if (!film || !film->value || !film->weight || !rgb || width <= 0 || height <= 0) {
         set_last_error("atrc_film_resolve: invalid argument");

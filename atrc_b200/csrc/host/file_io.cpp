@@ -226,20 +226,28 @@ void save_pfm(const std::string& fn, const float* rgb, int w, int h) {
 }
 
 void save_png8(const std::string& fn, const float* rgb, int w, int h, float gamma) {
-    // 8-bit RGB PNG with stored (uncompressed) deflate blocks.  Texels map as
-    // uint8(clamp(c^gamma, 0, 1) * 255), rows written top to bottom
-    // (save_to_img.cpp:36-49 flips the film vertically).
-    std::vector<uint8_t> raw;
-    raw.reserve(size_t(h) * (size_t(w) * 3 + 1));
+    // Texels map as uint8(clamp(c^gamma, 0, 1) * 255), rows written top to
+    // bottom (save_to_img.cpp:36-49 flips the film vertically).
+    std::vector<uint8_t> bytes(size_t(w) * h * 3);
     for (int y = 0; y < h; ++y) {
-        raw.push_back(0);
         const int src = h - 1 - y;
         for (int x = 0; x < w * 3; ++x) {
             float v = std::pow(rgb[size_t(src) * w * 3 + x], gamma);
             v = std::fmin(std::fmax(v, 0.0f), 1.0f);
             if (!(v == v)) v = 0;
-            raw.push_back(uint8_t(v * 255.0f));
+            bytes[size_t(y) * w * 3 + x] = uint8_t(v * 255.0f);
         }
+    }
+    write_png_bytes(fn, bytes.data(), w, h);
+}
+
+void write_png_bytes(const std::string& fn, const uint8_t* rgb8, int w, int h) {
+    // 8-bit RGB PNG with stored (uncompressed) deflate blocks, rows as given
+    std::vector<uint8_t> raw;
+    raw.reserve(size_t(h) * (size_t(w) * 3 + 1));
+    for (int y = 0; y < h; ++y) {
+        raw.push_back(0);
+        raw.insert(raw.end(), rgb8 + size_t(y) * w * 3, rgb8 + size_t(y + 1) * w * 3);
     }
     std::vector<uint8_t> z = {0x78, 0x01};
     size_t off = 0;

@@ -54,6 +54,8 @@ std::vector<float> load_triangle_mesh(const std::string& filename);
 // Writers used by the CLI's post processors; `rgb` is a film (row 0 = bottom).
 void save_pfm(const std::string& filename, const float* rgb, int w, int h);
 void save_png8(const std::string& filename, const float* rgb, int w, int h, float gamma);
+// 8-bit rows top to bottom.
+void write_png_bytes(const std::string& filename, const uint8_t* rgb8, int w, int h);
 void save_hdr_rgbe(const std::string& filename, const float* rgb, int w, int h);
 
 }  // namespace atrc

@@ -479,6 +479,36 @@ int atrc_save_image(const char* filename, const char* ext, const float* rgb,
  * weight == 0); host pointers. */
 int atrc_film_resolve(const AtrcFilm* film, int width, int height, float* rgb);
 
+/* Write 8-bit RGB (rows top to bottom, as atrc_cuda_encode_ldr produces)
+ * as a PNG file. */
+int atrc_save_png_bytes(const char* filename, const uint8_t* rgb8, int width, int height);
+
+/* ---- the output path on the device (the post_processor directory) ------ */
+typedef enum AtrcPostType {
+    ATRC_POST_GAMMA = 0,            /* c^value (gamma.cpp:19-31)              */
+    ATRC_POST_ACES = 1,             /* ACES curve of c * value (aces.cpp)     */
+    ATRC_POST_NORMAL_TO_COLOR = 2   /* (c + 1) / 2 (save_gbuffer.cpp:21-33)   */
+} AtrcPostType;
+
+/* value / weight (and albedo / weight, normal / weight when both pointers
+ * are given) of a device film into device images (3 floats per pixel, row 0
+ * = bottom of the picture, perpixel_renderer.cpp:180-191). */
+int atrc_cuda_film_resolve(const AtrcFilm* film, int width, int height,
+                           float* rgb, float* albedo, float* normal);
+/* One post-processing step on a device image, in place. */
+int atrc_cuda_post_apply(float* rgb, int width, int height, int32_t type, float value);
+/* The 8-bit encoding of save_to_img / save_gbuffer_to_png on the device:
+ * flipped vertically, uint8(clamp(c^gamma, 0, 1) * 255). */
+int atrc_cuda_encode_ldr(const float* rgb, int width, int height, float gamma, uint8_t* out);
+/* Run a rendering's post-processor list (the JSON array returned by
+ * atrc_config_post_processors) on a film (host or device): `gamma`, `aces`,
+ * `save_to_img` (png, hdr, pfm) and `save_gbuffer_to_png` on the device and
+ * in the listed order; `resize` and `oidn_denoiser` (third-party libraries)
+ * are skipped.  ${scene-directory} maps to scene_dir.  `log` (may be NULL)
+ * receives one line per file saved or step skipped. */
+int atrc_cuda_post_process(const AtrcFilm* film, int width, int height, const char* post_json,
+                           const char* scene_dir, char* log, size_t log_cap);
+
 /* ------------------------------------------------------------------------
  * Learned path guiding (no counterpart in the reference, whose `pt` samples
  * the BSDF only, path_tracing.cpp:150-169).  A guide is a small network --
