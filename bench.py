@@ -161,6 +161,13 @@ def reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes per closest ray of k_extend on the instanced workload, from one
+# ncu capture of every k_extend launch of a 2-spp step (dram__bytes_read.sum +
+# dram__bytes_write.sum over the launches / the step's closest rays); the
+# command and the figures are in profiles/k_extend_instanced_1080p_wide_bvh.md.
+K_EXTEND_DRAM_BYTES_PER_RAY = 248.1
+
+
 def cpu_baseline(args) -> dict:
     """Timed run of the oracle on all host cores: whole-film 1 spp passes of the
     same workload, repeated until at least 10 s of CPU work (at most 30 s)."""
@@ -439,7 +446,10 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                         "traffic": None, "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray,
+                         "traffic": (K_EXTEND_DRAM_BYTES_PER_RAY * rays_closest / max(ext_launches, 1)
+                                     if args.scene == "instanced" else None),
+                         "traffic_source": "ncu DRAM bytes per closest ray x closest rays per launch",
+                         "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray,
                          "tris_per_ray": tris_per_ray, "entities_per_ray": ents_per_ray,
                          "avg_launch_ms": ext_time / max(ext_launches, 1) * 1e3},
             "kernel_time_share": {"extend": ext_time / elapsed, "shade": shade_time / elapsed,
