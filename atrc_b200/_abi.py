@@ -34,7 +34,8 @@ class AtrcEntityDesc(C.Structure):
 class AtrcTexture2DDesc(C.Structure):
     _fields_ = [("type", C.c_int32), ("texel", C.c_float * 3), ("width", C.c_int32), ("height", C.c_int32),
                 ("data", c_float_p), ("nearest", C.c_int32), ("uv_transform", C.c_float * 6),
-                ("wrap_u", C.c_int32), ("wrap_v", C.c_int32), ("inv_gamma", C.c_float), ("pad_", C.c_int32)]
+                ("wrap_u", C.c_int32), ("wrap_v", C.c_int32), ("inv_gamma", C.c_float), ("grid_count", C.c_int32),
+                ("texel2", C.c_float * 3), ("pad_", C.c_int32)]
 
 
 class AtrcTexture3DDesc(C.Structure):

@@ -85,7 +85,7 @@ def build_library(verbose_ptxas: bool = False) -> Path:
     LIB.parent.mkdir(parents=True, exist_ok=True)
     if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
-        _run([NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"])
+        _run([NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread", "-lz"])
         os.replace(tmp, LIB)
     return LIB
 

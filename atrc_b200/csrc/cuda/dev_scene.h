@@ -60,6 +60,8 @@ struct Texture2D {
     int32_t type, width, height, nearest;
     float texel[3];
     float inv_gamma;
+    float texel2[3];         // checker board: second colour
+    float grid_size;         // checker board: 1 / grid_count
     float uv[6];
     int32_t wrap_u, wrap_v;
     int64_t data_offset;     // float offset into the texel pool

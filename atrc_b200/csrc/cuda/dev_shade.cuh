@@ -50,7 +50,10 @@ __device__ Vec3 tex2d_sample(const Scene& S, int ti, float u0, float v0) {
     const float u = wrap_coord(t.wrap_u, tu), v = wrap_coord(t.wrap_v, tv);
     const float* base = S.texels + t.data_offset;
     Vec3 r;
-    if (t.nearest) {
+    if (t.type == ATRC_TEX_CHECKER) {  // CheckerBoard::sample_spectrum_impl (checker_board.cpp:11-19)
+        const int ui = int(clampf(u, 0, 1) / t.grid_size), vi = int(clampf(v, 0, 1) / t.grid_size);
+        r = ((ui + vi) & 1) ? Vec3(t.texel[0], t.texel[1], t.texel[2]) : Vec3(t.texel2[0], t.texel2[1], t.texel2[2]);
+    } else if (t.nearest) {
         r = texel2(base, t.width, min(int(u * t.width), t.width - 1), min(int(v * t.height), t.height - 1));
     } else {
         const float fx = u * t.width - 0.5f, fy = v * t.height - 0.5f;
@@ -215,6 +218,15 @@ struct BSDF {
     float w_diffuse, w_specular, w_clearcoat, w_transmission;
     float eps;
     bool disney_fixed;  // sample the diffuse lobe instead of falling through
+    // mirror / metal: conductor Fresnel (eta_in / eta_out)^2, (k / eta_out)^2
+    // and the colour it is multiplied with
+    Vec3 eta2, etak2, rc;
+    // glass: ior (inside), reflection and refraction colours
+    float glass_ior;
+    Vec3 refl_c, refr_c;
+    // phong: diffuse and specular colours, exponent, component weights
+    Vec3 pd, ps;
+    float pns, wd, wsp;
 };
 
 __device__ __forceinline__ float one_minus_5(float x) { const float t = 1 - x, t2 = t * t; return t2 * t2 * t; }
@@ -298,6 +310,65 @@ __device__ __forceinline__ float normal_corr(const BSDF& b, Vec3 wi) {
     return dem < b.eps ? 1.0f : fabsf(cosv(b.shd.z, wi) / dem);
 }
 
+// ConductorPoint::eval (fresnel_point.h:44-64), per channel
+__device__ __forceinline__ Vec3 conductor_fresnel(const BSDF& b, float ci) {
+    if (ci <= 0) return Vec3();
+    const float cos2 = ci * ci, sin2 = fmaxf(0.0f, 1 - cos2);
+    const float e2[3] = {b.eta2.x, b.eta2.y, b.eta2.z}, k2[3] = {b.etak2.x, b.etak2.y, b.etak2.z};
+    float r[3];
+    for (int c = 0; c < 3; ++c) {
+        const float t0 = e2[c] - k2[c] - sin2;
+        const float a2b2 = sqrtf(t0 * t0 + 4 * e2[c] * k2[c]);
+        const float t1 = a2b2 + cos2;
+        const float a = sqrtf(0.5f * (a2b2 + t0));
+        const float t2 = 2 * ci * a;
+        const float rs = (t1 - t2) / (t1 + t2);
+        const float t3 = cos2 * a2b2 + sin2 * sin2;
+        const float t4 = t2 * sin2;
+        const float rp = rs * (t3 - t4) / (t3 + t4);
+        r[c] = 0.5f * (rp + rs);
+    }
+    return Vec3(r[0], r[1], r[2]);
+}
+
+// GGXMicrofacetReflectionComponent::eval / pdf (microfacet_refl_comp.cpp:9-55);
+// the Fresnel term is the coloured conductor of `metal`.
+__device__ __forceinline__ void ggx_refl(const BSDF& b, Vec3 lwi, Vec3 lwo, Vec3* f, float* pdf) {
+    if (lwi.z <= 0 || lwo.z <= 0) {
+        if (f) *f = Vec3();
+        if (pdf) *pdf = 0;
+        return;
+    }
+    const Vec3 lwh = normalize(lwi + lwo);
+    const float cd = dot(lwi, lwh);
+    float sph, cph, spi, cpi, spo, cpo;
+    sincos_phi(lwh, &sph, &cph);
+    sincos_phi(lwi, &spi, &cpi);
+    sincos_phi(lwo, &spo, &cpo);
+    const float D = aniso_gtr2(sph, cph, cos_2_sin(lwh.z), lwh.z, b.ax, b.ay);
+    const float Gi = smith_aniso_gtr2(cpi, spi, b.ax, b.ay, tan_theta(lwi));
+    const float Go = smith_aniso_gtr2(cpo, spo, b.ax, b.ay, tan_theta(lwo));
+    if (f) *f = b.rc * conductor_fresnel(b, cd) * (D * Gi * Go / fabsf(4 * lwi.z * lwo.z));
+    if (pdf) *pdf = Go * D / (4 * lwo.z);
+}
+
+// PhongSpecularComponent (phong_specular_comp.cpp:6-70): s (e+1)/2pi cos^e of
+// the angle to the mirror direction (a negative cosine with a fractional
+// exponent gives NaN, as in the reference)
+__device__ __forceinline__ float pow_cos_pdf(float e, float c) { return (e + 1) / (2 * kPi) * powf(c, e); }
+__device__ __forceinline__ Vec3 phong_spec_eval(const BSDF& b, Vec3 lwi, Vec3 lwo) {
+    if (lwi.z <= 0 || lwo.z <= 0) return Vec3();
+    const Vec3 ideal(-lwo.x, -lwo.y, lwo.z);  // refl_aux::reflect(lwo, z)
+    return b.ps * pow_cos_pdf(b.pns, cosv(ideal, lwi));
+}
+__device__ __forceinline__ float phong_spec_pdf(const BSDF& b, Vec3 lwi, Vec3 lwo) {
+    if (lwi.z <= 0 || lwo.z <= 0) return 0;
+    const Vec3 ideal(-lwo.x, -lwo.y, lwo.z);
+    const Vec3 l = coord_from_z(ideal).global_to_local(lwi);
+    if (l.z <= 0) return 0;
+    return pow_cos_pdf(b.pns, normalize(l).z);
+}
+
 __device__ void disney_init(BSDF& b, Vec3 base, float met, float rough, float trans, float trans_rough, float ior,
                             Vec3 spec_scale, float spec_tint, float aniso, float sheen, float sheen_tint, float cc,
                             float cc_gloss) {
@@ -363,7 +434,24 @@ __device__ Vec3 disney_f_inner(const BSDF& b, Vec3 lwi, Vec3 lwo) {
     return b.transmission * b.C * fabsf(F * D * G / (4 * lwi.z * lwo.z));
 }
 
+__device__ __forceinline__ bool is_aggregate(int type) { return type == ATRC_MAT_METAL || type == ATRC_MAT_PHONG; }
+
 __device__ Vec3 bsdf_eval(const BSDF& b, Vec3 wi, Vec3 wo) {
+    if (is_aggregate(b.type)) {  // AggregateBSDF::eval (component/aggregate.h)
+        if (fringes(b, wi) || fringes(b, wo)) {
+            if (!b.geo.positive(wi) || !b.geo.positive(wo)) return Vec3();
+            return b.albedo * kInvPi;
+        }
+        const Vec3 lwi = normalize(b.shd.global_to_local(wi)), lwo = normalize(b.shd.global_to_local(wo));
+        if (lwi.z == 0.0f || lwo.z == 0.0f) return Vec3();
+        if (b.type == ATRC_MAT_METAL) {
+            Vec3 f;
+            ggx_refl(b, lwi, lwo, &f, nullptr);
+            return f;
+        }
+        const Vec3 fd = (lwi.z <= 0 || lwo.z <= 0) ? Vec3() : b.pd * kInvPi;
+        return fd + phong_spec_eval(b, lwi, lwo);
+    }
     if (b.type == ATRC_MAT_IDEAL_DIFFUSE || b.type == ATRC_MAT_DISNEY) {
         if (fringes(b, wi) || fringes(b, wo)) {
             if (!b.geo.positive(wi) || !b.geo.positive(wo)) return Vec3();
@@ -437,12 +525,23 @@ __device__ float disney_pdf_trans(const BSDF& b, Vec3 lwi, Vec3 lwo) {
 }
 
 __device__ float bsdf_pdf(const BSDF& b, Vec3 wi, Vec3 wo) {
-    if (b.type != ATRC_MAT_IDEAL_DIFFUSE && b.type != ATRC_MAT_DISNEY) return 0;
+    if (b.type != ATRC_MAT_IDEAL_DIFFUSE && b.type != ATRC_MAT_DISNEY && !is_aggregate(b.type)) return 0;
     if (fringes(b, wi) || fringes(b, wo)) {
         if (b.geo.positive(wi) != b.geo.positive(wo)) return 0;
         return zweighted_pdf(normalize(b.geo.global_to_local(wi)).z);
     }
     const Vec3 lwi = normalize(b.shd.global_to_local(wi)), lwo = normalize(b.shd.global_to_local(wo));
+    if (is_aggregate(b.type)) {  // sum of weighted component pdfs / sum of weights
+        if (lwi.z == 0.0f || lwo.z == 0.0f) return 0;
+        if (b.type == ATRC_MAT_METAL) {
+            float pdf;
+            ggx_refl(b, lwi, lwo, nullptr, &pdf);
+            return pdf;
+        }
+        const float pdd = (lwi.z <= 0 || lwo.z <= 0) ? 0.0f : zweighted_pdf(lwi.z);
+        const float wsum = b.wd + b.wsp;
+        return wsum > 0 ? (b.wd * pdd + b.wsp * phong_spec_pdf(b, lwi, lwo)) / wsum : 0.0f;
+    }
     if (b.type == ATRC_MAT_IDEAL_DIFFUSE) {
         if (lwi.z <= 0 || lwo.z <= 0) return 0;
         return zweighted_pdf(lwi.z);
@@ -487,6 +586,109 @@ __device__ BSDFSample bsdf_sample(const BSDF& b, Vec3 wo, float u0, float u1, fl
         r.f = Vec3(1.0f / (c < b.eps ? 1.0f : c));
         r.pdf = 1;
         r.delta = true;
+        return r;
+    }
+    if (b.type == ATRC_MAT_MIRROR) {  // MirrorBSDF::sample (mirror.cpp:20-36)
+        const Vec3 lo = b.shd.global_to_local(wo);
+        if (lo.z <= 0) return r;
+        const Vec3 nwo = normalize(lo);
+        const Vec3 dir = b.shd.local_to_global(Vec3(0, 0, 2 * nwo.z) - nwo);
+        r.dir = dir;
+        r.f = conductor_fresnel(b, nwo.z) * b.rc / fabsf(nwo.z) * normal_corr(b, dir);
+        r.pdf = 1;
+        r.delta = true;
+        return r;
+    }
+    if (b.type == ATRC_MAT_GLASS) {  // GlassBSDF::sample (glass.cpp:34-70), radiance transport
+        const Vec3 nwo = normalize(b.shd.global_to_local(wo));
+        const Vec3 nor = nwo.z > 0 ? Vec3(0, 0, 1) : Vec3(0, 0, -1);
+        const float fr = dielectric_fresnel(b.glass_ior, 1.0f, nwo.z);
+        if (u0 < fr) {
+            const Vec3 lwi(-nwo.x, -nwo.y, nwo.z);
+            const Vec3 wi = b.shd.local_to_global(lwi);
+            r.dir = wi;
+            r.f = b.refl_c * fr / fabsf(lwi.z) * normal_corr(b, wi);
+            r.pdf = fr;
+            r.delta = true;
+            return r;
+        }
+        const float eta_i = nwo.z > 0 ? 1.0f : b.glass_ior, eta_t = nwo.z > 0 ? b.glass_ior : 1.0f;
+        const float eta = eta_i / eta_t;
+        const float ci = fabsf(nwo.z);
+        const float st2 = eta * eta * fmaxf(0.0f, 1 - ci * ci);
+        if (st2 >= 1) return r;
+        const float ct = sqrtf(1 - st2);
+        const Vec3 nwi = normalize((eta * ci - ct) * nor - eta * nwo);
+        const Vec3 dir = b.shd.local_to_global(nwi);
+        r.dir = dir;
+        r.f = eta * eta * b.refr_c * (1 - fr) / fabsf(nwi.z) * normal_corr(b, dir);
+        r.pdf = 1 - fr;
+        r.delta = true;
+        return r;
+    }
+    if (is_aggregate(b.type)) {  // AggregateBSDF::sample (component/aggregate.h)
+        if (fringes(b, wo)) {
+            if (!b.geo.positive(wo)) return r;
+            float pdf;
+            const Vec3 lwi = zweighted_on_hemisphere(u0, u1, &pdf);
+            if (pdf < b.eps) return r;
+            const Vec3 wi = normalize(b.geo.local_to_global(lwi));
+            r.dir = wi;
+            r.f = b.albedo * kInvPi * normal_corr(b, wi);
+            r.pdf = pdf;
+            return r;
+        }
+        const Vec3 lwo = normalize(b.shd.global_to_local(wo));
+        if (lwo.z == 0.0f) return r;
+        const bool metal = b.type == ATRC_MAT_METAL;
+        const float w0 = metal ? 1.0f : b.wd, w1 = metal ? 0.0f : b.wsp;
+        const int ncomp = metal ? 1 : 2;
+        float sel = (u0 - 0.001f) * (w0 + w1);
+        int comp = -1;
+        if (sel <= w0) comp = 0;
+        else if (ncomp > 1 && (sel -= w0) <= w1) comp = 1;
+        if (comp < 0) return r;
+        Vec3 lwi, f;
+        float pdf = 0;
+        if (lwo.z <= 0) return r;
+        if (metal) {
+            const Vec3 lwh = normalize(sample_gtr2_vnor(lwo, b.ax, b.ay, u1, u2, b.eps));
+            if (lwh.z <= 0) return r;
+            lwi = normalize(2 * dot(lwo, lwh) * lwh - lwo);
+            if (lwi.z <= 0) return r;
+            ggx_refl(b, lwi, lwo, &f, &pdf);
+        } else if (comp == 0) {  // DiffuseComponent::sample
+            lwi = zweighted_on_hemisphere(u1, u2, &pdf);
+            if (pdf < 0.001f) return r;
+            f = b.pd * kInvPi;
+        } else {  // PhongSpecularComponent::sample
+            const Vec3 ideal(-lwo.x, -lwo.y, lwo.z);
+            const float ct = powf(u1, 1 / (b.pns + 1));
+            const float st = cos_2_sin(ct);
+            float sp, cp;
+            sincosf(2 * kPi * u2, &sp, &cp);
+            const Vec3 local = normalize(Vec3(st * cp, st * sp, ct));
+            lwi = normalize(coord_from_z(ideal).local_to_global(local));
+            if (lwi.z <= 0) return r;
+            pdf = pow_cos_pdf(b.pns, local.z);
+            f = phong_spec_eval(b, lwi, lwo);
+        }
+        if (!(pdf > 0)) return r;
+        lwi = normalize(lwi);
+        pdf *= comp == 0 ? w0 : w1;
+        if (!metal) {  // the other component
+            if (comp == 0) {
+                f += phong_spec_eval(b, lwi, lwo);
+                pdf += phong_spec_pdf(b, lwi, lwo) * w1;
+            } else {
+                f += (lwi.z <= 0 || lwo.z <= 0) ? Vec3() : b.pd * kInvPi;
+                pdf += ((lwi.z <= 0 || lwo.z <= 0) ? 0.0f : zweighted_pdf(lwi.z)) * w0;
+            }
+        }
+        const Vec3 wi = b.shd.local_to_global(lwi);
+        r.dir = wi;
+        r.f = f * normal_corr(b, wi);
+        r.pdf = pdf;
         return r;
     }
     if (b.type != ATRC_MAT_IDEAL_DIFFUSE && b.type != ATRC_MAT_DISNEY) return r;
@@ -604,7 +806,8 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
     b.disney_fixed = S.disney_fixed != 0;
     b.albedo = Vec3();
     Coord shd = s.user;
-    if (m.normal_map >= 0 && (m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_DISNEY)) {
+    if (m.normal_map >= 0 && (m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_DISNEY ||
+                              m.type == ATRC_MAT_METAL || m.type == ATRC_MAT_PHONG)) {
         const Vec3 t = tex2d_sample(S, m.normal_map, s.u, s.v);  // NormalMapper::reorient
         const Vec3 ln = normalize(Vec3(t.x * 2 - 1, t.y * 2 - 1, t.z * 2 - 1));
         shd = rotate_to_new_z(s.user, s.user.local_to_global(ln));
@@ -624,6 +827,48 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
                         T(ATRC_DISNEY_SPECULAR_SCALE), T(ATRC_DISNEY_SPECULAR_TINT).x, T(ATRC_DISNEY_ANISOTROPIC).x,
                         T(ATRC_DISNEY_SHEEN).x, T(ATRC_DISNEY_SHEEN_TINT).x, T(ATRC_DISNEY_CLEARCOAT).x,
                         T(ATRC_DISNEY_CLEARCOAT_GLOSS).x);
+        }
+    } else if (m.type == ATRC_MAT_MIRROR || m.type == ATRC_MAT_GLASS || m.type == ATRC_MAT_METAL ||
+               m.type == ATRC_MAT_PHONG) {
+        auto T = [&](int slot) { return tex2d_sample(S, m.tex[slot], s.u, s.v); };
+        if (m.type == ATRC_MAT_MIRROR) {
+            // Mirror::shade (mirror.cpp:62-76): ConductorPoint(ior, 1, k) puts
+            // the ior on the OUTER side, so eta^2 = 1 / ior^2
+            const Vec3 rc = T(0), ior = T(1), k = T(2);
+            b.rc = rc;
+            b.eta2 = Vec3(1 / sqrf(ior.x), 1 / sqrf(ior.y), 1 / sqrf(ior.z));
+            b.etak2 = Vec3(sqrf(k.x / ior.x), sqrf(k.y / ior.y), sqrf(k.z / ior.z));
+            b.albedo = rc;
+        } else if (m.type == ATRC_MAT_GLASS) {  // Glass::shade (glass.cpp:127-150)
+            b.glass_ior = T(2).x;
+            b.refl_c = T(0);
+            const Vec3 rr = T(1);
+            b.refr_c = Vec3(sqrtf(rr.x), sqrtf(rr.y), sqrtf(rr.z));
+            b.albedo = 0.5f * (b.refl_c + b.refr_c);
+        } else if (m.type == ATRC_MAT_METAL) {  // Metal::shade (metal.cpp:25-46)
+            const Vec3 color = T(0), eta = T(1), k = T(2);
+            const float rough = T(3).x, aniso = T(4).x;
+            b.rc = color;  // ColoredConductorPoint(color, 1, eta, k)
+            b.eta2 = Vec3(sqrf(eta.x), sqrf(eta.y), sqrf(eta.z));
+            b.etak2 = Vec3(sqrf(k.x), sqrf(k.y), sqrf(k.z));
+            const float aspect = aniso > 0 ? sqrtf(1 - 0.9f * aniso) : 1.0f;
+            b.ax = fmaxf(0.001f, sqrf(rough) / aspect);
+            b.ay = fmaxf(0.001f, sqrf(rough) * aspect);
+            b.roughness = rough;
+            b.albedo = color;
+        } else {  // Phong::shade (phong.cpp:23-58)
+            Vec3 d = T(0), sp = T(1);
+            const float ns = T(2).x;
+            const float dem = fmaxf(1.0f, fmaxf(d.x + sp.x, fmaxf(d.y + sp.y, d.z + sp.z)));
+            d = d / dem;
+            sp = sp / dem;
+            const float dl = lum(d), sl = lum(sp);
+            b.wd = dl + sl > b.eps ? dl / (dl + sl) : 0.5f;
+            b.wsp = 1 - b.wd;
+            b.pd = d;
+            b.ps = sp;
+            b.pns = ns;
+            b.albedo = d + sp;
         }
     }
     return b;

@@ -429,6 +429,12 @@ __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d
     P.sh_c[k] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(slot));
 }
 
+// Materials the guide samples for: the non-delta BSDFs whose sampler
+// reports the density it samples with (with disney_fixed for Disney).
+__device__ __forceinline__ bool guidable(int type) {
+    return type == ATRC_MAT_IDEAL_DIFFUSE || type == ATRC_MAT_DISNEY || type == ATRC_MAT_METAL || type == ATRC_MAT_PHONG;
+}
+
 // Guide queries of the shade queue (same order as k_shade): surface hits
 // with a Lambert or Disney material, consistent frames and a depth the guide
 // serves are appended to a compact query list; gidx[i] is the query of
@@ -452,11 +458,11 @@ __global__ void k_guide_features(Scene S, Params p, Pool P, Counters* c) {
             const Surface s = make_surface(S, h, xyz(ro), xyz(rd));
             Vec3 sn;
             const BSDF b = shade(S, s, &sn);
-            if ((b.type == ATRC_MAT_IDEAL_DIFFUSE || b.type == ATRC_MAT_DISNEY) && !fringes(b, s.wr)) {
+            if (guidable(b.type) && !fringes(b, s.wr)) {
                 q.pos[0] = s.pos.x; q.pos[1] = s.pos.y; q.pos[2] = s.pos.z;
                 q.nrm[0] = sn.x; q.nrm[1] = sn.y; q.nrm[2] = sn.z;
                 q.wo[0] = s.wr.x; q.wo[1] = s.wr.y; q.wo[2] = s.wr.z;
-                q.rough = b.type == ATRC_MAT_DISNEY ? b.roughness : 1.0f;
+                q.rough = b.type == ATRC_MAT_DISNEY || b.type == ATRC_MAT_METAL ? b.roughness : 1.0f;
                 q.slot = slot;
             }
         }
@@ -602,7 +608,7 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                 const int gq_i = p.guide_on ? p.gf.gidx[i] : -1;
                 if (gq_i >= 0) {
                     const float* gm = p.gf.mixes + size_t(gq_i) * kGuideOut;
-                    guided = (b.type == ATRC_MAT_IDEAL_DIFFUSE || b.type == ATRC_MAT_DISNEY) && !fringes(b, s.wr);
+                    guided = guidable(b.type) && !fringes(b, s.wr);
                     if (guided) {
                         for (int k = 0; k < kGuideLobes; ++k) {
                             mix.mu[k][0] = gm[5 * k]; mix.mu[k][1] = gm[5 * k + 1]; mix.mu[k][2] = gm[5 * k + 2];

@@ -6,8 +6,12 @@
 // implemented here from their public specifications.  `.bm` follows
 // src/factory/src/utility/bin_mesh.cpp:7-27 (size_t count, then per triangle
 // three {position[3], normal[3], tex_coord[2]} float vertices).
+#include <zlib.h>
+
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <iterator>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -146,10 +150,101 @@ void png_chunk(std::ofstream& f, const char* type, const std::vector<uint8_t>& d
 
 }  // namespace
 
+// 8-bit PNG (gray, gray+alpha, RGB, RGBA; not interlaced) -> RGB floats
+// byte / 255, row 0 = top.  The IDAT stream is inflated with zlib and the
+// five scanline filters of the PNG specification are undone.
+std::vector<float> load_png(const std::string& fn, int* w, int* h) {
+    std::ifstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open file: " + fn);
+    std::vector<uint8_t> data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
+    if (data.size() < 8 || std::memcmp(data.data(), sig, 8) != 0) throw ConfigError("not a PNG file: " + fn);
+    auto be32 = [&](size_t o) {
+        return (uint32_t(data[o]) << 24) | (uint32_t(data[o + 1]) << 16) | (uint32_t(data[o + 2]) << 8) | data[o + 3];
+    };
+    uint32_t W = 0, H = 0;
+    int depth = 0, ctype = -1, interlace = 0;
+    std::vector<uint8_t> idat;
+    for (size_t pos = 8; pos + 12 <= data.size();) {
+        const uint32_t n = be32(pos);
+        if (pos + 12 + n > data.size()) throw ConfigError("truncated PNG chunk: " + fn);
+        const std::string kind(reinterpret_cast<const char*>(&data[pos + 4]), 4);
+        const uint8_t* body = &data[pos + 8];
+        if (kind == "IHDR" && n >= 13) {
+            W = be32(pos + 8);
+            H = be32(pos + 12);
+            depth = body[8];
+            ctype = body[9];
+            interlace = body[12];
+        } else if (kind == "IDAT") {
+            idat.insert(idat.end(), body, body + n);
+        } else if (kind == "IEND") {
+            break;
+        }
+        pos += 12 + n;
+    }
+    const int ch = ctype == 0 ? 1 : ctype == 4 ? 2 : ctype == 2 ? 3 : ctype == 6 ? 4 : 0;
+    if (depth != 8 || ch == 0 || interlace != 0 || W == 0 || H == 0 || W > (1u << 16) || H > (1u << 16))
+        throw ConfigError("unsupported PNG (8-bit gray / RGB / RGBA, not interlaced): " + fn);
+    const size_t stride = size_t(W) * ch;
+    std::vector<uint8_t> raw(size_t(H) * (stride + 1));
+    uLongf got = uLongf(raw.size());
+    if (uncompress(raw.data(), &got, idat.data(), uLong(idat.size())) != Z_OK || got != raw.size())
+        throw ConfigError("corrupt PNG data: " + fn);
+    std::vector<uint8_t> img(size_t(H) * stride);
+    for (uint32_t y = 0; y < H; ++y) {
+        const uint8_t ft = raw[y * (stride + 1)];
+        const uint8_t* src = &raw[y * (stride + 1) + 1];
+        uint8_t* dst = &img[y * stride];
+        const uint8_t* up = y ? &img[(y - 1) * stride] : nullptr;
+        for (size_t i = 0; i < stride; ++i) {
+            const int a = i >= size_t(ch) ? dst[i - ch] : 0, b = up ? up[i] : 0, c = (up && i >= size_t(ch)) ? up[i - ch] : 0;
+            int v = src[i];
+            if (ft == 1) v += a;
+            else if (ft == 2) v += b;
+            else if (ft == 3) v += (a + b) / 2;
+            else if (ft == 4) {
+                const int pp = a + b - c, pa = std::abs(pp - a), pb = std::abs(pp - b), pc = std::abs(pp - c);
+                v += (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
+            } else if (ft != 0) {
+                throw ConfigError("corrupt PNG filter: " + fn);
+            }
+            dst[i] = uint8_t(v);
+        }
+    }
+    *w = int(W);
+    *h = int(H);
+    std::vector<float> out(size_t(W) * H * 3);
+    for (size_t k = 0; k < size_t(W) * H; ++k)
+        for (int c = 0; c < 3; ++c) out[k * 3 + c] = float(img[k * ch + (ch >= 3 ? c : 0)]) / 255.0f;
+    return out;
+}
+
+// Binary PPM (P6, maxval 255) -> RGB floats byte / 255, row 0 = top.
+std::vector<float> load_ppm(const std::string& fn, int* w, int* h) {
+    std::ifstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open file: " + fn);
+    std::string magic;
+    int W = 0, H = 0, maxval = 0;
+    f >> magic >> W >> H >> maxval;
+    f.get();
+    if (magic != "P6" || W <= 0 || H <= 0 || maxval != 255) throw ConfigError("unsupported PPM (P6, 8-bit): " + fn);
+    std::vector<uint8_t> bytes(size_t(W) * H * 3);
+    f.read(reinterpret_cast<char*>(bytes.data()), std::streamsize(bytes.size()));
+    if (!f) throw ConfigError("truncated PPM: " + fn);
+    *w = W;
+    *h = H;
+    std::vector<float> out(bytes.size());
+    for (size_t k = 0; k < bytes.size(); ++k) out[k] = float(bytes[k]) / 255.0f;
+    return out;
+}
+
 std::vector<float> load_rgb_image(const std::string& fn, int* w, int* h) {
     if (has_ext(fn, ".pfm")) return load_pfm(fn, w, h);
     if (has_ext(fn, ".hdr")) return load_rgbe(fn, w, h);
-    throw ConfigError("unsupported image format (pt_cuda reads .pfm and .hdr): " + fn);
+    if (has_ext(fn, ".png")) return load_png(fn, w, h);
+    if (has_ext(fn, ".ppm")) return load_ppm(fn, w, h);
+    throw ConfigError("unsupported image format (pt_cuda reads .pfm, .hdr, .png and .ppm): " + fn);
 }
 
 std::vector<float> load_triangle_mesh(const std::string& fn) {

@@ -123,7 +123,11 @@ struct HostTex {
         tu = wrap(d->wrap_u, tu);
         tv = wrap(d->wrap_v, tv);
         Vec3 r;
-        if (d->nearest) {
+        if (d->type == ATRC_TEX_CHECKER) {
+            const float gs = 1.0f / float(d->grid_count);
+            const int ui = int(std::fmin(std::fmax(tu, 0.f), 1.f) / gs), vi = int(std::fmin(std::fmax(tv, 0.f), 1.f) / gs);
+            r = ((ui + vi) & 1) ? Vec3(d->texel[0], d->texel[1], d->texel[2]) : Vec3(d->texel2[0], d->texel2[1], d->texel2[2]);
+        } else if (d->nearest) {
             r = texel(std::min(int(tu * d->width), d->width - 1), std::min(int(tv * d->height), d->height - 1));
         } else {
             float fx = tu * d->width - 0.5f, fy = tv * d->height - 0.5f;
@@ -398,6 +402,11 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs) {
         dt.wrap_u = t.wrap_u;
         dt.wrap_v = t.wrap_v;
         dt.data_offset = -1;
+        if (t.type == ATRC_TEX_CHECKER) {
+            if (t.grid_count <= 0) throw std::runtime_error("invalid grid_count value");
+            std::memcpy(dt.texel2, t.texel2, sizeof(dt.texel2));
+            dt.grid_size = 1.0f / float(t.grid_count);
+        }
         if (t.type == ATRC_TEX_IMAGE) {
             if (t.width <= 0 || t.height <= 0 || !t.data) throw std::runtime_error("invalid image texture");
             dt.data_offset = int64_t(hs->texels.size());
@@ -433,12 +442,24 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs) {
         dm.type = m.type;
         std::memcpy(dm.tex, m.tex, sizeof(dm.tex));
         dm.normal_map = m.normal_map;
-        int slots = m.type == ATRC_MAT_DISNEY ? ATRC_DISNEY_SLOT_COUNT : (m.type == ATRC_MAT_IDEAL_DIFFUSE ? 1 : 0);
+        // texture slots each type reads; Lambert and Disney materials whose
+        // textures are all constant are folded into c[]
+        int slots = 0;
+        switch (m.type) {
+            case ATRC_MAT_DISNEY: slots = ATRC_DISNEY_SLOT_COUNT; break;
+            case ATRC_MAT_IDEAL_DIFFUSE: slots = 1; break;
+            case ATRC_MAT_MIRROR: case ATRC_MAT_GLASS: case ATRC_MAT_PHONG: slots = 3; break;
+            case ATRC_MAT_METAL: slots = 5; break;
+            case ATRC_MAT_IDEAL_BLACK: case ATRC_MAT_INVISIBLE_SURFACE: break;
+            default: throw std::runtime_error("unknown material type");
+        }
         bool all_const = m.normal_map < 0;
         for (int s = 0; s < slots; ++s) {
             if (m.tex[s] < 0 || uint32_t(m.tex[s]) >= d.texture2d_count) throw std::runtime_error("bad texture index");
             if (d.textures2d[m.tex[s]].type != ATRC_TEX_CONSTANT) all_const = false;
         }
+        if (m.normal_map >= 0 && uint32_t(m.normal_map) >= d.texture2d_count) throw std::runtime_error("bad texture index");
+        if (m.type != ATRC_MAT_DISNEY && m.type != ATRC_MAT_IDEAL_DIFFUSE) all_const = false;
         dm.all_constant = all_const;
         if (all_const && slots > 0) {
             auto T = [&](int s) { return d.textures2d[m.tex[s]].texel; };

@@ -177,8 +177,16 @@ public:
             t.type = ATRC_TEX_CONSTANT;
             t.texel[0] = texel.x; t.texel[1] = texel.y; t.texel[2] = texel.z;
             t.inv_gamma = 1.0f;
+        } else if (type == "checker_board") {  // CheckerBoardCreator (texture2d_creators.cpp:29-48)
+            t.type = ATRC_TEX_CHECKER;
+            t.grid_count = p.child_int("grid_count");
+            if (t.grid_count <= 0) throw ConfigError("invalid grid_count value: " + std::to_string(t.grid_count));
+            const Vec3 c1 = p.child_spectrum("color1"), c2 = p.child_spectrum("color2");
+            t.texel[0] = c1.x; t.texel[1] = c1.y; t.texel[2] = c1.z;
+            t.texel2[0] = c2.x; t.texel2[1] = c2.y; t.texel2[2] = c2.z;
         } else if (type == "hdr" || type == "image") {
-            // HDRTexture (hdr.cpp:11-72); `image` shares the float path
+            // HDRTexture (hdr.cpp:11-72) and ImageTexture (image.cpp): float
+            // texels, 8-bit images as byte / 255 (from_color3b)
             const std::string fn = map_path(p.child_str("filename"));
             const std::string sampler = p.child_str_or("sample", "linear");
             if (sampler != "linear" && sampler != "nearest") throw ConfigError("invalid sample method");
@@ -443,6 +451,36 @@ public:
             m.tex[ATRC_DISNEY_SHEEN_TINT] = child_texture_or_constant(p, "sheen_tint", 0);
             m.tex[ATRC_DISNEY_CLEARCOAT] = child_texture_or_constant(p, "clearcoat", 0);
             m.tex[ATRC_DISNEY_CLEARCOAT_GLOSS] = child_texture_or_constant(p, "clearcoat_gloss", 1);
+            if (auto n = p.find_child_group("normal_map")) m.normal_map = create_texture2d(*n);
+        } else if (type == "mirror") {  // MirrorCreator (material_creators.cpp:270-289)
+            m.type = ATRC_MAT_MIRROR;
+            m.tex[0] = create_texture2d(p.child_group("color_map"));
+            m.tex[1] = create_texture2d(p.child_group("eta"));
+            m.tex[2] = create_texture2d(p.child_group("k"));
+        } else if (type == "glass") {  // GlassCreator (material_creators.cpp:139-180)
+            m.type = ATRC_MAT_GLASS;
+            const int ior = create_texture2d(p.child_group("ior"));
+            int refl = -1, refr = -1;
+            if (auto n = p.find_child_group("color_map")) refl = refr = create_texture2d(*n);
+            if (auto n = p.find_child_group("color_reflection_map")) refl = create_texture2d(*n);
+            if (auto n = p.find_child_group("color_refraction_map")) refr = create_texture2d(*n);
+            if (refl < 0 || refr < 0) throw ConfigError("empty color reflection/refraction map");
+            m.tex[0] = refl;
+            m.tex[1] = refr;
+            m.tex[2] = ior;
+        } else if (type == "metal") {  // MetalCreator (material_creators.cpp:235-268)
+            m.type = ATRC_MAT_METAL;
+            m.tex[0] = create_texture2d(p.child_group("color"));
+            m.tex[1] = create_texture2d(p.child_group("eta"));
+            m.tex[2] = create_texture2d(p.child_group("k"));
+            m.tex[3] = create_texture2d(p.child_group("roughness"));
+            m.tex[4] = create_texture2d(p.child_group("anisotropic"));
+            if (auto n = p.find_child_group("normal_map")) m.normal_map = create_texture2d(*n);
+        } else if (type == "phong") {  // PhongCreator (material_creators.cpp:326-345)
+            m.type = ATRC_MAT_PHONG;
+            m.tex[0] = create_texture2d(p.child_group("d"));
+            m.tex[1] = create_texture2d(p.child_group("s"));
+            m.tex[2] = create_texture2d(p.child_group("ns"));
             if (auto n = p.find_child_group("normal_map")) m.normal_map = create_texture2d(*n);
         } else {
             throw ConfigError("material type '" + type + "' is not supported by pt_cuda");

@@ -114,7 +114,9 @@ typedef struct AtrcEntityDesc {
 
 typedef enum AtrcTextureType {
     ATRC_TEX_CONSTANT = 0,
-    ATRC_TEX_IMAGE    = 1        /* float RGB texels (`hdr`, `image`)        */
+    ATRC_TEX_IMAGE    = 1,       /* float RGB texels (`hdr`, `image`)        */
+    ATRC_TEX_CHECKER  = 2        /* `checker_board`: texel = color1,         */
+                                 /* texel2 = color2, grid_count cells        */
 } AtrcTextureType;
 
 typedef enum AtrcWrapMode {
@@ -132,6 +134,8 @@ typedef struct AtrcTexture2DDesc {
     float        uv_transform[6];/* 2x3 row-major affine applied to uv       */
     int32_t      wrap_u, wrap_v; /* AtrcWrapMode                             */
     float        inv_gamma;
+    int32_t      grid_count;     /* CHECKER                                  */
+    float        texel2[3];      /* CHECKER                                  */
     int32_t      pad_;
 } AtrcTexture2DDesc;
 
@@ -154,7 +158,13 @@ typedef enum AtrcMaterialType {
     ATRC_MAT_IDEAL_DIFFUSE     = 0,
     ATRC_MAT_IDEAL_BLACK       = 1,
     ATRC_MAT_DISNEY            = 2,
-    ATRC_MAT_INVISIBLE_SURFACE = 3
+    ATRC_MAT_INVISIBLE_SURFACE = 3,
+    ATRC_MAT_MIRROR            = 4,  /* tex[0] color_map, tex[1] eta, tex[2] k        */
+    ATRC_MAT_GLASS             = 5,  /* tex[0] reflection color, tex[1] refraction     */
+                                     /* color, tex[2] ior                             */
+    ATRC_MAT_METAL             = 6,  /* tex[0] color, tex[1] eta, tex[2] k,           */
+                                     /* tex[3] roughness, tex[4] anisotropic          */
+    ATRC_MAT_PHONG             = 7   /* tex[0] d, tex[1] s, tex[2] ns                 */
 } AtrcMaterialType;
 
 /* Disney texture slots, in the order of create_disney

@@ -138,8 +138,11 @@ def test_disney_defaults():
 
 def test_unknown_types_fail_loudly():
     q = json.loads(json.dumps(QUAD))
-    q["material"] = {"type": "glass", "ior": {"type": "constant", "texel": [1.5]}}
+    q["material"] = {"type": "paper", "color": {"type": "constant", "texel": [0.5]}}
     with pytest.raises(AtrcError, match="not supported"):
+        Config.from_string(base([q]))
+    q["material"] = {"type": "glass", "ior": {"type": "constant", "texel": [1.5]}}
+    with pytest.raises(AtrcError, match="empty color reflection/refraction map"):
         Config.from_string(base([q]))
     q["material"] = {"type": "no_such_thing"}
     with pytest.raises(AtrcError):
@@ -187,3 +190,81 @@ def test_post_processors_round_trip():
     c = base([QUAD], {"post_processors": [{"type": "save_to_img", "filename": "out.png", "inv_gamma": 2.2}]})
     pp = Config.from_string(c).post_processors(0)
     assert pp[0]["type"] == "save_to_img" and float(pp[0]["inv_gamma"]) == pytest.approx(2.2)
+
+
+def test_mirror_glass_metal_phong_and_checker_board():
+    c = lambda *v: {"type": "constant", "texel": list(v)}  # noqa: E731
+    mats = [("mirror", {"color_map": c(0.9), "eta": c(1.5), "k": c(2.0)}, 4, 3),
+            ("glass", {"ior": c(1.45), "color_map": c(0.8)}, 5, 3),
+            ("metal", {"color": c(0.9, 0.6, 0.3), "eta": c(0.2), "k": c(3.0), "roughness": c(0.3),
+                       "anisotropic": c(0.0)}, 6, 5),
+            ("phong", {"d": c(0.5), "s": c(0.4), "ns": c(30)}, 7, 3)]
+    for name, params, code, slots in mats:
+        q = json.loads(json.dumps(QUAD))
+        q["material"] = {"type": name, **params}
+        cfg = Config.from_string(base([q]))  # keep the config alive while reading its tables
+        s = cfg.scene_desc().contents
+        m = s.materials[0]
+        assert m.type == code and all(m.tex[k] >= 0 for k in range(slots))
+    # glass: one color_map serves reflection and refraction
+    q = json.loads(json.dumps(QUAD))
+    q["material"] = {"type": "glass", "ior": c(1.45), "color_map": c(0.8)}
+    cfg = Config.from_string(base([q]))
+    s = cfg.scene_desc().contents
+    assert s.materials[0].tex[0] == s.materials[0].tex[1]
+    # checker_board (texture2d_creators.cpp:29-48)
+    q = json.loads(json.dumps(QUAD))
+    q["material"] = {"type": "ideal_diffuse",
+                     "albedo": {"type": "checker_board", "grid_count": 4, "color1": [1, 0, 0], "color2": [0, 0, 1]}}
+    cfg = Config.from_string(base([q]))
+    s = cfg.scene_desc().contents
+    t = s.textures2d[s.materials[0].tex[0]]
+    assert t.type == 2 and t.grid_count == 4 and list(t.texel) == [1, 0, 0] and list(t.texel2) == [0, 0, 1]
+    q["material"]["albedo"]["grid_count"] = 0
+    with pytest.raises(AtrcError, match="grid_count"):
+        Config.from_string(base([q]))
+
+
+def test_png_and_ppm_textures(tmp_path):
+    # 8-bit images load as byte / 255, row 0 = top (PNG filters undone)
+    import zlib
+    import struct
+    rng = np.random.default_rng(3)
+    img = rng.integers(0, 256, (5, 7, 3), dtype=np.uint8)
+
+    def chunk(kind, body):
+        return struct.pack(">I", len(body)) + kind + body + struct.pack(">I", zlib.crc32(kind + body))
+    rows = b""
+    for y in range(5):  # rows with the Sub, Up, Paeth and None filters
+        ft = y % 5
+        r = img[y].astype(int).ravel()
+        prev = img[y - 1].astype(int).ravel() if y else np.zeros_like(r)
+        left = np.concatenate([[0, 0, 0], r[:-3]])
+        upleft = np.concatenate([[0, 0, 0], prev[:-3]])
+        if ft == 1:
+            f = r - left
+        elif ft == 2:
+            f = r - prev
+        elif ft == 3:
+            f = r - (left + prev) // 2
+        elif ft == 4:
+            p = left + prev - upleft
+            pa, pb, pc = abs(p - left), abs(p - prev), abs(p - upleft)
+            pred = np.where((pa <= pb) & (pa <= pc), left, np.where(pb <= pc, prev, upleft))
+            f = r - pred
+        else:
+            f = r
+        rows += bytes([ft]) + bytes((f % 256).astype(np.uint8))
+    png = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", 7, 5, 8, 2, 0, 0, 0)) + \
+        chunk(b"IDAT", zlib.compress(rows)) + chunk(b"IEND", b"")
+    (tmp_path / "t.png").write_bytes(png)
+    (tmp_path / "t.ppm").write_bytes(b"P6\n7 5\n255\n" + img.tobytes())
+    for fn in ("t.png", "t.ppm"):
+        q = json.loads(json.dumps(QUAD))
+        q["material"] = {"type": "ideal_diffuse", "albedo": {"type": "image", "filename": "${scene-directory}/" + fn}}
+        cfg = Config.from_string(base([q]), tmp_path)
+        s = cfg.scene_desc().contents
+        t = s.textures2d[s.materials[0].tex[0]]
+        assert (t.width, t.height) == (7, 5)
+        got = np.ctypeslib.as_array(t.data, shape=(5 * 7 * 3,)).reshape(5, 7, 3)
+        np.testing.assert_array_equal(got, img.astype(np.float32) / np.float32(255))
