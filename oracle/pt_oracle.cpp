@@ -292,6 +292,11 @@ struct Tex2D {
     // (i + 0.5) / size, edge texels clamped.
     V3 sample_impl(V2 uv) const {
         float u = clampf(uv.x, 0, 1), v = clampf(uv.y, 0, 1);
+        if (d.type == ATRC_TEX_CHECKER) {  // CheckerBoard::sample_spectrum_impl (checker_board.cpp:11-19)
+            float gs = 1.0f / float(d.grid_count);
+            int ui = int(u / gs), vi = int(v / gs);
+            return ((ui + vi) & 1) ? V3(d.texel) : V3(d.texel2);
+        }
         if (d.nearest) {
             int x = std::min(int(u * d.width), d.width - 1);
             int y = std::min(int(v * d.height), d.height - 1);
@@ -1087,6 +1092,14 @@ struct BSDF {
     float clearcoat = 0, transmission = 0, IOR = 1.5f, transmission_roughness = 0;
     float trans_ax = 0, trans_ay = 0, ax = 0, ay = 0, clearcoat_roughness = 0;
     float w_diffuse = 0.25f, w_specular = 0.25f, w_clearcoat = 0.25f, w_transmission = 0.25f;
+    // mirror / metal conductor Fresnel: eta^2, (eta k)^2 per channel, colour
+    V3 eta2, etak2, rc;
+    // glass (glass.cpp:127-150)
+    float glass_ior = 1.5f;
+    V3 refl_c, refr_c;
+    // phong (phong.cpp:23-58): diffuse / specular colours, exponent, weights
+    V3 pd, ps;
+    float pns = 1, wd = 0.5f, wsp = 0.5f;
 
     // ------------------------------------------------- LocalBSDF helpers
     // core/bsdf.h:113-202
@@ -1198,6 +1211,53 @@ struct BSDF {
         V3 nh = t_1 * t1 + t_2 * t2 + std::sqrt(std::max(0.0f, 1 - t_1 * t_1 - t_2 * t_2)) * vh;
         return normalize(V3(axx * nh.x, ayy * nh.y, std::max(0.0f, nh.z)));
     }
+
+    // ConductorPoint::eval (fresnel_point.h:44-64), per channel
+    V3 conductor_fresnel(float ci) const {
+        if (ci <= 0) return V3();
+        float cos2 = ci * ci, sin2 = std::max(0.0f, 1 - cos2);
+        float e2[3] = {eta2.x, eta2.y, eta2.z}, k2[3] = {etak2.x, etak2.y, etak2.z}, out[3];
+        for (int c = 0; c < 3; ++c) {
+            float t0 = e2[c] - k2[c] - sin2;
+            float a2b2 = std::sqrt(t0 * t0 + 4 * e2[c] * k2[c]);
+            float t1 = a2b2 + cos2;
+            float a = std::sqrt(0.5f * (a2b2 + t0));
+            float t2 = 2 * ci * a;
+            float rs = (t1 - t2) / (t1 + t2);
+            float t3 = cos2 * a2b2 + sin2 * sin2;
+            float t4 = t2 * sin2;
+            float rp = rs * (t3 - t4) / (t3 + t4);
+            out[c] = 0.5f * (rp + rs);
+        }
+        return V3(out[0], out[1], out[2]);
+    }
+    // GGXMicrofacetReflectionComponent::eval / pdf (microfacet_refl_comp.cpp:9-55)
+    void ggx_refl(V3 lwi, V3 lwo, V3* f, float* p) const {
+        if (lwi.z <= 0 || lwo.z <= 0) { if (f) *f = V3(); if (p) *p = 0; return; }
+        V3 lwh = normalize(lwi + lwo);
+        float cd = dot(lwi, lwh);
+        float ph = phi_of(lwh), pi_ = phi_of(lwi), po = phi_of(lwo);
+        float D = aniso_gtr2(std::sin(ph), std::cos(ph), cos_2_sin(lwh.z), lwh.z, ax, ay);
+        float Gi = smith_aniso_gtr2(std::cos(pi_), std::sin(pi_), ax, ay, tan_theta(lwi));
+        float Go = smith_aniso_gtr2(std::cos(po), std::sin(po), ax, ay, tan_theta(lwo));
+        if (f) *f = rc * conductor_fresnel(cd) * (D * Gi * Go / std::abs(4 * lwi.z * lwo.z));
+        if (p) *p = Go * D / (4 * lwo.z);
+    }
+    // PhongSpecularComponent (phong_specular_comp.cpp:6-70)
+    static float pow_cos_pdf(float e, float c) { return (e + 1) / (2 * PI) * std::pow(c, e); }
+    V3 phong_spec_eval(V3 lwi, V3 lwo) const {
+        if (lwi.z <= 0 || lwo.z <= 0) return V3();
+        V3 ideal(-lwo.x, -lwo.y, lwo.z);
+        return ps * pow_cos_pdf(pns, cosv(ideal, lwi));
+    }
+    float phong_spec_pdf(V3 lwi, V3 lwo) const {
+        if (lwi.z <= 0 || lwo.z <= 0) return 0;
+        V3 ideal(-lwo.x, -lwo.y, lwo.z);
+        V3 l = Coord::from_z(ideal).global_to_local(lwi);
+        if (l.z <= 0) return 0;
+        return pow_cos_pdf(pns, normalize(l).z);
+    }
+    V3 phong_diffuse(V3 lwi, V3 lwo) const { return (lwi.z <= 0 || lwo.z <= 0) ? V3() : pd / PI; }
 
     V3 f_diffuse(float ci, float co, float cd) const {
         V3 f_lambert = C / PI;
@@ -1396,7 +1456,15 @@ struct BSDF {
             V3 value = (1 - metallic) * (1 - transmission) * (diffuse + sheen_v) + specular + cc;
             return value * normal_corr(wi);
         }
-        default:
+        case ATRC_MAT_METAL:
+        case ATRC_MAT_PHONG: {  // AggregateBSDF::eval (component/aggregate.h:40-62)
+            if (black_fringes(wi, wo)) return eval_black_fringes(wi, wo);
+            V3 lwi = normalize(shd.global_to_local(wi)), lwo = normalize(shd.global_to_local(wo));
+            if (!lwi.z || !lwo.z) return V3();
+            if (type == ATRC_MAT_METAL) { V3 f; ggx_refl(lwi, lwo, &f, nullptr); return f; }
+            return phong_diffuse(lwi, lwo) + phong_spec_eval(lwi, lwo);
+        }
+        default:  // mirror and glass are delta: eval is 0 (mirror.cpp:38-41, glass.cpp:72-75)
             return V3();
         }
     }
@@ -1423,9 +1491,19 @@ struct BSDF {
             }
             if (lwi.z < 0) return w_transmission * pdf_transmission(lwi, lwo);
             float d = zweighted_pdf(lwi.z);
-            float ps, pc;
-            pdf_spec_cc(lwi, lwo, &ps, &pc);
-            return w_diffuse * d + w_specular * ps + w_clearcoat * pc;
+            float sp, pc;
+            pdf_spec_cc(lwi, lwo, &sp, &pc);
+            return w_diffuse * d + w_specular * sp + w_clearcoat * pc;
+        }
+        case ATRC_MAT_METAL:
+        case ATRC_MAT_PHONG: {  // AggregateBSDF::pdf (component/aggregate.h:200-225)
+            if (black_fringes(wi, wo)) return pdf_black_fringes(wi, wo);
+            V3 lwi = normalize(shd.global_to_local(wi)), lwo = normalize(shd.global_to_local(wo));
+            if (!lwi.z || !lwo.z) return 0;
+            if (type == ATRC_MAT_METAL) { float p; ggx_refl(lwi, lwo, nullptr, &p); return p; }
+            float pdd = (lwi.z <= 0 || lwo.z <= 0) ? 0.0f : zweighted_pdf(lwi.z);
+            float wsum = wd + wsp;
+            return wsum > 0 ? (wd * pdd + wsp * phong_spec_pdf(lwi, lwo)) / wsum : 0.0f;
         }
         default:
             return 0;
@@ -1487,6 +1565,95 @@ struct BSDF {
             r.f = eval(wi, wo);
             r.pdf = pdf(wi, wo);
             r.delta = false;
+            return r;
+        }
+        case ATRC_MAT_MIRROR: {  // MirrorBSDF::sample (mirror.cpp:20-36)
+            V3 lo = shd.global_to_local(wo);
+            if (lo.z <= 0) return r;
+            V3 nwo = normalize(lo);
+            V3 dir = shd.local_to_global(V3(0, 0, 2 * nwo.z) - nwo);
+            r.dir = dir;
+            r.f = conductor_fresnel(nwo.z) * rc / std::abs(nwo.z) * normal_corr(dir);
+            r.pdf = 1;
+            r.delta = true;
+            return r;
+        }
+        case ATRC_MAT_GLASS: {  // GlassBSDF::sample (glass.cpp:34-70), TransMode::Radiance
+            V3 nwo = normalize(shd.global_to_local(wo));
+            V3 nor = nwo.z > 0 ? V3(0, 0, 1) : V3(0, 0, -1);
+            float fr = dielectric_fresnel(glass_ior, 1, nwo.z);
+            r.delta = true;
+            if (sam[0] < fr) {
+                V3 lwi(-nwo.x, -nwo.y, nwo.z);
+                V3 wi = shd.local_to_global(lwi);
+                r.dir = wi;
+                r.f = refl_c * fr / std::abs(lwi.z) * normal_corr(wi);
+                r.pdf = fr;
+                return r;
+            }
+            float eta_i = nwo.z > 0 ? 1 : glass_ior, eta_t = nwo.z > 0 ? glass_ior : 1;
+            float eta = eta_i / eta_t;
+            float ci = std::abs(nwo.z);
+            float st2 = eta * eta * std::max(0.0f, 1 - ci * ci);
+            if (st2 >= 1) return BSDFSample();
+            float ct = std::sqrt(1 - st2);
+            V3 nwi = normalize((eta * ci - ct) * nor - eta * nwo);
+            V3 dir = shd.local_to_global(nwi);
+            r.dir = dir;
+            r.f = eta * eta * refr_c * (1 - fr) / std::abs(nwi.z) * normal_corr(dir);
+            r.pdf = 1 - fr;
+            return r;
+        }
+        case ATRC_MAT_METAL:
+        case ATRC_MAT_PHONG: {  // AggregateBSDF::sample (component/aggregate.h:64-139)
+            if (black_fringes(wo)) return sample_black_fringes(wo, sam);
+            V3 lwo = normalize(shd.global_to_local(wo));
+            if (!lwo.z) return r;
+            bool metal = type == ATRC_MAT_METAL;
+            float w0 = metal ? 1.0f : wd, w1 = metal ? 0.0f : wsp;
+            float sel = (sam[0] - 0.001f) * (w0 + w1);
+            int comp = -1;
+            if (sel <= w0) comp = 0;
+            else if (!metal && (sel -= w0) <= w1) comp = 1;
+            if (comp < 0) return r;
+            if (lwo.z <= 0) return r;
+            V3 lwi, f;
+            float p = 0;
+            if (metal) {  // GGXMicrofacetReflectionComponent::sample
+                V3 lwh = normalize(sample_aniso_gtr2_vnor(lwo, ax, ay, sam[1], sam[2]));
+                if (lwh.z <= 0) return r;
+                lwi = normalize(2 * dot(lwo, lwh) * lwh - lwo);
+                if (lwi.z <= 0) return r;
+                ggx_refl(lwi, lwo, &f, &p);
+            } else if (comp == 0) {  // DiffuseComponent::sample_bidir
+                lwi = zweighted_on_hemisphere(sam[1], sam[2], &p);
+                if (p < 0.001f) return r;
+                f = pd / PI;
+            } else {  // PhongSpecularComponent::sample
+                V3 ideal(-lwo.x, -lwo.y, lwo.z);
+                float ct = std::pow(sam[1], 1 / (pns + 1));
+                float st = cos_2_sin(ct);
+                float phi = 2 * PI * sam[2];
+                V3 local = normalize(V3(st * std::cos(phi), st * std::sin(phi), ct));
+                lwi = normalize(Coord::from_z(ideal).local_to_global(local));
+                if (lwi.z <= 0) return r;
+                p = pow_cos_pdf(pns, local.z);
+                f = phong_spec_eval(lwi, lwo);
+            }
+            if (!(p > 0)) return r;
+            lwi = normalize(lwi);
+            p *= comp == 0 ? w0 : w1;
+            if (!metal) {  // the other component's contribution
+                if (comp == 0) { f += phong_spec_eval(lwi, lwo); p += phong_spec_pdf(lwi, lwo) * w1; }
+                else {
+                    f += phong_diffuse(lwi, lwo);
+                    p += ((lwi.z <= 0 || lwo.z <= 0) ? 0.0f : zweighted_pdf(lwi.z)) * w0;
+                }
+            }
+            V3 wi = shd.local_to_global(lwi);
+            r.dir = wi;
+            r.f = f * normal_corr(wi);
+            r.pdf = p;
             return r;
         }
         case ATRC_MAT_INVISIBLE_SURFACE: {  // invisible_surface.cpp:22-28
@@ -1858,7 +2025,8 @@ struct OracleScene {
         b.type = m.type;
         b.geo = in.geo;
         Coord shd = in.user;
-        if (m.normal_map >= 0 && (m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_DISNEY)) {
+        if (m.normal_map >= 0 && (m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_DISNEY ||
+                                  m.type == ATRC_MAT_METAL || m.type == ATRC_MAT_PHONG)) {
             // NormalMapper::reorient (material.h:25-57)
             V3 s = tex2d[m.normal_map].sample(in.uv);
             V3 ln = normalize(V3(s.x * 2 - 1, s.y * 2 - 1, s.z * 2 - 1));
@@ -1878,6 +2046,54 @@ struct OracleScene {
                           R(ATRC_DISNEY_SHEEN), R(ATRC_DISNEY_SHEEN_TINT), R(ATRC_DISNEY_CLEARCOAT),
                           R(ATRC_DISNEY_CLEARCOAT_GLOSS), R(ATRC_DISNEY_TRANSMISSION),
                           R(ATRC_DISNEY_TRANSMISSION_ROUGHNESS), R(ATRC_DISNEY_IOR));
+            *shading_normal = shd.z;
+            break;
+        }
+        case ATRC_MAT_MIRROR: {  // Mirror::shade (mirror.cpp:62-76): ConductorPoint(ior, 1, k)
+            V3 c = tex2d[m.tex[0]].sample(in.uv), ior = tex2d[m.tex[1]].sample(in.uv), k = tex2d[m.tex[2]].sample(in.uv);
+            b.rc = c;
+            b.eta2 = V3(1 / sqr(ior.x), 1 / sqr(ior.y), 1 / sqr(ior.z));
+            b.etak2 = V3(sqr(k.x / ior.x), sqr(k.y / ior.y), sqr(k.z / ior.z));
+            b.albedo_ = c;
+            *shading_normal = shd.z;
+            break;
+        }
+        case ATRC_MAT_GLASS: {  // Glass::shade (glass.cpp:127-150)
+            b.glass_ior = tex2d[m.tex[2]].sample_real(in.uv);
+            b.refl_c = tex2d[m.tex[0]].sample(in.uv);
+            V3 rr = tex2d[m.tex[1]].sample(in.uv);
+            b.refr_c = V3(std::sqrt(rr.x), std::sqrt(rr.y), std::sqrt(rr.z));
+            b.albedo_ = 0.5f * (b.refl_c + b.refr_c);
+            *shading_normal = shd.z;
+            break;
+        }
+        case ATRC_MAT_METAL: {  // Metal::shade (metal.cpp:25-46)
+            V3 c = tex2d[m.tex[0]].sample(in.uv), eta = tex2d[m.tex[1]].sample(in.uv), k = tex2d[m.tex[2]].sample(in.uv);
+            float rough = tex2d[m.tex[3]].sample_real(in.uv), aniso = tex2d[m.tex[4]].sample_real(in.uv);
+            b.rc = c;
+            b.eta2 = V3(sqr(eta.x), sqr(eta.y), sqr(eta.z));
+            b.etak2 = V3(sqr(k.x), sqr(k.y), sqr(k.z));
+            float aspect = aniso > 0 ? std::sqrt(1 - 0.9f * aniso) : 1.0f;
+            b.ax = std::max(0.001f, sqr(rough) / aspect);
+            b.ay = std::max(0.001f, sqr(rough) * aspect);
+            b.roughness = rough;
+            b.albedo_ = c;
+            *shading_normal = shd.z;
+            break;
+        }
+        case ATRC_MAT_PHONG: {  // Phong::shade (phong.cpp:23-58)
+            V3 d = tex2d[m.tex[0]].sample(in.uv), sp = tex2d[m.tex[1]].sample(in.uv);
+            float ns = tex2d[m.tex[2]].sample_real(in.uv);
+            float dem = std::max(1.0f, std::max(d.x + sp.x, std::max(d.y + sp.y, d.z + sp.z)));
+            d = d / dem;
+            sp = sp / dem;
+            float dl = lum(d), sl = lum(sp);
+            b.wd = dl + sl > g_eps ? dl / (dl + sl) : 0.5f;
+            b.wsp = 1 - b.wd;
+            b.pd = d;
+            b.ps = sp;
+            b.pns = ns;
+            b.albedo_ = d + sp;
             *shading_normal = shd.z;
             break;
         }

@@ -158,3 +158,81 @@ def feature_scene(tmp: Path, renderer="pt", spp=256, width=48, height=36, gaussi
     if gaussian:
         cfg["rendering"]["film_filter"] = {"type": "gaussian", "radius": 1.5, "alpha": 2}
     return cfg
+
+
+def write_png8(path: Path, rgb: np.ndarray) -> None:
+    """(H, W, 3) uint8 -> 8-bit RGB PNG, filter 0 on every row, rows top first."""
+    import struct
+    import zlib
+    h, w, _ = rgb.shape
+    raw = b"".join(b"\x00" + rgb[y].astype(np.uint8).tobytes() for y in range(h))
+
+    def chunk(kind, body):
+        return struct.pack(">I", len(body)) + kind + body + struct.pack(">I", zlib.crc32(kind + body) & 0xFFFFFFFF)
+
+    path.write_bytes(b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)) +
+                     chunk(b"IDAT", zlib.compress(raw)) + chunk(b"IEND", b""))
+
+
+def materials_scene(tmp: Path, renderer="pt", spp=256, width=48, height=36) -> dict:
+    """The wider material set in one small scene: a mirror sphere, a glass
+    sphere, an anisotropic normal-mapped metal sphere, a phong box, a
+    checker_board floor (phong) and an 8-bit PNG image texture on the back
+    wall, lit by a sphere light and the native sky."""
+    from atrc_b200.scenes import _box_mesh, write_bm, write_pfm
+    rng = np.random.default_rng(91)
+    write_png8(tmp / "wall.png", np.kron(rng.integers(20, 235, (4, 6, 3)), np.ones((6, 6, 1), np.int64)))
+    nm = np.zeros((16, 16, 3), np.float32)
+    yy, xx = np.mgrid[0:16, 0:16] / 16.0
+    nm[..., 0] = 0.5 + 0.25 * np.sin(5 * xx)
+    nm[..., 1] = 0.5 + 0.25 * np.cos(7 * yy)
+    nm[..., 2] = 0.9
+    write_pfm(tmp / "bumps.pfm", nm)
+    p, n, uv = _box_mesh((0.35, 0.35, 0.35))
+    write_bm(tmp / "box.bm", p, n, uv)
+
+    def const(v):
+        return {"type": "constant", "texel": list(np.atleast_1d(v).astype(float))}
+
+    checker = {"type": "checker_board", "grid_count": 8, "color1": [0.8, 0.75, 0.7], "color2": [0.15, 0.2, 0.3]}
+    ents = [
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-4, -4, -1], "B": [4, -4, -1], "C": [4, 4, -1],
+                                           "D": [-4, 4, -1], "tA": [0, 0], "tB": [1, 0], "tC": [1, 1], "tD": [0, 1],
+                                           "transform": []},
+         "material": {"type": "phong", "d": checker, "s": const(0.25), "ns": const(30)}},
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-4, 3, -1], "B": [4, 3, -1], "C": [4, 3, 3],
+                                           "D": [-4, 3, 3], "tA": [0, 0], "tB": [1, 0], "tC": [1, 1], "tD": [0, 1],
+                                           "transform": []},
+         "material": {"type": "ideal_diffuse",
+                      "albedo": {"type": "image", "filename": "${scene-directory}/wall.png", "sample": "nearest"}}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.55,
+                                           "transform": [{"type": "translate", "offset": [-1.3, 0.4, -0.45]}]},
+         "material": {"type": "mirror", "color_map": const([0.9, 0.85, 0.8]), "eta": const([0.2, 0.9, 1.1]),
+                      "k": const([3.9, 2.4, 2.2])}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.5,
+                                           "transform": [{"type": "translate", "offset": [0.0, -0.4, -0.5]}]},
+         "material": {"type": "glass", "ior": const(1.5), "color_reflection_map": const(1.0),
+                      "color_refraction_map": const([0.9, 0.95, 1.0])}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.5,
+                                           "transform": [{"type": "translate", "offset": [1.3, 0.5, -0.5]}]},
+         "material": {"type": "metal", "color": const([0.95, 0.8, 0.5]), "eta": const([0.2, 0.4, 1.4]),
+                      "k": const([3.9, 2.4, 1.9]), "roughness": const(0.35), "anisotropic": const(0.6),
+                      "normal_map": {"type": "hdr", "filename": "${scene-directory}/bumps.pfm",
+                                     "wrap_u": "repeat", "wrap_v": "repeat"}}},
+        {"type": "geometric", "geometry": {"type": "transform_wrapper",
+                                           "transform": [{"type": "translate", "offset": [0.9, -1.0, -0.65]},
+                                                         {"type": "rotate_z", "deg": 25}],
+                                           "internal": {"type": "triangle_bvh", "filename": "${scene-directory}/box.bm",
+                                                        "transform": []}},
+         "material": {"type": "phong", "d": const([0.2, 0.5, 0.3]), "s": const([0.6, 0.6, 0.6]), "ns": const(8)}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.3,
+                                           "transform": [{"type": "translate", "offset": [-0.4, -0.8, 1.8]}]},
+         "material": {"type": "ideal_black"}, "emit_radiance": [8, 7, 6]},
+    ]
+    return {"scene": {"type": "default", "entities": ents,
+                      "env": {"type": "native_sky", "top": [0.4, 0.5, 0.8], "bottom": [0.1, 0.08, 0.05]}},
+            "rendering": {"camera": {"type": "thin_lens", "pos": [0, -5, 1.0], "dst": [0, 0, -0.3], "up": [0, 0, 1],
+                                     "fov": 50},
+                          "width": width, "height": height,
+                          "renderer": {"type": renderer, "spp": spp, "max_depth": 12, "min_depth": 3},
+                          "reporter": {"type": "noout"}}}

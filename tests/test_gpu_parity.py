@@ -153,6 +153,28 @@ def test_feature_scene_within_3_sigma(tmp_path, disney_fixed):
     assert np.mean(np.abs(gn - cn)) < 0.02
 
 
+def test_materials_scene_within_3_sigma(tmp_path):
+    # mirror, glass, anisotropic normal-mapped metal, phong, checker_board
+    # and an 8-bit PNG texture against the oracle
+    from tests import kat_scenes as K
+    cfg = Config.from_string(K.dumps(K.materials_scene(tmp_path, spp=512)), tmp_path)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    fg = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    fc = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    dev.render(desc, fg)
+    ora.render(desc, fc)
+    r = 0.5 - desc.eps
+    frac, allowed, info = band_test(fg, fc, 1 / (4 * r * r))
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fg, fc) < 4.0
+    # first-hit albedo (checker, PNG texels, material albedos) agrees
+    ga = fg.albedo.reshape(-1, 3) / fg.weight.reshape(-1, 1)
+    ca = fc.albedo.reshape(-1, 3) / fc.weight.reshape(-1, 1)
+    assert np.abs(ga - ca).mean() < 0.02
+
+
 def test_gaussian_filter_matches(tmp_path):
     from tests import kat_scenes as K
     cfg = Config.from_string(K.dumps(K.feature_scene(tmp_path, spp=128, gaussian=True)), tmp_path)

@@ -147,3 +147,112 @@ def test_fixed_disney_sampling_follows_its_pdf():
     f_u, _ = ora.bsdf_eval(0, wi, wo)
     ref = np.mean(f_u[:, 0] * wi[:, 2]) * 2 * math.pi
     assert abs(est - ref) < 0.02 * ref, (est, ref)
+
+
+def _const(v):
+    return {"type": "constant", "texel": list(np.atleast_1d(v).astype(float))}
+
+
+def _unit(v):
+    v = np.asarray(v, np.float64)
+    return (v / np.linalg.norm(v)).astype(np.float32)
+
+
+def _fresnel_conductor(cos_i, n):
+    """Exact Fresnel reflectance of unpolarised light at a conductor of
+    complex relative index n (Fresnel equations with Snell's law in C)."""
+    cos_i = np.asarray(cos_i, np.complex128)
+    sin2_t = (1 - cos_i ** 2) / n ** 2
+    cos_t = np.sqrt(1 - sin2_t)
+    rs = (cos_i - n * cos_t) / (cos_i + n * cos_t)
+    rp = (n * cos_i - cos_t) / (n * cos_i + cos_t)
+    return 0.5 * (np.abs(rs) ** 2 + np.abs(rp) ** 2)
+
+
+def _fresnel_dielectric(cos_i, n):
+    sin_t = np.sqrt(np.maximum(0, 1 - cos_i ** 2)) / n
+    cos_t = np.sqrt(np.maximum(0, 1 - sin_t ** 2))
+    rs = (cos_i - n * cos_t) / (cos_i + n * cos_t)
+    rp = (n * cos_i - cos_t) / (n * cos_i + cos_t)
+    return 0.5 * (rs ** 2 + rp ** 2)
+
+
+def test_mirror_reflects_with_the_conductor_fresnel_term():
+    # mirror.cpp:62-76 builds ConductorPoint(ior, 1, k): the medium of index
+    # `ior` is outside, so the relative complex index is (1 + i k) / ior
+    ior, k, col = np.array([1.3, 1.0, 0.8]), np.array([3.9, 2.4, 0.0]), np.array([0.9, 0.8, 0.7])
+    mat = {"type": "mirror", "color_map": _const(col), "eta": _const(ior), "k": _const(k)}
+    cfg, desc, ora = _oracle(K.material_probe(mat))
+    cos_i = np.linspace(0.05, 1.0, 64)
+    wo = np.stack([np.sqrt(1 - cos_i ** 2), np.zeros_like(cos_i), cos_i], 1).astype(np.float32)
+    wi, f, pdf, delta = ora.bsdf_sample(0, wo, np.full((64, 3), 0.5, np.float32))
+    assert delta.all() and np.all(pdf == 1)
+    np.testing.assert_allclose(wi, wo * np.float32([-1, -1, 1]), atol=2e-6)
+    want = col[None] * np.stack([_fresnel_conductor(cos_i, (1 + 1j * k[c]) / ior[c]) for c in range(3)], 1)
+    np.testing.assert_allclose(f * wi[:, 2:3] / pdf[:, None], want, rtol=2e-4, atol=1e-6)
+    # delta: eval and pdf are zero for every pair
+    ef, ep = ora.bsdf_eval(0, wi, wo)
+    assert not ef.any() and not ep.any()
+
+
+def test_glass_splits_by_the_dielectric_fresnel_term():
+    # glass.cpp:34-70: reflect with probability Fr, refract with 1 - Fr;
+    # Snell's law; radiance scaled by (eta_i / eta_t)^2 on refraction
+    mat = {"type": "glass", "ior": _const(1.5), "color_reflection_map": _const(0.9),
+           "color_refraction_map": _const([0.64, 0.81, 1.0])}
+    cfg, desc, ora = _oracle(K.material_probe(mat))
+    n = 40_000
+    for cz in (0.9, 0.4, -0.8, -0.5):
+        wo = np.tile(_unit([math.sqrt(1 - cz * cz), 0, cz]), (n, 1))
+        u = np.random.default_rng(5).random((n, 3)).astype(np.float32)
+        wi, f, pdf, delta = ora.bsdf_sample(0, wo, u)
+        assert delta.all()
+        inside = cz < 0
+        fr = 1.0 if inside and math.sqrt(1 - cz * cz) * 1.5 >= 1 else \
+            float(_fresnel_dielectric(abs(cz), 1 / 1.5 if inside else 1.5))
+        refl = wi[:, 2] * cz > 0
+        assert abs(refl.mean() - fr) < 4 * math.sqrt(fr * (1 - fr) / n) + 1e-6
+        np.testing.assert_allclose(pdf[refl], fr, rtol=1e-5)
+        np.testing.assert_allclose((f[refl] * np.abs(wi[refl, 2:3]) / pdf[refl, None]), 0.9, rtol=1e-5)
+        if fr < 1:
+            t = ~refl
+            eta = 1 / 1.5 if not inside else 1.5   # eta_i / eta_t along the light path
+            sin_o = math.sqrt(1 - cz * cz)
+            np.testing.assert_allclose(np.sqrt(1 - wi[t, 2] ** 2), eta * sin_o, rtol=1e-4)
+            got = f[t] * np.abs(wi[t, 2:3]) / pdf[t, None]
+            np.testing.assert_allclose(got, np.broadcast_to(np.float32(eta * eta) * np.float32([0.8, 0.9, 1.0]),
+                                                            got.shape), rtol=1e-5)
+    # total internal reflection: always reflected
+    wo = np.tile(_unit([0.9, 0, -0.3]), (1000, 1))
+    wi, f, pdf, _ = ora.bsdf_sample(0, wo, np.random.default_rng(6).random((1000, 3)).astype(np.float32))
+    assert np.all(wi[:, 2] < 0) and np.all(pdf == 1)
+
+
+@pytest.mark.parametrize("mat", [
+    {"type": "metal", "color": _const([0.95, 0.8, 0.5]), "eta": _const([0.2, 0.4, 1.4]), "k": _const([3.9, 2.4, 1.9]),
+     "roughness": _const(0.4), "anisotropic": _const(0.5)},
+    {"type": "phong", "d": _const([0.5, 0.3, 0.2]), "s": _const([0.4, 0.4, 0.4]), "ns": _const(12)},
+], ids=["metal", "phong"])
+def test_glossy_sampling_follows_its_pdf(mat):
+    # aggregate.h: the sampled f / pdf equal eval / pdf at the sampled
+    # direction; the pdf integrates to at most 1 over the hemisphere (the
+    # part of a lobe below the horizon is lost); the importance estimate of
+    # the directional albedo matches a uniform-hemisphere estimate and is <= 1
+    cfg, desc, ora = _oracle(K.material_probe(mat))
+    n = 400_000
+    wo = np.tile(_unit([0.5, 0.2, 0.8]), (n, 1))
+    s_wi, s_f, s_pdf, delta = ora.bsdf_sample(0, wo, np.random.default_rng(8).random((n, 3)).astype(np.float32))
+    assert not delta.any()
+    ok = s_pdf > 0
+    assert ok.mean() > 0.8
+    e_f, e_pdf = ora.bsdf_eval(0, s_wi[ok], wo[ok])
+    np.testing.assert_allclose(s_pdf[ok], e_pdf, rtol=2e-4)
+    np.testing.assert_allclose(s_f[ok], e_f, rtol=2e-4, atol=1e-7)
+    wi = _hemi(n, 10)
+    f_u, p_u = ora.bsdf_eval(0, wi, wo)
+    mass = np.mean(p_u) * 2 * math.pi
+    assert 0.85 < mass < 1.01, mass
+    est = np.sum(s_f[ok] * s_wi[ok, 2:3] / s_pdf[ok, None], 0) / n
+    ref = np.mean(f_u * wi[:, 2:3], 0) * 2 * math.pi
+    np.testing.assert_allclose(est, ref, rtol=0.03)
+    assert np.all(est <= 1.0)
