@@ -85,7 +85,9 @@ class AtrcRenderDesc(C.Structure):
                 ("filter_alpha", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64), ("first_spp", C.c_int32),
                 ("spp_count", C.c_int32), ("camera", AtrcCameraDesc), ("path_pool", C.c_int32),
                 ("count_traversal", C.c_int32), ("task_grid_size", C.c_int32), ("sort_mode", C.c_int32),
-                ("disney_fixed", C.c_int32), ("reserved_", C.c_int32)]
+                ("disney_fixed", C.c_int32), ("renderer", C.c_int32),
+                ("ao_sample_count", C.c_int32), ("ao_max_distance", C.c_float), ("ao_low", C.c_float * 3),
+                ("ao_high", C.c_float * 3), ("ao_background", C.c_float * 3), ("pad_", C.c_int32)]
 
 
 class AtrcFilm(C.Structure):

@@ -2,8 +2,8 @@
 // `CLI -d scene.json` / `CLI -s "<json>"` (src/cli/src/main.cpp:14-72,
 // src/cli/src/params.cpp:6-43).  Every `rendering` entry of the configuration
 // is rendered on the GPU through the C ABI and its `save_to_img` post
-// processors run.  `--renderer pt_cuda` renders entries written for the CPU
-// `pt` renderer unchanged.
+// processors run.  `--renderer pt_cuda` (or `--gpu`) renders entries written
+// for the CPU `pt` and `ao` renderers unchanged.
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -22,10 +22,11 @@ namespace {
 
 void usage() {
     std::printf(
-        "usage: atrc_cli (-d scene.json | -s '<json>') [--renderer pt_cuda] [--device N] [--quiet]\n"
+        "usage: atrc_cli (-d scene.json | -s '<json>') [--renderer pt_cuda | --gpu] [--device N] [--quiet]\n"
         "  -d, --scene-filename  scene description file\n"
         "  -s, --scene           scene description text\n"
-        "  --renderer pt_cuda    render entries whose renderer type is `pt` on the GPU as well\n");
+        "  --renderer pt_cuda    render entries whose renderer type is `pt` or `ao` on the GPU as well\n"
+        "  --gpu                 the same as --renderer pt_cuda\n");
 }
 
 bool check(int rc, const char* what) {
@@ -50,6 +51,7 @@ int main(int argc, char** argv) {
         if ((a == "-d" || a == "--scene-filename") && i + 1 < argc) file = argv[++i];
         else if ((a == "-s" || a == "--scene") && i + 1 < argc) text = argv[++i];
         else if (a == "--renderer" && i + 1 < argc) force = argv[++i];
+        else if (a == "--gpu") force = "pt_cuda";
         else if (a == "--device" && i + 1 < argc) device = std::atoi(argv[++i]);
         else if (a == "--quiet") quiet = true;
         else { usage(); return a == "-h" || a == "--help" ? 0 : 1; }
@@ -82,7 +84,7 @@ int main(int argc, char** argv) {
         char type[32];
         atrc_config_rendering(cfg, r, &desc, type, sizeof(type));
         if (std::string(type) != "pt_cuda" && force != "pt_cuda") {
-            std::fprintf(stderr, "rendering %d: renderer `%s` runs on the CPU reference; pass --renderer pt_cuda\n", r,
+            std::fprintf(stderr, "rendering %d: renderer `%s` runs on the CPU reference; pass --gpu\n", r,
                          type);
             rc_all = 1;
             continue;

@@ -181,6 +181,10 @@ struct Params {
     float cont_prob, eps;
     int guide_on;           // sample surface vertices with the learned guide
     GuideFrame gf;          // guide buffers of this call (zero when guide_on == 0)
+    int renderer;           // AtrcRendererType
+    int ao_count;           // ao: occlusion rays per camera sample
+    float ao_dist;          // ao: occlusion distance
+    float ao_low[3], ao_high[3], ao_bg[3];
 };
 
 struct Pool {
@@ -511,6 +515,37 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
             h.t = hv.x; h.u = hv.y; h.v = hv.z; h.entity = ent; h.tri = P.hit_tri[slot];
             s = make_surface(S, h, o, d);
             have_surface = true;
+        }
+        if (p.renderer == ATRC_RENDERER_AO) {
+            // trace_ao (path_tracing.cpp:383-415): the pixel is
+            // lerp(low, high, unblocked fraction); it starts at `low` and each
+            // unblocked occlusion ray adds (high - low) / count in k_shadow
+            if (!have_surface) {
+                L = Vec3(p.ao_bg[0], p.ao_bg[1], p.ao_bg[2]);
+            } else {
+                const Entity& e = S.entities[ent];
+                P.gb_albedo[slot] = make_float4(p.ao_high[0], p.ao_high[1], p.ao_high[2],
+                                                (e.flags & ENT_NO_DENOISE) ? 0.0f : 1.0f);
+                P.gb_normal[slot] = make_float4(s.geo.z.x, s.geo.z.y, s.geo.z.z, 0);
+                L = Vec3(p.ao_low[0], p.ao_low[1], p.ao_low[2]);
+                const Vec3 step = (Vec3(p.ao_high[0], p.ao_high[1], p.ao_high[2]) - L) / float(p.ao_count);
+                const Vec3 start = eps_offset(s, s.geo.z, eps);
+                for (int k = 0; k < p.ao_count; ++k) {
+                    const float u = rng.u(), v = rng.u();
+                    float pdf;
+                    const Vec3 dir = normalize(s.geo.local_to_global(zweighted_on_hemisphere(u, v, &pdf)));
+                    // Scene::visible(start, end): segment trimmed by eps at both ends
+                    const Vec3 seg = (start + dir * p.ao_dist) - start;
+                    const float dis = length(seg);
+                    push_shadow(P, c, start, normalize(seg), eps, dis - eps, step, slot);
+                }
+            }
+            store_rng(st, rng);
+            P.st[slot] = st;
+            P.L[slot] = make_float4(L.x, L.y, L.z, L4.w);
+            const int fi = warp_append(&c->n_finish, true);
+            P.q_finish[fi] = slot;
+            continue;
         }
         // (1) pending MIS-BSDF term of the previous vertex (direct_illum.cpp:130-192)
         if (flags & PF_MIS) {
@@ -1039,6 +1074,12 @@ Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
 }
 
 // Settings shared by the views of a render (taken from the first view).
+// Shadow rays one path emits per iteration: one per light (pt), or the
+// occlusion rays of a camera hit (ao).
+static int shadow_rays_per_path(const Scene& S, const AtrcRenderDesc& d) {
+    return d.renderer == ATRC_RENDERER_AO ? std::max(1, d.ao_sample_count) : std::max(1, S.light_count);
+}
+
 Params make_params(const AtrcRenderDesc& d) {
     Params p{};
     p.min_depth = d.min_depth;
@@ -1046,6 +1087,14 @@ Params make_params(const AtrcRenderDesc& d) {
     p.specular_depth = d.specular_depth;
     p.cont_prob = d.cont_prob;
     p.eps = d.eps;
+    p.renderer = d.renderer;
+    p.ao_count = d.ao_sample_count;
+    p.ao_dist = d.ao_max_distance;
+    for (int k = 0; k < 3; ++k) {
+        p.ao_low[k] = d.ao_low[k];
+        p.ao_high[k] = d.ao_high[k];
+        p.ao_bg[k] = d.ao_background[k];
+    }
     return p;
 }
 
@@ -1236,6 +1285,10 @@ static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid sort_mode");
     if (desc->filter_type == ATRC_FILTER_BOX ? !(desc->filter_radius - desc->eps > 0) : !(desc->filter_radius > 0 && desc->filter_alpha > 0))
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid film filter");
+    if (desc->renderer != ATRC_RENDERER_PT && desc->renderer != ATRC_RENDERER_AO)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid renderer");
+    if (desc->renderer == ATRC_RENDERER_AO && (desc->ao_sample_count <= 0 || desc->ao_sample_count > 4096))
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: ao_sample_count must be in [1, 4096]");
     return ATRC_OK;
 }
 
@@ -1282,8 +1335,9 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             tb += (tile_table_bytes(views[v]) + 255) & ~size_t(255);
         }
     }
-    // path pool: enough paths to fill the GPU; shadow capacity = pool x lights
-    const int nl = std::max(1, d.scene.light_count);
+    // path pool: enough paths to fill the GPU; shadow capacity = pool x
+    // shadow rays one path can emit in one iteration
+    const int nl = shadow_rays_per_path(d.scene, *desc);
     size_t cap = desc->path_pool > 0 ? size_t(desc->path_pool) : size_t(d.tuned_pool);
     cap = std::min<size_t>(cap, std::max<unsigned long long>(total, 1024ULL));
     cap = std::min<size_t>(cap, (size_t(1) << 28) / nl);
@@ -1512,6 +1566,8 @@ int atrc_cuda_render_guided(AtrcScene* scene, AtrcGuide* guide, const AtrcRender
     if (!guide) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_guided: null guide");
     const int rc = check_render_args(scene, desc, film);
     if (rc != ATRC_OK) return rc;
+    if (desc->renderer != ATRC_RENDERER_PT)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_guided: guiding needs the pt renderer");
     return guarded([&] {
         return render_impl(scene, desc, film, 1, nullptr, nullptr, nullptr, stats, guide_impl(guide), record != 0);
     });
@@ -1521,6 +1577,8 @@ int atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide, const AtrcRenderD
                            const AtrcFilm* films, double* view_seconds, AtrcRenderStats* stats) {
     if (!scene || !views || !films || n < 1) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_batch: null argument");
     if (n > kMaxViews) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_batch: more than 1024 views");
+    if (guide && views[0].renderer != ATRC_RENDERER_PT)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_batch: guiding needs the pt renderer");
     const AtrcRenderDesc& a = views[0];
     for (int v = 0; v < n; ++v) {
         const int rc = check_render_args(scene, views + v, films + v);
@@ -1530,9 +1588,14 @@ int atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide, const AtrcRenderD
         const AtrcRenderDesc& b = views[v];
         if (b.min_depth != a.min_depth || b.max_depth != a.max_depth || b.cont_prob != a.cont_prob ||
             b.specular_depth != a.specular_depth || b.eps != a.eps || b.sort_mode != a.sort_mode ||
-            b.disney_fixed != a.disney_fixed || b.path_pool != a.path_pool || b.count_traversal != a.count_traversal)
+            b.disney_fixed != a.disney_fixed || b.path_pool != a.path_pool || b.count_traversal != a.count_traversal ||
+            b.renderer != a.renderer || b.ao_sample_count != a.ao_sample_count ||
+            b.ao_max_distance != a.ao_max_distance ||
+            std::memcmp(b.ao_low, a.ao_low, sizeof(a.ao_low)) || std::memcmp(b.ao_high, a.ao_high, sizeof(a.ao_high)) ||
+            std::memcmp(b.ao_background, a.ao_background, sizeof(a.ao_background)))
             return fail(ATRC_ERR_INVALID_ARG,
-                        "atrc_cuda_render_batch: views must share depth, roulette, eps, sort, Disney and pool settings");
+                        "atrc_cuda_render_batch: views must share renderer, depth, roulette, eps, sort, Disney and "
+                        "pool settings");
     }
     return guarded([&] {
         return render_impl(scene, views, films, n, nullptr, nullptr, nullptr, stats, guide ? guide_impl(guide) : nullptr,
@@ -1598,7 +1661,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
         // pools whose workspace stays under a quarter of the free memory
         size_t free_b = 0, total_b = 0;
         CK(cudaMemGetInfo(&free_b, &total_b));
-        const int nl = std::max(1, d.scene.light_count);
+        const int nl = shadow_rays_per_path(d.scene, *desc);
         const int nkeys = std::max(d.scene.material_count, 4) + 2;
         // (the workspace held now is freed before a larger one is allocated)
         auto pool_fits = [&](int pool) {
@@ -1722,6 +1785,10 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
     if (desc->filter_type == ATRC_FILTER_BOX ? !(desc->filter_radius - desc->eps > 0)
                                              : !(desc->filter_radius > 0 && desc->filter_alpha > 0))
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid film filter");
+    if (desc->renderer != ATRC_RENDERER_PT && desc->renderer != ATRC_RENDERER_AO)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid renderer");
+    if (desc->renderer == ATRC_RENDERER_AO && (desc->ao_sample_count <= 0 || desc->ao_sample_count > 4096))
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: ao_sample_count must be in [1, 4096]");
     return guarded([&] {
         DeviceSceneImpl& d = scene->impl;
         CK(cudaSetDevice(d.device));
@@ -1736,7 +1803,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         view.start = 0;
         view.count = (unsigned long long)view.SW * view.SH * spp;
         const unsigned long long total = view.count;
-        const int nl = std::max(1, d.scene.light_count);
+        const int nl = shadow_rays_per_path(d.scene, *desc);
         // the array holds the counters, the view, the tile tables, then the path pool
         const size_t counters_bytes = 512;
         const size_t view_bytes = (sizeof(View) + 255) & ~size_t(255);

@@ -634,11 +634,28 @@ public:
         parse_camera(r.child_group("camera"), float(d.width) / float(d.height), &d.camera);
         const ConfigGroup& rp = r.child_group("renderer");
         e.renderer_type = rp.child_str("type");
-        if (e.renderer_type != "pt" && e.renderer_type != "pt_cuda")
-            throw ConfigError("renderer type '" + e.renderer_type + "' is not supported (pt, pt_cuda)");
-        // PathTracingRendererCreator (renderer_creators.cpp:115-151)
+        if (e.renderer_type != "pt" && e.renderer_type != "pt_cuda" && e.renderer_type != "ao")
+            throw ConfigError("renderer type '" + e.renderer_type + "' is not supported (pt, pt_cuda, ao)");
         d.spp = rp.child_int("spp");
         if (d.spp <= 0) throw ConfigError("invalid spp value");
+        d.renderer = e.renderer_type == "ao" ? ATRC_RENDERER_AO : ATRC_RENDERER_PT;
+        // AORendererCreator (renderer_creators.cpp:19-38)
+        d.ao_sample_count = rp.child_int_or("ao_sample_count", 5);
+        if (d.renderer == ATRC_RENDERER_AO && d.ao_sample_count <= 0)
+            throw ConfigError("invalid ao_sample_count value");
+        d.ao_max_distance = rp.child_real_or("max_occlusion_distance", 1);
+        {
+            const Vec3 lo = rp.child_spectrum_or("low_color", Vec3(0, 0, 0));
+            const Vec3 hi = rp.child_spectrum_or("high_color", Vec3(1, 1, 1));
+            const Vec3 bg = rp.child_spectrum_or("background_color", Vec3(0, 0, 0));
+            const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z}, b3[3] = {bg.x, bg.y, bg.z};
+            for (int k = 0; k < 3; ++k) {
+                d.ao_low[k] = l3[k];
+                d.ao_high[k] = h3[k];
+                d.ao_background[k] = b3[k];
+            }
+        }
+        // PathTracingRendererCreator (renderer_creators.cpp:115-151)
         d.min_depth = rp.child_int_or("min_depth", 5);
         d.max_depth = rp.child_int_or("max_depth", 10);
         d.cont_prob = rp.child_real_or("cont_prob", 0.9f);

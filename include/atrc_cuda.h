@@ -274,8 +274,24 @@ typedef struct AtrcRenderDesc {
                                      /* pdf); 1: the diffuse lobe is sampled */
                                      /* (sampling matches the pdf; needed by */
                                      /* guided rendering and error studies)  */
-    int32_t  reserved_;
+    int32_t  renderer;               /* AtrcRendererType                     */
+    /* `ao` renderer keys (renderer_creators.cpp:19-38, trace_ao in         */
+    /* path_tracing.cpp:383-415): a pixel is lerp(low, high, fraction of    */
+    /* ao_sample_count cosine-distributed rays from the first hit that are  */
+    /* not blocked within ao_max_distance); background on a miss            */
+    int32_t  ao_sample_count;        /* default 5                            */
+    float    ao_max_distance;        /* max_occlusion_distance, default 1    */
+    float    ao_low[3];              /* low_color, default 0                 */
+    float    ao_high[3];             /* high_color, default 1                */
+    float    ao_background[3];       /* background_color, default 0          */
+    int32_t  pad_;
 } AtrcRenderDesc;
+
+/* Renderer of a render call. */
+typedef enum AtrcRendererType {
+    ATRC_RENDERER_PT = 0,   /* `pt` / `pt_cuda`: volumetric path tracing with NEE and MIS */
+    ATRC_RENDERER_AO = 1    /* `ao`: ambient occlusion                                   */
+} AtrcRendererType;
 
 /* Sorting of hit records before shading (a counting sort by key). */
 typedef enum AtrcSortMode {

@@ -2292,6 +2292,32 @@ Pixel trace_std(const OracleScene& sc, const AtrcRenderDesc& p, Ray r, Sampler& 
     return px;
 }
 
+// render::trace_ao (path_tracing.cpp:383-415)
+Pixel trace_ao(const OracleScene& sc, const AtrcRenderDesc& p, Ray r, Sampler& s) {
+    Pixel px;
+    EntInct in;
+    if (!sc.closest(r, &in)) {
+        px.value = V3(p.ao_background);
+        return px;
+    }
+    const V3 low(p.ao_low), high(p.ao_high);
+    px.albedo = high;
+    px.normal = in.geo.z;
+    px.denoise = in.ent->no_denoise ? 0.0f : 1.0f;
+    const V3 start = in.eps_offset(in.geo.z);
+    float ao = 0;
+    for (int i = 0; i < p.ao_sample_count; ++i) {
+        const float u = s.u(), v = s.u();
+        float pdf;
+        const V3 dir = normalize(in.geo.local_to_global(zweighted_on_hemisphere(u, v, &pdf)));
+        if (sc.visible(start, start + dir * p.ao_max_distance)) ao += 1;
+    }
+    ao /= float(p.ao_sample_count);
+    const float t = clampf(ao, 0, 1);
+    px.value = low * (1 - t) + high * t;
+    return px;
+}
+
 // Film filter values (box_filter.cpp:6-34, gaussian_filter.cpp:6-78)
 struct Filter {
     int type = ATRC_FILTER_BOX;
@@ -2563,7 +2589,8 @@ int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film
                     V3 o = pos + fx * lens.x + fy * lens.y + fz * lens.z;
                     V3 ld = focal - lens;
                     V3 dir = normalize(fx * ld.x + fy * ld.y + fz * ld.z);
-                    Pixel pv = trace_std(*s, *d, Ray(o, dir), smp);
+                    Pixel pv = d->renderer == ATRC_RENDERER_AO ? trace_ao(*s, *d, Ray(o, dir), smp)
+                                                               : trace_std(*s, *d, Ray(o, dir), smp);
                     if (!finite3(pv.value)) continue;
                     // apply_image_filter (framebuffer.h:49-80)
                     const int xmin = std::max(x0, int(std::ceil(pixel_x - filter.radius - 0.5f)));

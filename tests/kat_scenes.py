@@ -236,3 +236,25 @@ def materials_scene(tmp: Path, renderer="pt", spp=256, width=48, height=36) -> d
                           "width": width, "height": height,
                           "renderer": {"type": renderer, "spp": spp, "max_depth": 12, "min_depth": 3},
                           "reporter": {"type": "noout"}}}
+
+
+def ao_slab(h=0.5, dist=1.0, spp=256, count=5, looking_up=False) -> dict:
+    """`ao` between two large parallel quads h apart, seen from between them.
+    A cosine-distributed ray from the floor meets the ceiling after
+    h / cos(theta), so it is unblocked within `dist` iff cos(theta) < h / dist:
+    the expected unblocked fraction is (h / dist)^2 (with the eps trims:
+    ((h - eps) / (dist - eps))^2)."""
+    def quad(z):
+        return {"type": "geometric", "geometry": {"type": "quad", "A": [-100, -100, z], "B": [100, -100, z],
+                                                  "C": [100, 100, z], "D": [-100, 100, z], "transform": []},
+                "material": {"type": "ideal_diffuse", "albedo": {"type": "constant", "texel": [0.5]}}}
+    ents = [quad(0.0), quad(h)] if not looking_up else [quad(0.0)]
+    dst = [0, 0, 1] if looking_up else [0, 0, 0]
+    return {"scene": {"type": "default", "entities": ents},
+            "rendering": {"camera": {"type": "thin_lens", "pos": [0, 0, 0.5 * h], "dst": dst, "up": [0, 1, 0],
+                                     "fov": 20},
+                          "width": 8, "height": 8,
+                          "renderer": {"type": "ao", "spp": spp, "ao_sample_count": count,
+                                       "max_occlusion_distance": dist, "low_color": [0.1, 0.2, 0.3],
+                                       "high_color": [0.9, 0.8, 0.7], "background_color": [0.05, 0.06, 0.07]},
+                          "reporter": {"type": "noout"}}}

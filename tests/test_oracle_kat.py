@@ -256,3 +256,31 @@ def test_glossy_sampling_follows_its_pdf(mat):
     ref = np.mean(f_u * wi[:, 2:3], 0) * 2 * math.pi
     np.testing.assert_allclose(est, ref, rtol=0.03)
     assert np.all(est <= 1.0)
+
+
+def test_ao_unblocked_fraction_between_parallel_planes():
+    # trace_ao (path_tracing.cpp:383-415): lerp(low, high, unblocked fraction)
+    cfg, desc, ora = _oracle(K.ao_slab(h=0.5, dist=1.0, spp=256))
+    assert desc.renderer == 1 and desc.ao_sample_count == 5
+    f = Film(desc.width, desc.height, gbuffer=True)
+    ora.render(desc, f)
+    img = f.image().reshape(-1, 3)
+    e = desc.eps
+    frac = ((0.5 - e) / (1.0 - e)) ** 2
+    low, high = np.array([0.1, 0.2, 0.3]), np.array([0.9, 0.8, 0.7])
+    want = low + (high - low) * frac
+    n = desc.width * desc.height * desc.spp
+    sigma = np.abs(high - low) * math.sqrt(frac * (1 - frac) / (n * 5))
+    assert np.all(np.abs(img.mean(0) - want) < 5 * sigma + 1e-6), (img.mean(0), want)
+    w = f.weight.reshape(-1, 1)
+    np.testing.assert_allclose(f.albedo.reshape(-1, 3) / w, np.broadcast_to(high, (64, 3)), rtol=1e-6)
+    np.testing.assert_allclose(np.abs(f.normal.reshape(-1, 3) / w)[:, 2], 1.0, rtol=1e-6)
+
+
+def test_ao_background_on_miss():
+    cfg, desc, ora = _oracle(K.ao_slab(spp=4, looking_up=True))
+    f = Film(desc.width, desc.height, gbuffer=True)
+    ora.render(desc, f)
+    np.testing.assert_allclose(f.image().reshape(-1, 3), np.broadcast_to(np.float32([0.05, 0.06, 0.07]), (64, 3)),
+                               rtol=1e-6)
+    assert not f.albedo.any()
