@@ -292,3 +292,34 @@ class DeviceScene:
                                               C.byref(cancel) if cancel is not None else None, cb, None,
                                               C.byref(st)))
         return {k: getattr(st, k) for k, _ in AtrcRenderStats._fields_}
+
+
+# ------------------------------------------------------------ BVH builders
+
+def bvh_build(boxes: np.ndarray, builder: str = "sah", device: int = 0) -> dict:
+    """Build a mesh tree over (n, 6) float32 boxes (lo xyz, hi xyz) with the
+    host SAH builder or the device PLOC builder; returns the build time, the
+    4-wide tree's surface-area cost, its node count, rounds and depth."""
+    b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+    info = abi.AtrcBvhBuildInfo()
+    kind = {"sah": 0, "ploc": 1}[builder]
+    _check(load_library().atrc_bvh_build(kind, device, b.ctypes.data_as(abi.c_float_p), len(b), C.byref(info)))
+    return {k: getattr(info, k) for k, _ in abi.AtrcBvhBuildInfo._fields_}
+
+
+def bvh_cluster_tree(boxes: np.ndarray, device: int = -1) -> dict:
+    """PLOC cluster tree over (n, 6) boxes on the host (device < 0) or on a
+    GPU: order, left, right, node boxes (internal node n + k), root, rounds."""
+    b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+    n = len(b)
+    order = np.zeros(n, np.uint32)
+    left = np.zeros(max(n - 1, 1), np.int32)
+    right = np.zeros(max(n - 1, 1), np.int32)
+    nb = np.zeros((max(n - 1, 1), 6), np.float32)
+    root, rounds = C.c_int32(), C.c_int32()
+    _check(load_library().atrc_bvh_cluster_tree(
+        device, b.ctypes.data_as(abi.c_float_p), n, order.ctypes.data_as(C.POINTER(C.c_uint32)),
+        left.ctypes.data_as(C.POINTER(C.c_int32)), right.ctypes.data_as(C.POINTER(C.c_int32)),
+        nb.ctypes.data_as(abi.c_float_p), C.byref(root), C.byref(rounds)))
+    return {"order": order, "left": left[:n - 1], "right": right[:n - 1], "boxes": nb[:n - 1],
+            "root": root.value, "rounds": rounds.value}

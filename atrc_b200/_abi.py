@@ -62,7 +62,7 @@ class AtrcEnvDesc(C.Structure):
 
 class AtrcSceneDesc(C.Structure):
     _fields_ = [("abi_version", C.c_uint32), ("aggregate", C.c_int32), ("aggregate_max_leaf_size", C.c_int32),
-                ("pad_", C.c_int32),
+                ("bvh_builder", C.c_int32),
                 ("meshes", C.POINTER(AtrcMeshDesc)), ("mesh_count", C.c_uint32),
                 ("geometries", C.POINTER(AtrcGeometryDesc)), ("geometry_count", C.c_uint32),
                 ("entities", C.POINTER(AtrcEntityDesc)), ("entity_count", C.c_uint32),
@@ -138,9 +138,14 @@ class AtrcGuideInfo(C.Structure):
                 ("max_select", C.c_float), ("pad2_", C.c_float)]
 
 
+class AtrcBvhBuildInfo(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("sah_cost", C.c_double), ("nodes", C.c_uint64), ("rounds", C.c_int32),
+                ("max_depth", C.c_int32)]
+
+
 STRUCT_ORDER = [AtrcSceneDesc, AtrcMeshDesc, AtrcGeometryDesc, AtrcEntityDesc, AtrcTexture2DDesc,
                 AtrcTexture3DDesc, AtrcMaterialDesc, AtrcMediumDesc, AtrcEnvDesc, AtrcRenderDesc, AtrcFilm,
-                AtrcRenderStats, AtrcRay, AtrcHit, AtrcDeviceInfo, AtrcTuning]
+                AtrcRenderStats, AtrcRay, AtrcHit, AtrcDeviceInfo, AtrcTuning, AtrcBvhBuildInfo]
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_double, C.c_void_p)
 
@@ -187,6 +192,10 @@ PROTOTYPES = {
     "atrc_guide_train_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.c_int, C.POINTER(C.c_float)]),
     "atrc_guide_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "atrc_cuda_scene_bounds": (C.c_int, [C.c_void_p, c_float_p, c_float_p]),
+    "atrc_bvh_build": (C.c_int, [C.c_int32, C.c_int32, c_float_p, C.c_uint64, C.POINTER(AtrcBvhBuildInfo)]),
+    "atrc_bvh_cluster_tree": (C.c_int, [C.c_int32, c_float_p, C.c_uint64, C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32), c_float_p,
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "atrc_cuda_render_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32,
                                          C.POINTER(AtrcFilm), C.POINTER(C.c_double), C.POINTER(AtrcRenderStats)]),
     "atrc_cuda_render_guided": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(AtrcRenderDesc), C.c_int32,

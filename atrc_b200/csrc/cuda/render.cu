@@ -1194,8 +1194,10 @@ int atrc_cuda_scene_create(const AtrcSceneDesc* desc, AtrcScene** out) {
     *out = nullptr;
     return guarded([&] {
         check_device_ready();
+        int device = 0;
+        CK(cudaGetDevice(&device));
         auto hs = std::make_unique<HostScene>();
-        build_host_scene(*desc, hs.get());
+        build_host_scene(*desc, hs.get(), device);
         auto sc = std::make_unique<AtrcScene>();
         DeviceSceneImpl& d = sc->impl;
         CK(cudaGetDevice(&d.device));

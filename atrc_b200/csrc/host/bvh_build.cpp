@@ -294,4 +294,272 @@ void validate_bvh4(const std::vector<Bvh4Node>& nodes, int32_t root, uint32_t pr
         if (!covered[k]) throw std::runtime_error("BVH primitive in no leaf");
 }
 
+// ------------------------------------------------------------------- PLOC
+
+namespace {
+
+uint64_t spread21(uint32_t v) {
+    uint64_t x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x1f00000000ffffULL;
+    x = (x | x << 16) & 0x1f0000ff0000ffULL;
+    x = (x | x << 8) & 0x100f00f00f00f00fULL;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
+    return x;
+}
+
+float box_area(const BuildPrim& b) {
+    const float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+BuildPrim box_union(const BuildPrim& a, const BuildPrim& b) {
+    BuildPrim u;
+    for (int k = 0; k < 3; ++k) {
+        u.lo[k] = std::min(a.lo[k], b.lo[k]);
+        u.hi[k] = std::max(a.hi[k], b.hi[k]);
+    }
+    return u;
+}
+
+// (min, max) of the position pair, compared lexicographically
+bool pair_before(uint32_t i, uint32_t j1, uint32_t j2) {
+    const uint32_t a1 = std::min(i, j1), b1 = std::max(i, j1), a2 = std::min(i, j2), b2 = std::max(i, j2);
+    return a1 != a2 ? a1 < a2 : b1 < b2;
+}
+
+}  // namespace
+
+uint64_t morton63(const BuildPrim& p, const float lo[3], const float inv_ext[3]) {
+    uint32_t q[3];
+    for (int a = 0; a < 3; ++a) {
+        const float c = 0.5f * (p.lo[a] + p.hi[a]);
+        float t = (c - lo[a]) * inv_ext[a];
+        if (!(t >= 0.0f)) t = 0.0f;
+        if (t > 1.0f) t = 1.0f;
+        q[a] = uint32_t(t * 2097151.0f);
+    }
+    return spread21(q[0]) | spread21(q[1]) << 1 | spread21(q[2]) << 2;
+}
+
+float union_area(const BuildPrim& a, const BuildPrim& b) {
+    const float dx = std::max(a.hi[0], b.hi[0]) - std::min(a.lo[0], b.lo[0]);
+    const float dy = std::max(a.hi[1], b.hi[1]) - std::min(a.lo[1], b.lo[1]);
+    const float dz = std::max(a.hi[2], b.hi[2]) - std::min(a.lo[2], b.lo[2]);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+ClusterTree ploc_build_host(const std::vector<BuildPrim>& prims, int radius) {
+    ClusterTree t;
+    const uint32_t n = uint32_t(prims.size());
+    t.n = n;
+    if (n == 0) return t;
+    if (radius < 1) throw std::runtime_error("PLOC radius must be positive");
+    float clo[3], chi[3], inv[3];
+    for (int a = 0; a < 3; ++a) {
+        clo[a] = std::numeric_limits<float>::infinity();
+        chi[a] = -std::numeric_limits<float>::infinity();
+    }
+    for (const BuildPrim& p : prims)
+        for (int a = 0; a < 3; ++a) {
+            if (!std::isfinite(p.lo[a]) || !std::isfinite(p.hi[a])) throw std::runtime_error("non-finite primitive bound");
+            const float c = 0.5f * (p.lo[a] + p.hi[a]);
+            clo[a] = std::min(clo[a], c);
+            chi[a] = std::max(chi[a], c);
+        }
+    for (int a = 0; a < 3; ++a) inv[a] = chi[a] > clo[a] ? 1.0f / (chi[a] - clo[a]) : 0.0f;
+    std::vector<std::pair<uint64_t, uint32_t>> keys(n);
+    for (uint32_t i = 0; i < n; ++i) keys[i] = {morton63(prims[i], clo, inv), i};
+    std::sort(keys.begin(), keys.end());
+    t.order.resize(n);
+    std::vector<BuildPrim> box(size_t(2) * n - 1);
+    for (uint32_t i = 0; i < n; ++i) {
+        t.order[i] = keys[i].second;
+        box[i] = prims[keys[i].second];
+    }
+    std::vector<int32_t> C(n), next_c(n), nn(n);
+    for (uint32_t i = 0; i < n; ++i) C[i] = int32_t(i);
+    t.left.reserve(n - 1);
+    t.right.reserve(n - 1);
+    t.box.reserve(n - 1);
+    uint32_t m = n, next = n;
+    while (m > 1) {
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t j0 = i > uint32_t(radius) ? i - uint32_t(radius) : 0;
+            const uint32_t j1 = std::min(m - 1, i + uint32_t(radius));
+            int32_t best = -1;
+            float best_a = 0.0f;
+            for (uint32_t j = j0; j <= j1; ++j) {
+                if (j == i) continue;
+                const float a = union_area(box[size_t(C[i])], box[size_t(C[j])]);
+                if (best < 0 || a < best_a || (a == best_a && pair_before(i, j, uint32_t(best)))) {
+                    best = int32_t(j);
+                    best_a = a;
+                }
+            }
+            nn[i] = best;
+        }
+        uint32_t merges = 0, w = 0;
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t j = uint32_t(nn[i]);
+            if (uint32_t(nn[j]) == i && i < j) {
+                const uint32_t k = next++;
+                t.left.push_back(C[i]);
+                t.right.push_back(C[j]);
+                box[k] = box_union(box[size_t(C[i])], box[size_t(C[j])]);
+                t.box.push_back(box[k]);
+                next_c[i] = int32_t(k);
+                ++merges;
+            } else {
+                next_c[i] = C[i];
+            }
+        }
+        if (merges == 0) throw std::runtime_error("PLOC made no progress");
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t j = uint32_t(nn[i]);
+            if (uint32_t(nn[j]) == i && j < i) continue;  // merged into position j
+            C[w++] = next_c[i];
+        }
+        m = w;
+        ++t.rounds;
+    }
+    t.root = C[0];
+    return t;
+}
+
+BvhResult bvh_from_clusters(const ClusterTree& t, const std::vector<BuildPrim>& prims, int max_leaf,
+                            float traversal_cost, float intersect_cost) {
+    BvhResult res;
+    const uint32_t n = t.n;
+    if (max_leaf < 1 || max_leaf > 16) throw std::runtime_error("max_leaf must be in [1, 16]");
+    if (n != prims.size() || t.order.size() != n || t.left.size() + 1 != std::max<size_t>(n, 1) ||
+        t.right.size() != t.left.size() || t.box.size() != t.left.size())
+        throw std::runtime_error("cluster tree does not match its primitives");
+    if (n == 0) {
+        res.root_link = 0;
+        for (int k = 0; k < 3; ++k) res.bound_lo[k] = res.bound_hi[k] = 0;
+        return res;
+    }
+    if (n >= (1u << 27)) throw std::runtime_error("too many primitives for one BVH");
+    const size_t total = size_t(2) * n - 1;
+    if (t.root < 0 || size_t(t.root) >= total) throw std::runtime_error("cluster tree root out of range");
+    auto box_of = [&](int32_t node) -> const BuildPrim& {
+        return uint32_t(node) < n ? prims[t.order[size_t(node)]] : t.box[size_t(node) - n];
+    };
+    // bottom-up: children are created before their parents
+    std::vector<uint32_t> count(total, 1);
+    std::vector<float> cost(total, intersect_cost);
+    std::vector<uint8_t> leaf(total, 1);
+    for (uint32_t k = 0; k + 1 < n; ++k) {
+        const size_t node = size_t(n) + k;
+        const int32_t l = t.left[k], r = t.right[k];
+        if (l < 0 || r < 0 || size_t(l) >= node || size_t(r) >= node)
+            throw std::runtime_error("cluster tree child out of order");
+        count[node] = count[size_t(l)] + count[size_t(r)];
+        const float A = box_area(t.box[k]);
+        const float cl = cost[size_t(l)], cr = cost[size_t(r)];
+        const float split = A > 0.0f ? traversal_cost + (box_area(box_of(l)) * cl + box_area(box_of(r)) * cr) / A
+                                     : traversal_cost + cl + cr;
+        const bool as_leaf = count[node] <= uint32_t(max_leaf) && float(count[node]) * intersect_cost <= split;
+        leaf[node] = as_leaf;
+        cost[node] = as_leaf ? float(count[node]) * intersect_cost : split;
+    }
+    res.order.reserve(n);
+    std::vector<int32_t> walk;
+    auto emit_leaf = [&](int32_t node) -> int32_t {
+        const uint32_t first = uint32_t(res.order.size());
+        walk.assign(1, node);
+        while (!walk.empty()) {
+            const int32_t x = walk.back();
+            walk.pop_back();
+            if (uint32_t(x) < n) {
+                res.order.push_back(t.order[size_t(x)]);
+            } else {
+                walk.push_back(t.right[size_t(x) - n]);
+                walk.push_back(t.left[size_t(x) - n]);
+            }
+        }
+        return leaf_link(first, uint32_t(res.order.size()) - first);
+    };
+    const BuildPrim& rb = box_of(t.root);
+    for (int k = 0; k < 3; ++k) {
+        res.bound_lo[k] = rb.lo[k];
+        res.bound_hi[k] = rb.hi[k];
+    }
+    if (leaf[size_t(t.root)]) {
+        res.root_link = emit_leaf(t.root);
+        return res;
+    }
+    struct Item {
+        int32_t node;
+        int32_t bin;
+        int depth;
+    };
+    std::vector<Item> stack{{t.root, 0, 1}};
+    res.nodes.reserve(n / 2 + 1);
+    res.nodes.push_back(BvhNode{});
+    res.root_link = 0;
+    while (!stack.empty()) {
+        const Item it = stack.back();
+        stack.pop_back();
+        res.max_depth = std::max(res.max_depth, it.depth);
+        const int32_t kids[2] = {t.left[size_t(it.node) - n], t.right[size_t(it.node) - n]};
+        int32_t links[2];
+        for (int c = 0; c < 2; ++c) {
+            if (leaf[size_t(kids[c])]) {
+                links[c] = emit_leaf(kids[c]);
+            } else {
+                links[c] = int32_t(res.nodes.size());
+                res.nodes.push_back(BvhNode{});
+                stack.push_back({kids[c], links[c], it.depth + 1});
+            }
+        }
+        BvhNode& nd = res.nodes[size_t(it.bin)];
+        const BuildPrim& lb = box_of(kids[0]);
+        const BuildPrim& rb2 = box_of(kids[1]);
+        nd.c0lo_x = lb.lo[0]; nd.c0hi_x = lb.hi[0]; nd.c0lo_y = lb.lo[1]; nd.c0hi_y = lb.hi[1];
+        nd.c1lo_x = rb2.lo[0]; nd.c1hi_x = rb2.hi[0]; nd.c1lo_y = rb2.lo[1]; nd.c1hi_y = rb2.hi[1];
+        nd.c0lo_z = lb.lo[2]; nd.c0hi_z = lb.hi[2]; nd.c1lo_z = rb2.lo[2]; nd.c1hi_z = rb2.hi[2];
+        nd.link0 = links[0];
+        nd.link1 = links[1];
+        nd.pad0 = nd.pad1 = 0;
+    }
+    if (res.order.size() != n) throw std::runtime_error("cluster tree leaves do not cover the primitives");
+    return res;
+}
+
+double bvh4_sah_cost(const std::vector<Bvh4Node>& nodes, int32_t root, float traversal_cost, float intersect_cost) {
+    auto slot_area = [](const Bvh4Node& w, int k) {
+        const double dx = double(w.hi_x[k]) - w.lo_x[k], dy = double(w.hi_y[k]) - w.lo_y[k],
+                     dz = double(w.hi_z[k]) - w.lo_z[k];
+        return dx * dy + dy * dz + dz * dx;
+    };
+    if (root < 0) return intersect_cost * double((uint32_t(~root) & 15) + 1);
+    const Bvh4Node& r = nodes[size_t(root)];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < 4; ++k) {
+        if (r.link[k] == kEmptyLink) continue;
+        lo[0] = std::min(lo[0], double(r.lo_x[k])); hi[0] = std::max(hi[0], double(r.hi_x[k]));
+        lo[1] = std::min(lo[1], double(r.lo_y[k])); hi[1] = std::max(hi[1], double(r.hi_y[k]));
+        lo[2] = std::min(lo[2], double(r.lo_z[k])); hi[2] = std::max(hi[2], double(r.hi_z[k]));
+    }
+    const double a0 = std::max(1e-300, (hi[0] - lo[0]) * (hi[1] - lo[1]) + (hi[1] - lo[1]) * (hi[2] - lo[2]) +
+                                           (hi[2] - lo[2]) * (hi[0] - lo[0]));
+    double cost = 0;
+    std::vector<std::pair<int32_t, double>> stack{{root, a0}};
+    while (!stack.empty()) {
+        const auto [link, area] = stack.back();
+        stack.pop_back();
+        cost += traversal_cost * area / a0;
+        const Bvh4Node& w = nodes[size_t(link)];
+        for (int k = 0; k < 4; ++k) {
+            const int32_t l = w.link[k];
+            if (l == kEmptyLink) continue;
+            if (l < 0) cost += intersect_cost * double((uint32_t(~l) & 15) + 1) * slot_area(w, k) / a0;
+            else stack.push_back({l, slot_area(w, k)});
+        }
+    }
+    return cost;
+}
+
 }  // namespace atrc

@@ -65,4 +65,55 @@ BvhResult build_bvh(const std::vector<BuildPrim>& prims, int max_leaf, float tra
 
 inline int32_t leaf_link(uint32_t first, uint32_t count) { return ~int32_t((first << 4) | (count - 1)); }
 
+// ------------------------------------------------------------- PLOC
+// Parallel locally-ordered clustering (Meister and Bittner 2018, "Parallel
+// Locally-Ordered Clustering for Bounding Volume Hierarchy Construction"):
+// primitives sorted by the 63-bit Morton code of their box centres start as
+// clusters; every round, each cluster finds the cluster within `radius`
+// positions whose union box has the smallest surface area, mutual nearest
+// neighbours merge (the new cluster keeps the lower position) and the list
+// is compacted, until one cluster is left.  Ties are broken by the pair of
+// positions, so the nearest-neighbour relation has a strict order, every
+// round merges at least one pair, and the tree does not depend on thread
+// timing: the device build (bvh_gpu.cu) and the serial build below give the
+// same tree bit for bit.
+//
+// The binary cluster tree: node i < n is the leaf of sorted primitive i,
+// node n + k is the k-th merge (children created before their parent).
+struct ClusterTree {
+    uint32_t n = 0;
+    int32_t root = -1;
+    std::vector<uint32_t> order;       // sorted position -> primitive index
+    std::vector<int32_t> left, right;  // children of internal node n + k
+    std::vector<BuildPrim> box;        // box of internal node n + k
+    int rounds = 0;
+};
+
+constexpr int kPlocRadius = 16;
+
+// Box centre quantised to 21 bits per axis, bits interleaved x-y-z (x in
+// the lowest position); lo / inv_ext map the centre bound to [0, 1].
+uint64_t morton63(const BuildPrim& p, const float lo[3], const float inv_ext[3]);
+
+// Surface-area measure of the union of two boxes, as the cluster distance.
+float union_area(const BuildPrim& a, const BuildPrim& b);
+
+// Serial PLOC (the specification of the device build; O(n radius) per round).
+ClusterTree ploc_build_host(const std::vector<BuildPrim>& prims, int radius = kPlocRadius);
+
+// Device PLOC on `device` (bvh_gpu.cu); throws std::runtime_error.
+ClusterTree ploc_build_device(const std::vector<BuildPrim>& prims, int device, int radius = kPlocRadius);
+
+// A cluster tree as a binary BVH with leaves of up to max_leaf primitives:
+// a subtree becomes a leaf where that is cheaper under the surface-area
+// heuristic (leaf: count * intersect_cost; split: traversal_cost + the
+// children's costs weighted by their area over the parent's).
+BvhResult bvh_from_clusters(const ClusterTree& t, const std::vector<BuildPrim>& prims, int max_leaf,
+                            float traversal_cost = 1.0f, float intersect_cost = 1.0f);
+
+// Surface-area cost of a 4-wide tree (interior visits weighted by area over
+// the root's area, plus leaf primitives likewise), for comparing builders.
+double bvh4_sah_cost(const std::vector<Bvh4Node>& nodes, int32_t root, float traversal_cost = 1.0f,
+                     float intersect_cost = 1.0f);
+
 }  // namespace atrc

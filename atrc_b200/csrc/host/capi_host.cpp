@@ -49,13 +49,13 @@ int atrc_abi_version(void) { return ATRC_ABI_VERSION; }
 const char* atrc_last_error(void) { return atrc::g_last_error.c_str(); }
 
 int atrc_abi_struct_sizes(uint64_t* sizes, int n) {
-    const uint64_t s[16] = {sizeof(AtrcSceneDesc), sizeof(AtrcMeshDesc), sizeof(AtrcGeometryDesc),
+    const uint64_t s[17] = {sizeof(AtrcSceneDesc), sizeof(AtrcMeshDesc), sizeof(AtrcGeometryDesc),
                             sizeof(AtrcEntityDesc), sizeof(AtrcTexture2DDesc), sizeof(AtrcTexture3DDesc),
                             sizeof(AtrcMaterialDesc), sizeof(AtrcMediumDesc), sizeof(AtrcEnvDesc),
                             sizeof(AtrcRenderDesc), sizeof(AtrcFilm), sizeof(AtrcRenderStats), sizeof(AtrcRay),
-                            sizeof(AtrcHit), sizeof(AtrcDeviceInfo), sizeof(AtrcTuning)};
-    for (int i = 0; sizes && i < n && i < 16; ++i) sizes[i] = s[i];
-    return 16;
+                            sizeof(AtrcHit), sizeof(AtrcDeviceInfo), sizeof(AtrcTuning), sizeof(AtrcBvhBuildInfo)};
+    for (int i = 0; sizes && i < n && i < 17; ++i) sizes[i] = s[i];
+    return 17;
 }
 
 int atrc_config_load_file(const char* path, AtrcConfig** out) {

@@ -149,8 +149,9 @@ float lum(Vec3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 
 }  // namespace
 
-void build_host_scene(const AtrcSceneDesc& d, HostScene* hs) {
+void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
     if (d.abi_version != ATRC_ABI_VERSION) throw std::runtime_error("scene description ABI version mismatch");
+    if (d.bvh_builder < ATRC_BVH_SAH || d.bvh_builder > ATRC_BVH_AUTO) throw std::runtime_error("invalid bvh_builder");
     *hs = HostScene();
     // ------------------------------------------------------------- leaves
     std::vector<LeafInfo> leaves(d.geometry_count);
@@ -266,7 +267,9 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs) {
             throw std::runtime_error("unknown geometry type");
         }
         // bottom-level BVH over this leaf's triangles
-        BvhResult bvh = build_bvh(prims, 4);
+        const bool ploc = device >= 0 && (d.bvh_builder == ATRC_BVH_PLOC ||
+                                          (d.bvh_builder == ATRC_BVH_AUTO && prims.size() >= (size_t(1) << 18)));
+        BvhResult bvh = ploc ? bvh_from_clusters(ploc_build_device(prims, device), prims, 4) : build_bvh(prims, 4);
         hs->max_blas_depth = std::max(hs->max_blas_depth, bvh.max_depth);
         const int32_t tri_off = int32_t(hs->tri_shade.size());
         auto fix_leaf = [&](int32_t link) -> int32_t {

@@ -33,6 +33,8 @@ struct HostScene {
 };
 
 // Throws std::runtime_error with a message on unsupported or invalid input.
-void build_host_scene(const AtrcSceneDesc& desc, HostScene* out);
+// `device` runs the PLOC builder where the description asks for it (-1:
+// build every tree on the host with the SAH builder).
+void build_host_scene(const AtrcSceneDesc& desc, HostScene* out, int device = -1);
 
 }  // namespace atrc

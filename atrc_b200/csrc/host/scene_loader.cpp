@@ -591,10 +591,20 @@ public:
                 throw ConfigError("unknown creator type name: " + at + " (aggregate)");
             }
         }
+        // pt_cuda-only key: builder of the device scene's mesh trees
+        int builder = ATRC_BVH_SAH;
+        if (p.find_child("bvh_builder")) {
+            const std::string b = p.child_str("bvh_builder");
+            if (b == "sah") builder = ATRC_BVH_SAH;
+            else if (b == "ploc") builder = ATRC_BVH_PLOC;
+            else if (b == "auto") builder = ATRC_BVH_AUTO;
+            else throw ConfigError("invalid bvh_builder value: " + b + " (expect sah/ploc/auto)");
+        }
         AtrcSceneDesc& s = out_.scene;
         s.abi_version = ATRC_ABI_VERSION;
         s.aggregate = agg;
         s.aggregate_max_leaf_size = leaf;
+        s.bvh_builder = builder;
         s.meshes = out_.meshes.data(); s.mesh_count = uint32_t(out_.meshes.size());
         s.geometries = out_.geometries.data(); s.geometry_count = uint32_t(out_.geometries.size());
         s.entities = out_.entities.data(); s.entity_count = uint32_t(out_.entities.size());

@@ -216,11 +216,20 @@ typedef enum AtrcAggregateType {
     ATRC_AGG_NATIVE = 0, ATRC_AGG_BVH = 1
 } AtrcAggregateType;
 
+/* Builder of the per-mesh bottom-level trees of the device scene.  Hit
+ * results do not depend on it; traversal cost and build time do. */
+typedef enum AtrcBvhBuilder {
+    ATRC_BVH_SAH  = 0,  /* binned SAH on the host (threads at the top levels)   */
+    ATRC_BVH_PLOC = 1,  /* parallel locally-ordered clustering on the device    */
+    ATRC_BVH_AUTO = 2   /* PLOC for meshes of at least 2^18 triangles, else SAH */
+} AtrcBvhBuilder;
+
 typedef struct AtrcSceneDesc {
     uint32_t abi_version;            /* ATRC_ABI_VERSION                     */
     int32_t  aggregate;              /* AtrcAggregateType (CPU semantics)    */
     int32_t  aggregate_max_leaf_size;
-    int32_t  pad_;
+    int32_t  bvh_builder;            /* AtrcBvhBuilder (pt_cuda scene key    */
+                                     /* "bvh_builder": sah / ploc / auto)    */
     const AtrcMeshDesc*      meshes;     uint32_t mesh_count;
     const AtrcGeometryDesc*  geometries; uint32_t geometry_count;
     const AtrcEntityDesc*    entities;   uint32_t entity_count;
@@ -620,6 +629,34 @@ int  atrc_cuda_scene_bounds(AtrcScene* scene, float lo[3], float hi[3]);
 int  atrc_cuda_render_guided(AtrcScene* scene, AtrcGuide* guide,
                              const AtrcRenderDesc* desc, int32_t record,
                              AtrcFilm* film, AtrcRenderStats* stats);
+
+/* ------------------------------------------------ scene ingestion (BVH) */
+/* The mesh trees of a device scene come from the builder its description
+ * names (AtrcSceneDesc.bvh_builder).  These two entries run a builder alone
+ * on a list of boxes, for comparing builders and checking the device build.
+ * No reference counterpart: the reference builds triangle_bvh.cpp:122-304
+ * on the CPU. */
+typedef struct AtrcBvhBuildInfo {
+    double   seconds;     /* tree, leaves, 4-wide collapse and validation    */
+    double   sah_cost;    /* surface-area cost of the 4-wide tree (unit     */
+                          /* traversal and intersection costs)              */
+    uint64_t nodes;       /* 4-wide nodes                                    */
+    int32_t  rounds;      /* PLOC rounds (0 for SAH)                         */
+    int32_t  max_depth;   /* depth of the binary tree                        */
+} AtrcBvhBuildInfo;
+
+/* boxes: n x 6 floats (lo x y z, hi x y z).  builder ATRC_BVH_SAH runs on
+ * the host, ATRC_BVH_PLOC on `device`. */
+int  atrc_bvh_build(int32_t builder, int32_t device, const float* boxes, uint64_t n,
+                    AtrcBvhBuildInfo* info);
+/* The PLOC cluster tree on the host (device < 0) or on `device`: order[n]
+ * (sorted position -> box index), left[n-1], right[n-1] and
+ * node_boxes[(n-1) x 6] of internal node n + k (nodes below n are the
+ * leaves in sorted order), the root and the number of rounds.  The host and
+ * the device give the same tree. */
+int  atrc_bvh_cluster_tree(int32_t device, const float* boxes, uint64_t n, uint32_t* order,
+                           int32_t* left, int32_t* right, float* node_boxes, int32_t* root,
+                           int32_t* rounds);
 
 #ifdef __cplusplus
 }

@@ -37,7 +37,7 @@ def test_struct_layouts_match():
     lib = atrc_b200.load_library()
     n = len(abi.STRUCT_ORDER)
     sizes = (C.c_uint64 * n)()
-    assert lib.atrc_abi_struct_sizes(sizes, n) == n == 16
+    assert lib.atrc_abi_struct_sizes(sizes, n) == n == 17
     for cls, size in zip(abi.STRUCT_ORDER, sizes):
         assert C.sizeof(cls) == size, cls.__name__
     assert C.sizeof(abi.AtrcRay) == 32 and C.sizeof(abi.AtrcHit) == 16

@@ -268,3 +268,26 @@ def test_png_and_ppm_textures(tmp_path):
         assert (t.width, t.height) == (7, 5)
         got = np.ctypeslib.as_array(t.data, shape=(5 * 7 * 3,)).reshape(5, 7, 3)
         np.testing.assert_array_equal(got, img.astype(np.float32) / np.float32(255))
+
+
+def test_ao_renderer_keys_and_bvh_builder():
+    # AORendererCreator (renderer_creators.cpp:19-38) defaults and keys
+    d, kind = Config.from_string(base([QUAD], {"renderer": {"type": "ao", "spp": 3}})).rendering(0)
+    assert kind == "ao" and d.renderer == 1 and d.spp == 3
+    assert (d.ao_sample_count, d.ao_max_distance) == (5, 1.0)
+    assert list(d.ao_low) == [0, 0, 0] and list(d.ao_high) == [1, 1, 1] and list(d.ao_background) == [0, 0, 0]
+    d, _ = Config.from_string(base([QUAD], {"renderer": {"type": "ao", "spp": 1, "ao_sample_count": 9,
+                                                         "max_occlusion_distance": 2.5, "low_color": [0.25],
+                                                         "high_color": [1, 0.5, 0.25]}})).rendering(0)
+    assert d.ao_sample_count == 9 and d.ao_max_distance == pytest.approx(2.5)
+    assert list(d.ao_low) == [0.25] * 3 and list(d.ao_high) == [1, 0.5, 0.25]
+    with pytest.raises(AtrcError, match="ao_sample_count"):
+        Config.from_string(base([QUAD], {"renderer": {"type": "ao", "spp": 1, "ao_sample_count": 0}}))
+    with pytest.raises(AtrcError, match="not supported"):
+        Config.from_string(base([QUAD], {"renderer": {"type": "bdpt", "spp": 1}}))
+    # pt_cuda scene key: builder of the device scene's mesh trees
+    assert Config.from_string(base([QUAD])).scene_desc().contents.bvh_builder == 0
+    for name, v in (("sah", 0), ("ploc", 1), ("auto", 2)):
+        assert Config.from_string(base([QUAD], bvh_builder=name)).scene_desc().contents.bvh_builder == v
+    with pytest.raises(AtrcError, match="bvh_builder"):
+        Config.from_string(base([QUAD], bvh_builder="lbvh"))

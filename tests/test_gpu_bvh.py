@@ -1,0 +1,77 @@
+"""The device PLOC builder (bvh_gpu.cu): the same cluster tree as its host
+specification bit for bit, a surface-area cost close to the binned-SAH
+builder's, and scenes built with it giving the oracle's closest hits."""
+import json
+
+import numpy as np
+import pytest
+
+import oracle
+from atrc_b200 import Config, DeviceScene, Film, bvh_build, bvh_cluster_tree
+from tests.parity import band_test, classify_closest, seeded_rays
+from tests.test_bvh_ploc import check_tree, random_boxes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n,surface", [(1, False), (2, True), (1000, False), (65537, True), (400000, False)])
+def test_device_cluster_tree_equals_host(n, surface):
+    boxes = random_boxes(n, 100 + n, surface)
+    h = bvh_cluster_tree(boxes, device=-1)
+    d = bvh_cluster_tree(boxes, device=0)
+    for k in ("order", "left", "right", "boxes"):
+        np.testing.assert_array_equal(d[k], h[k], err_msg=k)
+    assert (d["root"], d["rounds"]) == (h["root"], h["rounds"])
+    check_tree(boxes, d)
+
+
+def test_identical_boxes_on_device():
+    boxes = np.tile(np.float32([0, 0, 0, 1, 1, 1]), (4099, 1))
+    d = bvh_cluster_tree(boxes, device=0)
+    h = bvh_cluster_tree(boxes, device=-1)
+    np.testing.assert_array_equal(d["left"], h["left"])
+    np.testing.assert_array_equal(d["right"], h["right"])
+
+
+@pytest.mark.parametrize("surface", [False, True])
+def test_ploc_cost_close_to_sah(surface):
+    boxes = random_boxes(300_000, 7, surface)
+    s = bvh_build(boxes, "sah")
+    p = bvh_build(boxes, "ploc")
+    assert p["sah_cost"] < 1.25 * s["sah_cost"], (p, s)
+    assert p["rounds"] > 0 and p["nodes"] > 0
+
+
+@pytest.fixture(scope="module")
+def instanced_ploc(scene_dir):
+    from atrc_b200.scenes import instanced_disney
+    p = instanced_disney(scene_dir / "inst_small", ico_level=4, hf_res=128, width=64, height=36, spp=256)
+    cfgd = json.loads(open(p).read())
+    cfgd["scene"]["bvh_builder"] = "ploc"
+    from pathlib import Path
+    cfg = Config.from_string(json.dumps(cfgd), str(Path(p).parent))
+    desc, _ = cfg.rendering(0)
+    return cfg, desc, DeviceScene(cfg), oracle.OracleScene(cfg.scene_desc(), desc.eps)
+
+
+def test_ploc_scene_closest_hits_bit_exact(instanced_ploc):
+    cfg, desc, dev, ora = instanced_ploc
+    rays = seeded_rays(1_000_000, [-22.0] * 3, [22.0] * 3, list(desc.camera.pos), seed=12)
+    g = dev.trace_rays(rays, "closest", exact=True)
+    r = ora.trace_rays(rays, "closest")
+    c = classify_closest(rays, g, r, ora)
+    assert c["error"] == 0, c["errors"]
+    assert c["max_ulp_same_prim"] == 0
+    assert c["exact"] + c["tie"] + c["ref_fn"] == len(rays)
+    assert c["exact"] >= len(rays) * 0.9999, c
+
+
+def test_ploc_scene_image_within_3_sigma(instanced_ploc):
+    cfg, desc, dev, ora = instanced_ploc
+    fg = Film(desc.width, desc.height, value_sq=True)
+    fc = Film(desc.width, desc.height, value_sq=True)
+    dev.render(desc, fg)
+    ora.render(desc, fc)
+    r = 0.5 - desc.eps
+    frac, allowed, info = band_test(fg, fc, 1 / (4 * r * r))
+    assert frac <= allowed, (frac, allowed, info)
