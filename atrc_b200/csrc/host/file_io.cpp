@@ -247,6 +247,58 @@ std::vector<float> load_rgb_image(const std::string& fn, int* w, int* h) {
     throw ConfigError("unsupported image format (pt_cuda reads .pfm, .hdr, .png and .ppm): " + fn);
 }
 
+// STL triangle soup, binary (80-byte header, uint32 count, 50 bytes per
+// facet: normal, three vertices, attribute word) or ASCII (solid / facet
+// normal / outer loop / vertex x3).  A file is binary when its size is
+// 84 + 50 * count, whatever its first bytes say.  Vertex normals are the
+// facet normal, or the winding normal where the file's is zero; uv = 0.
+static std::vector<float> load_stl(const std::string& fn) {
+    std::ifstream f(fn, std::ios::binary);
+    if (!f) throw ConfigError("failed to open file: " + fn);
+    std::vector<char> data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    std::vector<float> out;
+    auto emit = [&](Vec3 n, const Vec3* v) {
+        const Vec3 w = cross(v[1] - v[0], v[2] - v[0]);
+        if (!(dot(n, n) > 0) || !std::isfinite(n.x + n.y + n.z)) n = dot(w, w) > 0 ? normalize(w) : Vec3(0, 0, 1);
+        else n = normalize(n);
+        for (int k = 0; k < 3; ++k) out.insert(out.end(), {v[k].x, v[k].y, v[k].z, n.x, n.y, n.z, 0.0f, 0.0f});
+    };
+    uint32_t count = 0;
+    if (data.size() >= 84) std::memcpy(&count, data.data() + 80, 4);
+    if (data.size() >= 84 && data.size() == 84 + size_t(count) * 50) {
+        out.reserve(size_t(count) * 24);
+        for (uint32_t t = 0; t < count; ++t) {
+            float r[12];
+            std::memcpy(r, data.data() + 84 + size_t(t) * 50, sizeof(r));
+            const Vec3 v[3] = {Vec3(r[3], r[4], r[5]), Vec3(r[6], r[7], r[8]), Vec3(r[9], r[10], r[11])};
+            emit(Vec3(r[0], r[1], r[2]), v);
+        }
+        return out;
+    }
+    std::istringstream ss(std::string(data.begin(), data.end()));
+    std::string tok;
+    if (!(ss >> tok) || tok != "solid") throw ConfigError("not an STL file: " + fn);
+    Vec3 n, v[3];
+    int nv = 0;
+    while (ss >> tok) {
+        if (tok == "facet") {
+            std::string kw;
+            ss >> kw >> n.x >> n.y >> n.z;
+            if (!ss || kw != "normal") throw ConfigError("bad STL facet: " + fn);
+            nv = 0;
+        } else if (tok == "vertex") {
+            if (nv >= 3) throw ConfigError("STL facet with more than three vertices: " + fn);
+            ss >> v[nv].x >> v[nv].y >> v[nv].z;
+            if (!ss) throw ConfigError("bad STL vertex: " + fn);
+            ++nv;
+        } else if (tok == "endfacet") {
+            if (nv != 3) throw ConfigError("STL facet without three vertices: " + fn);
+            emit(n, v);
+        }
+    }
+    return out;
+}
+
 std::vector<float> load_triangle_mesh(const std::string& fn) {
     if (has_ext(fn, ".bm")) {
         std::ifstream f(fn, std::ios::binary);
@@ -290,9 +342,7 @@ std::vector<float> load_triangle_mesh(const std::string& fn) {
                     const Idx tri[3] = {poly[0], poly[k], poly[k + 1]};
                     Vec3 P[3];
                     for (int i = 0; i < 3; ++i) {
-                        if (tri[i].p < 0 || size_t(tri[i].p) * 3 + 2 >= pos.size() + 0) {
-                            if (tri[i].p < 0 || size_t(tri[i].p) >= pos.size() / 3) throw ConfigError("OBJ index out of range");
-                        }
+                        if (tri[i].p < 0 || size_t(tri[i].p) >= pos.size() / 3) throw ConfigError("OBJ index out of range");
                         P[i] = Vec3(pos[tri[i].p * 3], pos[tri[i].p * 3 + 1], pos[tri[i].p * 3 + 2]);
                     }
                     Vec3 fn_ = normalize(cross(P[1] - P[0], P[2] - P[0]));
@@ -309,7 +359,8 @@ std::vector<float> load_triangle_mesh(const std::string& fn) {
         }
         return out;
     }
-    throw ConfigError("unsupported mesh format (pt_cuda reads .bm and .obj): " + fn);
+    if (has_ext(fn, ".stl")) return load_stl(fn);
+    throw ConfigError("unsupported mesh format (pt_cuda reads .bm, .obj and .stl): " + fn);
 }
 
 void save_pfm(const std::string& fn, const float* rgb, int w, int h) {

@@ -291,3 +291,41 @@ def test_ao_renderer_keys_and_bvh_builder():
         assert Config.from_string(base([QUAD], bvh_builder=name)).scene_desc().contents.bvh_builder == v
     with pytest.raises(AtrcError, match="bvh_builder"):
         Config.from_string(base([QUAD], bvh_builder="lbvh"))
+
+
+def _mesh_vertices(tmp_path, name):
+    q = {"type": "geometric", "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/" + name,
+                                           "transform": []},
+         "material": {"type": "ideal_black"}}
+    cfg = Config.from_string(base([q]), tmp_path)
+    m = cfg.scene_desc().contents.meshes[0]
+    return np.ctypeslib.as_array(m.vertices, shape=(int(m.triangle_count) * 24,)).reshape(-1, 3, 8).copy()
+
+
+def test_obj_and_stl_meshes(tmp_path):
+    # OBJ: positions / uvs / normals, negative indices, polygon fans
+    (tmp_path / "m.obj").write_text("v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nvt 0 0\nvt 1 0\nvt 1 1\nvt 0 1\n"
+                                    "vn 0 0 1\nf 1/1/1 2/2/1 3/3/1 4/4/1\nf -4 -2 -1\n")
+    v = _mesh_vertices(tmp_path, "m.obj")
+    assert v.shape == (3, 3, 8)
+    np.testing.assert_array_equal(v[1, :, :3], [[0, 0, 0], [1, 1, 0], [0, 1, 0]])
+    np.testing.assert_array_equal(v[1, :, 6:], [[0, 0], [1, 1], [0, 1]])
+    np.testing.assert_array_equal(v[2, :, 3:6], np.tile([0, 0, 1], (3, 1)))     # winding normal
+    # binary STL (its header starts with "solid", as some exporters write)
+    tris = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]], [[0, 0, 1], [0, 1, 1], [1, 0, 1]]], np.float32)
+    body = b"".join(np.float32([0, 0, 0]).tobytes() + t.tobytes() + b"\0\0" for t in tris)
+    (tmp_path / "b.stl").write_bytes(b"solid exported".ljust(80, b" ") + np.uint32(2).tobytes() + body)
+    v = _mesh_vertices(tmp_path, "b.stl")
+    np.testing.assert_array_equal(v[..., :3], tris)
+    np.testing.assert_allclose(v[0, :, 3:6], np.tile([0, 0, 1], (3, 1)))
+    np.testing.assert_allclose(v[1, :, 3:6], np.tile([0, 0, -1], (3, 1)))
+    assert not v[..., 6:].any()
+    # ASCII STL with its own facet normals
+    (tmp_path / "a.stl").write_text("solid t\n facet normal 0 0 2\n  outer loop\n   vertex 0 0 0\n   vertex 2 0 0\n"
+                                    "   vertex 0 2 0\n  endloop\n endfacet\nendsolid t\n")
+    v = _mesh_vertices(tmp_path, "a.stl")
+    np.testing.assert_array_equal(v[0, :, :3], [[0, 0, 0], [2, 0, 0], [0, 2, 0]])
+    np.testing.assert_allclose(v[0, :, 3:6], np.tile([0, 0, 1], (3, 1)))
+    (tmp_path / "bad.stl").write_text("solid t\n facet normal 0 0 1\n outer loop\n vertex 0 0 0\n endfacet\n")
+    with pytest.raises(AtrcError, match="three vertices"):
+        _mesh_vertices(tmp_path, "bad.stl")
