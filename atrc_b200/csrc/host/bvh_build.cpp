@@ -562,4 +562,18 @@ double bvh4_sah_cost(const std::vector<Bvh4Node>& nodes, int32_t root, float tra
     return cost;
 }
 
+int bvh4_depth(const std::vector<Bvh4Node>& nodes, int32_t root) {
+    if (root < 0) return 0;
+    int depth = 0;
+    std::vector<std::pair<int32_t, int>> stack{{root, 1}};
+    while (!stack.empty()) {
+        const auto [link, d] = stack.back();
+        stack.pop_back();
+        depth = std::max(depth, d);
+        for (int k = 0; k < 4; ++k)
+            if (nodes[size_t(link)].link[k] >= 0) stack.push_back({nodes[size_t(link)].link[k], d + 1});
+    }
+    return depth;
+}
+
 }  // namespace atrc

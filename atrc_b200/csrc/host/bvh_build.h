@@ -104,6 +104,24 @@ ClusterTree ploc_build_host(const std::vector<BuildPrim>& prims, int radius = kP
 // Device PLOC on `device` (bvh_gpu.cu); throws std::runtime_error.
 ClusterTree ploc_build_device(const std::vector<BuildPrim>& prims, int device, int radius = kPlocRadius);
 
+// A finished 4-wide tree: interior links index `nodes`, leaf links encode
+// (first, count) into `order` (leaf position -> primitive index).
+struct WideBvh {
+    std::vector<Bvh4Node> nodes;
+    std::vector<uint32_t> order;
+    int32_t root = 0;
+    float bound_lo[3] = {0, 0, 0}, bound_hi[3] = {0, 0, 0};
+    int rounds = 0;
+};
+
+// The whole mesh-tree build on `device`: PLOC, the surface-area leaves of
+// bvh_from_clusters (decided as the clusters merge) and the 4-wide collapse
+// of collapse_bvh4 (walked from the root round by round), so only the result
+// comes back.  The same tree as collapse_bvh4(bvh_from_clusters(
+// ploc_build_host(prims))) up to the numbering of its nodes.
+WideBvh ploc_wide_device(const std::vector<BuildPrim>& prims, int device, int max_leaf = 4,
+                         float traversal_cost = 1.0f, float intersect_cost = 1.0f);
+
 // A cluster tree as a binary BVH with leaves of up to max_leaf primitives:
 // a subtree becomes a leaf where that is cheaper under the surface-area
 // heuristic (leaf: count * intersect_cost; split: traversal_cost + the
@@ -115,5 +133,8 @@ BvhResult bvh_from_clusters(const ClusterTree& t, const std::vector<BuildPrim>& 
 // the root's area, plus leaf primitives likewise), for comparing builders.
 double bvh4_sah_cost(const std::vector<Bvh4Node>& nodes, int32_t root, float traversal_cost = 1.0f,
                      float intersect_cost = 1.0f);
+
+// Depth of a 4-wide tree (a leaf root has depth 0).
+int bvh4_depth(const std::vector<Bvh4Node>& nodes, int32_t root);
 
 }  // namespace atrc

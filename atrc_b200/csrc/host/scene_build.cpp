@@ -11,6 +11,7 @@
 #include "scene_build.h"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -269,18 +270,34 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
         // bottom-level BVH over this leaf's triangles
         const bool ploc = device >= 0 && (d.bvh_builder == ATRC_BVH_PLOC ||
                                           (d.bvh_builder == ATRC_BVH_AUTO && prims.size() >= (size_t(1) << 18)));
-        BvhResult bvh = ploc ? bvh_from_clusters(ploc_build_device(prims, device), prims, 4) : build_bvh(prims, 4);
-        hs->max_blas_depth = std::max(hs->max_blas_depth, bvh.max_depth);
+        WideBvh bvh;
+        if (ploc) {
+            bvh = ploc_wide_device(prims, device);
+        } else {
+            BvhResult bin = build_bvh(prims, 4);
+            bvh.root = collapse_bvh4(bin, &bvh.nodes);
+            bvh.order = std::move(bin.order);
+            std::copy(bin.bound_lo, bin.bound_lo + 3, bvh.bound_lo);
+            std::copy(bin.bound_hi, bin.bound_hi + 3, bvh.bound_hi);
+        }
+        hs->max_blas_depth = std::max(hs->max_blas_depth, bvh4_depth(bvh.nodes, bvh.root));
         const int32_t tri_off = int32_t(hs->tri_shade.size());
-        auto fix_leaf = [&](int32_t link) -> int32_t {
-            if (link >= 0 || link == kEmptyLink) return link;
+        const int32_t first_node = int32_t(hs->nodes.size());
+        // into the scene's node array: interior links shift by the nodes
+        // already there, leaf links by the triangles already there
+        auto place = [&](int32_t link) -> int32_t {
+            if (link == kEmptyLink) return link;
+            if (link >= 0) return link + first_node;
             uint32_t enc = uint32_t(~link);
             return leaf_link((enc >> 4) + uint32_t(tri_off), (enc & 15) + 1);
         };
-        const size_t first_node = hs->nodes.size();
-        L.root = fix_leaf(collapse_bvh4(bvh, &hs->nodes));
-        for (size_t k = first_node; k < hs->nodes.size(); ++k)
-            for (int32_t& l : hs->nodes[k].link) l = fix_leaf(l);
+        if (hs->nodes.size() + bvh.nodes.size() >= size_t(INT32_MAX)) throw std::runtime_error("too many BVH nodes");
+        for (Bvh4Node w : bvh.nodes) {
+            for (int32_t& l : w.link) l = place(l);
+            hs->nodes.push_back(w);
+        }
+        L.root = place(bvh.root);
+        if (bvh.order.size() != prims.size()) throw std::runtime_error("BVH leaf order does not cover the triangles");
         validate_bvh4(hs->nodes, L.root, uint32_t(tri_off), uint32_t(prims.size()));
         L.tri_first = tri_off;
         L.tri_count = int32_t(prims.size());
@@ -290,7 +307,10 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
             L.bound.hi = Vec3(bvh.bound_hi[0], bvh.bound_hi[1], bvh.bound_hi[2]);
             widen_degenerate(L.bound);
         }
+        std::vector<uint8_t> placed(prims.size(), 0);
         for (uint32_t k : bvh.order) {
+            if (k >= prims.size() || placed[k]) throw std::runtime_error("BVH leaf order is not a permutation");
+            placed[k] = 1;
             put_tri(hs, ta[k], tba[k], tca[k], tsh[k], torig[k]);
             L.tri_areas.push_back(double(tri_area(tba[k], tca[k])));
         }

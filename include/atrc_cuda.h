@@ -641,12 +641,13 @@ typedef struct AtrcBvhBuildInfo {
     double   sah_cost;    /* surface-area cost of the 4-wide tree (unit     */
                           /* traversal and intersection costs)              */
     uint64_t nodes;       /* 4-wide nodes                                    */
-    int32_t  rounds;      /* PLOC rounds (0 for SAH)                         */
-    int32_t  max_depth;   /* depth of the binary tree                        */
+    int32_t  rounds;      /* PLOC rounds on the device (0 otherwise)         */
+    int32_t  max_depth;   /* depth of the 4-wide tree                        */
 } AtrcBvhBuildInfo;
 
 /* boxes: n x 6 floats (lo x y z, hi x y z).  builder ATRC_BVH_SAH runs on
- * the host, ATRC_BVH_PLOC on `device`. */
+ * the host; ATRC_BVH_PLOC runs on `device`, or, with device < 0, as its
+ * serial host specification (the same tree, slowly). */
 int  atrc_bvh_build(int32_t builder, int32_t device, const float* boxes, uint64_t n,
                     AtrcBvhBuildInfo* info);
 /* The PLOC cluster tree on the host (device < 0) or on `device`: order[n]

@@ -249,9 +249,11 @@ def ao_slab(h=0.5, dist=1.0, spp=256, count=5, looking_up=False) -> dict:
                                                   "C": [100, 100, z], "D": [-100, 100, z], "transform": []},
                 "material": {"type": "ideal_diffuse", "albedo": {"type": "constant", "texel": [0.5]}}}
     ents = [quad(0.0), quad(h)] if not looking_up else [quad(0.0)]
-    dst = [0, 0, 1] if looking_up else [0, 0, 0]
+    # the view stays clear of the quads' diagonal edge, where the (not
+    # watertight) reference triangle test can let a ray through
+    dst = [0.3, 0.1, 1] if looking_up else [0.3, 0.1, 0]
     return {"scene": {"type": "default", "entities": ents},
-            "rendering": {"camera": {"type": "thin_lens", "pos": [0, 0, 0.5 * h], "dst": dst, "up": [0, 1, 0],
+            "rendering": {"camera": {"type": "thin_lens", "pos": [0.3, 0.1, 0.5 * h], "dst": dst, "up": [0, 1, 0],
                                      "fov": 20},
                           "width": 8, "height": 8,
                           "renderer": {"type": "ao", "spp": spp, "ao_sample_count": count,

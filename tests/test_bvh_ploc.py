@@ -71,3 +71,13 @@ def test_identical_boxes_still_merge():
     t = bvh_cluster_tree(boxes, device=-1)
     check_tree(boxes, t)
     np.testing.assert_array_equal(t["order"], np.arange(257))
+
+
+@pytest.mark.parametrize("surface", [False, True])
+def test_host_ploc_tree_cost_close_to_sah(surface):
+    from atrc_b200 import bvh_build
+    boxes = random_boxes(50_000, 3, surface)
+    s = bvh_build(boxes, "sah", device=-1)
+    p = bvh_build(boxes, "ploc", device=-1)
+    assert p["rounds"] == 0 and p["nodes"] > 0 and p["max_depth"] > 0
+    assert p["sah_cost"] < 1.25 * s["sah_cost"], (p, s)
