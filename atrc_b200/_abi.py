@@ -46,7 +46,7 @@ class AtrcTexture3DDesc(C.Structure):
 
 
 class AtrcMaterialDesc(C.Structure):
-    _fields_ = [("type", C.c_int32), ("tex", C.c_int32 * 13), ("normal_map", C.c_int32)]
+    _fields_ = [("type", C.c_int32), ("tex", C.c_int32 * 13), ("normal_map", C.c_int32), ("bssrdf", C.c_int32 * 3)]
 
 
 class AtrcMediumDesc(C.Structure):

@@ -88,6 +88,7 @@ struct Material {
                              // transmission, trans_rough, ior, spec_scale rgb,
                              // spec_tint, aniso, sheen, sheen_tint, clearcoat
     float cc_gloss;
+    int32_t bssrdf[3];       // subsurface A, dmfp, eta textures (-1: none)
 };
 
 struct Medium {

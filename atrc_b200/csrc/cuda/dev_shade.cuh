@@ -227,7 +227,13 @@ struct BSDF {
     // phong: diffuse and specular colours, exponent, component weights
     Vec3 pd, ps;
     float pns, wd, wsp;
+    // separable subsurface exit (kMatSeparable): eta in IOR, 1 - 2 FM1(1/eta)
+    float sep_ci;
 };
+
+// BSDF of the exit point of a subsurface walk (SeparableBSDF, separable.cpp:38-103);
+// not a material of the scene description.
+constexpr int kMatSeparable = 100;
 
 __device__ __forceinline__ float one_minus_5(float x) { const float t = 1 - x, t2 = t * t; return t2 * t2 * t; }
 __device__ __forceinline__ float cos_2_sin(float c) { return sqrtf(fmaxf(0.0f, 1 - c * c)); }
@@ -436,7 +442,15 @@ __device__ Vec3 disney_f_inner(const BSDF& b, Vec3 lwi, Vec3 lwo) {
 
 __device__ __forceinline__ bool is_aggregate(int type) { return type == ATRC_MAT_METAL || type == ATRC_MAT_PHONG; }
 
+// SeparableBSDF::eval (separable.cpp:50-60): (1 - Fr(cos wi)) / (c pi) eta^2
+// for any wi, below the surface too
+__device__ __forceinline__ Vec3 separable_eval(const BSDF& b, Vec3 wi) {
+    const float fr = dielectric_fresnel(b.IOR, 1.0f, cosv(wi, b.geo.z));
+    return Vec3((1.0f - fr) / (b.sep_ci * kPi) * b.IOR * b.IOR);
+}
+
 __device__ Vec3 bsdf_eval(const BSDF& b, Vec3 wi, Vec3 wo) {
+    if (b.type == kMatSeparable) return separable_eval(b, wi);
     if (is_aggregate(b.type)) {  // AggregateBSDF::eval (component/aggregate.h)
         if (fringes(b, wi) || fringes(b, wo)) {
             if (!b.geo.positive(wi) || !b.geo.positive(wo)) return Vec3();
@@ -525,6 +539,7 @@ __device__ float disney_pdf_trans(const BSDF& b, Vec3 lwi, Vec3 lwo) {
 }
 
 __device__ float bsdf_pdf(const BSDF& b, Vec3 wi, Vec3 wo) {
+    if (b.type == kMatSeparable) return zweighted_pdf(normalize(b.geo.global_to_local(wi)).z);
     if (b.type != ATRC_MAT_IDEAL_DIFFUSE && b.type != ATRC_MAT_DISNEY && !is_aggregate(b.type)) return 0;
     if (fringes(b, wi) || fringes(b, wo)) {
         if (b.geo.positive(wi) != b.geo.positive(wo)) return 0;
@@ -586,6 +601,14 @@ __device__ BSDFSample bsdf_sample(const BSDF& b, Vec3 wo, float u0, float u1, fl
         r.f = Vec3(1.0f / (c < b.eps ? 1.0f : c));
         r.pdf = 1;
         r.delta = true;
+        return r;
+    }
+    if (b.type == kMatSeparable) {  // SeparableBSDF::sample (separable.cpp:62-69)
+        float pdf;
+        const Vec3 lwi = zweighted_on_hemisphere(u0, u1, &pdf);
+        r.dir = b.geo.local_to_global(lwi);
+        r.f = separable_eval(b, r.dir);
+        r.pdf = pdf;
         return r;
     }
     if (b.type == ATRC_MAT_MIRROR) {  // MirrorBSDF::sample (mirror.cpp:20-36)
@@ -791,8 +814,61 @@ done:
 
 __device__ __forceinline__ Vec3 bsdf_albedo(const BSDF& b) {
     if (b.type == ATRC_MAT_INVISIBLE_SURFACE) return Vec3(1.0f);
-    if (b.type == ATRC_MAT_IDEAL_BLACK) return Vec3();
+    if (b.type == ATRC_MAT_IDEAL_BLACK || b.type == kMatSeparable) return Vec3();
     return b.albedo;
+}
+
+// ============================================================ subsurface
+// Normalized diffusion (Christensen and Burley 2015, "Approximate
+// reflectance profiles for efficient subsurface scattering";
+// normalized_diffusion.cpp:357-397).  With x = r / d:
+//   radial pdf   p(x) = (e^-x + e^-x/3) / 4           (integrates to 1)
+//   cdf          P(x) = 1 - e^-x / 4 - 3 e^-x/3 / 4
+// and the reference's profile eval_r(r) = A (e^-x + e^-x/3) / (8 pi d), i.e.
+// R(r) r, matched to a pdf in r dr dphi / (2 pi).
+
+// First moment of the dielectric Fresnel reflectance (the polynomial fits
+// of d'Eon and Irving 2011 used by separable.cpp:12-35).
+__device__ __forceinline__ float fresnel_moment1(float eta) {
+    const float e2 = eta * eta, e3 = e2 * eta, e4 = e2 * e2, e5 = e2 * e3;
+    if (eta < 1)
+        return 0.45966f - 1.73965f * eta + 3.37668f * e2 - 3.904945f * e3 + 2.49277f * e4 - 0.68441f * e5;
+    return -4.61686f + 11.1136f * eta - 10.4646f * e2 + 5.11455f * e3 - 1.27198f * e4 + 0.12746f * e5;
+}
+
+// P^-1(u) by Newton's method in double precision from a start that is
+// within a factor of two everywhere (P(x) ~ x / 2 near 0, 1 - 3 e^-x/3 / 4
+// far out); u is clamped below 1.
+__device__ __forceinline__ float nd_inv_cdf(float uf) {
+    const double u = fmin(fmax(double(uf), 0.0), 1.0 - 1e-7);
+    double x = u < 0.5 ? 2.0 * u : 3.0 * log(0.75 / (1.0 - u));
+    for (int k = 0; k < 24; ++k) {
+        const double e1 = exp(-x), e3 = exp(-x / 3.0);
+        const double f = 1.0 - 0.25 * e1 - 0.75 * e3 - u;
+        const double df = 0.25 * (e1 + e3);
+        const double step = f / df;
+        x = fmax(x - step, 0.0);
+        if (fabs(step) <= 1e-12 * fmax(x, 1e-12)) break;
+    }
+    return float(x);
+}
+
+__device__ __forceinline__ float nd_pdf_r(float d, float r) {  // pdf_r (normalized_diffusion.cpp:380-385)
+    const float x = r / d;
+    return 0.25f * (expf(-x) + expf(-x / 3.0f)) / d;
+}
+
+__device__ __forceinline__ Vec3 nd_eval_r(Vec3 A, Vec3 d, float r) {  // eval_r (normalized_diffusion.cpp:357-362)
+    return Vec3(A.x * (expf(-r / d.x) + expf(-r / (3.0f * d.x))) / (8.0f * kPi * d.x),
+                A.y * (expf(-r / d.y) + expf(-r / (3.0f * d.y))) / (8.0f * kPi * d.y),
+                A.z * (expf(-r / d.z) + expf(-r / (3.0f * d.z))) / (8.0f * kPi * d.z));
+}
+
+// Scattering distance d = dmfp / s with s = 3.5 + 100 (A - 0.33)^4
+// (NormalizedDiffusionBSSRDF ctor, normalized_diffusion.cpp:388-397).
+__device__ __forceinline__ float nd_scale(float a) {
+    const float t = a - 0.33f;
+    return 3.5f + 100.0f * t * t * t * t;
 }
 
 // Material::shade

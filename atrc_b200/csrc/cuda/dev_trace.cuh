@@ -366,5 +366,67 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
     return true;
 }
 
+// Closest hit of a ray with one entity in [tmin, tmax]
+// (GeometricEntity::closest_intersection), for the subsurface probe: the
+// entity's own tree only, depth-first with a private stack.  Returns false
+// on a miss; sets *watchdog when the stack or the step bound would be
+// exceeded.
+template <bool EXACT>
+__device__ bool trace_entity(const Scene& S, int32_t ei, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit,
+                             int* watchdog) {
+    const Entity& e = S.entities[ei];
+    Vec3 lo, ld;
+    to_entity_space<EXACT>(e, wo, wd, &lo, &ld);
+    if (e.kind != LEAF_TRIANGLES) {
+        RayState lr;
+        lr.o = lo; lr.d = ld; lr.tmin = tmin; lr.tmax = tmax; lr.inv = Vec3();
+        float t;
+        const bool h = e.kind == LEAF_SPHERE ? sphere_test<false>(lr, e.radius, tmax, &t) : disk_test(lr, e.radius, tmax, &t);
+        if (!h) return false;
+        hit->t = t; hit->u = 0; hit->v = 0; hit->entity = ei; hit->tri = -1;
+        return true;
+    }
+    RayState r;
+    r.o = lo; r.d = ld; r.inv = safe_inv(ld); r.tmin = tmin; r.tmax = tmax;
+    int32_t stack[kStackSize];
+    int sp = 0;
+    int32_t link = e.blas_root;
+    float best_t = tmax, best_u = 0, best_v = 0;
+    int32_t best_tri = -1;
+    for (int steps = 0;; ++steps) {
+        if (steps > kMaxTraversalSteps) { *watchdog = 1; return false; }
+        if (link >= 0) {
+            float tc[4];
+            int32_t lc[4];
+            box4(S.nodes + link, r, tc, lc);
+            sort4(tc, lc);
+            if (sp + 3 > kStackSize) { *watchdog = 1; return false; }
+            if (tc[3] != INFINITY) stack[sp++] = lc[3];
+            if (tc[2] != INFINITY) stack[sp++] = lc[2];
+            if (tc[1] != INFINITY) stack[sp++] = lc[1];
+            link = tc[0] != INFINITY ? lc[0] : (sp > 0 ? stack[--sp] : kDone);
+            continue;
+        }
+        if (link == kDone) break;
+        const uint32_t enc = uint32_t(~link);
+        const int32_t first = int32_t(enc >> 4), count = int32_t(enc & 15) + 1;
+        for (int32_t k = 0; k < count; ++k) {
+            const int32_t ti = first + k;
+            const float4* tp = reinterpret_cast<const float4*>(S.tris) + size_t(ti) * 3;
+            float t, u, v;
+            if (mt_test<EXACT, false>(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), best_t, &t, &u, &v)) {
+                if (t < best_t || (t == best_t && ti < best_tri)) {
+                    best_t = t; best_tri = ti; best_u = u; best_v = v;
+                    r.tmax = t;
+                }
+            }
+        }
+        link = sp > 0 ? stack[--sp] : kDone;
+    }
+    if (best_tri < 0) return false;
+    hit->t = best_t; hit->u = best_u; hit->v = best_v; hit->entity = ei; hit->tri = best_tri;
+    return true;
+}
+
 }  // namespace dev
 }  // namespace atrc

@@ -434,9 +434,94 @@ __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d
 }
 
 // Materials the guide samples for: the non-delta BSDFs whose sampler
-// reports the density it samples with (with disney_fixed for Disney).
-__device__ __forceinline__ bool guidable(int type) {
-    return type == ATRC_MAT_IDEAL_DIFFUSE || type == ATRC_MAT_DISNEY || type == ATRC_MAT_METAL || type == ATRC_MAT_PHONG;
+// reports the density it samples with (with disney_fixed for Disney), not
+// those with subsurface scattering.
+__device__ __forceinline__ bool guidable(const Material& m) {
+    const int type = m.type;
+    return (type == ATRC_MAT_IDEAL_DIFFUSE || type == ATRC_MAT_DISNEY || type == ATRC_MAT_METAL ||
+            type == ATRC_MAT_PHONG) && m.bssrdf[1] < 0;
+}
+
+constexpr int kMaxProbeHits = 64;  // entity crossings one subsurface probe records
+
+// SeparableBSSRDF::sample_pi (separable.cpp:107-220) of the normalized
+// diffusion profile, from entry surface `s` of entity `ei`: a colour channel,
+// a projection axis (the normal with 1/2, each tangent with 1/4) and a
+// radius r ~ p(r / d); the probe segment through the sphere of radius
+// r_max = P^-1(0.996) d crosses the entity at every point it meets, and one
+// crossing is kept uniformly.  On success *x is the exit point, *bx its
+// separable BSDF and *w = (1 - Fr(cos wo)) eval_r(|x - s|) / pdf.
+__device__ __noinline__ bool subsurface_sample(const Scene& S, const Material& m, const Surface& s, Rng& rng, int* wd, float eps,
+                                  Surface* x, BSDF* bx, Vec3* w) {
+    const Vec3 A = tex2d_sample(S, m.bssrdf[0], s.u, s.v);
+    const Vec3 dmfp = tex2d_sample(S, m.bssrdf[1], s.u, s.v);
+    const float eta = tex2d_sample(S, m.bssrdf[2], s.u, s.v).x;
+    const float dch[3] = {dmfp.x / nd_scale(A.x), dmfp.y / nd_scale(A.y), dmfp.z / nd_scale(A.z)};
+    const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+    const int ch = min(int(u0 * 3.0f), 2);  // extract_uniform_int
+    const float su = u0 * 3.0f - float(ch);
+    Coord proj;
+    float sv;
+    if (u1 < 0.5f) {
+        proj = s.geo;
+        sv = 2.0f * u1;
+    } else if (u1 < 0.75f) {
+        proj = Coord{s.geo.y, s.geo.z, s.geo.x};
+        sv = 4.0f * (u1 - 0.5f);
+    } else {
+        proj = Coord{s.geo.z, s.geo.x, s.geo.y};
+        sv = 4.0f * (u1 - 0.75f);
+    }
+    const float r = nd_inv_cdf(su) * dch[ch];
+    const float r_max = nd_inv_cdf(0.996f) * dch[ch];
+    if (!(r > 0.0f) || r > r_max) return false;
+    float sp, cp;
+    sincosf(2.0f * kPi * sv, &sp, &cp);
+    const float hl = sqrtf(fmaxf(0.0f, r_max * r_max - r * r));
+    Vec3 o = s.pos + proj.local_to_global(Vec3(r * cp, r * sp, hl));
+    const Vec3 dir = -proj.z;
+    float tmax = fmaxf(eps, 2.0f * hl);
+    int cnt = 0;
+    Hit pick{};
+    Vec3 pick_o;
+    for (int k = 0; k < kMaxProbeHits && eps < tmax; ++k) {
+        Hit h;
+        if (!trace_entity<false>(S, s.entity, o, dir, eps, tmax, &h, wd)) break;
+        ++cnt;
+        if (rng.u() * float(cnt) < 1.0f) {  // reservoir: each crossing kept with probability 1 / cnt
+            pick = h;
+            pick_o = o;
+        }
+        o = o + dir * (h.t + eps);
+        tmax -= h.t + eps;
+    }
+    (void)u2;
+    if (cnt == 0) return false;
+    *x = make_surface(S, pick, pick_o, dir);
+    // pdf_pi (separable.cpp:222-248): all three axes and channels
+    const Vec3 ld = s.geo.global_to_local(s.pos - x->pos);
+    const Vec3 ln = s.geo.global_to_local(x->geo.z);
+    const float rp[3] = {sqrtf(ld.y * ld.y + ld.z * ld.z), sqrtf(ld.z * ld.z + ld.x * ld.x),
+                         sqrtf(ld.x * ld.x + ld.y * ld.y)};
+    const float lnc[3] = {ln.x, ln.y, ln.z};
+    const float axis_pdf[3] = {0.25f, 0.25f, 0.5f};
+    float pr = 0.0f;
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) pr += fabsf(lnc[a]) * nd_pdf_r(dch[c], rp[a]) * axis_pdf[a];
+    pr *= 1.0f / 3.0f;
+    const float pdf = pr / (2.0f * kPi) / float(cnt);
+    if (!(pdf > 0.0f)) return false;
+    const float fro = 1.0f - dielectric_fresnel(eta, 1.0f, cosv(s.wr, s.geo.z));
+    *w = fro * nd_eval_r(A, Vec3(dch[0], dch[1], dch[2]), length(x->pos - s.pos)) / pdf;
+    BSDF b{};
+    b.type = kMatSeparable;
+    b.geo = x->geo;
+    b.shd = x->geo;
+    b.IOR = eta;
+    b.sep_ci = 1.0f - 2.0f * fresnel_moment1(1.0f / eta);
+    b.eps = eps;
+    *bx = b;
+    return true;
 }
 
 // Guide queries of the shade queue (same order as k_shade): surface hits
@@ -462,7 +547,7 @@ __global__ void k_guide_features(Scene S, Params p, Pool P, Counters* c) {
             const Surface s = make_surface(S, h, xyz(ro), xyz(rd));
             Vec3 sn;
             const BSDF b = shade(S, s, &sn);
-            if (guidable(b.type) && !fringes(b, s.wr)) {
+            if (guidable(S.materials[S.entities[ent].material]) && !fringes(b, s.wr)) {
                 q.pos[0] = s.pos.x; q.pos[1] = s.pos.y; q.pos[2] = s.pos.z;
                 q.nrm[0] = sn.x; q.nrm[1] = sn.y; q.nrm[2] = sn.z;
                 q.wo[0] = s.wr.x; q.wo[1] = s.wr.y; q.wo[2] = s.wr.z;
@@ -643,7 +728,7 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                 const int gq_i = p.guide_on ? p.gf.gidx[i] : -1;
                 if (gq_i >= 0) {
                     const float* gm = p.gf.mixes + size_t(gq_i) * kGuideOut;
-                    guided = guidable(b.type) && !fringes(b, s.wr);
+                    guided = guidable(S.materials[e.material]) && !fringes(b, s.wr);
                     if (guided) {
                         for (int k = 0; k < kGuideLobes; ++k) {
                             mix.mu[k][0] = gm[5 * k]; mix.mu[k][1] = gm[5 * k + 1]; mix.mu[k][2] = gm[5 * k + 2];
@@ -659,38 +744,47 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                 };
                 if (depth == 1 && (e.flags & ENT_LIGHT)) L += coef * area_light_radiance(e, s.geo.z, s.wr);
                 // next-event estimation over every light (path_tracing.cpp:134-146)
-                for (int li = 0; li < S.light_count; ++li) {
-                    const int le_i = S.light_entity[li];
-                    const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
-                    if (le_i < 0) {
-                        float lpdf;
-                        const Vec3 dir = env_sample(S, u0, u1, u2, &lpdf);
-                        const Vec3 rad = env_radiance(S, dir);
-                        if (black(rad)) continue;
-                        const Vec3 lpos = env_emit_pos(S, s.pos, dir);
-                        const Vec3 to_light = normalize(lpos - s.pos);
-                        const Vec3 bf = bsdf_eval(b, to_light, s.wr);
-                        if (black(bf)) continue;
-                        const Vec3 contrib = coef * rad * bf *
-                                             (fabsf(cosv(to_light, s.geo.z)) / (lpdf + side_pdf(to_light, bsdf_pdf(b, to_light, s.wr))));
-                        push_shadow(P, c, s.pos, to_light, eps, length(s.pos - lpos) - eps, contrib, slot);
-                    } else {
-                        const Entity& le = S.entities[le_i];
-                        LightSample ls;
-                        if (!area_light_sample(S, le, s.pos, u0, u1, u2, &ls)) continue;
-                        if (black(ls.rad) || ls.pdf == 0.0f) continue;
-                        const float slen = length(ls.pos - s.pos) - eps;
-                        if (slen <= eps) continue;
-                        const Vec3 to_light = normalize(ls.pos - s.pos);
-                        const Vec3 bf = bsdf_eval(b, to_light, s.wr);
-                        if (black(bf)) continue;
-                        Vec3 tr(1.0f);
-                        if (S.has_media) tr = medium_tr(S, medium_of(s, e, to_light), ls.pos, s.pos, rng, &wd);
-                        const Vec3 contrib = coef * tr * ls.rad * bf *
-                                             (fabsf(cosv(to_light, s.geo.z)) / (ls.pdf + side_pdf(to_light, bsdf_pdf(b, to_light, s.wr))));
-                        push_shadow(P, c, s.pos, to_light, eps, slen, contrib, slot);
+                // at surface sv with BSDF bv (the BSDF-side pdf includes the
+                // guide where `with_guide`)
+                auto nee = [&](const Surface& sv, const BSDF& bv, bool with_guide) {
+                    for (int li = 0; li < S.light_count; ++li) {
+                        const int le_i = S.light_entity[li];
+                        const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+                        if (le_i < 0) {
+                            float lpdf;
+                            const Vec3 dir = env_sample(S, u0, u1, u2, &lpdf);
+                            const Vec3 rad = env_radiance(S, dir);
+                            if (black(rad)) continue;
+                            const Vec3 lpos = env_emit_pos(S, sv.pos, dir);
+                            const Vec3 to_light = normalize(lpos - sv.pos);
+                            const Vec3 bf = bsdf_eval(bv, to_light, sv.wr);
+                            if (black(bf)) continue;
+                            const float pb = bsdf_pdf(bv, to_light, sv.wr);
+                            const Vec3 contrib = coef * rad * bf *
+                                                 (fabsf(cosv(to_light, sv.geo.z)) /
+                                                  (lpdf + (with_guide ? side_pdf(to_light, pb) : pb)));
+                            push_shadow(P, c, sv.pos, to_light, eps, length(sv.pos - lpos) - eps, contrib, slot);
+                        } else {
+                            const Entity& le = S.entities[le_i];
+                            LightSample ls;
+                            if (!area_light_sample(S, le, sv.pos, u0, u1, u2, &ls)) continue;
+                            if (black(ls.rad) || ls.pdf == 0.0f) continue;
+                            const float slen = length(ls.pos - sv.pos) - eps;
+                            if (slen <= eps) continue;
+                            const Vec3 to_light = normalize(ls.pos - sv.pos);
+                            const Vec3 bf = bsdf_eval(bv, to_light, sv.wr);
+                            if (black(bf)) continue;
+                            Vec3 tr(1.0f);
+                            if (S.has_media) tr = medium_tr(S, medium_of(sv, e, to_light), ls.pos, sv.pos, rng, &wd);
+                            const float pb = bsdf_pdf(bv, to_light, sv.wr);
+                            const Vec3 contrib = coef * tr * ls.rad * bf *
+                                                 (fabsf(cosv(to_light, sv.geo.z)) /
+                                                  (ls.pdf + (with_guide ? side_pdf(to_light, pb) : pb)));
+                            push_shadow(P, c, sv.pos, to_light, eps, slen, contrib, slot);
+                        }
                     }
-                }
+                };
+                nee(s, b, true);
                 // BSDF sample: MIS-BSDF ray and continuation (path_tracing.cpp:148-169)
                 BSDFSample bs;
                 float pdf_bsdf = 0.0f;
@@ -735,6 +829,32 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                             flags |= PF_REC_PENDING;
                         }
                     }
+                    // subsurface scattering (path_tracing.cpp:173-221): a
+                    // direction into the surface re-emerges at a probed exit
+                    // point, which gets its own light samples and continues
+                    // the path with a sample of its separable BSDF.  The
+                    // entry's MIS-BSDF term is the continuation's, which
+                    // re-emerges instead: exact while the inside of the
+                    // object holds no light.
+                    const Material& mat = S.materials[e.material];
+                    if (mat.bssrdf[1] >= 0 && bs.pdf >= eps && !s.geo.positive(bs.dir) && s.geo.positive(s.wr)) {
+                        coef = coef * bs.f * (fabsf(cosv(s.geo.z, bs.dir)) / bs.pdf);
+                        Surface x;
+                        BSDF bx;
+                        Vec3 w;
+                        bool alive = subsurface_sample(S, mat, s, rng, &wd, eps, &x, &bx, &w);
+                        if (alive) {
+                            coef = coef * w;
+                            nee(x, bx, false);
+                            const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+                            bs = bsdf_sample(bx, x.wr, u0, u1, u2);
+                            alive = !black(bs.f);
+                            s = x;
+                        }
+                        if (!alive) finish = true;
+                    }
+                }
+                if (!finish) {
                     const Vec3 dir = normalize(bs.dir);
                     const float gcos = fabsf(dot(s.geo.z, dir));
                     mf4 = make_float4(coef.x * bs.f.x * gcos, coef.y * bs.f.y * gcos, coef.z * bs.f.z * gcos, mf4.w);

@@ -482,6 +482,12 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
             if (d.textures2d[m.tex[s]].type != ATRC_TEX_CONSTANT) all_const = false;
         }
         if (m.normal_map >= 0 && uint32_t(m.normal_map) >= d.texture2d_count) throw std::runtime_error("bad texture index");
+        const bool sss = m.bssrdf[1] >= 0;
+        for (int s = 0; s < 3; ++s) {
+            dm.bssrdf[s] = sss ? m.bssrdf[s] : -1;
+            if (sss && (m.type != ATRC_MAT_DISNEY || m.bssrdf[s] < 0 || uint32_t(m.bssrdf[s]) >= d.texture2d_count))
+                throw std::runtime_error("bad subsurface texture index (Disney materials only)");
+        }
         if (m.type != ATRC_MAT_DISNEY && m.type != ATRC_MAT_IDEAL_DIFFUSE) all_const = false;
         dm.all_constant = all_const;
         if (all_const && slots > 0) {

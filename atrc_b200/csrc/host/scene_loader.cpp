@@ -421,8 +421,7 @@ public:
         AtrcMaterialDesc m{};
         for (int i = 0; i < ATRC_DISNEY_SLOT_COUNT; ++i) m.tex[i] = -1;
         m.normal_map = -1;
-        if (p.find_child("bssrdf_dmfp"))
-            throw ConfigError("bssrdf_dmfp: BSSRDF materials are not supported by pt_cuda");
+        m.bssrdf[0] = m.bssrdf[1] = m.bssrdf[2] = -1;
         if (type == "ideal_diffuse") {
             // material_creators.cpp (IdealDiffuseCreator)
             m.type = ATRC_MAT_IDEAL_DIFFUSE;
@@ -452,6 +451,16 @@ public:
             m.tex[ATRC_DISNEY_CLEARCOAT] = child_texture_or_constant(p, "clearcoat", 0);
             m.tex[ATRC_DISNEY_CLEARCOAT_GLOSS] = child_texture_or_constant(p, "clearcoat_gloss", 1);
             if (auto n = p.find_child_group("normal_map")) m.normal_map = create_texture2d(*n);
+            // init_bssrdf_surface (material_creators.cpp:20-45): subsurface
+            // scattering when bssrdf_dmfp is given; A defaults to the base
+            // colour and eta to the ior
+            if (p.find_child("bssrdf_dmfp")) {
+                m.bssrdf[1] = create_texture2d(p.child_group("bssrdf_dmfp"));
+                m.bssrdf[0] = p.find_child_group("bssrdf_A") ? create_texture2d(p.child_group("bssrdf_A"))
+                                                             : m.tex[ATRC_DISNEY_BASE_COLOR];
+                m.bssrdf[2] = p.find_child_group("bssrdf_eta") ? create_texture2d(p.child_group("bssrdf_eta"))
+                                                               : m.tex[ATRC_DISNEY_IOR];
+            }
         } else if (type == "mirror") {  // MirrorCreator (material_creators.cpp:270-289)
             m.type = ATRC_MAT_MIRROR;
             m.tex[0] = create_texture2d(p.child_group("color_map"));

@@ -183,6 +183,11 @@ typedef struct AtrcMaterialDesc {
     int32_t tex[ATRC_DISNEY_SLOT_COUNT]; /* texture2d indices; IDEAL_DIFFUSE */
                                      /* uses tex[0] as albedo                */
     int32_t normal_map;              /* texture2d index or -1                */
+    int32_t bssrdf[3];               /* DISNEY subsurface scattering         */
+                                     /* (init_bssrdf_surface, material_      */
+                                     /* creators.cpp:20-45): texture2d       */
+                                     /* indices of A, dmfp and eta; -1 each  */
+                                     /* when the material has none           */
 } AtrcMaterialDesc;
 
 typedef enum AtrcMediumType {

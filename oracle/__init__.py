@@ -42,6 +42,8 @@ def load() -> C.CDLL:
                                          abi.c_float_p, abi.c_float_p]
         lib.oracle_bsdf_sample.argtypes = [C.c_void_p, C.c_int, abi.c_float_p, abi.c_float_p, C.c_size_t,
                                            abi.c_float_p, abi.c_float_p, abi.c_float_p, C.POINTER(C.c_int), C.c_int]
+        lib.oracle_subsurface.argtypes = [C.c_void_p, abi.c_float_p, abi.c_float_p, C.c_size_t, C.c_uint64,
+                                          abi.c_float_p, abi.c_float_p]
         _lib = lib
     return _lib
 
@@ -109,6 +111,16 @@ class OracleScene:
         pdf = np.empty(len(wi), dtype=np.float32)
         _check(load().oracle_bsdf_eval(self._h, material, _fp(wi), _fp(wo), len(wi), _fp(f), _fp(pdf)))
         return f, pdf
+
+    def subsurface(self, o, d, n: int, seed: int = 1):
+        """n subsurface probes from the closest hit of ray (o, d): weights
+        (n, 3) (zero for invalid samples) and exit points (n, 3)."""
+        o = np.ascontiguousarray(o, dtype=np.float32)
+        d = np.ascontiguousarray(d, dtype=np.float32)
+        w = np.empty((n, 3), dtype=np.float32)
+        x = np.empty((n, 3), dtype=np.float32)
+        _check(load().oracle_subsurface(self._h, _fp(o), _fp(d), n, seed, _fp(w), _fp(x)))
+        return w, x
 
     def bsdf_sample(self, material: int, wo: np.ndarray, u3: np.ndarray, disney_fixed: bool = False):
         wo = np.ascontiguousarray(wo, dtype=np.float32)

@@ -77,6 +77,12 @@ int oracle_bsdf_eval(OracleScene* s, int material, const float* wi,
 int oracle_bsdf_sample(OracleScene* s, int material, const float* wo,
                        const float* u3, size_t n, float* wi, float* f,
                        float* pdf, int* is_delta, int disney_fixed);
+/* Subsurface probe (SeparableBSSRDF::sample_pi) from the closest hit of the
+ * ray (o, d), which must meet an entity whose material has subsurface
+ * scattering: n samples of the weight coef / pdf -> w[3] (0 when the
+ * sample is invalid) and the exit point -> exit_pos[3]. */
+int oracle_subsurface(OracleScene* s, const float* o, const float* d, size_t n, uint64_t seed,
+                      float* w, float* exit_pos);
 
 #ifdef __cplusplus
 }

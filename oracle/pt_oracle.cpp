@@ -1100,6 +1100,14 @@ struct BSDF {
     // phong (phong.cpp:23-58): diffuse / specular colours, exponent, weights
     V3 pd, ps;
     float pns = 1, wd = 0.5f, wsp = 0.5f;
+    // exit point of a subsurface walk (SeparableBSDF, separable.cpp:38-103):
+    // eta in IOR, sep_ci = 1 - 2 FM1(1 / eta)
+    float sep_ci = 1;
+    static constexpr int kSeparable = 100;
+    V3 separable_eval(V3 wi) const {  // separable.cpp:50-60, any wi
+        float fr = dielectric_fresnel(IOR, 1, cosv(wi, geo.z));
+        return V3((1 - fr) / (sep_ci * PI) * IOR * IOR);
+    }
 
     // ------------------------------------------------- LocalBSDF helpers
     // core/bsdf.h:113-202
@@ -1417,6 +1425,7 @@ struct BSDF {
 
     // ------------------------------------------------- interface
     V3 eval(V3 wi, V3 wo) const {
+        if (type == kSeparable) return separable_eval(wi);
         switch (type) {
         case ATRC_MAT_IDEAL_DIFFUSE: {  // AggregateBSDF::eval (component/aggregate.h:40-62)
             if (black_fringes(wi, wo)) return eval_black_fringes(wi, wo);
@@ -1470,6 +1479,7 @@ struct BSDF {
     }
 
     float pdf(V3 wi, V3 wo) const {
+        if (type == kSeparable) return zweighted_pdf(normalize(geo.global_to_local(wi)).z);
         switch (type) {
         case ATRC_MAT_IDEAL_DIFFUSE: {  // AggregateBSDF::pdf (component/aggregate.h:200-225)
             if (black_fringes(wi, wo)) return pdf_black_fringes(wi, wo);
@@ -1512,6 +1522,14 @@ struct BSDF {
 
     BSDFSample sample(V3 wo, const float* sam) const {
         BSDFSample r;
+        if (type == kSeparable) {  // separable.cpp:62-69
+            float p;
+            V3 lwi = zweighted_on_hemisphere(sam[0], sam[1], &p);
+            r.dir = geo.local_to_global(lwi);
+            r.f = separable_eval(r.dir);
+            r.pdf = p;
+            return r;
+        }
         switch (type) {
         case ATRC_MAT_IDEAL_DIFFUSE: {  // AggregateBSDF::sample (component/aggregate.h:64-139)
             if (black_fringes(wo)) return sample_black_fringes(wo, sam);
@@ -1671,7 +1689,7 @@ struct BSDF {
 
     V3 albedo() const {
         if (type == ATRC_MAT_INVISIBLE_SURFACE) return V3(1.0f);
-        if (type == ATRC_MAT_IDEAL_BLACK) return V3();
+        if (type == ATRC_MAT_IDEAL_BLACK || type == kSeparable) return V3();
         return albedo_;
     }
 };
@@ -2222,6 +2240,95 @@ struct Pixel {
     float denoise = 1;
 };
 
+// ---------------------------------------------------------- subsurface
+// Normalized diffusion profile (normalized_diffusion.cpp:357-397): radial
+// pdf p(x) = (e^-x + e^-x/3) / 4 in x = r / d, eval_r(r) = A (e^-x +
+// e^-x/3) / (8 pi d), d = dmfp / (3.5 + 100 (A - 0.33)^4).  The reference
+// samples r from a tabulated inverse cdf (agz-utils sample_inv_cdf_table,
+// not in this container); this inverts the cdf by Newton's method.
+float nd_inv_cdf(float uf) {
+    double u = std::min(std::max(double(uf), 0.0), 1.0 - 1e-7);
+    double x = u < 0.5 ? 2.0 * u : 3.0 * std::log(0.75 / (1.0 - u));
+    for (int k = 0; k < 24; ++k) {
+        double e1 = std::exp(-x), e3 = std::exp(-x / 3.0);
+        double step = (1.0 - 0.25 * e1 - 0.75 * e3 - u) / (0.25 * (e1 + e3));
+        x = std::max(x - step, 0.0);
+        if (std::abs(step) <= 1e-12 * std::max(x, 1e-12)) break;
+    }
+    return float(x);
+}
+float nd_pdf_r(float d, float r) { float x = r / d; return 0.25f * (std::exp(-x) + std::exp(-x / 3.0f)) / d; }
+float nd_scale(float a) { float t = a - 0.33f; return 3.5f + 100.0f * t * t * t * t; }
+// first Fresnel moment, the polynomial fits used by separable.cpp:12-35
+float fresnel_moment1(float eta) {
+    float e2 = eta * eta, e3 = e2 * eta, e4 = e2 * e2, e5 = e2 * e3;
+    if (eta < 1) return 0.45966f - 1.73965f * eta + 3.37668f * e2 - 3.904945f * e3 + 2.49277f * e4 - 0.68441f * e5;
+    return -4.61686f + 11.1136f * eta - 10.4646f * e2 + 5.11455f * e3 - 1.27198f * e4 + 0.12746f * e5;
+}
+
+// SeparableBSSRDF::sample_pi (separable.cpp:107-220) from entry `po`:
+// exit point `pi` with its separable BSDF, and the weight coef / pdf.
+bool subsurface_sample(const OracleScene& sc, const AtrcMaterialDesc& m, const EntInct& po, Sampler& s,
+                       EntInct* pi, BSDF* bx, V3* w) {
+    const V3 A = sc.tex2d[m.bssrdf[0]].sample(po.uv), dmfp = sc.tex2d[m.bssrdf[1]].sample(po.uv);
+    const float eta = sc.tex2d[m.bssrdf[2]].sample_real(po.uv);
+    const float d[3] = {dmfp.x / nd_scale(A.x), dmfp.y / nd_scale(A.y), dmfp.z / nd_scale(A.z)};
+    float sam[3] = {s.u(), s.u(), s.u()};
+    int ch = std::min(int(sam[0] * 3), 2);  // extract_uniform_int
+    float su = sam[0] * 3 - float(ch);
+    Coord proj;
+    float sv;
+    if (sam[1] < 0.5f) { proj = po.geo; sv = 2 * sam[1]; }
+    else if (sam[1] < 0.75f) { proj = Coord(po.geo.y, po.geo.z, po.geo.x); sv = 4 * (sam[1] - 0.5f); }
+    else { proj = Coord(po.geo.z, po.geo.x, po.geo.y); sv = 4 * (sam[1] - 0.75f); }
+    float r = nd_inv_cdf(su) * d[ch];
+    float r_max = nd_inv_cdf(0.996f) * d[ch];
+    if (!(r > 0) || r > r_max) return false;
+    float phi = 2 * PI * sv;
+    float hl = std::sqrt(std::max(0.0f, r_max * r_max - r * r));
+    Ray probe(po.pos + proj.local_to_global(V3(r * std::cos(phi), r * std::sin(phi), hl)), -proj.z, g_eps,
+              std::max(g_eps, 2 * hl));
+    // every crossing of the same entity along the probe, one kept uniformly
+    int cnt = 0;
+    GeoInct pick;
+    for (int k = 0; k < 64; ++k) {
+        if (probe.t_min >= probe.t_max) break;
+        GeoInct g;
+        if (!po.ent->closest(probe, &g)) break;
+        ++cnt;
+        if (s.u() * float(cnt) < 1) pick = g;
+        probe.o = probe.at(g.t + g_eps);
+        probe.t_max -= g.t + g_eps;
+    }
+    if (!cnt) return false;
+    static_cast<GeoInct&>(*pi) = pick;
+    pi->ent = po.ent;
+    // pdf_pi (separable.cpp:222-248)
+    V3 ld = po.geo.global_to_local(po.pos - pi->pos), ln = po.geo.global_to_local(pi->geo.z);
+    float rp[3] = {std::sqrt(ld.y * ld.y + ld.z * ld.z), std::sqrt(ld.z * ld.z + ld.x * ld.x),
+                   std::sqrt(ld.x * ld.x + ld.y * ld.y)};
+    float lnc[3] = {ln.x, ln.y, ln.z}, axis_pdf[3] = {0.25f, 0.25f, 0.5f};
+    float pr = 0;
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) pr += std::abs(lnc[a]) * nd_pdf_r(d[c], rp[a]) * axis_pdf[a];
+    pr /= 3;
+    float pdf = pr / (2 * PI) / float(cnt);
+    if (!(pdf > 0)) return false;
+    float fro = 1 - BSDF::dielectric_fresnel(eta, 1, cosv(po.wr, po.geo.z));
+    float dist = len(pi->pos - po.pos);
+    V3 ev(A.x * (std::exp(-dist / d[0]) + std::exp(-dist / (3 * d[0]))) / (8 * PI * d[0]),
+          A.y * (std::exp(-dist / d[1]) + std::exp(-dist / (3 * d[1]))) / (8 * PI * d[1]),
+          A.z * (std::exp(-dist / d[2]) + std::exp(-dist / (3 * d[2]))) / (8 * PI * d[2]));
+    *w = fro * ev / pdf;
+    BSDF b;
+    b.type = BSDF::kSeparable;
+    b.geo = b.shd = pi->geo;
+    b.IOR = eta;
+    b.sep_ci = 1 - 2 * fresnel_moment1(1 / eta);
+    *bx = b;
+    return true;
+}
+
 // render::trace_std (path_tracing.cpp:15-225), direct_illum_sample_count = 1
 Pixel trace_std(const OracleScene& sc, const AtrcRenderDesc& p, Ray r, Sampler& s) {
     V3 coef(1);
@@ -2283,10 +2390,33 @@ Pixel trace_std(const OracleScene& sc, const AtrcRenderDesc& p, Ray r, Sampler& 
         float sam[3] = {s.u(), s.u(), s.u()};
         BSDFSample bs = b.sample(in.wr, sam);
         if (bs.f.black() || bs.pdf < sc.eps) return px;
-        const bool delta = bs.delta;
+        bool delta = bs.delta;
         const float abscos = std::abs(cosv(in.geo.z, bs.dir));
         coef *= bs.f * abscos / bs.pdf;
         r = Ray(in.eps_offset(bs.dir), normalize(bs.dir));
+        // bssrdf (path_tracing.cpp:173-221)
+        const AtrcMaterialDesc& mat = sc.materials[in.ent->material];
+        if (mat.type == ATRC_MAT_DISNEY && mat.bssrdf[1] >= 0 && !in.geo.in_positive_z_hemisphere(bs.dir) &&
+            in.geo.in_positive_z_hemisphere(in.wr)) {
+            EntInct x;
+            BSDF bx;
+            V3 w;
+            if (!subsurface_sample(sc, mat, in, s, &x, &bx, &w)) return px;
+            coef *= w;
+            V3 di2;
+            for (const Light& l : sc.lights) {
+                if (l.is_env) di2 += coef * mis_env_surface(sc, x, bx, s);
+                else di2 += coef * mis_area_surface(sc, l.ent, x, bx, s);
+            }
+            di2 += coef * mis_bsdf_surface(sc, x, bx, s);
+            px.value += di2;
+            float sam2[3] = {s.u(), s.u(), s.u()};
+            BSDFSample bs2 = bx.sample(x.wr, sam2);
+            if (bs2.f.black()) return px;
+            coef *= bs2.f * std::abs(cosv(x.geo.z, bs2.dir)) / bs2.pdf;
+            r = Ray(x.eps_offset(bs2.dir), normalize(bs2.dir));
+            delta = false;
+        }
         if (delta && depth >= 2 && s_depth <= p.specular_depth) { --depth; ++s_depth; }
     }
     return px;
@@ -2687,6 +2817,25 @@ int oracle_bsdf_sample(OracleScene* s, int material, const float* wo, const floa
         f[3 * i] = r.f.x; f[3 * i + 1] = r.f.y; f[3 * i + 2] = r.f.z;
         pdf[i] = r.pdf;
         is_delta[i] = r.delta;
+    }
+    return ATRC_OK;
+}
+
+int oracle_subsurface(OracleScene* s, const float* o, const float* d, size_t n, uint64_t seed, float* w,
+                      float* exit_pos) {
+    if (!s || !o || !d || !w || !exit_pos) return ATRC_ERR_INVALID_ARG;
+    EntInct in;
+    if (!s->closest(Ray(V3(o), normalize(V3(d))), &in)) return ATRC_ERR_INVALID_ARG;
+    const AtrcMaterialDesc& m = s->materials[in.ent->material];
+    if (m.type != ATRC_MAT_DISNEY || m.bssrdf[1] < 0) return ATRC_ERR_INVALID_ARG;
+    Sampler smp(seed, 7);
+    for (size_t i = 0; i < n; ++i) {
+        EntInct x;
+        BSDF bx;
+        V3 wv;
+        if (!subsurface_sample(*s, m, in, smp, &x, &bx, &wv)) { wv = V3(); x.pos = V3(); }
+        w[3 * i] = wv.x; w[3 * i + 1] = wv.y; w[3 * i + 2] = wv.z;
+        exit_pos[3 * i] = x.pos.x; exit_pos[3 * i + 1] = x.pos.y; exit_pos[3 * i + 2] = x.pos.z;
     }
     return ATRC_OK;
 }

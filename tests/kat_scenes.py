@@ -260,3 +260,61 @@ def ao_slab(h=0.5, dist=1.0, spp=256, count=5, looking_up=False) -> dict:
                                        "max_occlusion_distance": dist, "low_color": [0.1, 0.2, 0.3],
                                        "high_color": [0.9, 0.8, 0.7], "background_color": [0.05, 0.06, 0.07]},
                           "reporter": {"type": "noout"}}}
+
+
+def subsurface_plane(A=(0.5, 0.5, 0.5), dmfp=(0.1, 0.1, 0.1), ior=1.3, spp=16) -> dict:
+    """A large flat quad of Disney material with subsurface scattering
+    (bssrdf_dmfp; A from bssrdf_A), seen straight down."""
+    def const(v):
+        return {"type": "constant", "texel": list(map(float, np.atleast_1d(v)))}
+    mat = {"type": "disney", "base_color": const([0.8, 0.8, 0.8]), "metallic": const(0), "roughness": const(0.5),
+           "transmission": const(1.0), "ior": const(ior), "bssrdf_dmfp": const(list(dmfp)), "bssrdf_A": const(list(A))}
+    return {"scene": {"type": "default",
+                      "entities": [{"type": "geometric",
+                                    "geometry": {"type": "quad", "A": [-50, -50, 0], "B": [50, -50, 0],
+                                                 "C": [50, 50, 0], "D": [-50, 50, 0], "transform": []},
+                                    "material": mat}]},
+            "rendering": {"camera": {"type": "thin_lens", "pos": [0.3, 0.1, 2], "dst": [0.3, 0.1, 0], "up": [0, 1, 0],
+                                     "fov": 20},
+                          "width": 4, "height": 4, "renderer": {"type": "pt", "spp": spp},
+                          "reporter": {"type": "noout"}}}
+
+
+def subsurface_scene(tmp: Path, spp=256, width=40, height=30) -> dict:
+    """Disney materials with subsurface scattering on a sphere and a mesh
+    box over a diffuse floor, lit by a sphere light and the native sky."""
+    from atrc_b200.scenes import _box_mesh, write_bm
+    p, n, uv = _box_mesh((0.45, 0.45, 0.45))
+    write_bm(tmp / "sss_box.bm", p, n, uv)
+
+    def const(v):
+        return {"type": "constant", "texel": list(map(float, np.atleast_1d(v)))}
+
+    def skin(color, A, dmfp, trans=0.8):
+        return {"type": "disney", "base_color": const(color), "metallic": const(0), "roughness": const(0.4),
+                "transmission": const(trans), "ior": const(1.4), "bssrdf_dmfp": const(dmfp), "bssrdf_A": const(A)}
+    ents = [
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-4, -4, -1], "B": [4, -4, -1], "C": [4, 4, -1],
+                                           "D": [-4, 4, -1], "transform": []},
+         "material": {"type": "ideal_diffuse", "albedo": const([0.6, 0.6, 0.6])}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.6,
+                                           "transform": [{"type": "translate", "offset": [-0.7, 0.2, -0.4]}]},
+         "material": skin([0.9, 0.6, 0.5], [0.9, 0.55, 0.4], [0.3, 0.15, 0.08])},
+        {"type": "geometric", "geometry": {"type": "transform_wrapper",
+                                           "transform": [{"type": "translate", "offset": [0.8, -0.2, -0.55]},
+                                                         {"type": "rotate_z", "deg": 30}],
+                                           "internal": {"type": "triangle_bvh",
+                                                        "filename": "${scene-directory}/sss_box.bm",
+                                                        "transform": []}},
+         "material": skin([0.5, 0.7, 0.9], [0.5, 0.7, 0.9], [0.1, 0.2, 0.3], trans=1.0)},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.3,
+                                           "transform": [{"type": "translate", "offset": [0.2, -1.0, 1.6]}]},
+         "material": {"type": "ideal_black"}, "emit_radiance": [10, 9, 8]},
+    ]
+    return {"scene": {"type": "default", "entities": ents,
+                      "env": {"type": "native_sky", "top": [0.3, 0.35, 0.5], "bottom": [0.05, 0.05, 0.05]}},
+            "rendering": {"camera": {"type": "thin_lens", "pos": [0, -4.5, 1.2], "dst": [0, 0, -0.4], "up": [0, 0, 1],
+                                     "fov": 40},
+                          "width": width, "height": height,
+                          "renderer": {"type": "pt", "spp": spp, "max_depth": 10, "min_depth": 3},
+                          "reporter": {"type": "noout"}}}

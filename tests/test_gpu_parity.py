@@ -175,6 +175,25 @@ def test_materials_scene_within_3_sigma(tmp_path):
     assert np.abs(ga - ca).mean() < 0.02
 
 
+def test_subsurface_scene_within_3_sigma(tmp_path):
+    # Disney subsurface scattering (normalized diffusion probe, separable
+    # exit BSDF) on a sphere and an instanced mesh against the oracle
+    from tests import kat_scenes as K
+    cfg = Config.from_string(K.dumps(K.subsurface_scene(tmp_path, spp=512)), tmp_path)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    fg = Film(desc.width, desc.height, value_sq=True)
+    fc = Film(desc.width, desc.height, value_sq=True)
+    stats = dev.render(desc, fg)
+    assert stats["watchdog_flags"] == 0
+    ora.render(desc, fc)
+    r = 0.5 - desc.eps
+    frac, allowed, info = band_test(fg, fc, 1 / (4 * r * r))
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fg, fc) < 4.0
+
+
 def test_gaussian_filter_matches(tmp_path):
     from tests import kat_scenes as K
     cfg = Config.from_string(K.dumps(K.feature_scene(tmp_path, spp=128, gaussian=True)), tmp_path)

@@ -284,3 +284,47 @@ def test_ao_background_on_miss():
     np.testing.assert_allclose(f.image().reshape(-1, 3), np.broadcast_to(np.float32([0.05, 0.06, 0.07]), (64, 3)),
                                rtol=1e-6)
     assert not f.albedo.any()
+
+
+def _nd_cdf(x):
+    return 1 - 0.25 * np.exp(-x) - 0.75 * np.exp(-x / 3)
+
+
+def _nd_inv_cdf(u):
+    lo, hi = 0.0, 200.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if _nd_cdf(mid) < u else (lo, mid)
+    return 0.5 * (lo + hi)
+
+
+@pytest.mark.parametrize("A", [(0.5, 0.5, 0.5), (0.8, 0.5, 0.2)])
+def test_subsurface_weight_on_a_plane(A):
+    # separable.cpp:107-248 on a flat surface: only the normal-axis probe
+    # (probability 1/2) meets the plane, once; its pdf_pi keeps 1/2 of the
+    # axis term, so E[w_c] = (1 - Fr(eta, cos 0)) * 2 pi * integral of
+    # eval_r,c(r) * (sum over sampled channels whose r_max covers r of
+    # pdf_r) / (sum of pdf_r) dr -- for a grey A exactly (1 - Fr) A P(x_max)
+    ior, dmfp = 1.3, 0.1
+    cfg, desc, ora = _oracle(K.subsurface_plane(A=A, dmfp=(dmfp,) * 3, ior=ior))
+    n = 400_000
+    w, x = ora.subsurface([0.3, 0.1, 2.0], [0, 0, -1], n, seed=3)
+    A = np.array(A, np.float64)
+    d = dmfp / (3.5 + 100 * (A - 0.33) ** 4)
+    xm = _nd_inv_cdf(0.996)
+    fro = 1 - ((ior - 1) / (ior + 1)) ** 2
+    r = np.linspace(0, xm * d.max(), 400_001)
+    pdf_r = 0.25 * (np.exp(-r[None] / d[:, None]) + np.exp(-r[None] / (3 * d[:, None]))) / d[:, None]
+    covered = (r[None] <= xm * d[:, None]) * pdf_r
+    ratio = covered.sum(0) / pdf_r.sum(0)
+    want = np.array([fro * 2 * np.pi * np.trapezoid(
+        A[c] * (np.exp(-r / d[c]) + np.exp(-r / (3 * d[c]))) / (8 * np.pi * d[c]) * ratio, r) for c in range(3)])
+    if np.all(A == A[0]):
+        np.testing.assert_allclose(want, fro * A * 0.996, rtol=1e-4)
+    valid = w[:, 0] > 0
+    assert abs(valid.mean() - 0.5 * np.mean([1.0])) < 0.01        # the normal axis only
+    se = w.std(0) / math.sqrt(n)
+    assert np.all(np.abs(w.mean(0) - want) < 5 * se), (w.mean(0), want, se)
+    # exit points on the plane, within r_max of the entry
+    dist = np.linalg.norm(x[valid] - np.float32([0.3, 0.1, 0]), axis=1)
+    assert np.all(np.abs(x[valid, 2]) < 1e-5) and dist.max() <= xm * d.max() * 1.0001
