@@ -223,6 +223,18 @@ class DeviceScene:
     def handle(self) -> C.c_void_p:
         return self._h
 
+    def subsurface_probe(self, o, d, n: int, seed: int = 1):
+        """n subsurface walks from the closest hit of ray (o, d)
+        (atrc_cuda_subsurface_probe): weights (n, 3), exit points (n, 3)."""
+        o = np.ascontiguousarray(o, np.float32)
+        d = np.ascontiguousarray(d, np.float32)
+        w = np.zeros((n, 3), np.float32)
+        x = np.zeros((n, 3), np.float32)
+        fp = abi.c_float_p
+        _check(load_library().atrc_cuda_subsurface_probe(self._h, o.ctypes.data_as(fp), d.ctypes.data_as(fp), n, seed,
+                                                         w.ctypes.data_as(fp), x.ctypes.data_as(fp)))
+        return w, x
+
     def trace_rays(self, rays: np.ndarray, mode: str = "closest", exact: bool = True) -> np.ndarray:
         """rays: RAY_DTYPE array (or (n, 8) float32).  Returns HIT_DTYPE."""
         r = np.ascontiguousarray(rays)

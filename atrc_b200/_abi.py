@@ -35,7 +35,7 @@ class AtrcTexture2DDesc(C.Structure):
     _fields_ = [("type", C.c_int32), ("texel", C.c_float * 3), ("width", C.c_int32), ("height", C.c_int32),
                 ("data", c_float_p), ("nearest", C.c_int32), ("uv_transform", C.c_float * 6),
                 ("wrap_u", C.c_int32), ("wrap_v", C.c_int32), ("inv_gamma", C.c_float), ("grid_count", C.c_int32),
-                ("texel2", C.c_float * 3), ("pad_", C.c_int32)]
+                ("texel2", C.c_float * 3), ("tex3d", C.c_int32)]
 
 
 class AtrcTexture3DDesc(C.Structure):
@@ -192,6 +192,8 @@ PROTOTYPES = {
     "atrc_guide_train_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.c_int, C.POINTER(C.c_float)]),
     "atrc_guide_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "atrc_cuda_scene_bounds": (C.c_int, [C.c_void_p, c_float_p, c_float_p]),
+    "atrc_cuda_subsurface_probe": (C.c_int, [C.c_void_p, c_float_p, c_float_p, C.c_int32, C.c_uint64, c_float_p,
+                                             c_float_p]),
     "atrc_bvh_build": (C.c_int, [C.c_int32, C.c_int32, c_float_p, C.c_uint64, C.POINTER(AtrcBvhBuildInfo)]),
     "atrc_bvh_cluster_tree": (C.c_int, [C.c_int32, c_float_p, C.c_uint64, C.POINTER(C.c_uint32),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32), c_float_p,

@@ -65,6 +65,8 @@ struct Texture2D {
     float uv[6];
     int32_t wrap_u, wrap_v;
     int64_t data_offset;     // float offset into the texel pool
+    int32_t tex3d;           // solid image: the 3D texture behind it
+    int32_t pad_;
 };
 
 struct Texture3D {

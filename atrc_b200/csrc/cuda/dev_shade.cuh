@@ -42,15 +42,20 @@ __device__ __forceinline__ Vec3 texel2(const float* base, int w, int x, int y) {
     return Vec3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
+template <bool REAL_ONLY>
+__device__ Vec3 tex3d_sample(const Scene& S, int ti, Vec3 uvw0);
+
 __device__ Vec3 tex2d_sample(const Scene& S, int ti, float u0, float v0) {
     const Texture2D& t = S.tex2d[ti];
     if (t.type == 0) return Vec3(t.texel[0], t.texel[1], t.texel[2]);
     const float tu = t.uv[0] * u0 + t.uv[1] * v0 + t.uv[2];
     const float tv = t.uv[3] * u0 + t.uv[4] * v0 + t.uv[5];
     const float u = wrap_coord(t.wrap_u, tu), v = wrap_coord(t.wrap_v, tv);
+    // SolidImageTexture::sample_spectrum_impl (solid_image.cpp:12-15)
+    if (t.type == ATRC_TEX_SOLID) return tex3d_sample<false>(S, t.tex3d, Vec3(u, v, 0.0f));
     const float* base = S.texels + t.data_offset;
     Vec3 r;
-    if (t.type == ATRC_TEX_CHECKER) {  // CheckerBoard::sample_spectrum_impl (checker_board.cpp:11-19)
+    if (t.type == ATRC_TEX_CHECKER) {  // CheckerBoard::sample_spectrum_impl (checker_board.cpp:15-22)
         const int ui = int(clampf(u, 0, 1) / t.grid_size), vi = int(clampf(v, 0, 1) / t.grid_size);
         r = ((ui + vi) & 1) ? Vec3(t.texel[0], t.texel[1], t.texel[2]) : Vec3(t.texel2[0], t.texel2[1], t.texel2[2]);
     } else if (t.nearest) {
@@ -69,6 +74,13 @@ __device__ Vec3 tex2d_sample(const Scene& S, int ti, float u0, float v0) {
     }
     if (t.inv_gamma != 1.0f) r = Vec3(powf(r.x, t.inv_gamma), powf(r.y, t.inv_gamma), powf(r.z, t.inv_gamma));
     return r;
+}
+
+// Texture2D::sample_spectrum(inct): the solid image reads its 3D texture at
+// the world position (solid_image.cpp:25-33), every other texture at uv.
+__device__ __forceinline__ Vec3 tex2d_sample_at(const Scene& S, int ti, float u, float v, Vec3 pos) {
+    if (S.tex2d[ti].type == ATRC_TEX_SOLID) return tex3d_sample<false>(S, S.tex2d[ti].tex3d, pos);
+    return tex2d_sample(S, ti, u, v);
 }
 
 __device__ __forceinline__ float tex3d_at(const float* base, const Texture3D& t, int x, int y, int z, int c) {
@@ -358,7 +370,7 @@ __device__ __forceinline__ void ggx_refl(const BSDF& b, Vec3 lwi, Vec3 lwo, Vec3
     if (pdf) *pdf = Go * D / (4 * lwo.z);
 }
 
-// PhongSpecularComponent (phong_specular_comp.cpp:6-70): s (e+1)/2pi cos^e of
+// PhongSpecularComponent (phong_specular_comp.cpp:7-96): s (e+1)/2pi cos^e of
 // the angle to the mirror direction (a negative cosine with a fractional
 // exponent gives NaN, as in the reference)
 __device__ __forceinline__ float pow_cos_pdf(float e, float c) { return (e + 1) / (2 * kPi) * powf(c, e); }
@@ -611,7 +623,7 @@ __device__ BSDFSample bsdf_sample(const BSDF& b, Vec3 wo, float u0, float u1, fl
         r.pdf = pdf;
         return r;
     }
-    if (b.type == ATRC_MAT_MIRROR) {  // MirrorBSDF::sample (mirror.cpp:20-36)
+    if (b.type == ATRC_MAT_MIRROR) {  // MirrorBSDF::sample (mirror.cpp:32-50)
         const Vec3 lo = b.shd.global_to_local(wo);
         if (lo.z <= 0) return r;
         const Vec3 nwo = normalize(lo);
@@ -622,7 +634,7 @@ __device__ BSDFSample bsdf_sample(const BSDF& b, Vec3 wo, float u0, float u1, fl
         r.delta = true;
         return r;
     }
-    if (b.type == ATRC_MAT_GLASS) {  // GlassBSDF::sample (glass.cpp:34-70), radiance transport
+    if (b.type == ATRC_MAT_GLASS) {  // GlassBSDF::sample (glass.cpp:52-91), radiance transport
         const Vec3 nwo = normalize(b.shd.global_to_local(wo));
         const Vec3 nor = nwo.z > 0 ? Vec3(0, 0, 1) : Vec3(0, 0, -1);
         const float fr = dielectric_fresnel(b.glass_ior, 1.0f, nwo.z);
@@ -891,7 +903,8 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
     b.shd = shd;
     *shading_normal = m.type == ATRC_MAT_INVISIBLE_SURFACE || m.type == ATRC_MAT_IDEAL_BLACK ? s.user.z : shd.z;
     if (m.type == ATRC_MAT_IDEAL_DIFFUSE) {
-        b.albedo = m.all_constant ? Vec3(m.c[0], m.c[1], m.c[2]) : tex2d_sample(S, m.tex[0], s.u, s.v);
+        // IdealDiffuse::shade samples by intersection (ideal_diffuse.cpp:27)
+        b.albedo = m.all_constant ? Vec3(m.c[0], m.c[1], m.c[2]) : tex2d_sample_at(S, m.tex[0], s.u, s.v, s.pos);
     } else if (m.type == ATRC_MAT_DISNEY) {
         if (m.all_constant) {
             disney_init(b, Vec3(m.c[0], m.c[1], m.c[2]), m.c[3], m.c[4], m.c[5], m.c[6], m.c[7],
@@ -908,20 +921,21 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
                m.type == ATRC_MAT_PHONG) {
         auto T = [&](int slot) { return tex2d_sample(S, m.tex[slot], s.u, s.v); };
         if (m.type == ATRC_MAT_MIRROR) {
-            // Mirror::shade (mirror.cpp:62-76): ConductorPoint(ior, 1, k) puts
+            // Mirror::shade (mirror.cpp:98-115): ConductorPoint(ior, 1, k) puts
             // the ior on the OUTER side, so eta^2 = 1 / ior^2
             const Vec3 rc = T(0), ior = T(1), k = T(2);
             b.rc = rc;
             b.eta2 = Vec3(1 / sqrf(ior.x), 1 / sqrf(ior.y), 1 / sqrf(ior.z));
             b.etak2 = Vec3(sqrf(k.x / ior.x), sqrf(k.y / ior.y), sqrf(k.z / ior.z));
             b.albedo = rc;
-        } else if (m.type == ATRC_MAT_GLASS) {  // Glass::shade (glass.cpp:127-150)
-            b.glass_ior = T(2).x;
-            b.refl_c = T(0);
-            const Vec3 rr = T(1);
+        } else if (m.type == ATRC_MAT_GLASS) {  // Glass::shade (glass.cpp:180-206), by intersection
+            auto TP = [&](int slot) { return tex2d_sample_at(S, m.tex[slot], s.u, s.v, s.pos); };
+            b.glass_ior = TP(2).x;
+            b.refl_c = TP(0);
+            const Vec3 rr = TP(1);
             b.refr_c = Vec3(sqrtf(rr.x), sqrtf(rr.y), sqrtf(rr.z));
             b.albedo = 0.5f * (b.refl_c + b.refr_c);
-        } else if (m.type == ATRC_MAT_METAL) {  // Metal::shade (metal.cpp:25-46)
+        } else if (m.type == ATRC_MAT_METAL) {  // Metal::shade (metal.cpp:39-62)
             const Vec3 color = T(0), eta = T(1), k = T(2);
             const float rough = T(3).x, aniso = T(4).x;
             b.rc = color;  // ColoredConductorPoint(color, 1, eta, k)
@@ -932,7 +946,7 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
             b.ay = fmaxf(0.001f, sqrf(rough) * aspect);
             b.roughness = rough;
             b.albedo = color;
-        } else {  // Phong::shade (phong.cpp:23-58)
+        } else {  // Phong::shade (phong.cpp:33-79)
             Vec3 d = T(0), sp = T(1);
             const float ns = T(2).x;
             const float dem = fmaxf(1.0f, fmaxf(d.x + sp.x, fmaxf(d.y + sp.y, d.z + sp.z)));

@@ -53,7 +53,13 @@ struct RayState {
     float tmin, tmax;
 };
 
-__device__ __forceinline__ Vec3 safe_inv(Vec3 d) { return Vec3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z); }
+// Reciprocal direction for the slab tests.  The slab test evaluates
+// lo * inv - o * inv (one FMA per plane), which for a zero component would
+// be inf - inf = NaN and cull every box; a zero (or denormal-small)
+// component is replaced by +-1e-20 (sign kept), so the slab of that axis is
+// a huge finite interval on the correct side.
+__device__ __forceinline__ float safe_rcp(float x) { return 1.0f / (fabsf(x) > 1e-20f ? x : copysignf(1e-20f, x)); }
+__device__ __forceinline__ Vec3 safe_inv(Vec3 d) { return Vec3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z)); }
 
 // Moller-Trumbore.  ANY selects has_intersection_with_triangle (alpha <= 1
 // also checked), otherwise closest_intersection_with_triangle.

@@ -1396,6 +1396,36 @@ int atrc_cuda_trace_rays(AtrcScene* scene, const AtrcRay* rays, size_t n, AtrcHi
     });
 }
 
+// n subsurface probes from the closest hit of one ray (a check of
+// subsurface_sample against the oracle's; thread i draws its own stream).
+__global__ void k_subsurface_probe(Scene S, Vec3 o, Vec3 d, int n, uint64_t seed, float eps, float* w, float* x,
+                                   int* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec3 wv, xp;
+    Hit h;
+    int wd = 0;
+    if (!trace_ray<false, false>(S, o, d, 0.0f, INFINITY, &h, &wd)) {
+        if (i == 0) *status = 1;
+    } else {
+        const Surface s = make_surface(S, h, o, d);
+        const Material& m = S.materials[S.entities[h.entity].material];
+        if (m.bssrdf[1] < 0) {
+            if (i == 0) *status = 2;
+        } else {
+            Rng rng;
+            rng.state = mix64(seed ^ (uint64_t(i) * 0x9E3779B97F4A7C15ULL));
+            Surface ex;
+            BSDF bx;
+            if (subsurface_sample(S, m, s, rng, &wd, eps, &ex, &bx, &wv)) xp = ex.pos;
+            else wv = Vec3();
+        }
+    }
+    if (wd) *status = 3;
+    w[3 * i] = wv.x; w[3 * i + 1] = wv.y; w[3 * i + 2] = wv.z;
+    x[3 * i] = xp.x; x[3 * i + 1] = xp.y; x[3 * i + 2] = xp.z;
+}
+
 static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const AtrcFilm* film) {
     if (!scene || !desc || !film || !film->value || !film->weight)
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: null argument");
@@ -1413,6 +1443,35 @@ static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: ao_sample_count must be in [1, 4096]");
     return ATRC_OK;
 }
+
+int atrc_cuda_subsurface_probe(AtrcScene* scene, const float o[3], const float d[3], int32_t n, uint64_t seed,
+                               float* w, float* exit_pos) {
+    if (!scene || !o || !d || !w || !exit_pos || n <= 0)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_subsurface_probe: null argument");
+    return guarded([&] {
+        DeviceSceneImpl& dv = scene->impl;
+        CK(cudaSetDevice(dv.device));
+        DevBuf bw, bx, bs;
+        bw.alloc(size_t(n) * 12);
+        bx.alloc(size_t(n) * 12);
+        bs.alloc(4);
+        CK(cudaMemsetAsync(bs.p, 0, 4, dv.stream));
+        const Vec3 ov(o[0], o[1], o[2]), dvv = normalize(Vec3(d[0], d[1], d[2]));
+        k_subsurface_probe<<<(n + 127) / 128, 128, 0, dv.stream>>>(dv.scene, ov, dvv, n, seed, dv.scene.eps,
+                                                                 bw.as<float>(), bx.as<float>(), bs.as<int>());
+        CK(cudaGetLastError());
+        int status = 0;
+        CK(cudaMemcpyAsync(w, bw.p, size_t(n) * 12, cudaMemcpyDeviceToHost, dv.stream));
+        CK(cudaMemcpyAsync(exit_pos, bx.p, size_t(n) * 12, cudaMemcpyDeviceToHost, dv.stream));
+        CK(cudaMemcpyAsync(&status, bs.p, 4, cudaMemcpyDeviceToHost, dv.stream));
+        CK(cudaStreamSynchronize(dv.stream));
+        if (status == 1) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_subsurface_probe: the ray hits nothing");
+        if (status == 2) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_subsurface_probe: no subsurface material");
+        if (status == 3) return fail(ATRC_ERR_WATCHDOG, "atrc_cuda_subsurface_probe: traversal bound exceeded");
+        return int(ATRC_OK);
+    });
+}
+
 
 // The wavefront render behind atrc_cuda_render (arguments already checked;
 // CUDA failures throw).  Launch shapes, path pool and sort mode left to

@@ -435,6 +435,13 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
             dt.data_offset = int64_t(hs->texels.size());
             hs->texels.insert(hs->texels.end(), t.data, t.data + size_t(t.width) * t.height * 3);
         }
+        dt.tex3d = -1;
+        if (t.type == ATRC_TEX_SOLID) {
+            if (t.tex3d < 0 || uint32_t(t.tex3d) >= d.texture3d_count) throw std::runtime_error("bad solid_image texture");
+            dt.tex3d = t.tex3d;
+        } else if (t.type != ATRC_TEX_CONSTANT && t.type != ATRC_TEX_IMAGE && t.type != ATRC_TEX_CHECKER) {
+            throw std::runtime_error("unknown texture2d type");
+        }
         hs->tex2d.push_back(dt);
     }
     for (uint32_t i = 0; i < d.texture3d_count; ++i) {
@@ -573,6 +580,7 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
             if (d.env.tex < 0 || uint32_t(d.env.tex) >= d.texture2d_count) throw std::runtime_error("bad env texture");
             // EnvironmentLightSampler (env_sampler.h:15-104), table in FP64
             const AtrcTexture2DDesc& td = d.textures2d[d.env.tex];
+            if (td.type == ATRC_TEX_SOLID) throw std::runtime_error("solid_image is not supported as an environment map");
             const bool uniform = d.env.no_importance_sampling || td.type == ATRC_TEX_CONSTANT;
             const int tw = uniform ? 1 : td.width, th = uniform ? 1 : td.height;
             const int pw = std::min(tw, 200), ph = std::min(th, 200);

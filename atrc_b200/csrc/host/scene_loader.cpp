@@ -141,6 +141,7 @@ public:
             return r;
         }
         AtrcTexture2DDesc t{};
+        t.tex3d = -1;
         // Texture2DCommonParams::from_params / full_transform (texture2d.h:8-53)
         const bool inv_u = p.child_int_or("inv_u", 0) != 0;
         const bool inv_v = p.child_int_or("inv_v", 0) != 0;
@@ -184,6 +185,16 @@ public:
             const Vec3 c1 = p.child_spectrum("color1"), c2 = p.child_spectrum("color2");
             t.texel[0] = c1.x; t.texel[1] = c1.y; t.texel[2] = c1.z;
             t.texel2[0] = c2.x; t.texel2[1] = c2.y; t.texel2[2] = c2.z;
+        } else if (type == "solid_image") {
+            // SolidImageCreator (texture2d_creators.cpp:148-163): a 3D
+            // texture behind the 2D interface, without the 2D common
+            // parameters (identity uv transform, clamp, no gamma)
+            t.type = ATRC_TEX_SOLID;
+            t.tex3d = create_texture3d(p.child_group("tex3d"));
+            const float id[6] = {1, 0, 0, 0, 1, 0};
+            std::memcpy(t.uv_transform, id, sizeof(id));
+            t.wrap_u = t.wrap_v = ATRC_WRAP_CLAMP;
+            t.inv_gamma = 1.0f;
         } else if (type == "hdr" || type == "image") {
             // HDRTexture (hdr.cpp:11-72) and ImageTexture (image.cpp): float
             // texels, 8-bit images as byte / 255 (from_color3b)

@@ -115,8 +115,13 @@ typedef struct AtrcEntityDesc {
 typedef enum AtrcTextureType {
     ATRC_TEX_CONSTANT = 0,
     ATRC_TEX_IMAGE    = 1,       /* float RGB texels (`hdr`, `image`)        */
-    ATRC_TEX_CHECKER  = 2        /* `checker_board`: texel = color1,         */
+    ATRC_TEX_CHECKER  = 2,       /* `checker_board`: texel = color1,         */
                                  /* texel2 = color2, grid_count cells        */
+    ATRC_TEX_SOLID    = 3        /* `solid_image` (solid_image.cpp:6-45):    */
+                                 /* the texture3d `tex3d` read at (u, v, 0), */
+                                 /* or at the world position where the       */
+                                 /* material passes the intersection (ideal  */
+                                 /* diffuse albedo, glass maps)              */
 } AtrcTextureType;
 
 typedef enum AtrcWrapMode {
@@ -136,7 +141,7 @@ typedef struct AtrcTexture2DDesc {
     float        inv_gamma;
     int32_t      grid_count;     /* CHECKER                                  */
     float        texel2[3];      /* CHECKER                                  */
-    int32_t      pad_;
+    int32_t      tex3d;          /* SOLID: texture3d index                   */
 } AtrcTexture2DDesc;
 
 /* Texture3D (src/tracer/include/agz/tracer/core/texture3d.h:30-223). */
@@ -627,6 +632,13 @@ int  atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide,
                             const AtrcRenderDesc* views, int32_t n,
                             const AtrcFilm* films, double* view_seconds,
                             AtrcRenderStats* stats);
+/* Subsurface probe check: n samples of the subsurface walk (normalized
+ * diffusion, separable.cpp:107-248) from the closest hit of the ray (o, d),
+ * which must meet a Disney material with subsurface scattering: the weight
+ * coef / pdf (zero for an invalid sample) -> w[3 n] and the exit point ->
+ * exit_pos[3 n].  Uses the scene's eps of the last render (3e-4 before). */
+int  atrc_cuda_subsurface_probe(AtrcScene* scene, const float o[3], const float d[3], int32_t n,
+                                uint64_t seed, float* w, float* exit_pos);
 /* Scene bound (for atrc_guide_create). */
 int  atrc_cuda_scene_bounds(AtrcScene* scene, float lo[3], float hi[3]);
 /* atrc_cuda_render with the guide sampling surface vertices; record = 1

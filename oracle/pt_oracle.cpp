@@ -22,6 +22,7 @@
 #include <mutex>
 #include <queue>
 #include <stack>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -292,7 +293,7 @@ struct Tex2D {
     // (i + 0.5) / size, edge texels clamped.
     V3 sample_impl(V2 uv) const {
         float u = clampf(uv.x, 0, 1), v = clampf(uv.y, 0, 1);
-        if (d.type == ATRC_TEX_CHECKER) {  // CheckerBoard::sample_spectrum_impl (checker_board.cpp:11-19)
+        if (d.type == ATRC_TEX_CHECKER) {  // CheckerBoard::sample_spectrum_impl (checker_board.cpp:15-22)
             float gs = 1.0f / float(d.grid_count);
             int ui = int(u / gs), vi = int(v / gs);
             return ((ui + vi) & 1) ? V3(d.texel) : V3(d.texel2);
@@ -318,11 +319,18 @@ struct Tex2D {
         if (d.type == ATRC_TEX_CONSTANT) return V3(d.texel);
         const float* m = d.uv_transform;
         V2 t(m[0] * uv.x + m[1] * uv.y + m[2], m[3] * uv.x + m[4] * uv.y + m[5]);
-        V3 r = sample_impl(V2(wrap_apply(d.wrap_u, t.x), wrap_apply(d.wrap_v, t.y)));
+        V2 w(wrap_apply(d.wrap_u, t.x), wrap_apply(d.wrap_v, t.y));
+        if (d.type == ATRC_TEX_SOLID) return solid_sample(V3(w.x, w.y, 0));  // solid_image.cpp:12-15
+        V3 r = sample_impl(w);
         if (d.inv_gamma != 1) r = V3(std::pow(r.x, d.inv_gamma), std::pow(r.y, d.inv_gamma), std::pow(r.z, d.inv_gamma));
         return r;
     }
     float sample_real(V2 uv) const { return sample(uv).x; }
+    // Texture2D::sample_spectrum(inct): a solid image at the world position
+    // (solid_image.cpp:25-33), every other texture at uv
+    V3 sample_at(V2 uv, V3 pos) const { return d.type == ATRC_TEX_SOLID ? solid_sample(pos) : sample(uv); }
+    const struct Tex3D* solid = nullptr;  // the 3D texture of a solid image
+    V3 solid_sample(V3 p) const;
 };
 
 struct Tex3D {
@@ -367,6 +375,7 @@ struct Tex3D {
     }
     float sample_real(V3 uvw) const { return sample(uvw).x; }
 };
+V3 Tex2D::solid_sample(V3 p) const { return solid->sample(p); }
 
 // ============================================================ intersections
 struct SurfacePoint {
@@ -1094,10 +1103,10 @@ struct BSDF {
     float w_diffuse = 0.25f, w_specular = 0.25f, w_clearcoat = 0.25f, w_transmission = 0.25f;
     // mirror / metal conductor Fresnel: eta^2, (eta k)^2 per channel, colour
     V3 eta2, etak2, rc;
-    // glass (glass.cpp:127-150)
+    // glass (glass.cpp:180-206)
     float glass_ior = 1.5f;
     V3 refl_c, refr_c;
-    // phong (phong.cpp:23-58): diffuse / specular colours, exponent, weights
+    // phong (phong.cpp:33-79): diffuse / specular colours, exponent, weights
     V3 pd, ps;
     float pns = 1, wd = 0.5f, wsp = 0.5f;
     // exit point of a subsurface walk (SeparableBSDF, separable.cpp:38-103):
@@ -1251,7 +1260,7 @@ struct BSDF {
         if (f) *f = rc * conductor_fresnel(cd) * (D * Gi * Go / std::abs(4 * lwi.z * lwo.z));
         if (p) *p = Go * D / (4 * lwo.z);
     }
-    // PhongSpecularComponent (phong_specular_comp.cpp:6-70)
+    // PhongSpecularComponent (phong_specular_comp.cpp:7-96)
     static float pow_cos_pdf(float e, float c) { return (e + 1) / (2 * PI) * std::pow(c, e); }
     V3 phong_spec_eval(V3 lwi, V3 lwo) const {
         if (lwi.z <= 0 || lwo.z <= 0) return V3();
@@ -1473,7 +1482,7 @@ struct BSDF {
             if (type == ATRC_MAT_METAL) { V3 f; ggx_refl(lwi, lwo, &f, nullptr); return f; }
             return phong_diffuse(lwi, lwo) + phong_spec_eval(lwi, lwo);
         }
-        default:  // mirror and glass are delta: eval is 0 (mirror.cpp:38-41, glass.cpp:72-75)
+        default:  // mirror and glass are delta: eval is 0 (mirror.cpp:27-30, glass.cpp:47-50)
             return V3();
         }
     }
@@ -1585,7 +1594,7 @@ struct BSDF {
             r.delta = false;
             return r;
         }
-        case ATRC_MAT_MIRROR: {  // MirrorBSDF::sample (mirror.cpp:20-36)
+        case ATRC_MAT_MIRROR: {  // MirrorBSDF::sample (mirror.cpp:32-50)
             V3 lo = shd.global_to_local(wo);
             if (lo.z <= 0) return r;
             V3 nwo = normalize(lo);
@@ -1596,7 +1605,7 @@ struct BSDF {
             r.delta = true;
             return r;
         }
-        case ATRC_MAT_GLASS: {  // GlassBSDF::sample (glass.cpp:34-70), TransMode::Radiance
+        case ATRC_MAT_GLASS: {  // GlassBSDF::sample (glass.cpp:52-91), TransMode::Radiance
             V3 nwo = normalize(shd.global_to_local(wo));
             V3 nor = nwo.z > 0 ? V3(0, 0, 1) : V3(0, 0, -1);
             float fr = dielectric_fresnel(glass_ior, 1, nwo.z);
@@ -2053,7 +2062,7 @@ struct OracleScene {
         b.shd = shd;
         switch (m.type) {
         case ATRC_MAT_IDEAL_DIFFUSE:
-            b.albedo_ = tex2d[m.tex[0]].sample(in.uv);
+            b.albedo_ = tex2d[m.tex[0]].sample_at(in.uv, in.pos);  // ideal_diffuse.cpp:27, by intersection
             *shading_normal = shd.z;
             break;
         case ATRC_MAT_DISNEY: {
@@ -2067,7 +2076,7 @@ struct OracleScene {
             *shading_normal = shd.z;
             break;
         }
-        case ATRC_MAT_MIRROR: {  // Mirror::shade (mirror.cpp:62-76): ConductorPoint(ior, 1, k)
+        case ATRC_MAT_MIRROR: {  // Mirror::shade (mirror.cpp:98-115): ConductorPoint(ior, 1, k)
             V3 c = tex2d[m.tex[0]].sample(in.uv), ior = tex2d[m.tex[1]].sample(in.uv), k = tex2d[m.tex[2]].sample(in.uv);
             b.rc = c;
             b.eta2 = V3(1 / sqr(ior.x), 1 / sqr(ior.y), 1 / sqr(ior.z));
@@ -2076,16 +2085,16 @@ struct OracleScene {
             *shading_normal = shd.z;
             break;
         }
-        case ATRC_MAT_GLASS: {  // Glass::shade (glass.cpp:127-150)
-            b.glass_ior = tex2d[m.tex[2]].sample_real(in.uv);
-            b.refl_c = tex2d[m.tex[0]].sample(in.uv);
-            V3 rr = tex2d[m.tex[1]].sample(in.uv);
+        case ATRC_MAT_GLASS: {  // Glass::shade (glass.cpp:180-206)
+            b.glass_ior = tex2d[m.tex[2]].sample_at(in.uv, in.pos).x;  // by intersection
+            b.refl_c = tex2d[m.tex[0]].sample_at(in.uv, in.pos);
+            V3 rr = tex2d[m.tex[1]].sample_at(in.uv, in.pos);
             b.refr_c = V3(std::sqrt(rr.x), std::sqrt(rr.y), std::sqrt(rr.z));
             b.albedo_ = 0.5f * (b.refl_c + b.refr_c);
             *shading_normal = shd.z;
             break;
         }
-        case ATRC_MAT_METAL: {  // Metal::shade (metal.cpp:25-46)
+        case ATRC_MAT_METAL: {  // Metal::shade (metal.cpp:39-62)
             V3 c = tex2d[m.tex[0]].sample(in.uv), eta = tex2d[m.tex[1]].sample(in.uv), k = tex2d[m.tex[2]].sample(in.uv);
             float rough = tex2d[m.tex[3]].sample_real(in.uv), aniso = tex2d[m.tex[4]].sample_real(in.uv);
             b.rc = c;
@@ -2099,7 +2108,7 @@ struct OracleScene {
             *shading_normal = shd.z;
             break;
         }
-        case ATRC_MAT_PHONG: {  // Phong::shade (phong.cpp:23-58)
+        case ATRC_MAT_PHONG: {  // Phong::shade (phong.cpp:33-79)
             V3 d = tex2d[m.tex[0]].sample(in.uv), sp = tex2d[m.tex[1]].sample(in.uv);
             float ns = tex2d[m.tex[2]].sample_real(in.uv);
             float dem = std::max(1.0f, std::max(d.x + sp.x, std::max(d.y + sp.y, d.z + sp.z)));
@@ -2489,6 +2498,11 @@ int oracle_scene_create(const AtrcSceneDesc* d, float eps, OracleScene** out) {
         for (uint32_t i = 0; i < d->texture2d_count; ++i) sc->tex2d[i].d = d->textures2d[i];
         sc->tex3d.resize(d->texture3d_count);
         for (uint32_t i = 0; i < d->texture3d_count; ++i) sc->tex3d[i].d = d->textures3d[i];
+        for (Tex2D& t : sc->tex2d)
+            if (t.d.type == ATRC_TEX_SOLID) {
+                if (t.d.tex3d < 0 || uint32_t(t.d.tex3d) >= d->texture3d_count) throw std::runtime_error("bad solid_image");
+                t.solid = &sc->tex3d[size_t(t.d.tex3d)];
+            }
         sc->materials.assign(d->materials, d->materials + d->material_count);
         sc->media.resize(d->medium_count);
         for (uint32_t i = 0; i < d->medium_count; ++i) {
@@ -2545,6 +2559,8 @@ int oracle_scene_create(const AtrcSceneDesc* d, float eps, OracleScene** out) {
             l.is_env = true;
             sc->lights.push_back(l);
             if (d->env.type == ATRC_ENV_IBL) {
+                if (sc->tex2d[d->env.tex].d.type == ATRC_TEX_SOLID)
+                    throw std::runtime_error("solid_image is not supported as an environment map");
                 sc->env.tex = &sc->tex2d[d->env.tex];
                 const Tex2D* t = sc->env.tex;
                 if (d->env.no_importance_sampling) {

@@ -107,6 +107,27 @@ def test_closest_hits_bit_exact_instanced(instanced):
     assert 0.02 < (g["entity"] >= 0).mean() < 0.98
 
 
+def test_axis_aligned_rays_match(instanced):
+    # directions with exact zero components (the slab test must not turn
+    # 0 * inf into NaN and cull every box)
+    from tests.parity import RAY_DTYPE
+    cfg, desc, dev, ora = instanced
+    rng = np.random.default_rng(21)
+    n = 60_000
+    rays = np.zeros(n, dtype=RAY_DTYPE)
+    rays["o"] = rng.uniform(-20, 20, (n, 3))
+    axes = np.concatenate([np.eye(3), -np.eye(3)]).astype(np.float32)
+    rays["d"] = axes[rng.integers(0, 6, n)]
+    rays["t_min"] = 0
+    rays["t_max"] = np.inf
+    g = dev.trace_rays(rays, "closest", exact=True)
+    r = ora.trace_rays(rays, "closest")
+    c = classify_closest(rays, g, r, ora)
+    assert c["error"] == 0, c["errors"]
+    assert c["exact"] + c["tie"] + c["ref_fn"] == len(rays)
+    assert 0.05 < (g["entity"] >= 0).mean() and c["exact"] >= len(rays) * 0.999, c
+
+
 def test_instanced_disney_ibl_image_within_3_sigma(instanced):
     cfg, desc, dev, ora = instanced
     fg = Film(desc.width, desc.height, value_sq=True)
@@ -235,3 +256,28 @@ def test_closest_hits_bit_exact_1e7_full_workload():
     assert c["max_ulp_same_prim"] == 0
     assert c["exact"] + c["tie"] + c["ref_fn"] == len(rays)
     assert c["exact"] >= len(rays) * 0.9999, c
+
+
+@pytest.mark.parametrize("case", ["plane", "sphere", "box"])
+def test_subsurface_probe_matches_oracle(tmp_path, case):
+    # the device's subsurface walk (subsurface_sample) and the oracle's: the
+    # fraction of valid samples and the mean weight per channel agree to
+    # sampling noise, on a plane, a sphere and an instanced mesh box
+    import json
+    from tests import kat_scenes as K
+    if case == "plane":
+        c, o, d = K.subsurface_plane(A=(0.8, 0.5, 0.2)), [0.3, 0.1, 2.0], [0, 0, -1]
+    else:
+        c = K.subsurface_scene(tmp_path)
+        o, d = ([-0.7, -3.0, -0.4], [0, 1, 0]) if case == "sphere" else ([0.8, -3.0, -0.55], [0.01, 1, 0.02])
+    cfg = Config.from_string(json.dumps(c), tmp_path)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    n = 200_000
+    wg, xg = dev.subsurface_probe(o, d, n, seed=5)
+    wo, xo = ora.subsurface(o, d, n, seed=5)
+    pg, po = (wg[:, 0] > 0).mean(), (wo[:, 0] > 0).mean()
+    assert abs(pg - po) < 5 * np.sqrt(po * (1 - po) * 2 / n) + 1e-6, (pg, po)
+    se = np.sqrt(wg.var(0) / n + wo.var(0) / n)
+    assert np.all(np.abs(wg.mean(0) - wo.mean(0)) < 5 * se + 1e-6), (wg.mean(0), wo.mean(0), se)
