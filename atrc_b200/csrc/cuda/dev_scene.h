@@ -133,6 +133,7 @@ struct Scene {
     const Medium* media;
     int32_t medium_count;
     int32_t has_media;              // any non-void medium referenced
+    int32_t has_subsurface;         // any material with subsurface scattering
     const float* alias_prob;        // triangle-area alias tables (all leaves)
     const int32_t* alias_idx;
     int32_t light_count;            // lights: env first (if any), then areas

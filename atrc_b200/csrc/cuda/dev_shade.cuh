@@ -42,17 +42,22 @@ __device__ __forceinline__ Vec3 texel2(const float* base, int w, int x, int y) {
     return Vec3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
-template <bool REAL_ONLY>
-__device__ Vec3 tex3d_sample(const Scene& S, int ti, Vec3 uvw0);
+// A solid image's 3D lookup (defined after the 3D filter).
+__device__ Vec3 solid_sample(const Scene& S, int t3, Vec3 p);
 
-__device__ Vec3 tex2d_sample(const Scene& S, int ti, float u0, float v0) {
+// Texture2D::sample_spectrum.  With SOLID, a solid image reads its 3D
+// texture at (u, v, 0) (solid_image.cpp:12-15), or at `pos` where the
+// material samples by intersection (solid_image.cpp:25-33); lookups that
+// never meet a solid image (the environment map) pass SOLID = false.
+template <bool SOLID>
+__device__ __forceinline__ Vec3 tex2d_lookup(const Scene& S, int ti, float u0, float v0, Vec3 pos, bool at_pos) {
     const Texture2D& t = S.tex2d[ti];
     if (t.type == 0) return Vec3(t.texel[0], t.texel[1], t.texel[2]);
+    if (SOLID && t.type == ATRC_TEX_SOLID && at_pos) return solid_sample(S, t.tex3d, pos);
     const float tu = t.uv[0] * u0 + t.uv[1] * v0 + t.uv[2];
     const float tv = t.uv[3] * u0 + t.uv[4] * v0 + t.uv[5];
     const float u = wrap_coord(t.wrap_u, tu), v = wrap_coord(t.wrap_v, tv);
-    // SolidImageTexture::sample_spectrum_impl (solid_image.cpp:12-15)
-    if (t.type == ATRC_TEX_SOLID) return tex3d_sample<false>(S, t.tex3d, Vec3(u, v, 0.0f));
+    if (SOLID && t.type == ATRC_TEX_SOLID) return solid_sample(S, t.tex3d, Vec3(u, v, 0.0f));
     const float* base = S.texels + t.data_offset;
     Vec3 r;
     if (t.type == ATRC_TEX_CHECKER) {  // CheckerBoard::sample_spectrum_impl (checker_board.cpp:15-22)
@@ -76,11 +81,8 @@ __device__ Vec3 tex2d_sample(const Scene& S, int ti, float u0, float v0) {
     return r;
 }
 
-// Texture2D::sample_spectrum(inct): the solid image reads its 3D texture at
-// the world position (solid_image.cpp:25-33), every other texture at uv.
-__device__ __forceinline__ Vec3 tex2d_sample_at(const Scene& S, int ti, float u, float v, Vec3 pos) {
-    if (S.tex2d[ti].type == ATRC_TEX_SOLID) return tex3d_sample<false>(S, S.tex2d[ti].tex3d, pos);
-    return tex2d_sample(S, ti, u, v);
+__device__ __forceinline__ Vec3 tex2d_sample(const Scene& S, int ti, float u, float v) {
+    return tex2d_lookup<true>(S, ti, u, v, Vec3(), false);
 }
 
 __device__ __forceinline__ float tex3d_at(const float* base, const Texture3D& t, int x, int y, int z, int c) {
@@ -126,6 +128,8 @@ __device__ Vec3 tex3d_sample(const Scene& S, int ti, Vec3 uvw0) {
     if (t.inv_gamma != 1.0f) r = Vec3(powf(r.x, t.inv_gamma), powf(r.y, t.inv_gamma), powf(r.z, t.inv_gamma));
     return r;
 }
+
+__device__ Vec3 solid_sample(const Scene& S, int t3, Vec3 p) { return tex3d_sample<false>(S, t3, p); }
 
 // ====================================================== surface interaction
 struct Surface {
@@ -894,9 +898,24 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
     b.disney_fixed = S.disney_fixed != 0;
     b.albedo = Vec3();
     Coord shd = s.user;
-    if (m.normal_map >= 0 && (m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_DISNEY ||
-                              m.type == ATRC_MAT_METAL || m.type == ATRC_MAT_PHONG)) {
-        const Vec3 t = tex2d_sample(S, m.normal_map, s.u, s.v);  // NormalMapper::reorient
+    // every texture slot the material reads, and its normal map last, from
+    // one lookup site (the lookup is inlined once; its values stay in tv)
+    const bool nmap = m.normal_map >= 0 && (m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_DISNEY ||
+                                            m.type == ATRC_MAT_METAL || m.type == ATRC_MAT_PHONG);
+    int nsl = 0;
+    if (!m.all_constant) {
+        nsl = m.type == ATRC_MAT_DISNEY ? 13 : m.type == ATRC_MAT_IDEAL_DIFFUSE ? 1 : m.type == ATRC_MAT_METAL ? 5
+            : (m.type == ATRC_MAT_MIRROR || m.type == ATRC_MAT_GLASS || m.type == ATRC_MAT_PHONG) ? 3 : 0;
+    }
+    // IdealDiffuse and Glass sample by intersection (ideal_diffuse.cpp:27, glass.cpp:184-192)
+    const bool at_pos = m.type == ATRC_MAT_IDEAL_DIFFUSE || m.type == ATRC_MAT_GLASS;
+    const int ntex = nsl + (nmap ? 1 : 0);
+    Vec3 tv[14];
+#pragma unroll 1
+    for (int k = 0; k < ntex; ++k)
+        tv[k] = tex2d_lookup<true>(S, k < nsl ? m.tex[k] : m.normal_map, s.u, s.v, s.pos, at_pos && k < nsl);
+    if (nmap) {
+        const Vec3 t = tv[nsl];  // NormalMapper::reorient
         const Vec3 ln = normalize(Vec3(t.x * 2 - 1, t.y * 2 - 1, t.z * 2 - 1));
         shd = rotate_to_new_z(s.user, s.user.local_to_global(ln));
     }
@@ -904,13 +923,13 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
     *shading_normal = m.type == ATRC_MAT_INVISIBLE_SURFACE || m.type == ATRC_MAT_IDEAL_BLACK ? s.user.z : shd.z;
     if (m.type == ATRC_MAT_IDEAL_DIFFUSE) {
         // IdealDiffuse::shade samples by intersection (ideal_diffuse.cpp:27)
-        b.albedo = m.all_constant ? Vec3(m.c[0], m.c[1], m.c[2]) : tex2d_sample_at(S, m.tex[0], s.u, s.v, s.pos);
+        b.albedo = m.all_constant ? Vec3(m.c[0], m.c[1], m.c[2]) : tv[0];
     } else if (m.type == ATRC_MAT_DISNEY) {
         if (m.all_constant) {
             disney_init(b, Vec3(m.c[0], m.c[1], m.c[2]), m.c[3], m.c[4], m.c[5], m.c[6], m.c[7],
                         Vec3(m.c[8], m.c[9], m.c[10]), m.c[11], m.c[12], m.c[13], m.c[14], m.c[15], m.cc_gloss);
         } else {
-            auto T = [&](int slot) { return tex2d_sample(S, m.tex[slot], s.u, s.v); };
+            auto T = [&](int slot) { return tv[slot]; };
             disney_init(b, T(ATRC_DISNEY_BASE_COLOR), T(ATRC_DISNEY_METALLIC).x, T(ATRC_DISNEY_ROUGHNESS).x,
                         T(ATRC_DISNEY_TRANSMISSION).x, T(ATRC_DISNEY_TRANSMISSION_ROUGHNESS).x, T(ATRC_DISNEY_IOR).x,
                         T(ATRC_DISNEY_SPECULAR_SCALE), T(ATRC_DISNEY_SPECULAR_TINT).x, T(ATRC_DISNEY_ANISOTROPIC).x,
@@ -919,7 +938,7 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
         }
     } else if (m.type == ATRC_MAT_MIRROR || m.type == ATRC_MAT_GLASS || m.type == ATRC_MAT_METAL ||
                m.type == ATRC_MAT_PHONG) {
-        auto T = [&](int slot) { return tex2d_sample(S, m.tex[slot], s.u, s.v); };
+        auto T = [&](int slot) { return tv[slot]; };
         if (m.type == ATRC_MAT_MIRROR) {
             // Mirror::shade (mirror.cpp:98-115): ConductorPoint(ior, 1, k) puts
             // the ior on the OUTER side, so eta^2 = 1 / ior^2
@@ -929,10 +948,9 @@ __device__ BSDF shade(const Scene& S, const Surface& s, Vec3* shading_normal) {
             b.etak2 = Vec3(sqrf(k.x / ior.x), sqrf(k.y / ior.y), sqrf(k.z / ior.z));
             b.albedo = rc;
         } else if (m.type == ATRC_MAT_GLASS) {  // Glass::shade (glass.cpp:180-206), by intersection
-            auto TP = [&](int slot) { return tex2d_sample_at(S, m.tex[slot], s.u, s.v, s.pos); };
-            b.glass_ior = TP(2).x;
-            b.refl_c = TP(0);
-            const Vec3 rr = TP(1);
+            b.glass_ior = T(2).x;
+            b.refl_c = T(0);
+            const Vec3 rr = T(1);
             b.refr_c = Vec3(sqrtf(rr.x), sqrtf(rr.y), sqrtf(rr.z));
             b.albedo = 0.5f * (b.refl_c + b.refr_c);
         } else if (m.type == ATRC_MAT_METAL) {  // Metal::shade (metal.cpp:39-62)
@@ -1104,7 +1122,7 @@ __device__ Vec3 env_radiance(const Scene& S, Vec3 d) {
     }
     const float u = clampf(phi_of(dir) / (2 * kPi), 0, 1);
     const float v = clampf(acosf(clampf(dir.z, -1, 1)) / kPi, 0, 1);
-    return tex2d_sample(S, env.tex, u, v);
+    return tex2d_lookup<false>(S, env.tex, u, v, Vec3(), false);
 }
 
 __device__ float env_pdf(const Scene& S, Vec3 d) {

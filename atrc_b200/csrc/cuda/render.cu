@@ -115,6 +115,7 @@ struct Counters {
     int n_ext, n_next;        // paths to extend / continuations written
     int n_shadow, n_finish;
     int n_guide;              // guide queries this iteration
+    int n_sss;                // subsurface walks queued this iteration
     int n_free, n_new, n_cont, free_base;
     unsigned long long gen_base, issued, total, completed;
     unsigned long long rays_closest, rays_shadow, iterations;
@@ -204,6 +205,7 @@ struct Pool {
     int* key_count;               // per key: entries this iteration
     int* key_cursor;              // per key: next write position in q_sorted
     int* q_finish;
+    int* q_sss;                   // paths whose BSDF sample entered a subsurface material
     int* free_list;
     float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
     int shadow_cap;
@@ -243,6 +245,7 @@ __global__ void k_begin(Counters* c) {
     c->n_shadow = 0;
     c->n_finish = 0;
     c->n_guide = 0;
+    c->n_sss = 0;
     if (c->n_ext == 0) c->done = 1;
 }
 
@@ -442,6 +445,50 @@ __device__ __forceinline__ bool guidable(const Material& m) {
             type == ATRC_MAT_PHONG) && m.bssrdf[1] < 0;
 }
 
+// Next-event estimation at surface vertex sv over every light
+// (path_tracing.cpp:134-146, direct_illum.cpp:11-128): one light sample
+// each, MIS-weighted against the BSDF-side pdf -- the guide's one-sample
+// mixture where `guided` -- and pushed to the shadow queue.
+__device__ __forceinline__ void nee_surface(const Scene& S, Pool& P, Counters* c, int slot, const Surface& sv,
+                                            const BSDF& bv, const Entity& e, Vec3 coef, bool guided,
+                                            const GuideMix& mix, Rng& rng, int* wd, float eps) {
+    auto side_pdf = [&](Vec3 dir, float pb) {
+        return guided ? mix.c * guide_pdf(mix, dir) + (1.0f - mix.c) * pb : pb;
+    };
+    for (int li = 0; li < S.light_count; ++li) {
+        const int le_i = S.light_entity[li];
+        const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+        if (le_i < 0) {
+            float lpdf;
+            const Vec3 dir = env_sample(S, u0, u1, u2, &lpdf);
+            const Vec3 rad = env_radiance(S, dir);
+            if (black(rad)) continue;
+            const Vec3 lpos = env_emit_pos(S, sv.pos, dir);
+            const Vec3 to_light = normalize(lpos - sv.pos);
+            const Vec3 bf = bsdf_eval(bv, to_light, sv.wr);
+            if (black(bf)) continue;
+            const Vec3 contrib = coef * rad * bf *
+                                 (fabsf(cosv(to_light, sv.geo.z)) / (lpdf + side_pdf(to_light, bsdf_pdf(bv, to_light, sv.wr))));
+            push_shadow(P, c, sv.pos, to_light, eps, length(sv.pos - lpos) - eps, contrib, slot);
+        } else {
+            const Entity& le = S.entities[le_i];
+            LightSample ls;
+            if (!area_light_sample(S, le, sv.pos, u0, u1, u2, &ls)) continue;
+            if (black(ls.rad) || ls.pdf == 0.0f) continue;
+            const float slen = length(ls.pos - sv.pos) - eps;
+            if (slen <= eps) continue;
+            const Vec3 to_light = normalize(ls.pos - sv.pos);
+            const Vec3 bf = bsdf_eval(bv, to_light, sv.wr);
+            if (black(bf)) continue;
+            Vec3 tr(1.0f);
+            if (S.has_media) tr = medium_tr(S, medium_of(sv, e, to_light), ls.pos, sv.pos, rng, wd);
+            const Vec3 contrib = coef * tr * ls.rad * bf *
+                                 (fabsf(cosv(to_light, sv.geo.z)) / (ls.pdf + side_pdf(to_light, bsdf_pdf(bv, to_light, sv.wr))));
+            push_shadow(P, c, sv.pos, to_light, eps, slen, contrib, slot);
+        }
+    }
+}
+
 constexpr int kMaxProbeHits = 64;  // entity crossings one subsurface probe records
 
 // SeparableBSSRDF::sample_pi (separable.cpp:107-220) of the normalized
@@ -585,7 +632,7 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
         Vec3 L = xyz(L4);
         float4 mf4 = P.mis_f[slot];
         int wd = 0;
-        bool finish = false, cont = false;
+        bool finish = false, cont = false, subsurface = false;
         if (flags & PF_REC_PENDING) {
             // radiance gathered up to this vertex: the previous record's
             // incident radiance is what the path brings back from here on
@@ -744,47 +791,7 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                 };
                 if (depth == 1 && (e.flags & ENT_LIGHT)) L += coef * area_light_radiance(e, s.geo.z, s.wr);
                 // next-event estimation over every light (path_tracing.cpp:134-146)
-                // at surface sv with BSDF bv (the BSDF-side pdf includes the
-                // guide where `with_guide`)
-                auto nee = [&](const Surface& sv, const BSDF& bv, bool with_guide) {
-                    for (int li = 0; li < S.light_count; ++li) {
-                        const int le_i = S.light_entity[li];
-                        const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
-                        if (le_i < 0) {
-                            float lpdf;
-                            const Vec3 dir = env_sample(S, u0, u1, u2, &lpdf);
-                            const Vec3 rad = env_radiance(S, dir);
-                            if (black(rad)) continue;
-                            const Vec3 lpos = env_emit_pos(S, sv.pos, dir);
-                            const Vec3 to_light = normalize(lpos - sv.pos);
-                            const Vec3 bf = bsdf_eval(bv, to_light, sv.wr);
-                            if (black(bf)) continue;
-                            const float pb = bsdf_pdf(bv, to_light, sv.wr);
-                            const Vec3 contrib = coef * rad * bf *
-                                                 (fabsf(cosv(to_light, sv.geo.z)) /
-                                                  (lpdf + (with_guide ? side_pdf(to_light, pb) : pb)));
-                            push_shadow(P, c, sv.pos, to_light, eps, length(sv.pos - lpos) - eps, contrib, slot);
-                        } else {
-                            const Entity& le = S.entities[le_i];
-                            LightSample ls;
-                            if (!area_light_sample(S, le, sv.pos, u0, u1, u2, &ls)) continue;
-                            if (black(ls.rad) || ls.pdf == 0.0f) continue;
-                            const float slen = length(ls.pos - sv.pos) - eps;
-                            if (slen <= eps) continue;
-                            const Vec3 to_light = normalize(ls.pos - sv.pos);
-                            const Vec3 bf = bsdf_eval(bv, to_light, sv.wr);
-                            if (black(bf)) continue;
-                            Vec3 tr(1.0f);
-                            if (S.has_media) tr = medium_tr(S, medium_of(sv, e, to_light), ls.pos, sv.pos, rng, &wd);
-                            const float pb = bsdf_pdf(bv, to_light, sv.wr);
-                            const Vec3 contrib = coef * tr * ls.rad * bf *
-                                                 (fabsf(cosv(to_light, sv.geo.z)) /
-                                                  (ls.pdf + (with_guide ? side_pdf(to_light, pb) : pb)));
-                            push_shadow(P, c, sv.pos, to_light, eps, slen, contrib, slot);
-                        }
-                    }
-                };
-                nee(s, b, true);
+                nee_surface(S, P, c, slot, s, b, e, coef, guided, mix, rng, &wd, eps);
                 // BSDF sample: MIS-BSDF ray and continuation (path_tracing.cpp:148-169)
                 BSDFSample bs;
                 float pdf_bsdf = 0.0f;
@@ -831,30 +838,17 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                     }
                     // subsurface scattering (path_tracing.cpp:173-221): a
                     // direction into the surface re-emerges at a probed exit
-                    // point, which gets its own light samples and continues
-                    // the path with a sample of its separable BSDF.  The
-                    // entry's MIS-BSDF term is the continuation's, which
-                    // re-emerges instead: exact while the inside of the
-                    // object holds no light.
-                    const Material& mat = S.materials[e.material];
-                    if (mat.bssrdf[1] >= 0 && bs.pdf >= eps && !s.geo.positive(bs.dir) && s.geo.positive(s.wr)) {
+                    // point; the walk runs in k_subsurface.  The entry's
+                    // MIS-BSDF term is the continuation's, which re-emerges
+                    // instead: exact while the inside of the object holds
+                    // no light.
+                    if (S.has_subsurface && S.materials[e.material].bssrdf[1] >= 0 && bs.pdf >= eps &&
+                        !s.geo.positive(bs.dir) && s.geo.positive(s.wr)) {
                         coef = coef * bs.f * (fabsf(cosv(s.geo.z, bs.dir)) / bs.pdf);
-                        Surface x;
-                        BSDF bx;
-                        Vec3 w;
-                        bool alive = subsurface_sample(S, mat, s, rng, &wd, eps, &x, &bx, &w);
-                        if (alive) {
-                            coef = coef * w;
-                            nee(x, bx, false);
-                            const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
-                            bs = bsdf_sample(bx, x.wr, u0, u1, u2);
-                            alive = !black(bs.f);
-                            s = x;
-                        }
-                        if (!alive) finish = true;
+                        subsurface = true;
                     }
                 }
-                if (!finish) {
+                if (!finish && !subsurface) {
                     const Vec3 dir = normalize(bs.dir);
                     const float gcos = fabsf(dot(s.geo.z, dir));
                     mf4 = make_float4(coef.x * bs.f.x * gcos, coef.y * bs.f.y * gcos, coef.z * bs.f.z * gcos, mf4.w);
@@ -879,6 +873,73 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
         P.L[slot] = make_float4(L.x, L.y, L.z, L4.w);
         P.mis_f[slot] = mf4;
         P.ctr[slot] = make_int4(depth, s_depth, scat, (flags & 0xff) | (ray_med << 8));
+        const int qi = warp_append(&c->n_next, cont);
+        if (cont) P.q[out][qi] = slot;
+        if (S.has_subsurface) {
+            const int si = warp_append(&c->n_sss, subsurface);
+            if (subsurface) P.q_sss[si] = slot;
+        }
+        const bool ends = !cont && !subsurface;
+        const int fi = warp_append(&c->n_finish, ends);
+        if (ends) P.q_finish[fi] = slot;
+    }
+}
+
+// Subsurface walks queued by k_shade (path_tracing.cpp:173-221): the probe
+// from the entry point, light samples at the exit point with its separable
+// BSDF, and the exit's BSDF sample that continues the path (its MIS-BSDF
+// term pending like every other vertex).  Paths end here when the probe
+// finds no exit or the exit sample is black.
+__global__ void __launch_bounds__(128) k_subsurface(Scene S, Params p, Pool P, Counters* c) {
+    const int n = c->n_sss, out = c->out;
+    const float eps = p.eps;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = P.q_sss[i];
+        const int4 ct = P.ctr[slot];
+        int depth = ct.x, flags = ct.w & 0xff, ray_med = ct.w >> 8;
+        uint4 st = P.st[slot];
+        Rng rng = load_rng(st);
+        const float4 ro = P.ray_o[slot], rd = P.ray_d[slot], hv = P.hit[slot];
+        Hit h;
+        h.t = hv.x; h.u = hv.y; h.v = hv.z; h.entity = __float_as_int(hv.w); h.tri = P.hit_tri[slot];
+        const Surface s = make_surface(S, h, xyz(ro), xyz(rd));
+        const Entity& e = S.entities[h.entity];
+        float4 coef4 = P.coef[slot];
+        Vec3 coef = xyz(coef4);
+        float4 mf4 = P.mis_f[slot];
+        int wd = 0;
+        bool cont = false;
+        Surface x;
+        BSDF bx;
+        Vec3 w;
+        if (subsurface_sample(S, S.materials[e.material], s, rng, &wd, eps, &x, &bx, &w)) {
+            coef = coef * w;
+            GuideMix none;
+            nee_surface(S, P, c, slot, x, bx, e, coef, false, none, rng, &wd, eps);
+            const float u0 = rng.u(), u1 = rng.u(), u2 = rng.u();
+            const BSDFSample bs = bsdf_sample(bx, x.wr, u0, u1, u2);
+            if (!black(bs.f)) {
+                const Vec3 dir = normalize(bs.dir);
+                const float gcos = fabsf(dot(x.geo.z, dir));
+                mf4 = make_float4(coef.x * bs.f.x * gcos, coef.y * bs.f.y * gcos, coef.z * bs.f.z * gcos, mf4.w);
+                coef4.w = bs.pdf;
+                flags |= PF_MIS;
+                ray_med = medium_of(x, e, dir);
+                if (bs.pdf < eps) flags |= PF_TERMINATE;
+                else coef = coef * bs.f * (fabsf(cosv(x.geo.z, bs.dir)) / bs.pdf);
+                const Vec3 no = eps_offset(x, bs.dir, eps);
+                P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                P.ray_d[slot] = make_float4(dir.x, dir.y, dir.z, INFINITY);
+                ++depth;
+                cont = true;
+            }
+        }
+        if (wd) atomicMax(&c->watchdog, wd);
+        store_rng(st, rng);
+        P.st[slot] = st;
+        P.coef[slot] = make_float4(coef.x, coef.y, coef.z, coef4.w);
+        P.mis_f[slot] = mf4;
+        P.ctr[slot] = make_int4(depth, ct.y, ct.z, (flags & 0xff) | (ray_med << 8));
         const int qi = warp_append(&c->n_next, cont);
         if (cont) P.q[out][qi] = slot;
         const int fi = warp_append(&c->n_finish, !cont);
@@ -1160,6 +1221,7 @@ PoolLayout pool_layout(size_t cap, size_t shadow_cap, int nkeys) {
     take(11, cap * 4); take(12, cap * 4); take(13, cap * 4); take(14, cap * 4);
     take(15, shadow_cap * 16); take(16, shadow_cap * 16); take(17, shadow_cap * 16);
     take(18, cap * 4); take(19, cap * 4); take(20, size_t(nkeys) * 4); take(21, size_t(nkeys) * 4);
+    take(22, cap * 4);
     L.total = (o + 255) & ~size_t(255);
     return L;
 }
@@ -1189,6 +1251,7 @@ Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
     P.keys = reinterpret_cast<int*>(b + L.off[19]);
     P.key_count = reinterpret_cast<int*>(b + L.off[20]);
     P.key_cursor = reinterpret_cast<int*>(b + L.off[21]);
+    P.q_sss = reinterpret_cast<int*>(b + L.off[22]);
     P.shadow_cap = int(shadow_cap);
     return P;
 }
@@ -1620,6 +1683,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
                 guide_infer(guide, &c->n_guide, s);
             }
             k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
+            if (d.scene.has_subsurface) k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
             if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
             else k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
@@ -1635,7 +1699,8 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     }
     for (int iter_block = 0;; ++iter_block) {
         CK(cudaGraphLaunch(d.window_exec, s));
-        launches += (6 + (p.sort_mode != ATRC_SORT_NONE ? 2 : 0) + (guide ? 2 : 0)) * window;
+        launches += (6 + (p.sort_mode != ATRC_SORT_NONE ? 2 : 0) + (guide ? 2 : 0) + (d.scene.has_subsurface ? 1 : 0)) *
+                    window;
         ext_launches += window;
         CK(cudaStreamSynchronize(s));
         hc = *pinned;
@@ -2039,6 +2104,10 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
                     launches += 2;
                 }
                 k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
+                if (d.scene.has_subsurface) {
+                    k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
+                    launches += 1;
+                }
                 k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 k_finish<<<gsm, 128, 0, s>>>(p, P, c);
                 launches += 6;

@@ -490,6 +490,7 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
         }
         if (m.normal_map >= 0 && uint32_t(m.normal_map) >= d.texture2d_count) throw std::runtime_error("bad texture index");
         const bool sss = m.bssrdf[1] >= 0;
+        if (sss) hs->scene.has_subsurface = 1;
         for (int s = 0; s < 3; ++s) {
             dm.bssrdf[s] = sss ? m.bssrdf[s] : -1;
             if (sss && (m.type != ATRC_MAT_DISNEY || m.bssrdf[s] < 0 || uint32_t(m.bssrdf[s]) >= d.texture2d_count))

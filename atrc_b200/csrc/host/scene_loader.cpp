@@ -221,6 +221,7 @@ public:
         t.texel[0] = t.texel[1] = t.texel[2] = v;
         t.uv_transform[0] = 1; t.uv_transform[4] = 1;
         t.inv_gamma = 1;
+        t.tex3d = -1;
         out_.textures2d.push_back(t);
         return int(out_.textures2d.size() - 1);
     }

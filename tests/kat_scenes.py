@@ -318,3 +318,43 @@ def subsurface_scene(tmp: Path, spp=256, width=40, height=30) -> dict:
                           "width": width, "height": height,
                           "renderer": {"type": "pt", "spp": spp, "max_depth": 10, "min_depth": 3},
                           "reporter": {"type": "noout"}}}
+
+
+def solid_image_scene(tmp: Path, spp=256, width=40, height=30) -> dict:
+    """`solid_image` textures: a floor whose ideal-diffuse albedo reads an RGB
+    3D image at the world position (scaled into the texture's unit cube), a
+    glass sphere whose refraction colour does the same, and a Disney sphere
+    whose base colour reads the same 3D image at (u, v, 0)."""
+    rng = np.random.default_rng(5)
+    grid = rng.uniform(0.05, 0.95, (8, 8, 8, 3)).astype(np.float32)   # (d, h, w, rgb)
+    (tmp / "solid.bin").write_bytes(np.int32([8, 8, 8]).tobytes() + grid.tobytes())
+    tex3d = {"type": "image3d", "format": "spec", "binary_filename": "${scene-directory}/solid.bin",
+             "sample": "nearest", "wrap_u": "repeat", "wrap_v": "repeat", "wrap_w": "repeat",
+             "transform": [{"type": "scale", "ratio": 0.25}, {"type": "translate", "offset": [4, 4, 4]}]}
+    solid = {"type": "solid_image", "tex3d": tex3d}
+    plain = {"type": "solid_image", "tex3d": dict(tex3d, transform=[])}
+
+    def const(v):
+        return {"type": "constant", "texel": list(map(float, np.atleast_1d(v)))}
+    ents = [
+        {"type": "geometric", "geometry": {"type": "quad", "A": [-4, -4, -1], "B": [4, -4, -1], "C": [4, 4, -1],
+                                           "D": [-4, 4, -1], "transform": []},
+         "material": {"type": "ideal_diffuse", "albedo": solid}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.6,
+                                           "transform": [{"type": "translate", "offset": [-0.8, 0.3, -0.4]}]},
+         "material": {"type": "disney", "base_color": plain, "metallic": const(0), "roughness": const(0.5)}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.5,
+                                           "transform": [{"type": "translate", "offset": [0.8, -0.2, -0.5]}]},
+         "material": {"type": "glass", "ior": const(1.5), "color_reflection_map": const(0.9),
+                      "color_refraction_map": solid}},
+        {"type": "geometric", "geometry": {"type": "sphere", "radius": 0.3,
+                                           "transform": [{"type": "translate", "offset": [0.2, -1.0, 1.6]}]},
+         "material": {"type": "ideal_black"}, "emit_radiance": [10, 9, 8]},
+    ]
+    return {"scene": {"type": "default", "entities": ents,
+                      "env": {"type": "native_sky", "top": [0.3, 0.35, 0.5], "bottom": [0.05, 0.05, 0.05]}},
+            "rendering": {"camera": {"type": "thin_lens", "pos": [0, -4.5, 1.2], "dst": [0, 0, -0.4], "up": [0, 0, 1],
+                                     "fov": 40},
+                          "width": width, "height": height,
+                          "renderer": {"type": "pt", "spp": spp, "max_depth": 10, "min_depth": 3},
+                          "reporter": {"type": "noout"}}}

@@ -329,3 +329,17 @@ def test_obj_and_stl_meshes(tmp_path):
     (tmp_path / "bad.stl").write_text("solid t\n facet normal 0 0 1\n outer loop\n vertex 0 0 0\n endfacet\n")
     with pytest.raises(AtrcError, match="three vertices"):
         _mesh_vertices(tmp_path, "bad.stl")
+
+
+def test_solid_image_texture():
+    # SolidImageCreator (texture2d_creators.cpp:148-163): a 3D texture behind
+    # the 2D interface, without the 2D common parameters
+    q = json.loads(json.dumps(QUAD))
+    q["material"]["albedo"] = {"type": "solid_image", "transform": [{"type": "scale", "ratio": 3}],
+                               "tex3d": {"type": "constant", "texel": [0.2, 0.4, 0.6]}}
+    cfg = Config.from_string(base([q]))
+    s = cfg.scene_desc().contents
+    t = [s.textures2d[i] for i in range(s.texture2d_count) if s.textures2d[i].type == 3]
+    assert len(t) == 1 and 0 <= t[0].tex3d < s.texture3d_count
+    assert list(t[0].uv_transform) == [1, 0, 0, 0, 1, 0] and t[0].wrap_u == 0 and t[0].inv_gamma == 1
+    assert list(s.textures3d[t[0].tex3d].texel) == pytest.approx([0.2, 0.4, 0.6])

@@ -215,6 +215,26 @@ def test_subsurface_scene_within_3_sigma(tmp_path):
     assert global_mean_z(fg, fc) < 4.0
 
 
+def test_solid_image_scene_within_3_sigma(tmp_path):
+    # solid_image read at the world position (ideal diffuse albedo, glass
+    # refraction colour) and at (u, v, 0) (Disney base colour)
+    from tests import kat_scenes as K
+    cfg = Config.from_string(K.dumps(K.solid_image_scene(tmp_path, spp=512)), tmp_path)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    fg = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    fc = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    dev.render(desc, fg)
+    ora.render(desc, fc)
+    r = 0.5 - desc.eps
+    frac, allowed, info = band_test(fg, fc, 1 / (4 * r * r))
+    assert frac <= allowed, (frac, allowed, info)
+    ga = fg.albedo.reshape(-1, 3) / fg.weight.reshape(-1, 1)
+    ca = fc.albedo.reshape(-1, 3) / fc.weight.reshape(-1, 1)
+    assert np.abs(ga - ca).mean() < 0.02
+
+
 def test_gaussian_filter_matches(tmp_path):
     from tests import kat_scenes as K
     cfg = Config.from_string(K.dumps(K.feature_scene(tmp_path, spp=128, gaussian=True)), tmp_path)
