@@ -83,9 +83,11 @@ __device__ __forceinline__ void tmem_row(uint32_t tbase, int col0, int n, float*
 }
 
 // ------------------------------------------------------------ inference
-// shared memory of k_guide_mlp (bytes)
-constexpr int kInfX = 0;                              // X 128 x 112, later H2 128 x 64
-constexpr int kInfH = kInfX + kTile * kGuideIn * 2;   // H1 / H3 128 x 64
+// shared memory of k_guide_mlp (bytes): two input buffers (each holds an
+// encoded tile, then H2, then the tile's outputs), H1 / H3, the weights and
+// the barriers (MMA completion, one per input buffer)
+constexpr int kInfX = 0;                                  // X[0], X[1]: 128 x 112 each
+constexpr int kInfH = kInfX + 2 * kGuideTileBytes;        // H1 / H3 128 x 64
 constexpr int kInfW1 = kInfH + kTile * kGuideHidden * 2;
 constexpr int kInfW2 = kInfW1 + kGuideHidden * kGuideIn * 2;
 constexpr int kInfW3 = kInfW2 + kGuideHidden * kGuideHidden * 2;
@@ -93,7 +95,9 @@ constexpr int kInfW4 = kInfW3 + kGuideHidden * kGuideHidden * 2;
 constexpr int kInfBar = kInfW4 + kGuideOut * kGuideHidden * 2;
 constexpr int kInfSmem = kInfBar + 64;
 constexpr uint32_t kInfTmemCols = 64;
-static_assert(kInfX == 0 && kGuideTileBytes == kInfH, "an encoded tile fills X");
+static_assert(kGuideTileBytes == kTile * kGuideIn * 2 && kGuideTileBytes % 16 == 0, "an encoded tile fills X");
+static_assert(kTile * kGuideOut * 4 <= kGuideTileBytes, "a tile's outputs fit its input buffer");
+static_assert(2 * (kInfSmem + 1024) <= 228 * 1024, "two CTAs per SM");
 
 // One MMA group: thread 0 issues, all wait.  Returns false (uniformly) when
 // the wait gave up.
@@ -136,38 +140,68 @@ __global__ void k_guide_encode(HashGrid grid, const T* __restrict__ table, const
 
 // The MLP over encoded tiles: *n_dev rows.  DECODE writes the decoded
 // mixture (GuideMix order, kGuideOut floats per row), else the raw outputs.
-// One CTA of 128 threads per tile (persistent over tiles); thread t owns row
-// t and TMEM lane t; the four layers run on the same 64 TMEM columns.
+// Persistent CTAs of 128 threads, two per SM; thread t owns row t and TMEM
+// lane t, and the four layers run on the same 64 TMEM columns.  While a
+// tile runs through the tensor core, the CTA's next tile streams into the
+// other input buffer (one bulk copy, completion counted on that buffer's
+// mbarrier); the finished tile's outputs are staged in its input buffer and
+// leave in coalesced 16-byte stores.
 template <bool DECODE>
 __global__ void __launch_bounds__(kTile, 2) k_guide_mlp(NetView net, const uint8_t* __restrict__ xtiles,
                                                        const int* __restrict__ n_dev, float* __restrict__ out,
                                                        int* err) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* X = smem + kInfX;
     uint8_t* H = smem + kInfH;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kInfBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kInfBar + 8);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kInfBar);       // MMA completion
+    uint64_t* bar_in = reinterpret_cast<uint64_t*>(smem + kInfBar + 8);  // [2] input copies
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kInfBar + 24);
     const int n = *n_dev;
     const int ntiles = (n + kTile - 1) / kTile;
     if (int(blockIdx.x) >= ntiles) return;  // uniform per CTA, before any TMEM use
+    const int t = threadIdx.x;
+    if (t == 0) {
+        tc::mbar_init(bar, 1);
+        tc::mbar_init(bar_in, 1);
+        tc::mbar_init(bar_in + 1, 1);
+        // the first tile starts streaming before the weights are staged
+        tc::mbar_arrive_expect_tx(bar_in, kGuideTileBytes);
+        tc::bulk_g2s(smem + kInfX, xtiles + size_t(blockIdx.x) * kGuideTileBytes, kGuideTileBytes, bar_in);
+    }
     load_weights(smem + kInfW1, net.w + kOffW1, kGuideHidden, kGuideIn, false, kGuideHidden);
     load_weights(smem + kInfW2, net.w + kOffW2, kGuideHidden, kGuideHidden, false, kGuideHidden);
     load_weights(smem + kInfW3, net.w + kOffW3, kGuideHidden, kGuideHidden, false, kGuideHidden);
     load_weights(smem + kInfW4, net.w + kOffW4, kGuideOut, kGuideHidden, false, kGuideOut);
-    if (threadIdx.x == 0) tc::mbar_init(bar, 1);
-    if (threadIdx.x < 32) tc::tmem_alloc(tslot, kInfTmemCols);
+    if (t < 32) tc::tmem_alloc(tslot, kInfTmemCols);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t sX = tc::smem_addr(X), sH = tc::smem_addr(H);
-    uint32_t phase = 0;
-    const int t = threadIdx.x;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        // the tile's encoded inputs (rows past n hold stale values; every
-        // output row depends on its own input row only, and is not written)
-        const uint4* src = reinterpret_cast<const uint4*>(xtiles + size_t(tile) * kGuideTileBytes);
-        for (int k = t; k < kGuideTileBytes / 16; k += kTile) reinterpret_cast<uint4*>(X)[k] = __ldg(src + k);
+    const uint32_t sH = tc::smem_addr(H);
+    uint32_t phase = 0, phase_in[2] = {0, 0};
+    bool pending[2] = {true, false};  // a copy into the buffer not waited for yet
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int buf = it & 1;
+        uint8_t* X = smem + kInfX + buf * kGuideTileBytes;
+        const uint32_t sX = tc::smem_addr(X);
+        // the next tile into the other buffer (its last use, the previous
+        // tile's output staging, ended at the barrier closing that tile)
+        const int next = tile + int(gridDim.x);
+        if (next < ntiles) {
+            if (t == 0) {
+                uint8_t* Xn = smem + kInfX + (buf ^ 1) * kGuideTileBytes;
+                tc::fence_async_smem();
+                tc::mbar_arrive_expect_tx(bar_in + (buf ^ 1), kGuideTileBytes);
+                tc::bulk_g2s(Xn, xtiles + size_t(next) * kGuideTileBytes, kGuideTileBytes, bar_in + (buf ^ 1));
+            }
+            pending[buf ^ 1] = true;
+        }
+        // this tile's inputs (rows past n hold stale values; every output row
+        // depends on its own input row only, and is not written)
+        const bool ok = tc::mbar_wait(bar_in + buf, phase_in[buf], err);
+        if (!__syncthreads_and(ok)) break;
+        phase_in[buf] ^= 1u;
+        pending[buf] = false;
         if (!run_mma(bar, &phase, err, tmem, sX, tc::smem_addr(smem + kInfW1), kGuideIn, kGuideHidden, false)) break;
         relu_row(tmem, H, t);
         if (!run_mma(bar, &phase, err, tmem, sH, tc::smem_addr(smem + kInfW2), kGuideHidden, kGuideHidden, false)) break;
@@ -177,28 +211,39 @@ __global__ void __launch_bounds__(kTile, 2) k_guide_mlp(NetView net, const uint8
         if (!run_mma(bar, &phase, err, tmem, sH, tc::smem_addr(smem + kInfW4), kGuideHidden, kGuideOut, false)) break;
         float v[kGuideOut];
         tmem_row(tmem, 0, kGuideOut, v);
-        const int i = tile * kTile + t;
-        if (i < n) {
-            float* o = out + size_t(i) * kGuideOut;
-            if (DECODE) {
-                GuideMix m;
-                guide_decode(v, &m);
-                for (int k = 0; k < kGuideLobes; ++k) {
-                    o[5 * k] = m.mu[k][0];
-                    o[5 * k + 1] = m.mu[k][1];
-                    o[5 * k + 2] = m.mu[k][2];
-                    o[5 * k + 3] = m.kappa[k];
-                    o[5 * k + 4] = m.w[k];
-                }
-                o[kGuideUsed - 1] = m.c;
-            } else {
-                for (int k = 0; k < kGuideOut; ++k) o[k] = v[k];
+        // stage row t (H2 in X was read by the layer-3 MMA, complete now)
+        float* o = reinterpret_cast<float*>(X) + t * kGuideOut;
+        if (DECODE) {
+            GuideMix m;
+            guide_decode(v, &m);
+            for (int k = 0; k < kGuideLobes; ++k) {
+                o[5 * k] = m.mu[k][0];
+                o[5 * k + 1] = m.mu[k][1];
+                o[5 * k + 2] = m.mu[k][2];
+                o[5 * k + 3] = m.kappa[k];
+                o[5 * k + 4] = m.w[k];
             }
+            o[kGuideUsed - 1] = m.c;
+            for (int k = kGuideUsed; k < kGuideOut; ++k) o[k] = 0.0f;
+        } else {
+            for (int k = 0; k < kGuideOut; ++k) o[k] = v[k];
         }
+        __syncthreads();
+        // the tile's valid rows leave as one contiguous block
+        const int rows = min(kTile, n - tile * kTile);
+        const uint4* src = reinterpret_cast<const uint4*>(X);
+        uint4* dst = reinterpret_cast<uint4*>(out + size_t(tile) * kTile * kGuideOut);
+        for (int k = t; k < rows * kGuideOut / 4; k += kTile) dst[k] = src[k];
+        __syncthreads();
     }
+    // copies still in flight (the loop left early) land before the CTA
+    // exits; these waits are bounded like the others
+    if (t == 0)
+        for (int b = 0; b < 2; ++b)
+            if (pending[b]) tc::mbar_wait(bar_in + b, phase_in[b], err, 1u << 16);
     tc::fence_before_sync();
     __syncthreads();
-    if (threadIdx.x < 32) tc::tmem_dealloc(tmem, kInfTmemCols);
+    if (t < 32) tc::tmem_dealloc(tmem, kInfTmemCols);
 }
 
 // ------------------------------------------------------------- training
