@@ -1,0 +1,79 @@
+"""Fixed workloads for profiling the kernels under ncu (each runs its scene
+through the public API and exits; the renders are the same ones the bench
+times).
+
+    python -m atrc_b200.workloads instanced [--spp 2] [--warmup 3] [--steps 1]
+        the 1920x1080 instanced Disney + IBL scene: scene build, autotune,
+        warm-up steps, then `steps` steps of `spp` samples per pixel; each
+        timed step is wrapped in an NVTX range named "step"
+    python -m atrc_b200.workloads guided-room [--train-passes 3] [--passes 3]
+        the 1280x720 indoor room: plain passes, guided passes that record and
+        train, then guided passes that only sample (1 spp each)
+"""
+from __future__ import annotations
+
+import argparse
+
+
+def instanced(spp: int, warmup: int, steps: int) -> None:
+    import torch
+
+    from . import Config, DeviceScene, Film, scenes
+    cfg = Config.from_file(scenes.instanced_disney())
+    desc, _ = cfg.rendering(0)
+    scene = DeviceScene(cfg)
+    scene.autotune(desc, trial_spp=2)
+    film = Film(desc.width, desc.height, device=True)
+    desc.spp_count = spp
+    for k in range(warmup + steps):
+        desc.first_spp = k * spp
+        if k >= warmup:
+            torch.cuda.nvtx.range_push("step")
+        stats = scene.render(desc, film)
+        if k >= warmup:
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
+            print(f"step {k - warmup}: closest rays {stats['rays_closest']}, shadow rays {stats['rays_shadow']}")
+
+
+def guided_room(train_passes: int, passes: int) -> None:
+    from . import Config, DeviceScene, Film, scenes
+    from .guide import Guide
+    cfg = Config.from_file(scenes.indoor_room())
+    desc, _ = cfg.rendering(0)
+    scene = DeviceScene(cfg)
+    film = Film(desc.width, desc.height, device=True)
+    desc.spp_count = 1
+    for k in range(3):
+        desc.first_spp = k
+        scene.render(desc, film)
+    guide = Guide.for_scene(scene)
+    for k in range(train_passes):
+        desc.first_spp = 3 + k
+        scene.render_guided(guide, desc, film, record=True)
+        guide.train(steps=4)
+    for k in range(passes):
+        desc.first_spp = 3 + train_passes + k
+        scene.render_guided(guide, desc, film, record=False)
+    guide.close()
+
+
+def main() -> None:
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    sub = p.add_subparsers(dest="workload", required=True)
+    a = sub.add_parser("instanced")
+    a.add_argument("--spp", type=int, default=2)
+    a.add_argument("--warmup", type=int, default=3)
+    a.add_argument("--steps", type=int, default=1)
+    b = sub.add_parser("guided-room")
+    b.add_argument("--train-passes", type=int, default=3)
+    b.add_argument("--passes", type=int, default=3)
+    args = p.parse_args()
+    if args.workload == "instanced":
+        instanced(args.spp, args.warmup, args.steps)
+    else:
+        guided_room(args.train_passes, args.passes)
+
+
+if __name__ == "__main__":
+    main()
