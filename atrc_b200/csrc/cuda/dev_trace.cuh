@@ -196,9 +196,11 @@ struct TraceCount {
     uint32_t ents;   // entity (instance) visits
 };
 
-// Trace one ray.  Returns true if something was hit (ANY: occluded).
-// `watchdog` is set when the traversal stack would overflow.  With COUNT the
-// work done is added to *cnt.
+// Traversal of one ray, resumable: step() runs one round of the traversal
+// (descend to leaves, then the leaves) and says whether the ray is done, so
+// a kernel can refill the lanes of finished rays between rounds (k_extend);
+// trace_ray() runs the rounds to the end.  ANY stops at the first hit
+// (occlusion); with COUNT the work done is added to a TraceCount.
 //
 // Structure (after Aila and Laine, "Understanding the efficiency of ray
 // traversal on GPUs", 2009): a thread that reaches a leaf while descending
@@ -206,60 +208,73 @@ struct TraceCount {
 // once every active lane holds a leaf, so node and leaf code run with most
 // lanes converged.  Top-level leaves (entities) switch the ray into the
 // entity's space and push a sentinel that restores the world ray when the
-// bottom-level tree is exhausted.
+// bottom-level tree is exhausted.  A ray whose stack would overflow or
+// whose visits exceed kMaxTraversalSteps ends with the watchdog set.
+// The traversal stack is the caller's local array (kStackSize entries, the
+// deeper ones past a shared-memory ring with ATRC_STACK_RING), kept out of
+// the struct so that the scalar state stays in registers.
 template <bool EXACT, bool ANY, bool COUNT = false>
-__device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog,
-                          TraceCount* cnt = nullptr) {
-    if (S.entity_count == 0) return false;
+struct Tracer {
 #if ATRC_STACK_RING > 0
-    __shared__ int32_t s_ring[kStackRing * kTraceBlock];
-    int32_t* const ring = s_ring + threadIdx.x;
-    int32_t spill[kStackSize - kStackRing];
-#else
-    int32_t stack[kStackSize];
+    int32_t* ring;
 #endif
-    int sp = 0;
+    int32_t* stack;
+    int sp;
     RayState r;
-    r.o = wo; r.d = wd; r.inv = safe_inv(wd); r.tmin = tmin; r.tmax = tmax;
-    const Vec3 winv = r.inv;
-    float best_t = tmax;
-    int32_t best_e = -1, best_tri = -1;
-    float best_u = 0, best_v = 0;
-    int32_t cur_entity = -1;
-    int32_t link = S.tlas_root;
-    int32_t held = 0;  // parked leaf (negative) or 0
-    bool overflow = false;
+    Vec3 wo, wd, winv;
+    float tmin0, best_t, best_u, best_v;
+    int32_t best_e, best_tri, cur_entity, link, held;
+    int steps;
+    bool overflow, found;
+
+    __device__ __forceinline__ void init(const Scene& S, int32_t* stk, Vec3 o, Vec3 d, float tmin, float tmax) {
+        stack = stk;
+#if ATRC_STACK_RING > 0
+        // entry i sits in ring slot i % R; pushing entry sp evicts entry
+        // sp - R to the spill array, popping entry sp refills its slot
+        __shared__ int32_t s_ring[kStackRing * kTraceBlock];
+        ring = s_ring + threadIdx.x;
+#endif
+        sp = 0;
+        wo = o; wd = d; winv = safe_inv(d);
+        r.o = o; r.d = d; r.inv = winv; r.tmin = tmin; r.tmax = tmax;
+        tmin0 = tmin;
+        best_t = tmax; best_u = 0; best_v = 0;
+        best_e = -1; best_tri = -1; cur_entity = -1;
+        link = S.entity_count == 0 ? kDone : S.tlas_root;
+        held = 0;
+        steps = 0;
+        overflow = false;
+        found = false;
+    }
 
 #if ATRC_STACK_RING > 0
-    // entry i sits in ring slot i % R; pushing entry sp evicts entry sp - R
-    // to the spill array, popping entry sp refills its slot with sp - R
-    auto push = [&](int32_t v) {
+    __device__ __forceinline__ void push(int32_t v) {
         if (sp >= kStackSize) { overflow = true; return; }
         int32_t& slot = ring[(sp & (kStackRing - 1)) * kTraceBlock];
-        if (sp >= kStackRing) spill[sp - kStackRing] = slot;
+        if (sp >= kStackRing) stack[sp - kStackRing] = slot;
         slot = v;
         ++sp;
-    };
-    auto pop = [&]() -> int32_t {
+    }
+    __device__ __forceinline__ int32_t pop() {
         if (sp <= 0) return kDone;
         --sp;
         int32_t& slot = ring[(sp & (kStackRing - 1)) * kTraceBlock];
         const int32_t v = slot;
-        if (sp >= kStackRing) slot = spill[sp - kStackRing];
+        if (sp >= kStackRing) slot = stack[sp - kStackRing];
         return v;
-    };
+    }
 #else
-    auto push = [&](int32_t v) {
+    __device__ __forceinline__ void push(int32_t v) {
         if (sp >= kStackSize) { overflow = true; return; }
         stack[sp++] = v;
-    };
-    auto pop = [&]() -> int32_t { return sp > 0 ? stack[--sp] : kDone; };
+    }
+    __device__ __forceinline__ int32_t pop() { return sp > 0 ? stack[--sp] : kDone; }
 #endif
 
     // Visit leaf `lf`; `next` is what follows it.  Returns the new link.
     // Sets `found` in ANY mode when something was hit.
-    bool found = false;
-    auto visit_leaf = [&](int32_t lf, int32_t next) -> int32_t {
+    __device__ __forceinline__ int32_t visit_leaf(const Scene& S, int32_t lf, int32_t next, TraceCount* cnt) {
         const uint32_t enc = uint32_t(~lf);
         const int32_t first = int32_t(enc >> 4), count = int32_t(enc & 15) + 1;
         if (cur_entity < 0) {
@@ -278,7 +293,7 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
                     return e.blas_root;
                 }
                 RayState lr;
-                lr.o = lo; lr.d = ld; lr.tmin = tmin; lr.inv = Vec3();
+                lr.o = lo; lr.d = ld; lr.tmin = tmin0; lr.inv = Vec3();
                 float t;
                 const bool h = e.kind == LEAF_SPHERE ? sphere_test<ANY>(lr, e.radius, best_t, &t)
                                                      : disk_test(lr, e.radius, best_t, &t);
@@ -307,11 +322,12 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
             }
         }
         return next;
-    };
+    }
 
-    int steps = 0;
-    for (;;) {
-        // descend interior nodes, parking the first leaf found
+    // One round: descend (parking the first leaf found) until every active
+    // lane holds a leaf, then the leaves.  Returns true when the ray is done.
+    __device__ __forceinline__ bool step(const Scene& S, int* watchdog, TraceCount* cnt) {
+        if (link == kDone && held == 0) return true;
         while (link >= 0) {
             if (++steps > kMaxTraversalSteps) { overflow = true; break; }
             if (COUNT) cnt->nodes++;
@@ -336,12 +352,12 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
             if (overflow) break;
             if (!__any_sync(__activemask(), held == 0)) break;
         }
-        if (overflow) { *watchdog = 1; break; }
+        if (overflow) { *watchdog = 1; return true; }
         // leaves: the parked one first, then any leaf / sentinel in `link`
         if (held != 0) {
-            link = visit_leaf(held, link);
+            link = visit_leaf(S, held, link, cnt);
             held = 0;
-            if (found) break;
+            if (found) return true;
         }
         while (link < 0) {
             if (link == kDone) break;
@@ -353,23 +369,40 @@ __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tm
                 continue;
             }
             const int32_t next = pop();
-            link = visit_leaf(link, next);
+            link = visit_leaf(S, link, next, cnt);
             if (found) break;
         }
-        if (overflow) { *watchdog = 1; break; }
-        if (found || link == kDone) break;
+        if (overflow) { *watchdog = 1; return true; }
+        return found || link == kDone;
     }
-    if (ANY) {
-        if (found) { hit->entity = best_e; hit->t = best_t; }
-        return found;
+
+    // The result once step() said done: true if something was hit.
+    __device__ __forceinline__ bool result(Hit* hit) const {
+        if (ANY) {
+            if (found) { hit->entity = best_e; hit->t = best_t; }
+            return found;
+        }
+        if (best_e < 0) return false;
+        hit->t = best_t;
+        hit->u = best_u;
+        hit->v = best_v;
+        hit->entity = best_e;
+        hit->tri = best_tri;
+        return true;
     }
-    if (best_e < 0) return false;
-    hit->t = best_t;
-    hit->u = best_u;
-    hit->v = best_v;
-    hit->entity = best_e;
-    hit->tri = best_tri;
-    return true;
+};
+
+// Trace one ray to the end.  Returns true if something was hit (ANY:
+// occluded); `watchdog` is set when the traversal stack would overflow.
+template <bool EXACT, bool ANY, bool COUNT = false>
+__device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog,
+                          TraceCount* cnt = nullptr) {
+    int32_t stack[kStackSize];
+    Tracer<EXACT, ANY, COUNT> t;
+    t.init(S, stack, wo, wd, tmin, tmax);
+    while (!t.step(S, watchdog, cnt)) {
+    }
+    return t.result(hit);
 }
 
 // Closest hit of a ray with one entity in [tmin, tmax]

@@ -116,6 +116,7 @@ struct Counters {
     int n_shadow, n_finish;
     int n_guide;              // guide queries this iteration
     int n_sss;                // subsurface walks queued this iteration
+    int ext_cursor;           // next extend-queue entry for k_extend_fetch
     int n_free, n_new, n_cont, free_base;
     unsigned long long gen_base, issued, total, completed;
     unsigned long long rays_closest, rays_shadow, iterations;
@@ -246,6 +247,7 @@ __global__ void k_begin(Counters* c) {
     c->n_finish = 0;
     c->n_guide = 0;
     c->n_sss = 0;
+    c->ext_cursor = 0;
     if (c->n_ext == 0) c->done = 1;
 }
 
@@ -424,6 +426,59 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(S
         P.hit_tri[slot] = h.tri;
         if (sort_mode != ATRC_SORT_NONE) count_key(S, P, sort_mode, nkeys, i, slot, hit, h.entity);
     }
+    if (COUNT) flush_count(c->cnt_closest, tc);
+}
+
+// k_extend with dynamic ray fetch (Aila and Laine 2009): persistent warps
+// trace the queue round by round (Tracer::step), and whenever at least
+// kRefillLanes lanes of a warp have finished their rays, those lanes take
+// the next queue entries (one atomic per warp).  Lanes whose rays end early
+// no longer idle until the warp's longest ray is done, which is where the
+// one-ray-per-thread kernel loses most of its SIMD lanes on secondary rays.
+// Results, sort keys and counts are those of k_extend.
+constexpr int kRefillLanes = 16;
+
+template <bool EXACT, bool COUNT>
+__global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend_fetch(Scene S, Pool P, Counters* c,
+                                                                                    int sort_mode, int nkeys) {
+    const int n = c->n_ext, in = c->in;
+    const int lane = threadIdx.x & 31;
+    TraceCount tc{0, 0, 0};
+    int32_t stack[kStackSize];
+    Tracer<EXACT, false, COUNT> tr;
+    int i = -1, slot = -1, wd = 0;
+    bool drained = false;
+    for (;;) {
+        const unsigned idle = __ballot_sync(0xffffffffu, i < 0);
+        if (!drained && __popc(idle) >= kRefillLanes) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&c->ext_cursor, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + __popc(idle) >= n) drained = true;
+            if (i < 0) {
+                const int k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < n) {
+                    i = k;
+                    slot = P.q[in][i];
+                    const float4 o = P.ray_o[slot], d = P.ray_d[slot];
+                    tr.init(S, stack, xyz(o), xyz(d), o.w, d.w);
+                }
+            }
+        }
+        if (drained && __all_sync(0xffffffffu, i < 0)) break;
+        if (i >= 0 && tr.step(S, &wd, &tc)) {
+            Hit h;
+            h.entity = -1;
+            h.tri = -1;
+            h.t = h.u = h.v = 0.0f;
+            const bool hit = tr.result(&h);
+            P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.entity : -1));
+            P.hit_tri[slot] = h.tri;
+            if (sort_mode != ATRC_SORT_NONE) count_key(S, P, sort_mode, nkeys, i, slot, hit, h.entity);
+            i = -1;
+        }
+    }
+    if (wd) atomicMax(&c->watchdog, wd);
     if (COUNT) flush_count(c->cnt_closest, tc);
 }
 
@@ -1132,6 +1187,7 @@ struct DeviceSceneImpl {
     int tuned_gen_blocks = 16;    // k_generate / k_finish blocks per SM
     int tuned_gen_threads = 256;  // k_generate block
     int tuned_fin_threads = 128;  // k_finish block
+    int tuned_fetch = 0;          // k_extend_fetch instead of k_extend
     int tuned_trials = 0;
     double tuned_ms = 0, default_ms = 0;
     DevBuf tune_film;
@@ -1671,8 +1727,15 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             k_begin<<<1, 1, 0, s>>>(c);
             k_generate<<<gsm, d.tuned_gen_threads, 0, s>>>(d.scene, p, P, c);
             CK(cudaEventRecordWithFlags(kev[k * 4 + 0], s, cudaEventRecordExternal));
-            if (count) k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
-            else k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+            if (d.tuned_fetch) {
+                const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
+                if (count) k_extend_fetch<false, true><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                else k_extend_fetch<false, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+            } else if (count) {
+                k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+            } else {
+                k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+            }
             if (p.sort_mode != ATRC_SORT_NONE) {
                 k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
                 k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
@@ -1858,6 +1921,8 @@ static void tuning_out(const DeviceSceneImpl& d, AtrcTuning* out) {
     out->trials = d.tuned_trials;
     out->ms_per_msample = d.tuned_ms;
     out->default_ms_per_msample = d.default_ms;
+    out->extend_fetch = d.tuned_fetch;
+    out->pad_ = 0;
 }
 
 int atrc_cuda_get_tuning(AtrcScene* scene, AtrcTuning* out) {
@@ -1870,7 +1935,8 @@ static bool tuning_valid(const AtrcTuning& t) {
     auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
     return t.path_pool >= 1024 && t.path_pool <= (1 << 26) && t.sort_mode >= ATRC_SORT_NONE &&
            t.sort_mode <= ATRC_SORT_MATERIAL && t.gen_blocks_per_sm >= 1 && t.gen_blocks_per_sm <= 64 &&
-           pow2_in(t.gen_threads, 32, 1024) && pow2_in(t.finish_threads, 32, 1024);
+           pow2_in(t.gen_threads, 32, 1024) && pow2_in(t.finish_threads, 32, 1024) &&
+           (t.extend_fetch == 0 || t.extend_fetch == 1);
 }
 
 int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
@@ -1882,6 +1948,7 @@ int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
     d.tuned_gen_blocks = in->gen_blocks_per_sm;
     d.tuned_gen_threads = in->gen_threads;
     d.tuned_fin_threads = in->finish_threads;
+    d.tuned_fetch = in->extend_fetch;
     return ATRC_OK;
 }
 
@@ -1932,7 +1999,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
             return best;
         };
         // defaults first (one warm-up trial compiles nothing but pages in)
-        AtrcTuning base{1 << 21, ATRC_SORT_NONE, 16, 256, 128, 0, 0, 0};
+        AtrcTuning base{1 << 21, ATRC_SORT_NONE, 16, 256, 128, 0, 0, 0, 0, 0};
         if (!pool_fits(base.path_pool)) base.path_pool = 1 << 19;
         measure(base);
         const double base_ms = measure(base);
@@ -1943,6 +2010,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
             const double ms = measure(c);
             if (ms < best_ms * 0.99) { best_ms = ms; best = c; }
         };
+        { AtrcTuning c = best; c.extend_fetch = 1; consider(c); }
         for (int m : {ATRC_SORT_TYPE, ATRC_SORT_MATERIAL}) { AtrcTuning c = best; c.sort_mode = m; consider(c); }
         const AtrcTuning after_sort = best;
         for (int pool : {1 << 19, 1 << 20, 1 << 22}) { AtrcTuning c = after_sort; c.path_pool = pool; consider(c); }
@@ -2097,7 +2165,11 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
             for (int k = 0; k < DeviceSceneImpl::kWindow; ++k) {
                 k_begin<<<1, 1, 0, s>>>(c);
                 k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
-                k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                if (d.tuned_fetch)
+                    k_extend_fetch<false, false><<<d.sm_count * ATRC_TRACE_MIN_BLOCKS, kTraceBlock, 0, s>>>(
+                        d.scene, P, c, p.sort_mode, p.nkeys);
+                else
+                    k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
                 if (p.sort_mode != ATRC_SORT_NONE) {
                     k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
                     k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);

@@ -471,13 +471,18 @@ typedef struct AtrcTuning {
     int32_t trials;             /* trial renders measured by the last autotune   */
     double  ms_per_msample;     /* device ms per million samples, chosen config  */
     double  default_ms_per_msample; /* the same for the built-in defaults        */
+    int32_t extend_fetch;       /* closest-hit traversal: 1 = persistent warps   */
+                                /* that refill finished lanes with new rays, 0 = */
+                                /* one ray per thread                            */
+    int32_t pad_;
 } AtrcTuning;
 
 /* Project autotuner (the reference has no counterpart: it renders with a
  * fixed thread pool and 32x32 tiles, renderer_creators.cpp:127-128).  Renders
  * short trials of `desc` (each `trial_spp` samples per pixel, or enough for
- * about 4M samples when trial_spp <= 0) into scratch memory, searching sort
- * granularity, then path-pool size, then the generate / finish launch shapes
+ * about 4M samples when trial_spp <= 0) into scratch memory, searching the
+ * closest-hit kernel (extend_fetch), sort granularity, then path-pool size,
+ * then the generate / finish launch shapes
  * (coordinate descent, best of two timings each), and stores the fastest
  * configuration in the scene.  The caller's films are untouched. */
 int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc,

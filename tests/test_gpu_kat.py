@@ -201,3 +201,32 @@ def test_autotune_picks_a_valid_configuration(cornell_path):
         dev.set_tuning(gen_threads=100)
     dev.set_tuning(sort_mode=2, path_pool=4096)
     assert dev.tuning()["sort_mode"] == 2 and dev.tuning()["path_pool"] == 4096
+
+
+@pytest.mark.parametrize("sort_mode", [0, 2])
+def test_extend_fetch_matches_one_ray_per_thread(scene_dir, sort_mode):
+    # k_extend_fetch (persistent warps refilling finished lanes) finds the
+    # same closest hits as k_extend: the same paths, traversal work and film
+    from atrc_b200.scenes import instanced_disney
+    p = instanced_disney(scene_dir / "inst_small", ico_level=4, hf_res=128, width=64, height=36, spp=64)
+    cfg = Config.from_file(p)
+    desc, _ = cfg.rendering(0)
+    desc.sort_mode, desc.count_traversal = sort_mode, 1
+    dev = DeviceScene(cfg)
+    out = []
+    for fetch in (0, 1):
+        dev.set_tuning(extend_fetch=fetch, path_pool=1 << 14)
+        f = Film(desc.width, desc.height)
+        st = dev.render(desc, f)
+        assert st["watchdog_flags"] == 0
+        out.append((f, st))
+    (fa, sa), (fb, sb) = out
+    for k in ("samples", "rays_closest", "rays_shadow"):
+        assert sa[k] == sb[k], k
+    # the work differs a little: a lane visits its parked leaf when its whole
+    # warp holds leaves, and which rays share a warp differs between kernels
+    for k in ("nodes_closest", "tris_closest", "ents_closest"):
+        assert abs(sa[k] - sb[k]) <= 0.01 * sa[k], k
+    # (shadow contributions are FP32 atomics, whose order may differ)
+    np.testing.assert_allclose(fb.value, fa.value, rtol=2e-6, atol=1e-9)
+    np.testing.assert_array_equal(fb.weight, fa.weight)
