@@ -336,14 +336,26 @@ struct Tracer {
             float tc[4];
             int32_t lc[4];
             box4(S.nodes + link, r, tc, lc);
-            sort4(tc, lc);
-            if (tc[0] == INFINITY) {
-                link = pop();
+            if (ANY) {
+                // occlusion needs any hit, not the nearest: children in slot
+                // order, no sort
+                int32_t nxt = kDone;
+                for (int k = 3; k >= 0; --k) {
+                    if (tc[k] == INFINITY) continue;
+                    if (nxt != kDone) push(nxt);
+                    nxt = lc[k];
+                }
+                link = nxt != kDone ? nxt : pop();
             } else {
-                if (tc[3] != INFINITY) push(lc[3]);
-                if (tc[2] != INFINITY) push(lc[2]);
-                if (tc[1] != INFINITY) push(lc[1]);
-                link = lc[0];
+                sort4(tc, lc);
+                if (tc[0] == INFINITY) {
+                    link = pop();
+                } else {
+                    if (tc[3] != INFINITY) push(lc[3]);
+                    if (tc[2] != INFINITY) push(lc[2]);
+                    if (tc[1] != INFINITY) push(lc[1]);
+                    link = lc[0];
+                }
             }
             if (link < 0 && link != kSentinel && link != kDone && held == 0) {
                 held = link;
