@@ -1164,6 +1164,8 @@ struct DeviceSceneImpl {
     // per-call resources kept between render calls
     static constexpr int kWindow = 4;  // wavefront iterations between host checks
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, kev[kWindow * 4] = {};
+    static constexpr int kCopyChunks = 16;  // host-film download in pieces
+    cudaEvent_t copy_ev[kCopyChunks] = {};
     void* pinned_counters = nullptr;
     DevBuf views_buf;                   // view table (+ per-view completion counters)
     void* view_stage = nullptr;         // pinned copy of the completion counters
@@ -1200,6 +1202,7 @@ struct DeviceSceneImpl {
             CK(cudaEventCreate(&ev0));
             CK(cudaEventCreate(&ev1));
             for (auto& e : kev) CK(cudaEventCreate(&e));
+            for (auto& e : copy_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
         if (!pinned_counters) CK(cudaMallocHost(&pinned_counters, 512));
     }
@@ -1215,6 +1218,7 @@ struct DeviceSceneImpl {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (auto& e : kev) if (e) cudaEventDestroy(e);
+        for (auto& e : copy_ev) if (e) cudaEventDestroy(e);
         if (window_exec) cudaGraphExecDestroy(window_exec);
         if (view_stage) cudaFreeHost(view_stage);
         if (pinned_counters) cudaFreeHost(pinned_counters);
@@ -1804,24 +1808,39 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
         for (auto& t : host_targets) doubles += t.second;
         d.ensure_stage(doubles * sizeof(double));
         const double* tmp = static_cast<const double*>(d.stage);
-        CK(cudaMemcpyAsync(d.stage, local_film.p, doubles * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        d2h += doubles * sizeof(double);
-        // accumulate into the caller's arrays with a few host threads
-        size_t off = 0;
-        for (auto& t : host_targets) {
-            const size_t n_el = t.second;
-            const unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
-            std::vector<std::thread> th;
-            for (unsigned k = 0; k < nt; ++k) {
-                const size_t b0 = n_el * k / nt, b1 = n_el * (k + 1) / nt;
-                double* dst = t.first;
-                const double* src = tmp + off;
-                th.emplace_back([=] { for (size_t q = b0; q < b1; ++q) dst[q] += src[q]; });
-            }
-            for (auto& x : th) x.join();
-            off += n_el;
+        // the download runs in chunks, each followed by an event; host threads
+        // add chunk k into the caller's arrays while chunk k + 1 is in flight
+        constexpr int kc = DeviceSceneImpl::kCopyChunks;
+        const size_t chunk = ((doubles + kc - 1) / kc + 511) / 512 * 512;
+        int nchunks = 0;
+        for (size_t c0 = 0; c0 < doubles; c0 += chunk, ++nchunks) {
+            const size_t n_el = std::min(chunk, doubles - c0);
+            CK(cudaMemcpyAsync(static_cast<double*>(d.stage) + c0, local_film.as<double>() + c0, n_el * sizeof(double),
+                               cudaMemcpyDeviceToHost, s));
+            CK(cudaEventRecord(d.copy_ev[nchunks], s));
         }
+        d2h += doubles * sizeof(double);
+        std::vector<size_t> start(host_targets.size() + 1, 0);  // target k covers [start[k], start[k + 1])
+        for (size_t k = 0; k < host_targets.size(); ++k) start[k + 1] = start[k] + host_targets[k].second;
+        const unsigned nt = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+        std::atomic<int> copy_err{0};
+        auto add = [&](unsigned t) {
+            for (int k = 0; k < nchunks; ++k) {
+                if (cudaEventSynchronize(d.copy_ev[k]) != cudaSuccess) { copy_err = 1; return; }
+                const size_t c0 = size_t(k) * chunk, c1 = std::min(doubles, c0 + chunk);
+                const size_t a = c0 + (c1 - c0) * t / nt, b = c0 + (c1 - c0) * (t + 1) / nt;
+                for (size_t j = 0; j < host_targets.size(); ++j) {
+                    const size_t lo = std::max(a, start[j]), hi = std::min(b, start[j + 1]);
+                    double* dst = host_targets[j].first;
+                    for (size_t q = lo; q < hi; ++q) dst[q - start[j]] += tmp[q];
+                }
+            }
+        };
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; ++t) th.emplace_back(add, t);
+        add(0);
+        for (auto& x : th) x.join();
+        if (copy_err) throw CudaError("atrc_cuda_render: film download failed");
     }
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
