@@ -351,6 +351,9 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
     }
 }
 
+constexpr int kMaterialTypes = 8;  // AtrcMaterialType values 0..7: type-sort keys 1..8
+static_assert(ATRC_MAT_PHONG + 1 == kMaterialTypes, "one sort key per material type");
+
 // Material key of a hit record: 0 for a miss, nkeys - 1 for a path inside a
 // medium (its next step is medium sampling), else 1 + the material type or
 // index of the hit entity.  Counted per warp (one atomic per distinct key).
@@ -1195,7 +1198,7 @@ struct DeviceSceneImpl {
     DevBuf tune_film;
     void resolve_sort(Params* p, int requested) const {
         p->sort_mode = requested == ATRC_SORT_AUTO ? tuned_sort : requested;
-        p->nkeys = std::max(scene.material_count, 4) + 2;
+        p->nkeys = std::max(scene.material_count, kMaterialTypes) + 2;
     }
     void ensure_render_resources() {
         if (!ev0) {
@@ -1994,7 +1997,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
         size_t free_b = 0, total_b = 0;
         CK(cudaMemGetInfo(&free_b, &total_b));
         const int nl = shadow_rays_per_path(d.scene, *desc);
-        const int nkeys = std::max(d.scene.material_count, 4) + 2;
+        const int nkeys = std::max(d.scene.material_count, kMaterialTypes) + 2;
         // (the workspace held now is freed before a larger one is allocated)
         auto pool_fits = [&](int pool) {
             return pool_layout(size_t(pool), size_t(pool) * nl, nkeys).total < (free_b + d.pool_buf.bytes) / 4;

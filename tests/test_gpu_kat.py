@@ -139,14 +139,21 @@ def test_empty_scene_and_threads(tmp_path):
     assert abs(out[0] - 1) < 1e-5 and abs(out[1] - 1) < 0.05
 
 
-@pytest.mark.parametrize("scene", ["cornell", "media"])
-def test_shade_queue_sort_changes_nothing(scene, cornell_path, scene_dir):
+@pytest.mark.parametrize("scene", ["cornell", "media", "phong", "materials"])
+def test_shade_queue_sort_changes_nothing(scene, cornell_path, scene_dir, tmp_path):
     # sorting hit records by material key only reorders the shade queue: every
     # path keeps its own random stream, so the films agree up to the order in
-    # which the FP32 shadow-ray results of several lights add into one path
+    # which the FP32 shadow-ray results of several lights add into one path.
+    # "phong": three materials, one of the last type (type-sort key 8 with
+    # fewer materials than types); "materials": every surface type but two
     from atrc_b200 import scenes
-    path = cornell_path if scene == "cornell" else scenes.media_scene(scene_dir)
-    cfg = Config.from_file(path)
+    if scene in ("phong", "materials"):
+        d = K.materials_scene(tmp_path)
+        if scene == "phong":
+            d["scene"]["entities"] = [d["scene"]["entities"][k] for k in (0, 5, 6)]
+        cfg = Config.from_string(K.dumps(d), str(tmp_path))
+    else:
+        cfg = Config.from_file(cornell_path if scene == "cornell" else scenes.media_scene(scene_dir))
     desc, _ = cfg.rendering(0)
     desc.width, desc.height, desc.spp = 64, 48, 8
     dev = DeviceScene(cfg)
