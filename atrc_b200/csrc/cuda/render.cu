@@ -119,6 +119,7 @@ struct Counters {
     int ext_cursor;           // next extend-queue entry for k_extend_fetch
     int n_free, n_new, n_cont;
     int gen_ticket;           // k_generate: free slots claimed this iteration
+    int ext_ticket;           // k_generate: extend-queue entries written (slot order)
     unsigned long long gen_base, issued, total, completed;
     unsigned long long rays_closest, rays_shadow, iterations;
     unsigned long long cnt_closest[3], cnt_shadow[3];  // nodes, tris, entities
@@ -180,6 +181,7 @@ struct Params {
     const View* views;                 // device array
     unsigned long long* view_done;     // per view: finished samples (batch renders; else null)
     int sort_mode, nkeys;   // shade-queue sort (AtrcSortMode, resolved) and key count
+    int slot_queue;         // 1: extend queue in slot order (AtrcTuning::queue_order)
     int min_depth, max_depth, specular_depth;
     float cont_prob, eps;
     int guide_on;           // sample surface vertices with the learned guide
@@ -189,6 +191,10 @@ struct Params {
     float ao_dist;          // ao: occlusion distance
     float ao_low[3], ao_high[3], ao_bg[3];
 };
+
+// Slot states: free, holding a path that continues next iteration, or
+// holding a path between its queue entry and its continuation / finish.
+constexpr int kSlotBusy = 0, kSlotFree = 1, kSlotCont = 2;
 
 struct Pool {
     float4 *ray_o, *ray_d;        // o.xyz tmin / d.xyz tmax
@@ -208,14 +214,14 @@ struct Pool {
     int* key_cursor;              // per key: next write position in q_sorted
     int* q_finish;
     int* q_sss;                   // paths whose BSDF sample entered a subsurface material
-    int* free_flag;               // per slot: 1 while the slot holds no path
+    int* slot_state;              // per slot: kSlotFree / kSlotCont / kSlotBusy
     float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
     int cap, shadow_cap;
 };
 
 __global__ void k_init(Pool P, int cap, int nkeys, Counters* c, unsigned long long total) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < cap) P.free_flag[i] = 1;
+    if (i < cap) P.slot_state[i] = kSlotFree;
     if (i < nkeys) P.key_count[i] = 0;
     if (i == 0) {
         memset(c, 0, sizeof(Counters));
@@ -238,6 +244,7 @@ __global__ void k_begin(Counters* c) {
     c->gen_base = c->issued;
     c->issued += n_new;
     c->gen_ticket = 0;
+    c->ext_ticket = 0;
     c->n_free -= n_new;
     c->n_new = n_new;
     c->n_cont = n_cont;
@@ -304,29 +311,51 @@ __device__ __forceinline__ int tile_of(const int4* t, int n, int e0, int u, int*
     return g;
 }
 
-// New samples go into free slots taken in ascending slot order: each warp
-// scans 32 consecutive slots and claims the free ones with one ticket atomic,
-// ticket t (< n_new) becoming sample gen_base + t at extend-queue position
-// n_cont + t.  A slot's path state is then written by neighbouring lanes,
-// whatever order the paths finished in.  The sample -> pixel / random stream
-// map does not depend on the slot, so the image does not either.
+// New samples go into free slots taken in ascending slot order: a warp looks
+// at 32 consecutive slots and takes sample tickets for its free ones with
+// one atomic (ticket t < n_new becomes sample gen_base + t), so new path
+// state is written by neighbouring lanes whatever order the paths finished
+// in.  Extend-queue positions: n_cont + t after the continuations k_shade
+// appended (shade order), or, with p.slot_queue, one more ticket per warp
+// for its new paths and for its slots whose path continues, so the whole
+// queue runs in slot order.  The sample -> pixel / random stream map does
+// not depend on the slot, so the image does not either.
 __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
     const int n = c->n_new;
-    if (n == 0) return;
-    const int base = c->n_cont, in = c->in, lane = threadIdx.x & 31;
+    if (p.slot_queue ? c->n_ext == 0 : n == 0) return;
+    const int in = c->in, n_cont = c->n_cont, lane = threadIdx.x & 31;
     const unsigned long long gen = c->gen_base;
     for (int i0 = blockIdx.x * blockDim.x; i0 < P.cap; i0 += gridDim.x * blockDim.x) {
         const int slot = i0 + int(threadIdx.x);
-        const bool is_free = slot < P.cap && P.free_flag[slot] != 0;
-        const unsigned m = __ballot_sync(0xffffffffu, is_free);
-        if (m == 0) continue;
-        int t0 = 0;
-        if (lane == 0) t0 = atomicAdd(&c->gen_ticket, __popc(m));
-        t0 = __shfl_sync(0xffffffffu, t0, 0);
-        if (t0 >= n) return;  // tickets only grow: every sample of this iteration is placed
-        const int i = t0 + __popc(m & ((1u << lane) - 1u));
-        if (!is_free || i >= n) continue;
-        P.free_flag[slot] = 0;
+        const int state = slot < P.cap ? P.slot_state[slot] : kSlotBusy;
+        const bool is_free = state == kSlotFree && n > 0;
+        const unsigned mf = __ballot_sync(0xffffffffu, is_free);
+        int i = n;
+        if (mf != 0) {
+            int t0 = 0;
+            if (lane == 0) t0 = atomicAdd(&c->gen_ticket, __popc(mf));
+            t0 = __shfl_sync(0xffffffffu, t0, 0);
+            // tickets only grow: past n_new every sample of this iteration is placed
+            if (t0 >= n && !p.slot_queue) return;
+            i = t0 + __popc(mf & ((1u << lane) - 1u));
+        }
+        const bool fresh = is_free && i < n;
+        int qpos = n_cont + i;
+        if (p.slot_queue) {
+            const bool enqueue = fresh || state == kSlotCont;
+            const unsigned me = __ballot_sync(0xffffffffu, enqueue);
+            if (me == 0) continue;
+            int q0 = 0;
+            if (lane == 0) q0 = atomicAdd(&c->ext_ticket, __popc(me));
+            q0 = __shfl_sync(0xffffffffu, q0, 0);
+            if (!enqueue) continue;
+            qpos = q0 + __popc(me & ((1u << lane) - 1u));
+        } else if (!fresh) {
+            continue;
+        }
+        P.slot_state[slot] = kSlotBusy;
+        P.q[in][qpos] = slot;
+        if (!fresh) continue;
         const unsigned long long k = gen + i;
         const int vi = view_of(p, k);
         const View& v = p.views[vi];
@@ -366,7 +395,6 @@ __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
         store_rng(st, rng);
         P.st[slot] = st;
         P.ctr[slot] = make_int4(1, 1, 0, 0);
-        P.q[in][base + i] = slot;
     }
 }
 
@@ -951,7 +979,10 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
         P.mis_f[slot] = mf4;
         P.ctr[slot] = make_int4(depth, s_depth, scat, (flags & 0xff) | (ray_med << 8));
         const int qi = warp_append(&c->n_next, cont);
-        if (cont) P.q[out][qi] = slot;
+        if (cont) {
+            if (p.slot_queue) P.slot_state[slot] = kSlotCont;
+            else P.q[out][qi] = slot;
+        }
         if (S.has_subsurface) {
             const int si = warp_append(&c->n_sss, subsurface);
             if (subsurface) P.q_sss[si] = slot;
@@ -1018,7 +1049,10 @@ __global__ void __launch_bounds__(128) k_subsurface(Scene S, Params p, Pool P, C
         P.mis_f[slot] = mf4;
         P.ctr[slot] = make_int4(depth, ct.y, ct.z, (flags & 0xff) | (ray_med << 8));
         const int qi = warp_append(&c->n_next, cont);
-        if (cont) P.q[out][qi] = slot;
+        if (cont) {
+            if (p.slot_queue) P.slot_state[slot] = kSlotCont;
+            else P.q[out][qi] = slot;
+        }
         const int fi = warp_append(&c->n_finish, !cont);
         if (!cont) P.q_finish[fi] = slot;
     }
@@ -1125,7 +1159,7 @@ __global__ void k_finish(Params p, Pool P, Counters* c) {
                 }
             }
         }
-        P.free_flag[slot] = 1;
+        P.slot_state[slot] = kSlotFree;
     }
 }
 
@@ -1212,11 +1246,13 @@ struct DeviceSceneImpl {
     int tuned_gen_threads = 256;  // k_generate block
     int tuned_fin_threads = 128;  // k_finish block
     int tuned_fetch = 0;          // k_extend_fetch instead of k_extend
+    int tuned_queue = 0;          // extend queue in slot order (1) or shade order (0)
     int tuned_trials = 0;
     double tuned_ms = 0, default_ms = 0;
     DevBuf tune_film;
     void resolve_sort(Params* p, int requested) const {
         p->sort_mode = requested == ATRC_SORT_AUTO ? tuned_sort : requested;
+        p->slot_queue = tuned_queue;
         p->nkeys = std::max(scene.material_count, kMaterialTypes) + 2;
     }
     void ensure_render_resources() {
@@ -1325,7 +1361,7 @@ Pool pool_from(void* base, const PoolLayout& L, size_t cap, size_t shadow_cap) {
     P.q[0] = reinterpret_cast<int*>(b + L.off[11]);
     P.q[1] = reinterpret_cast<int*>(b + L.off[12]);
     P.q_finish = reinterpret_cast<int*>(b + L.off[13]);
-    P.free_flag = reinterpret_cast<int*>(b + L.off[14]);
+    P.slot_state = reinterpret_cast<int*>(b + L.off[14]);
     P.sh_o = reinterpret_cast<float4*>(b + L.off[15]);
     P.sh_d = reinterpret_cast<float4*>(b + L.off[16]);
     P.sh_c = reinterpret_cast<float4*>(b + L.off[17]);
@@ -1964,7 +2000,7 @@ static void tuning_out(const DeviceSceneImpl& d, AtrcTuning* out) {
     out->ms_per_msample = d.tuned_ms;
     out->default_ms_per_msample = d.default_ms;
     out->extend_fetch = d.tuned_fetch;
-    out->pad_ = 0;
+    out->queue_order = d.tuned_queue;
 }
 
 int atrc_cuda_get_tuning(AtrcScene* scene, AtrcTuning* out) {
@@ -1978,7 +2014,7 @@ static bool tuning_valid(const AtrcTuning& t) {
     return t.path_pool >= 1024 && t.path_pool <= (1 << 26) && t.sort_mode >= ATRC_SORT_NONE &&
            t.sort_mode <= ATRC_SORT_MATERIAL && t.gen_blocks_per_sm >= 1 && t.gen_blocks_per_sm <= 64 &&
            pow2_in(t.gen_threads, 32, 1024) && pow2_in(t.finish_threads, 32, 1024) &&
-           (t.extend_fetch == 0 || t.extend_fetch == 1);
+           (t.extend_fetch == 0 || t.extend_fetch == 1) && (t.queue_order == 0 || t.queue_order == 1);
 }
 
 int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
@@ -1991,6 +2027,7 @@ int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
     d.tuned_gen_threads = in->gen_threads;
     d.tuned_fin_threads = in->finish_threads;
     d.tuned_fetch = in->extend_fetch;
+    d.tuned_queue = in->queue_order;
     return ATRC_OK;
 }
 
@@ -2025,21 +2062,22 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
         AtrcTuning cur{};
         tuning_out(d, &cur);
         int trials = 0;
-        auto measure = [&](const AtrcTuning& c) {
+        auto measure_on = [&](const AtrcTuning& c, AtrcRenderDesc& trial) {
             atrc_cuda_set_tuning(scene, &c);
-            t.sort_mode = ATRC_SORT_AUTO;
-            t.path_pool = 0;
+            trial.sort_mode = ATRC_SORT_AUTO;
+            trial.path_pool = 0;
             double best = 1e30;
             for (int rep = 0; rep < 2; ++rep) {
                 CK(cudaMemsetAsync(d.tune_film.p, 0, npix * 4 * sizeof(double), d.stream));
                 AtrcRenderStats st{};
-                const int r = render_impl(scene, &t, &film, 1, nullptr, nullptr, nullptr, &st);
+                const int r = render_impl(scene, &trial, &film, 1, nullptr, nullptr, nullptr, &st);
                 if (r != ATRC_OK) throw CudaError(std::string("autotune trial failed: ") + atrc_last_error());
                 best = std::min(best, st.kernel_seconds * 1e3 / (double(st.samples) / 1e6));
                 ++trials;
             }
             return best;
         };
+        auto measure = [&](const AtrcTuning& c) { return measure_on(c, t); };
         // defaults first (one warm-up trial compiles nothing but pages in)
         AtrcTuning base{1 << 21, ATRC_SORT_NONE, 16, 256, 128, 0, 0, 0, 0, 0};
         if (!pool_fits(base.path_pool)) base.path_pool = 1 << 19;
@@ -2053,7 +2091,27 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
             if (ms < best_ms * 0.99) { best_ms = ms; best = c; }
         };
         { AtrcTuning c = best; c.extend_fetch = 1; consider(c); }
-        for (int m : {ATRC_SORT_TYPE, ATRC_SORT_MATERIAL}) { AtrcTuning c = best; c.sort_mode = m; consider(c); }
+        // Sort granularity with the extend-queue order.  The queue order only
+        // matters once slots are reused, so these trials render at least three
+        // pools of samples (up to the view's spp).
+        {
+            AtrcRenderDesc tq = t;
+            const size_t three_pools = 3 * size_t(best.path_pool);
+            tq.spp_count = int32_t(std::min<size_t>(size_t(desc->spp),
+                                                    std::max<size_t>(size_t(t.spp_count), (three_pools + npix - 1) / npix)));
+            const AtrcTuning after_fetch = best;
+            double q_ms = measure_on(after_fetch, tq);
+            for (int q : {0, 1})
+                for (int m : {ATRC_SORT_NONE, ATRC_SORT_TYPE, ATRC_SORT_MATERIAL}) {
+                    AtrcTuning c = after_fetch;
+                    c.sort_mode = m;
+                    c.queue_order = q;
+                    if ((q == after_fetch.queue_order && m == after_fetch.sort_mode) || !tuning_valid(c)) continue;
+                    const double ms = measure_on(c, tq);
+                    if (ms < q_ms * 0.99) { q_ms = ms; best = c; }
+                }
+            best_ms = measure(best);  // the later steps compare on the short trial
+        }
         const AtrcTuning after_sort = best;
         for (int pool : {1 << 19, 1 << 20, 1 << 22}) { AtrcTuning c = after_sort; c.path_pool = pool; consider(c); }
         const AtrcTuning after_pool = best;
@@ -2088,7 +2146,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
 // cudaMallocHost and no allocating library call.
 //
 // The array is shared by every call on a device and keeps the previous call's
-// contents; the counters and the free-slot flags are rewritten at the start of each
+// contents; the counters and the slot states are rewritten at the start of each
 // call, and every other word is written before it is read.  Calls whose work
 // overlaps on the GPU (two threads, two streams, or two scenes on the same
 // device at once) race on the array: serialise them.
@@ -2196,7 +2254,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         Pool P = pool_from(base + counters_bytes + tiles_bytes, L, cap, shadow_cap);
         const int gsm = grid_for(d.sm_count, 16);
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
-        // k_init rewrites the counters and the free-slot flags (all state that must
+        // k_init rewrites the counters and the slot states (all state that must
         // start from a known value)
         k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
         CK(cudaGetLastError());

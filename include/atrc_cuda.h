@@ -474,14 +474,18 @@ typedef struct AtrcTuning {
     int32_t extend_fetch;       /* closest-hit traversal: 1 = persistent warps   */
                                 /* that refill finished lanes with new rays, 0 = */
                                 /* one ray per thread                            */
-    int32_t pad_;
+    int32_t queue_order;        /* extend queue: 0 = continuing paths in the     */
+                                /* order they were shaded, then new samples; 1 = */
+                                /* every queued path in ascending slot order     */
 } AtrcTuning;
 
 /* Project autotuner (the reference has no counterpart: it renders with a
  * fixed thread pool and 32x32 tiles, renderer_creators.cpp:127-128).  Renders
  * short trials of `desc` (each `trial_spp` samples per pixel, or enough for
  * about 4M samples when trial_spp <= 0) into scratch memory, searching the
- * closest-hit kernel (extend_fetch), sort granularity, then path-pool size,
+ * closest-hit kernel (extend_fetch), sort granularity with the extend-queue
+ * order (queue_order; these on a trial of at least three path pools of
+ * samples, where slots are reused), then path-pool size,
  * then the generate / finish launch shapes
  * (coordinate descent, best of two timings each), and stores the fastest
  * configuration in the scene.  The caller's films are untouched. */

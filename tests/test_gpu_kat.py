@@ -237,3 +237,38 @@ def test_extend_fetch_matches_one_ray_per_thread(scene_dir, sort_mode):
     # (shadow contributions are FP32 atomics, whose order may differ)
     np.testing.assert_allclose(fb.value, fa.value, rtol=2e-6, atol=1e-9)
     np.testing.assert_array_equal(fb.weight, fa.weight)
+
+
+@pytest.mark.parametrize("scene", ["instanced", "media", "subsurface"])
+@pytest.mark.parametrize("sort_mode", [0, 2])
+def test_queue_order_changes_nothing(scene, sort_mode, scene_dir, tmp_path):
+    # the extend queue in slot order (continuations marked per slot, queued
+    # by the slot scan) or in shade order (continuations appended by k_shade
+    # and k_subsurface) holds the same paths: same samples, rays and film,
+    # with a pool small enough that slots are reused many times
+    from atrc_b200 import scenes
+    if scene == "instanced":
+        cfg = Config.from_file(scenes.instanced_disney(scene_dir / "inst_small", ico_level=4, hf_res=128,
+                                                       width=64, height=36, spp=64))
+    elif scene == "media":
+        cfg = Config.from_file(scenes.media_scene(scene_dir))
+    else:
+        cfg = Config.from_string(K.dumps(K.subsurface_scene(tmp_path)), str(tmp_path))
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 64, 36, 32
+    desc.sort_mode = sort_mode
+    dev = DeviceScene(cfg)
+    out = []
+    for q in (0, 1):
+        dev.set_tuning(queue_order=q, path_pool=1 << 13)
+        assert dev.tuning()["queue_order"] == q
+        f = Film(desc.width, desc.height)
+        st = dev.render(desc, f)
+        assert st["watchdog_flags"] == 0
+        out.append((f, st))
+    (fa, sa), (fb, sb) = out
+    assert sa["samples"] == sb["samples"] == desc.width * desc.height * desc.spp
+    for k in ("rays_closest", "rays_shadow"):
+        assert sa[k] == sb[k], k
+    np.testing.assert_allclose(fb.value, fa.value, rtol=2e-6, atol=1e-9)
+    np.testing.assert_array_equal(fb.weight, fa.weight)
