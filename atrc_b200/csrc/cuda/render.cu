@@ -311,48 +311,63 @@ __device__ __forceinline__ int tile_of(const int4* t, int n, int e0, int u, int*
     return g;
 }
 
-// New samples go into free slots taken in ascending slot order: a warp looks
-// at 32 consecutive slots and takes sample tickets for its free ones with
-// one atomic (ticket t < n_new becomes sample gen_base + t), so new path
+// Block-wide ticket: the lanes with `pred` get consecutive values from
+// *counter in thread order (one atomic per block); every thread receives its
+// own ticket (or -1) and, in *first, the block's base.  All threads of the
+// block call it together.
+__device__ __forceinline__ int block_ticket(int* counter, bool pred, int* smem, int* first) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (lane == 0) smem[w] = __popc(m);
+    __syncthreads();
+    if (w == 0) {
+        const int v = lane < nw ? smem[lane] : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        int base = 0;
+        if (lane == 0 && total > 0) base = atomicAdd(counter, total);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (lane < nw) smem[lane] = base + incl - v;
+        if (lane == 0) smem[32] = base;
+    }
+    __syncthreads();
+    const int t = pred ? smem[w] + __popc(m & ((1u << lane) - 1u)) : -1;
+    *first = smem[32];
+    __syncthreads();
+    return t;
+}
+
+// New samples go into free slots taken in ascending slot order: a block looks
+// at blockDim consecutive slots and takes sample tickets for its free ones
+// with one atomic (ticket t < n_new becomes sample gen_base + t), so new path
 // state is written by neighbouring lanes whatever order the paths finished
 // in.  Extend-queue positions: n_cont + t after the continuations k_shade
-// appended (shade order), or, with p.slot_queue, one more ticket per warp
+// appended (shade order), or, with p.slot_queue, one more ticket per block
 // for its new paths and for its slots whose path continues, so the whole
 // queue runs in slot order.  The sample -> pixel / random stream map does
 // not depend on the slot, so the image does not either.
 __global__ void k_generate(Scene S, Params p, Pool P, Counters* c) {
+    __shared__ int tick[33];
     const int n = c->n_new;
     if (p.slot_queue ? c->n_ext == 0 : n == 0) return;
-    const int in = c->in, n_cont = c->n_cont, lane = threadIdx.x & 31;
+    const int in = c->in, n_cont = c->n_cont;
     const unsigned long long gen = c->gen_base;
-    for (int i0 = blockIdx.x * blockDim.x; i0 < P.cap; i0 += gridDim.x * blockDim.x) {
+    for (int i0 = blockIdx.x * blockDim.x; i0 < P.cap; i0 += gridDim.x * blockDim.x) {  // block-uniform
         const int slot = i0 + int(threadIdx.x);
         const int state = slot < P.cap ? P.slot_state[slot] : kSlotBusy;
         const bool is_free = state == kSlotFree && n > 0;
-        const unsigned mf = __ballot_sync(0xffffffffu, is_free);
-        int i = n;
-        if (mf != 0) {
-            int t0 = 0;
-            if (lane == 0) t0 = atomicAdd(&c->gen_ticket, __popc(mf));
-            t0 = __shfl_sync(0xffffffffu, t0, 0);
-            // tickets only grow: past n_new every sample of this iteration is placed
-            if (t0 >= n && !p.slot_queue) return;
-            i = t0 + __popc(mf & ((1u << lane) - 1u));
-        }
+        int first;
+        int i = block_ticket(&c->gen_ticket, is_free, tick, &first);
+        // tickets only grow: past n_new every sample of this iteration is placed
+        if (first >= n && !p.slot_queue) return;  // block-uniform
         const bool fresh = is_free && i < n;
         int qpos = n_cont + i;
-        if (p.slot_queue) {
-            const bool enqueue = fresh || state == kSlotCont;
-            const unsigned me = __ballot_sync(0xffffffffu, enqueue);
-            if (me == 0) continue;
-            int q0 = 0;
-            if (lane == 0) q0 = atomicAdd(&c->ext_ticket, __popc(me));
-            q0 = __shfl_sync(0xffffffffu, q0, 0);
-            if (!enqueue) continue;
-            qpos = q0 + __popc(me & ((1u << lane) - 1u));
-        } else if (!fresh) {
-            continue;
-        }
+        if (p.slot_queue) qpos = block_ticket(&c->ext_ticket, fresh || state == kSlotCont, tick, &first);
+        if (qpos < 0 || (!p.slot_queue && !fresh)) continue;
         P.slot_state[slot] = kSlotBusy;
         P.q[in][qpos] = slot;
         if (!fresh) continue;
