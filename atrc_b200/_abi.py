@@ -122,7 +122,7 @@ class AtrcTuning(C.Structure):
     _fields_ = [("path_pool", C.c_int32), ("sort_mode", C.c_int32), ("gen_blocks_per_sm", C.c_int32),
                 ("gen_threads", C.c_int32), ("finish_threads", C.c_int32), ("trials", C.c_int32),
                 ("ms_per_msample", C.c_double), ("default_ms_per_msample", C.c_double), ("extend_fetch", C.c_int32),
-                ("queue_order", C.c_int32)]
+                ("queue_order", C.c_int32), ("shadow_fetch", C.c_int32), ("pad_", C.c_int32)]
 
 
 class AtrcGuideDesc(C.Structure):

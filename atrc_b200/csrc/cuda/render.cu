@@ -117,6 +117,7 @@ struct Counters {
     int n_guide;              // guide queries this iteration
     int n_sss;                // subsurface walks queued this iteration
     int ext_cursor;           // next extend-queue entry for k_extend_fetch
+    int sh_cursor;            // next shadow-queue entry for k_shadow_fetch
     int n_free, n_new, n_cont;
     int gen_ticket;           // k_generate: free slots claimed this iteration
     int ext_ticket;           // k_generate: extend-queue entries written (slot order)
@@ -256,6 +257,7 @@ __global__ void k_begin(Counters* c) {
     c->n_guide = 0;
     c->n_sss = 0;
     c->ext_cursor = 0;
+    c->sh_cursor = 0;
     if (c->n_ext == 0) c->done = 1;
 }
 
@@ -1095,6 +1097,52 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_shadow(S
     if (COUNT) flush_count(c->cnt_shadow, tc);
 }
 
+// k_shadow with dynamic ray fetch, as k_extend_fetch: persistent warps
+// step their any-hit traversals round by round and refill the lanes whose
+// rays are done (occluded at the first hit, or through the scene) from the
+// shadow queue.  Contributions and counts are those of k_shadow.
+template <bool EXACT, bool COUNT>
+__global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_shadow_fetch(Scene S, Pool P, Counters* c) {
+    const int n = min(c->n_shadow, P.shadow_cap);
+    const int lane = threadIdx.x & 31;
+    TraceCount tc{0, 0, 0};
+    int32_t stack[kStackSize];
+    Tracer<EXACT, true, COUNT> tr;
+    int i = -1, wd = 0;
+    bool drained = false;
+    for (;;) {
+        const unsigned idle = __ballot_sync(0xffffffffu, i < 0);
+        if (!drained && __popc(idle) >= kRefillLanes) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&c->sh_cursor, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + __popc(idle) >= n) drained = true;
+            if (i < 0) {
+                const int k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < n) {
+                    i = k;
+                    const float4 o = P.sh_o[i], d = P.sh_d[i];
+                    tr.init(S, stack, xyz(o), xyz(d), o.w, d.w);
+                }
+            }
+        }
+        if (drained && __all_sync(0xffffffffu, i < 0)) break;
+        if (i >= 0 && tr.step(S, &wd, &tc)) {
+            Hit h;
+            if (!tr.result(&h)) {
+                const float4 cc = P.sh_c[i];
+                float* l = reinterpret_cast<float*>(P.L + __float_as_int(cc.w));
+                atomicAdd(l, cc.x);
+                atomicAdd(l + 1, cc.y);
+                atomicAdd(l + 2, cc.z);
+            }
+            i = -1;
+        }
+    }
+    if (wd) atomicMax(&c->watchdog, wd);
+    if (COUNT) flush_count(c->cnt_shadow, tc);
+}
+
 __device__ __forceinline__ float filter_eval(const View& p, float x, float y) {
     if (p.filter_type == ATRC_FILTER_BOX) return p.filter_value;
     const float gx = fmaxf(0.0f, __expf(-p.filter_alpha * x * x) - p.filter_exp);
@@ -1262,6 +1310,7 @@ struct DeviceSceneImpl {
     int tuned_fin_threads = 128;  // k_finish block
     int tuned_fetch = 0;          // k_extend_fetch instead of k_extend
     int tuned_queue = 0;          // extend queue in slot order (1) or shade order (0)
+    int tuned_shadow_fetch = 0;   // k_shadow_fetch instead of k_shadow
     int tuned_trials = 0;
     double tuned_ms = 0, default_ms = 0;
     DevBuf tune_film;
@@ -1826,8 +1875,15 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             if (d.scene.has_subsurface) k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
-            if (count) k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
-            else k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+            if (d.tuned_shadow_fetch) {
+                const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
+                if (count) k_shadow_fetch<false, true><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+                else k_shadow_fetch<false, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+            } else if (count) {
+                k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+            } else {
+                k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+            }
             CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
             k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, c);
         }
@@ -2016,6 +2072,8 @@ static void tuning_out(const DeviceSceneImpl& d, AtrcTuning* out) {
     out->default_ms_per_msample = d.default_ms;
     out->extend_fetch = d.tuned_fetch;
     out->queue_order = d.tuned_queue;
+    out->shadow_fetch = d.tuned_shadow_fetch;
+    out->pad_ = 0;
 }
 
 int atrc_cuda_get_tuning(AtrcScene* scene, AtrcTuning* out) {
@@ -2029,7 +2087,8 @@ static bool tuning_valid(const AtrcTuning& t) {
     return t.path_pool >= 1024 && t.path_pool <= (1 << 26) && t.sort_mode >= ATRC_SORT_NONE &&
            t.sort_mode <= ATRC_SORT_MATERIAL && t.gen_blocks_per_sm >= 1 && t.gen_blocks_per_sm <= 64 &&
            pow2_in(t.gen_threads, 32, 1024) && pow2_in(t.finish_threads, 32, 1024) &&
-           (t.extend_fetch == 0 || t.extend_fetch == 1) && (t.queue_order == 0 || t.queue_order == 1);
+           (t.extend_fetch == 0 || t.extend_fetch == 1) && (t.queue_order == 0 || t.queue_order == 1) &&
+           (t.shadow_fetch == 0 || t.shadow_fetch == 1);
 }
 
 int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
@@ -2043,6 +2102,7 @@ int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
     d.tuned_fin_threads = in->finish_threads;
     d.tuned_fetch = in->extend_fetch;
     d.tuned_queue = in->queue_order;
+    d.tuned_shadow_fetch = in->shadow_fetch;
     return ATRC_OK;
 }
 
@@ -2061,8 +2121,10 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
         film.weight = film.value + npix * 3;
         film.on_device = 1;
         AtrcRenderDesc t = *desc;
-        if (trial_spp <= 0) trial_spp = int32_t(std::max<size_t>(1, ((size_t(1) << 22) + npix - 1) / npix));
-        t.spp_count = std::min(trial_spp, desc->spp);
+        // at least three default path pools of samples: the extend-queue
+        // order only matters once slots are reused
+        const int32_t three_pools = int32_t((3 * (size_t(1) << 21) + npix - 1) / npix);
+        t.spp_count = std::min(std::max(trial_spp, three_pools), desc->spp);
         t.first_spp = 0;
         t.count_traversal = 0;
         // pools whose workspace stays under a quarter of the free memory
@@ -2077,22 +2139,21 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
         AtrcTuning cur{};
         tuning_out(d, &cur);
         int trials = 0;
-        auto measure_on = [&](const AtrcTuning& c, AtrcRenderDesc& trial) {
+        auto measure = [&](const AtrcTuning& c) {
             atrc_cuda_set_tuning(scene, &c);
-            trial.sort_mode = ATRC_SORT_AUTO;
-            trial.path_pool = 0;
+            t.sort_mode = ATRC_SORT_AUTO;
+            t.path_pool = 0;
             double best = 1e30;
             for (int rep = 0; rep < 2; ++rep) {
                 CK(cudaMemsetAsync(d.tune_film.p, 0, npix * 4 * sizeof(double), d.stream));
                 AtrcRenderStats st{};
-                const int r = render_impl(scene, &trial, &film, 1, nullptr, nullptr, nullptr, &st);
+                const int r = render_impl(scene, &t, &film, 1, nullptr, nullptr, nullptr, &st);
                 if (r != ATRC_OK) throw CudaError(std::string("autotune trial failed: ") + atrc_last_error());
                 best = std::min(best, st.kernel_seconds * 1e3 / (double(st.samples) / 1e6));
                 ++trials;
             }
             return best;
         };
-        auto measure = [&](const AtrcTuning& c) { return measure_on(c, t); };
         // defaults first (one warm-up trial compiles nothing but pages in)
         AtrcTuning base{1 << 21, ATRC_SORT_NONE, 16, 256, 128, 0, 0, 0, 0, 0};
         if (!pool_fits(base.path_pool)) base.path_pool = 1 << 19;
@@ -2106,27 +2167,15 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
             if (ms < best_ms * 0.99) { best_ms = ms; best = c; }
         };
         { AtrcTuning c = best; c.extend_fetch = 1; consider(c); }
-        // Sort granularity with the extend-queue order.  The queue order only
-        // matters once slots are reused, so these trials render at least three
-        // pools of samples (up to the view's spp).
-        {
-            AtrcRenderDesc tq = t;
-            const size_t three_pools = 3 * size_t(best.path_pool);
-            tq.spp_count = int32_t(std::min<size_t>(size_t(desc->spp),
-                                                    std::max<size_t>(size_t(t.spp_count), (three_pools + npix - 1) / npix)));
-            const AtrcTuning after_fetch = best;
-            double q_ms = measure_on(after_fetch, tq);
-            for (int q : {0, 1})
-                for (int m : {ATRC_SORT_NONE, ATRC_SORT_TYPE, ATRC_SORT_MATERIAL}) {
-                    AtrcTuning c = after_fetch;
-                    c.sort_mode = m;
-                    c.queue_order = q;
-                    if ((q == after_fetch.queue_order && m == after_fetch.sort_mode) || !tuning_valid(c)) continue;
-                    const double ms = measure_on(c, tq);
-                    if (ms < q_ms * 0.99) { q_ms = ms; best = c; }
-                }
-            best_ms = measure(best);  // the later steps compare on the short trial
-        }
+        { AtrcTuning c = best; c.shadow_fetch = 1; consider(c); }
+        const AtrcTuning after_fetch = best;
+        for (int q : {0, 1})
+            for (int m : {ATRC_SORT_NONE, ATRC_SORT_TYPE, ATRC_SORT_MATERIAL}) {
+                AtrcTuning c = after_fetch;
+                c.sort_mode = m;
+                c.queue_order = q;
+                if (q != after_fetch.queue_order || m != after_fetch.sort_mode) consider(c);
+            }
         const AtrcTuning after_sort = best;
         for (int pool : {1 << 19, 1 << 20, 1 << 22}) { AtrcTuning c = after_sort; c.path_pool = pool; consider(c); }
         const AtrcTuning after_pool = best;
@@ -2295,7 +2344,10 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
                     k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
                     launches += 1;
                 }
-                k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+                if (d.tuned_shadow_fetch)
+                    k_shadow_fetch<false, false><<<d.sm_count * ATRC_TRACE_MIN_BLOCKS, kTraceBlock, 0, s>>>(d.scene, P, c);
+                else
+                    k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 k_finish<<<gsm, 128, 0, s>>>(p, P, c);
                 launches += 6;
                 ext_launches += 1;

@@ -337,7 +337,7 @@ def batch_comparison(args) -> dict:
     small_r = compare(small)
     return {"workload": f"indoor_room_{args.batch_views}_views", "spp_scale": args.batch_spp_scale,
             "tuning": {k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
-                                              "finish_threads", "extend_fetch", "queue_order")},
+                                              "finish_threads", "extend_fetch", "queue_order", "shadow_fetch")},
             **full, "small_views": small_r}
 
 
@@ -356,7 +356,7 @@ def ingest_comparison(args, cfg, desc, tuning, sah_build_s: float, sah_value: fl
     scene = DeviceScene(pcfg)
     ploc_s = time.perf_counter() - t0
     scene.set_tuning(**{k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
-                                               "finish_threads", "extend_fetch", "queue_order")})
+                                               "finish_threads", "extend_fetch", "queue_order", "shadow_fetch")})
     film = Film(desc.width, desc.height, device=True)
     for k in range(args.warmup):
         desc.first_spp = k * desc.spp_count
@@ -496,7 +496,7 @@ def main():
                        "l2": "inputs larger than L2 (BVH + triangles + shading data > 126 MB)",
                        "scene_build_s": round(build_s, 3), "autotune_s": round(tune_s, 3),
                        "tuning": {k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
-                                                         "finish_threads", "extend_fetch", "queue_order", "trials")}},
+                                                         "finish_threads", "extend_fetch", "queue_order", "shadow_fetch", "trials")}},
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -477,18 +477,21 @@ typedef struct AtrcTuning {
     int32_t queue_order;        /* extend queue: 0 = continuing paths in the     */
                                 /* order they were shaded, then new samples; 1 = */
                                 /* every queued path in ascending slot order     */
+    int32_t shadow_fetch;       /* any-hit traversal: 1 = persistent warps that  */
+                                /* refill finished lanes, 0 = one ray per thread */
+    int32_t pad_;
 } AtrcTuning;
 
 /* Project autotuner (the reference has no counterpart: it renders with a
  * fixed thread pool and 32x32 tiles, renderer_creators.cpp:127-128).  Renders
- * short trials of `desc` (each `trial_spp` samples per pixel, or enough for
- * about 4M samples when trial_spp <= 0) into scratch memory, searching the
- * closest-hit kernel (extend_fetch), sort granularity with the extend-queue
- * order (queue_order; these on a trial of at least three path pools of
- * samples, where slots are reused), then path-pool size,
- * then the generate / finish launch shapes
- * (coordinate descent, best of two timings each), and stores the fastest
- * configuration in the scene.  The caller's films are untouched. */
+ * short trials of `desc` into scratch memory, each max(trial_spp, the spp
+ * of three default path pools = 3 * 2^21 samples) samples per pixel, capped
+ * at desc->spp (the extend-queue order only matters once path slots are
+ * reused).  It searches the closest-hit and any-hit kernels (extend_fetch,
+ * shadow_fetch), sort granularity with the extend-queue order
+ * (queue_order), then path-pool size, then the generate / finish launch
+ * shapes (coordinate descent, best of two timings each), and stores the
+ * fastest configuration in the scene.  The caller's films are untouched. */
 int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc,
                        int32_t trial_spp, AtrcTuning* out);
 /* Read or replace a scene's launch configuration (e.g. a cached tuning). */

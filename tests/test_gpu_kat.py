@@ -272,3 +272,37 @@ def test_queue_order_changes_nothing(scene, sort_mode, scene_dir, tmp_path):
         assert sa[k] == sb[k], k
     np.testing.assert_allclose(fb.value, fa.value, rtol=2e-6, atol=1e-9)
     np.testing.assert_array_equal(fb.weight, fa.weight)
+
+
+@pytest.mark.parametrize("scene", ["instanced", "media"])
+def test_shadow_fetch_matches_one_ray_per_thread(scene, scene_dir):
+    # k_shadow_fetch (persistent warps refilling finished lanes from the
+    # shadow queue) decides the same occlusions as k_shadow: same rays,
+    # traversal work and film
+    from atrc_b200 import scenes
+    if scene == "instanced":
+        p = scenes.instanced_disney(scene_dir / "inst_small", ico_level=4, hf_res=128, width=64, height=36, spp=64)
+    else:
+        p = scenes.media_scene(scene_dir)
+    cfg = Config.from_file(p)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 64, 36, 32
+    desc.count_traversal = 1
+    dev = DeviceScene(cfg)
+    out = []
+    for fetch in (0, 1):
+        dev.set_tuning(shadow_fetch=fetch, path_pool=1 << 14)
+        assert dev.tuning()["shadow_fetch"] == fetch
+        f = Film(desc.width, desc.height)
+        st = dev.render(desc, f)
+        assert st["watchdog_flags"] == 0
+        out.append((f, st))
+    (fa, sa), (fb, sb) = out
+    for k in ("samples", "rays_closest", "rays_shadow"):
+        assert sa[k] == sb[k], k
+    assert sa["rays_shadow"] > 0
+    # which rays share a warp differs, and with it leaf postponement's visits
+    for k in ("nodes_shadow", "tris_shadow", "ents_shadow"):
+        assert abs(sa[k] - sb[k]) <= 0.01 * sa[k], k
+    np.testing.assert_allclose(fb.value, fa.value, rtol=2e-6, atol=1e-9)
+    np.testing.assert_array_equal(fb.weight, fa.weight)
