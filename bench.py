@@ -165,8 +165,8 @@ def reference_arm(args, rank: int, world: int) -> None:
 # DRAM bytes per closest ray of k_extend on the instanced workload, from one
 # ncu capture of every k_extend launch of an NVTX-marked 2-spp step
 # (dram__bytes_read.sum + dram__bytes_write.sum summed over the launches,
-# divided by the step's closest rays: 1,242.4 MB / 5,306,689 rays).
-K_EXTEND_DRAM_BYTES_PER_RAY = 234.1
+# divided by the step's closest rays: 1,247.9 MB / 5,306,689 rays).
+K_EXTEND_DRAM_BYTES_PER_RAY = 235.2
 
 
 def cpu_baseline(args) -> dict:
