@@ -465,16 +465,52 @@ __global__ void __launch_bounds__(1024) k_sort_scan(Pool P, int nkeys) {
 }
 
 // Scatter the extend queue into key order (order within a key is arbitrary).
-__global__ void k_sort_scatter(Pool P, Counters* c) {
-    const int n = c->n_ext, in = c->in;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int key = P.keys[i];
-        const unsigned same = __match_any_sync(__activemask(), key);
-        const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(P.key_cursor + key, __popc(same));
-        base = __shfl_sync(same, base, leader);
-        P.q_sorted[base + __popc(same & ((1u << lane) - 1u))] = P.q[in][i];
+// A block takes kScatterPer x blockDim entries per pass, counts them per key
+// in shared memory and reserves each key's run with one global atomic, so the
+// few key cursors see one atomic per key per block pass instead of one per
+// warp (same-address atomics serialise in L2).  More keys than kScatterKeys
+// (material sort of a large scene): one atomic per key per warp.
+constexpr int kScatterKeys = 1024, kScatterPer = 8;
+
+__global__ void k_sort_scatter(Pool P, Counters* c, int nkeys) {
+    __shared__ int run[kScatterKeys];
+    const int n = c->n_ext, in = c->in, lane = threadIdx.x & 31;
+    if (nkeys > kScatterKeys) {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            const int key = P.keys[i];
+            const unsigned same = __match_any_sync(__activemask(), key);
+            const int leader = __ffs(same) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(P.key_cursor + key, __popc(same));
+            base = __shfl_sync(same, base, leader);
+            P.q_sorted[base + __popc(same & ((1u << lane) - 1u))] = P.q[in][i];
+        }
+        return;
+    }
+    const int span = kScatterPer * blockDim.x;
+    for (int i0 = blockIdx.x * span; i0 < n; i0 += gridDim.x * span) {  // block-uniform
+        for (int k = threadIdx.x; k < nkeys; k += blockDim.x) run[k] = 0;
+        __syncthreads();
+        int key[kScatterPer], rank[kScatterPer], slot[kScatterPer];
+#pragma unroll
+        for (int e = 0; e < kScatterPer; ++e) {
+            const int i = i0 + e * int(blockDim.x) + int(threadIdx.x);
+            key[e] = i < n ? P.keys[i] : -1;
+            slot[e] = i < n ? P.q[in][i] : 0;
+            const unsigned same = __match_any_sync(0xffffffffu, key[e]);
+            const int leader = __ffs(same) - 1;
+            int r = 0;
+            if (lane == leader && key[e] >= 0) r = atomicAdd(run + key[e], __popc(same));
+            rank[e] = __shfl_sync(0xffffffffu, r, leader) + __popc(same & ((1u << lane) - 1u));
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < nkeys; k += blockDim.x)
+            if (run[k] > 0) run[k] = atomicAdd(P.key_cursor + k, run[k]);
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < kScatterPer; ++e)
+            if (key[e] >= 0) P.q_sorted[run[key[e]] + rank[e]] = slot[e];
+        __syncthreads();
     }
 }
 
@@ -1868,7 +1904,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             }
             if (p.sort_mode != ATRC_SORT_NONE) {
                 k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
-                k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
+                k_sort_scatter<<<d.sm_count * 8, 128, 0, s>>>(P, c, p.nkeys);
             }
             CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
             if (guide) {
@@ -2339,7 +2375,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
                     k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
                 if (p.sort_mode != ATRC_SORT_NONE) {
                     k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
-                    k_sort_scatter<<<g_path, 128, 0, s>>>(P, c);
+                    k_sort_scatter<<<d.sm_count * 8, 128, 0, s>>>(P, c, p.nkeys);
                     launches += 2;
                 }
                 k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
