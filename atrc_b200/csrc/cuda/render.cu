@@ -2206,7 +2206,6 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
             if (ms < best_ms * 0.99) { best_ms = ms; best = c; }
         };
         { AtrcTuning c = best; c.extend_fetch = 1; consider(c); }
-        { AtrcTuning c = best; c.shadow_fetch = 1; consider(c); }
         const AtrcTuning after_fetch = best;
         for (int q : {0, 1})
             for (int m : {ATRC_SORT_NONE, ATRC_SORT_TYPE, ATRC_SORT_MATERIAL}) {

@@ -479,6 +479,7 @@ typedef struct AtrcTuning {
                                 /* every queued path in ascending slot order     */
     int32_t shadow_fetch;       /* any-hit traversal: 1 = persistent warps that  */
                                 /* refill finished lanes, 0 = one ray per thread */
+                                /* (set by the caller; the autotuner leaves 0)   */
     int32_t pad_;
 } AtrcTuning;
 
@@ -487,8 +488,8 @@ typedef struct AtrcTuning {
  * short trials of `desc` into scratch memory, each max(trial_spp, the spp
  * of three default path pools = 3 * 2^21 samples) samples per pixel, capped
  * at desc->spp (the extend-queue order only matters once path slots are
- * reused).  It searches the closest-hit and any-hit kernels (extend_fetch,
- * shadow_fetch), sort granularity with the extend-queue order
+ * reused).  It searches the closest-hit kernel (extend_fetch), sort
+ * granularity with the extend-queue order
  * (queue_order), then path-pool size, then the generate / finish launch
  * shapes (coordinate descent, best of two timings each), and stores the
  * fastest configuration in the scene.  The caller's films are untouched. */
