@@ -196,10 +196,9 @@ struct Params {
     float ao_low[3], ao_high[3], ao_bg[3];
 };
 
-// Slot states: free, holding a path that continues next iteration, holding
-// a finished path that k_finish splats, or holding a path between its queue
-// entry and its continuation / finish.
-constexpr int kSlotBusy = 0, kSlotFree = 1, kSlotCont = 2, kSlotDone = 3;
+// Slot states: free, holding a path that continues next iteration, or
+// holding a path between its queue entry and its continuation / finish.
+constexpr int kSlotBusy = 0, kSlotFree = 1, kSlotCont = 2;
 
 struct Pool {
     float4 *ray_o, *ray_d;        // o.xyz tmin / d.xyz tmax
@@ -217,6 +216,7 @@ struct Pool {
     int* keys;                    // material key per extend-queue entry
     int* key_count;               // per key: entries this iteration
     int* key_cursor;              // per key: next write position in q_sorted
+    int* q_finish;
     int* q_sss;                   // paths whose BSDF sample entered a subsurface material
     int* slot_state;              // per slot: kSlotFree / kSlotCont / kSlotBusy
     float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
@@ -836,8 +836,8 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
             store_rng(st, rng);
             P.st[slot] = st;
             P.L[slot] = make_float4(L.x, L.y, L.z, L4.w);
-            warp_append(&c->n_finish, true);
-            P.slot_state[slot] = kSlotDone;
+            const int fi = warp_append(&c->n_finish, true);
+            P.q_finish[fi] = slot;
             continue;
         }
         // (1) pending MIS-BSDF term of the previous vertex (direct_illum.cpp:130-192)
@@ -1044,8 +1044,8 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
             if (subsurface) P.q_sss[si] = slot;
         }
         const bool ends = !cont && !subsurface;
-        warp_append(&c->n_finish, ends);
-        if (ends) P.slot_state[slot] = kSlotDone;
+        const int fi = warp_append(&c->n_finish, ends);
+        if (ends) P.q_finish[fi] = slot;
     }
 }
 
@@ -1109,8 +1109,8 @@ __global__ void __launch_bounds__(128) k_subsurface(Scene S, Params p, Pool P, C
             if (p.slot_queue) P.slot_state[slot] = kSlotCont;
             else P.q[out][qi] = slot;
         }
-        warp_append(&c->n_finish, !cont);
-        if (!cont) P.slot_state[slot] = kSlotDone;
+        const int fi = warp_append(&c->n_finish, !cont);
+        if (!cont) P.q_finish[fi] = slot;
     }
 }
 
@@ -1189,13 +1189,10 @@ __device__ __forceinline__ float filter_eval(const View& p, float x, float y) {
     return gx * gy;
 }
 
-// Finished paths are found by a scan of the slot states in ascending order,
-// so neighbouring lanes splat paths that were generated together: mostly
-// neighbouring pixels, whose FP64 atomics share L2 sectors.
 __global__ void k_finish(Params p, Pool P, Counters* c) {
-    if (c->n_finish == 0) return;
-    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < P.cap; slot += gridDim.x * blockDim.x) {
-        if (P.slot_state[slot] != kSlotDone) continue;
+    const int n = c->n_finish;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = P.q_finish[i];
         const float4 L = P.L[slot];
         const float sx = L.w, sy = P.mis_f[slot].w;
         const uint32_t vt = P.st[slot].w;
@@ -1442,7 +1439,7 @@ PoolLayout pool_layout(size_t cap, size_t shadow_cap, int nkeys) {
     take(0, cap * 16); take(1, cap * 16); take(2, cap * 16); take(3, cap * 4);
     take(4, cap * 16); take(5, cap * 16); take(6, cap * 16); take(7, cap * 16); take(8, cap * 16);
     take(9, cap * 16); take(10, cap * 16);
-    take(11, cap * 4); take(12, cap * 4); take(13, 0); take(14, cap * 4);  // 13: empty (finished paths are marked in the slot states)
+    take(11, cap * 4); take(12, cap * 4); take(13, cap * 4); take(14, cap * 4);
     take(15, shadow_cap * 16); take(16, shadow_cap * 16); take(17, shadow_cap * 16);
     take(18, cap * 4); take(19, cap * 4); take(20, size_t(nkeys) * 4); take(21, size_t(nkeys) * 4);
     take(22, cap * 4);
@@ -1466,6 +1463,7 @@ Pool pool_from(void* base, const PoolLayout& L, size_t cap, size_t shadow_cap) {
     P.ctr = reinterpret_cast<int4*>(b + L.off[10]);
     P.q[0] = reinterpret_cast<int*>(b + L.off[11]);
     P.q[1] = reinterpret_cast<int*>(b + L.off[12]);
+    P.q_finish = reinterpret_cast<int*>(b + L.off[13]);
     P.slot_state = reinterpret_cast<int*>(b + L.off[14]);
     P.sh_o = reinterpret_cast<float4*>(b + L.off[15]);
     P.sh_d = reinterpret_cast<float4*>(b + L.off[16]);
