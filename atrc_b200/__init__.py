@@ -295,14 +295,15 @@ class DeviceScene:
                                                      C.byref(f), C.byref(st)))
         return {k: getattr(st, k) for k, _ in AtrcRenderStats._fields_}
 
-    def render(self, desc: AtrcRenderDesc, film: Film, cancel: Optional[C.c_int] = None,
+    def render(self, desc: AtrcRenderDesc, film: Film, should_stop: Optional[Callable[[], bool]] = None,
                progress: Optional[Callable[[float], None]] = None) -> dict:
+        """atrc_cuda_render: `should_stop` is polled between wavefront
+        iterations (a true result cancels), `progress` gets percentages."""
         st = AtrcRenderStats()
         f = film.as_struct()
         cb = abi.PROGRESS_FN(lambda pct, user: progress(pct)) if progress else abi.PROGRESS_FN()
-        _check(load_library().atrc_cuda_render(self._h, C.byref(desc), C.byref(f),
-                                              C.byref(cancel) if cancel is not None else None, cb, None,
-                                              C.byref(st)))
+        stop = abi.CANCEL_FN(lambda user: 1 if should_stop() else 0) if should_stop else abi.CANCEL_FN()
+        _check(load_library().atrc_cuda_render(self._h, C.byref(desc), C.byref(f), stop, cb, None, C.byref(st)))
         return {k: getattr(st, k) for k, _ in AtrcRenderStats._fields_}
 
 

@@ -149,6 +149,7 @@ STRUCT_ORDER = [AtrcSceneDesc, AtrcMeshDesc, AtrcGeometryDesc, AtrcEntityDesc, A
                 AtrcRenderStats, AtrcRay, AtrcHit, AtrcDeviceInfo, AtrcTuning, AtrcBvhBuildInfo]
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_double, C.c_void_p)
+CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
 
 # name -> (restype, argtypes)
 PROTOTYPES = {
@@ -170,7 +171,7 @@ PROTOTYPES = {
                                        C.c_int]),
     "atrc_cuda_trace_rays_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int]),
     "atrc_cuda_render": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
-                                   C.POINTER(C.c_int), PROGRESS_FN, C.c_void_p, C.POINTER(AtrcRenderStats)]),
+                                   CANCEL_FN, PROGRESS_FN, C.c_void_p, C.POINTER(AtrcRenderStats)]),
     "atrc_cuda_render_noalloc": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
                                            C.POINTER(AtrcRenderStats)]),
     "atrc_film_resolve": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, c_float_p]),

@@ -1561,6 +1561,8 @@ View make_view(const AtrcRenderDesc& d) {
 
 size_t tile_table_bytes(const View& p) { return size_t(p.TX + p.TY + 2) * sizeof(int4); }
 
+void* noalloc_scratch(int device);  // static scratch of atrc_cuda_render_noalloc (below)
+
 // Point a view at its tile table (filled on the device by k_tiles).
 void set_tiles(View* v, void* table) {
     v->tile_cols = static_cast<int4*>(table);
@@ -1630,6 +1632,9 @@ int atrc_cuda_scene_create(const AtrcSceneDesc* desc, AtrcScene** out) {
         S.eps = 3e-4f;
         d.scene = S;
         d.watchdog.alloc(sizeof(int));
+        // load the module's static scratch onto this device now, so that
+        // atrc_cuda_render_noalloc neither allocates nor looks it up itself
+        noalloc_scratch(d.device);
         CK(cudaStreamSynchronize(s));
         *out = sc.release();
         return int(ATRC_OK);
@@ -1767,7 +1772,7 @@ int atrc_cuda_subsurface_probe(AtrcScene* scene, const float o[3], const float d
 // receives the time from the start of the call at which each view's last
 // sample was splatted, observed at window granularity.
 static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const AtrcFilm* films, int nviews,
-                       volatile const int* cancel, AtrcProgressFn progress, void* user, AtrcRenderStats* stats,
+                       AtrcCancelFn should_stop, AtrcProgressFn progress, void* user, AtrcRenderStats* stats,
                        GuideImpl* guide = nullptr, bool record = false, double* view_seconds = nullptr) {
     const auto t_start = std::chrono::steady_clock::now();
     const AtrcRenderDesc* desc = descs;
@@ -1964,7 +1969,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
         if (hc.watchdog) { status = ATRC_ERR_WATCHDOG; break; }
         if (hc.done) break;
         if (progress) progress(100.0 * double(hc.completed) / double(std::max(1ULL, total)), user);
-        if (cancel && *cancel) { status = ATRC_ERR_CANCELLED; break; }
+        if (should_stop && should_stop(user)) { status = ATRC_ERR_CANCELLED; break; }
     }
     CK(cudaEventRecord(ev1, s));
     CK(cudaEventSynchronize(ev1));
@@ -2042,11 +2047,11 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     return int(ATRC_OK);
 }
 
-int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* film, volatile const int* cancel,
+int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc, AtrcFilm* film, AtrcCancelFn should_stop,
                      AtrcProgressFn progress, void* user, AtrcRenderStats* stats) {
     const int rc = check_render_args(scene, desc, film);
     if (rc != ATRC_OK) return rc;
-    return guarded([&] { return render_impl(scene, desc, film, 1, cancel, progress, user, stats); });
+    return guarded([&] { return render_impl(scene, desc, film, 1, should_stop, progress, user, stats); });
 }
 
 int atrc_cuda_scene_bounds(AtrcScene* scene, float lo[3], float hi[3]) {
@@ -2241,11 +2246,15 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
 // driver's allocator (cudaMalloc can synchronise the device and its latency is
 // unbounded).  atrc_cuda_render_noalloc serves them: the wavefront's scratch
 // memory (path pool, queues, shadow rays, counters) lives in the file-scope
-// array below, which the driver reserves once when the library is loaded onto
-// a device and which every GPU that loads the library keeps until the process
-// exits.  The caller passes the scene (created beforehand) and a film of
-// device pointers; the call itself makes no cudaMalloc / cudaFree /
-// cudaMallocHost and no allocating library call.
+// array below, which every GPU that loads this file's module keeps until the
+// process exits.  Under CUDA's lazy module loading (the default since 12.2)
+// the module, and with it the array, is loaded onto a device the first time
+// the module is used there, which would be an allocation of its own; so
+// atrc_cuda_scene_create resolves the array's address on its device, and the
+// array is reserved before any render call or stream capture.  The caller
+// passes the scene (created beforehand) and a film of device pointers; the
+// call itself makes no cudaMalloc / cudaFree / cudaMallocHost and no
+// allocating library call.
 //
 // The array is shared by every call on a device and keeps the previous call's
 // contents; the counters and the slot states are rewritten at the start of each
@@ -2265,8 +2274,9 @@ std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[kMaxDevices] = {};
 
 // Device address of the static scratch array on the current device.  The
-// first call on a device looks the symbol up (cudaGetSymbolAddress); that
-// first call must therefore not happen inside a stream capture.
+// first call on a device looks the symbol up (cudaGetSymbolAddress, which
+// also loads the module there under lazy loading); atrc_cuda_scene_create
+// makes that first call, outside any stream capture.
 void* noalloc_scratch(int device) {
     if (device < 0 || device >= kMaxDevices) throw CudaError("device index out of range for the static scratch");
     std::lock_guard<std::mutex> lk(g_noalloc_mutex);
@@ -2319,6 +2329,10 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         view.start = 0;
         view.count = (unsigned long long)view.SW * view.SH * spp;
         const unsigned long long total = view.count;
+        // the path state packs (view << kTileBits) | tile: a larger tile grid
+        // would spill into the view bits
+        if (size_t(view.TX) * view.TY >= (size_t(1) << kTileBits))
+            return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: film too large: more than 2^22 filter tiles");
         const int nl = shadow_rays_per_path(d.scene, *desc);
         // the array holds the counters, the view, the tile tables, then the path pool
         const size_t counters_bytes = 512;
@@ -2330,8 +2344,9 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         size_t cap = 0;
         for (size_t c = 256; pool_layout(c, c * nl, p.nkeys).total <= budget; c += 256) cap = c;
         if (cap < 1024)
-            return fail(ATRC_ERR_UNSUPPORTED, "atrc_cuda_render_noalloc: the scene's " + std::to_string(nl) +
-                                                  " lights leave room for fewer than 1024 paths in the " +
+            return fail(ATRC_ERR_UNSUPPORTED, "atrc_cuda_render_noalloc: " + std::to_string(nl) +
+                                                  " shadow / occlusion rays per path (one per light for pt, "
+                                                  "ao_sample_count for ao) leave room for fewer than 1024 paths in the " +
                                                   std::to_string(ATRC_NOALLOC_SCRATCH_BYTES) + "-byte scratch");
         if (desc->path_pool > 0) {
             if (size_t(desc->path_pool) > cap)
@@ -2354,7 +2369,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         p.view_done = nullptr;
         k_tiles<<<1, 32, 0, s>>>(p);
         Pool P = pool_from(base + counters_bytes + tiles_bytes, L, cap, shadow_cap);
-        const int gsm = grid_for(d.sm_count, 16);
+        const int gsm = grid_for(d.sm_count, d.tuned_gen_blocks);
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
         // k_init rewrites the counters and the slot states (all state that must
         // start from a known value)
@@ -2366,7 +2381,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         for (;;) {
             for (int k = 0; k < DeviceSceneImpl::kWindow; ++k) {
                 k_begin<<<1, 1, 0, s>>>(c);
-                k_generate<<<gsm, 256, 0, s>>>(d.scene, p, P, c);
+                k_generate<<<gsm, d.tuned_gen_threads, 0, s>>>(d.scene, p, P, c);
                 if (d.tuned_fetch)
                     k_extend_fetch<false, false><<<d.sm_count * ATRC_TRACE_MIN_BLOCKS, kTraceBlock, 0, s>>>(
                         d.scene, P, c, p.sort_mode, p.nkeys);
@@ -2386,7 +2401,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
                     k_shadow_fetch<false, false><<<d.sm_count * ATRC_TRACE_MIN_BLOCKS, kTraceBlock, 0, s>>>(d.scene, P, c);
                 else
                     k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
-                k_finish<<<gsm, 128, 0, s>>>(p, P, c);
+                k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, c);
                 launches += 6;
                 ext_launches += 1;
             }

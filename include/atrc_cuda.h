@@ -43,7 +43,7 @@
 extern "C" {
 #endif
 
-#define ATRC_ABI_VERSION 1
+#define ATRC_ABI_VERSION 2
 
 /* ---------------------------------------------------------------- status */
 
@@ -53,7 +53,7 @@ typedef enum AtrcStatus {
     ATRC_ERR_CONFIG       = -2,  /* malformed JSON / unknown creator / file  */
     ATRC_ERR_OUT_OF_MEMORY= -3,  /* host or device allocation failed         */
     ATRC_ERR_CUDA         = -4,  /* CUDA runtime error or no usable device   */
-    ATRC_ERR_CANCELLED    = -5,  /* the cancel flag was raised               */
+    ATRC_ERR_CANCELLED    = -5,  /* the cancel callback asked to stop        */
     ATRC_ERR_WATCHDOG     = -6,  /* a device loop hit its iteration cap      */
     ATRC_ERR_UNSUPPORTED  = -7   /* scene feature outside pt_cuda's support  */
 } AtrcStatus;
@@ -357,6 +357,13 @@ typedef struct AtrcRenderStats {
  * iterations with a percentage in [0, 100]. */
 typedef void (*AtrcProgressFn)(double percent, void* user);
 
+/* Cancel poll, called on the calling thread between wavefront iterations;
+ * a non-zero return stops the render.  The reference's cancel flag is a
+ * `std::atomic<bool> stop_rendering_` member of Renderer
+ * (src/tracer/include/agz/tracer/core/renderer.h:20), which C cannot read
+ * portably; a binding returns `stop_rendering_.load()` from this callback. */
+typedef int (*AtrcCancelFn)(void* user);
+
 /* ------------------------------------------------------------ ray queries */
 
 typedef struct AtrcRay {       /* 32 bytes */
@@ -452,11 +459,14 @@ int atrc_cuda_trace_rays_device(AtrcScene* scene, const AtrcRay* d_rays,
                                 size_t n, AtrcHit* d_hits, int mode, int exact);
 
 /* Render `desc` (a pt_cuda / pt configuration) and ADD the samples into
- * `film`.  `cancel` (may be NULL) is polled between wavefront iterations;
- * raising it ends the call with ATRC_ERR_CANCELLED after the samples already
- * taken are in the film.  `progress` (may be NULL) is called on this thread. */
+ * `film`.  `should_stop` (may be NULL) is called with `user` between
+ * wavefront iterations; a non-zero return ends the call with
+ * ATRC_ERR_CANCELLED after the samples already taken are in the film (this
+ * is the contract of Renderer::render_async / stop_async,
+ * src/tracer/src/core/core/renderer.cpp:5-38).
+ * `progress` (may be NULL) is called with the same `user` on this thread. */
 int atrc_cuda_render(AtrcScene* scene, const AtrcRenderDesc* desc,
-                     AtrcFilm* film, volatile const int* cancel,
+                     AtrcFilm* film, AtrcCancelFn should_stop,
                      AtrcProgressFn progress, void* user,
                      AtrcRenderStats* stats);
 
@@ -509,13 +519,22 @@ int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in);
  * reference, whose CPU renderer allocates per tile and per sample.
  *  - The wavefront scratch (path pool, queues, shadow rays, counters) lives in
  *    a static device array of ATRC_NOALLOC_SCRATCH_BYTES that every GPU which
- *    loads this library keeps reserved until the process exits.  The pool
- *    holds as many paths as fit (about 100k with one light); scenes whose
- *    lights leave room for fewer than 1024 paths, and a desc->path_pool above
- *    that maximum, are rejected (ATRC_ERR_UNSUPPORTED / ATRC_ERR_INVALID_ARG).
+ *    loads this library keeps reserved until the process exits.  A path
+ *    takes 192 bytes plus 48 per shadow ray it may emit in one iteration (one
+ *    per light for pt, ao_sample_count for ao), so the pool holds about 100k
+ *    paths with one light.  Calls that leave room for fewer than 1024 paths
+ *    (more than 508 lights, or ao_sample_count above 508) are rejected with
+ *    ATRC_ERR_UNSUPPORTED; a desc->path_pool above the maximum, and a film
+ *    of 2^22 or more filter tiles, with ATRC_ERR_INVALID_ARG.  Nothing is
+ *    launched before these checks.
  *  - `film` must hold device pointers (on_device = 1); samples are added.
- *  - The first call on a device looks up the array's device address; make
- *    that first call before capturing any stream.
+ *  - Under CUDA's lazy module loading the array is reserved on a device when
+ *    the library's module is first loaded there; atrc_cuda_scene_create
+ *    loads it and looks up the array's device address on the scene's device,
+ *    so this call neither allocates nor looks anything up.  Create the scene
+ *    before capturing any stream.
+ *  - The launch shapes and traversal kernels are the scene's tuning
+ *    (atrc_cuda_autotune / atrc_cuda_set_tuning), as for atrc_cuda_render.
  *  - All calls share the array and it keeps the last call's contents (each
  *    call resets the counters it needs).  Calls that overlap on the GPU race
  *    on it: serialise them.

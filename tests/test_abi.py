@@ -44,7 +44,7 @@ def test_struct_layouts_match():
 
 
 def test_abi_version():
-    assert atrc_b200.load_library().atrc_abi_version() == 1
+    assert atrc_b200.load_library().atrc_abi_version() == 2
 
 
 def test_errors_are_reported_without_a_gpu():

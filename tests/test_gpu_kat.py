@@ -82,15 +82,15 @@ def test_cancel_returns_partial_film(cornell_path):
     desc.path_pool = 1 << 16
     dev = DeviceScene(cfg)
     f = Film(256, 256)
-    flag = C.c_int(0)
+    flag = [False]
     seen = []
 
     def progress(p):
         seen.append(p)
         if len(seen) == 3:
-            flag.value = 1
+            flag[0] = True
     with pytest.raises(AtrcError, match="CANCELLED"):
-        dev.render(desc, f, cancel=flag, progress=progress)
+        dev.render(desc, f, should_stop=lambda: flag[0], progress=progress)
     done = f.weight.sum() * 4 * (0.5 - 3e-4) ** 2
     assert 0 < done < 256 * 256 * 4096
 
