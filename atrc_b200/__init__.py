@@ -235,8 +235,11 @@ class DeviceScene:
                                                          w.ctypes.data_as(fp), x.ctypes.data_as(fp)))
         return w, x
 
-    def trace_rays(self, rays: np.ndarray, mode: str = "closest", exact: bool = True) -> np.ndarray:
-        """rays: RAY_DTYPE array (or (n, 8) float32).  Returns HIT_DTYPE."""
+    def trace_rays(self, rays: np.ndarray, mode: str = "closest", exact: bool = True,
+                   isect: Optional[int] = None) -> np.ndarray:
+        """rays: RAY_DTYPE array (or (n, 8) float32).  Returns HIT_DTYPE.
+        `isect` (an AtrcIsectMode: 0 fast, 1 reference-exact Moller-Trumbore,
+        2 watertight) overrides `exact`."""
         r = np.ascontiguousarray(rays)
         if r.dtype != RAY_DTYPE:
             r = np.ascontiguousarray(r, dtype=np.float32).reshape(-1, 8).view(RAY_DTYPE).reshape(-1)
@@ -244,7 +247,7 @@ class DeviceScene:
         m = 0 if mode == "closest" else 1
         _check(load_library().atrc_cuda_trace_rays(
             self._h, r.ctypes.data_as(C.POINTER(abi.AtrcRay)), len(r), hits.ctypes.data_as(C.POINTER(abi.AtrcHit)),
-            m, 1 if exact else 0))
+            m, isect if isect is not None else (1 if exact else 0)))
         return hits
 
     def trace_rays_device(self, d_rays_ptr: int, n: int, d_hits_ptr: int, mode: str = "closest",

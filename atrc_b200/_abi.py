@@ -87,7 +87,7 @@ class AtrcRenderDesc(C.Structure):
                 ("count_traversal", C.c_int32), ("task_grid_size", C.c_int32), ("sort_mode", C.c_int32),
                 ("disney_fixed", C.c_int32), ("renderer", C.c_int32),
                 ("ao_sample_count", C.c_int32), ("ao_max_distance", C.c_float), ("ao_low", C.c_float * 3),
-                ("ao_high", C.c_float * 3), ("ao_background", C.c_float * 3), ("pad_", C.c_int32)]
+                ("ao_high", C.c_float * 3), ("ao_background", C.c_float * 3), ("isect_mode", C.c_int32)]
 
 
 class AtrcFilm(C.Structure):
@@ -172,6 +172,7 @@ PROTOTYPES = {
     "atrc_cuda_trace_rays_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int]),
     "atrc_cuda_render": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
                                    CANCEL_FN, PROGRESS_FN, C.c_void_p, C.POINTER(AtrcRenderStats)]),
+    "atrc_cuda_stream_read_gbs": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_double)]),
     "atrc_cuda_render_noalloc": (C.c_int, [C.c_void_p, C.POINTER(AtrcRenderDesc), C.POINTER(AtrcFilm),
                                            C.POINTER(AtrcRenderStats)]),
     "atrc_film_resolve": (C.c_int, [C.POINTER(AtrcFilm), C.c_int, C.c_int, c_float_p]),
@@ -192,6 +193,7 @@ PROTOTYPES = {
     "atrc_guide_train": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
     "atrc_guide_pdf": (C.c_int, [C.c_void_p, c_float_p, c_float_p, C.c_size_t, c_float_p, c_float_p]),
     "atrc_guide_train_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.c_int, C.POINTER(C.c_float)]),
+    "atrc_guide_gradients": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, c_float_p, c_float_p, c_float_p]),
     "atrc_guide_records": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "atrc_cuda_scene_bounds": (C.c_int, [C.c_void_p, c_float_p, c_float_p]),
     "atrc_cuda_subsurface_probe": (C.c_int, [C.c_void_p, c_float_p, c_float_p, C.c_int32, C.c_uint64, c_float_p,

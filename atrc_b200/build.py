@@ -38,7 +38,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-ffp
 
 HOST_SOURCES = ["host/config.cpp", "host/scene_loader.cpp", "host/file_io.cpp", "host/bvh_build.cpp",
                 "host/scene_build.cpp", "host/capi_host.cpp"]
-CUDA_SOURCES = ["cuda/render.cu", "cuda/guide.cu", "cuda/post.cu", "cuda/bvh_gpu.cu"]
+CUDA_SOURCES = ["cuda/render.cu", "cuda/guide.cu", "cuda/post.cu", "cuda/bvh_gpu.cu", "cuda/membench.cu"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -119,6 +119,7 @@ struct Env {
 struct Scene {
     const Bvh4Node* nodes;          // all 4-wide BVH nodes (every BLAS + the TLAS)
     const float* tris;              // 12 floats per triangle: A,_, B-A,_, C-A,_
+    const float* tri_bc;            // 8 floats per triangle: the exact vertices B,_, C,_ (watertight test)
     const TriShade* tri_shade;
     const uint32_t* tri_orig;       // original index per pool triangle
     const Entity* entities;

@@ -167,7 +167,7 @@ __device__ Surface make_surface(const Scene& S, const Hit& h, Vec3 wo, Vec3 wd) 
     Surface s;
     s.entity = h.entity;
     Vec3 lo, ld;
-    to_entity_space<false>(e, wo, wd, &lo, &ld);
+    to_entity_space(e, wo, wd, &lo, &ld);
     Vec3 p = lo + h.t * ld;
     if (e.kind == LEAF_TRIANGLES) {
         const TriShade& sh = S.tri_shade[h.tri];

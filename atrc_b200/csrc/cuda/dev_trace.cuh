@@ -7,9 +7,18 @@
 // transform_wrapper.cpp:51-68), the per-mesh BVH
 // (src/tracer/src/core/geometry/triangle_bvh.cpp:363-488) and the
 // Moller-Trumbore test (src/tracer/include/agz/tracer/utility/
-// triangle_aux.h:9-69).  In EXACT mode every float operation of the ray
-// transform and of Moller-Trumbore is evaluated in the reference's order
-// without fused multiply-adds, so hit distances are bit-identical.
+// triangle_aux.h:9-69).  The intersection mode (IsectMode) is a template
+// parameter of the traversal:
+//   ISECT_FAST       Moller-Trumbore as the compiler schedules it (FMAs);
+//   ISECT_EXACT      every float operation of the ray transform and of
+//                    Moller-Trumbore in the reference's order without fused
+//                    multiply-adds, so hit distances are bit-identical;
+//   ISECT_WATERTIGHT the watertight triangle test of Woop, Benthin and Wald
+//                    (JCGT 2(1), 2013) on the triangles' exact vertices, and
+//                    sphere roots without cancellation.  A ray through an
+//                    edge or vertex shared by two triangles of a mesh hits at
+//                    least one of them; Moller-Trumbore with alpha >= 0 and
+//                    alpha + beta <= 1 rounded per triangle can miss both.
 #pragma once
 
 #include <climits>
@@ -61,6 +70,8 @@ struct RayState {
 __device__ __forceinline__ float safe_rcp(float x) { return 1.0f / (fabsf(x) > 1e-20f ? x : copysignf(1e-20f, x)); }
 __device__ __forceinline__ Vec3 safe_inv(Vec3 d) { return Vec3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z)); }
 
+enum IsectMode : int { ISECT_FAST = 0, ISECT_EXACT = 1, ISECT_WATERTIGHT = 2 };
+
 // Moller-Trumbore.  ANY selects has_intersection_with_triangle (alpha <= 1
 // also checked), otherwise closest_intersection_with_triangle.
 template <bool EXACT, bool ANY>
@@ -104,6 +115,77 @@ __device__ __forceinline__ bool mt_test(const RayState& r, const float4& p0, con
     }
 }
 
+// Per-ray constants of the watertight test: the axis of the largest
+// direction component becomes z (kz), kx and ky follow cyclically and swap
+// when d[kz] < 0 (which keeps the triangles' winding), and the shear that
+// maps the direction onto +z.
+struct WtRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+__device__ __forceinline__ float comp(const Vec3& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ WtRay wt_setup(const Vec3& d) {
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    WtRay w;
+    w.kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    w.kx = w.kz == 2 ? 0 : w.kz + 1;
+    w.ky = w.kx == 2 ? 0 : w.kx + 1;
+    const float dz = comp(d, w.kz);
+    if (dz < 0) {
+        const int t = w.kx;
+        w.kx = w.ky;
+        w.ky = t;
+    }
+    w.sx = __fdiv_rn(comp(d, w.kx), dz);
+    w.sy = __fdiv_rn(comp(d, w.ky), dz);
+    w.sz = __fdiv_rn(1.0f, dz);
+    return w;
+}
+
+// Watertight ray-triangle test on the exact vertices A, B, C (Woop, Benthin
+// and Wald 2013).  The vertices are moved to the ray origin and sheared so
+// that the ray is the +z axis; the signs of the three 2D edge functions
+// decide the hit.  An edge function is evaluated from the same two rounded
+// vertex coordinates in both triangles that share the edge, with opposite
+// signs, so no ray passes between them; edge functions that round to zero
+// are evaluated again in double precision, where the products are exact.
+// Both windings are accepted (no culling).  alpha / beta are the weights of
+// B and C, as Moller-Trumbore's.  No fused multiply-adds: a contracted
+// a*b - c*d is not antisymmetric under the swap that the neighbour makes.
+template <bool ANY>
+__device__ __forceinline__ bool wt_test(const RayState& r, const WtRay& w, const float4& pa, const float4& pb,
+                                        const float4& pc, float tmax, float* t_out, float* u_out, float* v_out) {
+    const Vec3 A = sub_rn(Vec3(pa.x, pa.y, pa.z), r.o);
+    const Vec3 B = sub_rn(Vec3(pb.x, pb.y, pb.z), r.o);
+    const Vec3 C = sub_rn(Vec3(pc.x, pc.y, pc.z), r.o);
+    const float az = comp(A, w.kz), bz = comp(B, w.kz), cz = comp(C, w.kz);
+    const float Ax = __fsub_rn(comp(A, w.kx), __fmul_rn(w.sx, az)), Ay = __fsub_rn(comp(A, w.ky), __fmul_rn(w.sy, az));
+    const float Bx = __fsub_rn(comp(B, w.kx), __fmul_rn(w.sx, bz)), By = __fsub_rn(comp(B, w.ky), __fmul_rn(w.sy, bz));
+    const float Cx = __fsub_rn(comp(C, w.kx), __fmul_rn(w.sx, cz)), Cy = __fsub_rn(comp(C, w.ky), __fmul_rn(w.sy, cz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = __double2float_rn(__dsub_rn(__dmul_rn(double(Cx), double(By)), __dmul_rn(double(Cy), double(Bx))));
+        V = __double2float_rn(__dsub_rn(__dmul_rn(double(Ax), double(Cy)), __dmul_rn(double(Ay), double(Cx))));
+        W = __double2float_rn(__dsub_rn(__dmul_rn(double(Bx), double(Ay)), __dmul_rn(double(By), double(Ax))));
+    }
+    if ((U < 0 || V < 0 || W < 0) && (U > 0 || V > 0 || W > 0)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (det == 0.0f) return false;
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, __fmul_rn(w.sz, az)), __fmul_rn(V, __fmul_rn(w.sz, bz))),
+                              __fmul_rn(W, __fmul_rn(w.sz, cz)));
+    const float rcp = __fdiv_rn(1.0f, det);
+    const float t = __fmul_rn(T, rcp);
+    if (!(r.tmin <= t && t <= tmax)) return false;
+    *t_out = t;
+    *u_out = __fmul_rn(V, rcp);
+    *v_out = __fmul_rn(W, rcp);
+    return true;
+}
+
 // Sphere (sphere_aux.h:53-86) in local space.
 template <bool ANY>
 __device__ __forceinline__ bool sphere_test(const RayState& r, float radius, float tmax, float* t_out) {
@@ -113,6 +195,41 @@ __device__ __forceinline__ bool sphere_test(const RayState& r, float radius, flo
     delta = sqrtf(delta);
     const float inv2A = 0.5f / A;
     const float t0 = (-B - delta) * inv2A, t1 = (-B + delta) * inv2A;
+    if (ANY) {
+        if (r.tmin <= t0 && t0 <= tmax) { *t_out = t0; return true; }
+        if (r.tmin <= t1 && t1 <= tmax) { *t_out = t1; return true; }
+        return false;
+    }
+    if (tmax < t0 || t1 < r.tmin) return false;
+    const bool not_t0 = t0 < r.tmin;
+    if (not_t0 && t1 > tmax) return false;
+    *t_out = not_t0 ? t1 : t0;
+    return true;
+}
+
+// Sphere without cancellation (watertight mode): with b = o.d, the
+// discriminant is a (r^2 - |o - (b/a) d|^2) instead of b^2 - a (o.o - r^2),
+// which loses every digit when the ray passes far from the centre, and the
+// roots are q / a and c / q with q = -(b + sign(b) sqrt(disc)) instead of
+// (-b -+ sqrt(disc)) / a, which cancels for the root near the origin (Haines
+// et al., "Precision Improvements for Ray/Sphere Intersection", Ray Tracing
+// Gems, 2019).  Same root selection as sphere_test.
+template <bool ANY>
+__device__ __forceinline__ bool sphere_test_robust(const RayState& r, float radius, float tmax, float* t_out) {
+    const float a = dot(r.d, r.d);
+    if (!(a > 0)) return false;
+    const float b = dot(r.o, r.d);
+    const Vec3 l = r.o - (b / a) * r.d;
+    const float disc = a * (radius * radius - dot(l, l));
+    if (disc < 0) return false;
+    const float c = dot(r.o, r.o) - radius * radius;
+    const float q = -(b + copysignf(sqrtf(disc), b));
+    float t0 = q / a, t1 = q != 0.0f ? c / q : t0;
+    if (t0 > t1) {
+        const float tt = t0;
+        t0 = t1;
+        t1 = tt;
+    }
     if (ANY) {
         if (r.tmin <= t0 && t0 <= tmax) { *t_out = t0; return true; }
         if (r.tmin <= t1 && t1 <= tmax) { *t_out = t1; return true; }
@@ -175,7 +292,6 @@ __device__ __forceinline__ void sort4(float* t, int32_t* l) {
 
 // Move a world ray into an entity's primitive space (wrapper, then the
 // geometry's own transform), as transform_wrapper / TransformedGeometry do.
-template <bool EXACT>
 __device__ __forceinline__ void to_entity_space(const Entity& e, Vec3 o, Vec3 d, Vec3* lo, Vec3* ld) {
     if (e.flags & ENT_WRAP) {
         o = apply_point_rn(e.wrap_inv, o);
@@ -213,7 +329,7 @@ struct TraceCount {
 // The traversal stack is the caller's local array (kStackSize entries, the
 // deeper ones past a shared-memory ring with ATRC_STACK_RING), kept out of
 // the struct so that the scalar state stays in registers.
-template <bool EXACT, bool ANY, bool COUNT = false>
+template <int ISECT, bool ANY, bool COUNT = false>
 struct Tracer {
 #if ATRC_STACK_RING > 0
     int32_t* ring;
@@ -221,6 +337,7 @@ struct Tracer {
     int32_t* stack;
     int sp;
     RayState r;
+    WtRay w;  // watertight mode: shear of the current (world or entity) ray
     Vec3 wo, wd, winv;
     float tmin0, best_t, best_u, best_v;
     int32_t best_e, best_tri, cur_entity, link, held;
@@ -238,6 +355,7 @@ struct Tracer {
         sp = 0;
         wo = o; wd = d; winv = safe_inv(d);
         r.o = o; r.d = d; r.inv = winv; r.tmin = tmin; r.tmax = tmax;
+        if (ISECT == ISECT_WATERTIGHT) w = wt_setup(d);
         tmin0 = tmin;
         best_t = tmax; best_u = 0; best_v = 0;
         best_e = -1; best_tri = -1; cur_entity = -1;
@@ -284,19 +402,22 @@ struct Tracer {
                 const Entity& e = S.entities[ei];
                 if (COUNT) cnt->ents++;
                 Vec3 lo, ld;
-                to_entity_space<EXACT>(e, wo, wd, &lo, &ld);
+                to_entity_space(e, wo, wd, &lo, &ld);
                 if (e.kind == LEAF_TRIANGLES) {
                     push(next);
                     push(kSentinel);
                     r.o = lo; r.d = ld; r.inv = safe_inv(ld);
+                    if (ISECT == ISECT_WATERTIGHT) w = wt_setup(ld);
                     cur_entity = ei;
                     return e.blas_root;
                 }
                 RayState lr;
                 lr.o = lo; lr.d = ld; lr.tmin = tmin0; lr.inv = Vec3();
                 float t;
-                const bool h = e.kind == LEAF_SPHERE ? sphere_test<ANY>(lr, e.radius, best_t, &t)
-                                                     : disk_test(lr, e.radius, best_t, &t);
+                const bool h = e.kind == LEAF_SPHERE
+                                   ? (ISECT == ISECT_WATERTIGHT ? sphere_test_robust<ANY>(lr, e.radius, best_t, &t)
+                                                                : sphere_test<ANY>(lr, e.radius, best_t, &t))
+                                   : disk_test(lr, e.radius, best_t, &t);
                 if (h) {
                     if (ANY) { best_e = ei; best_t = t; found = true; return kDone; }
                     if (t < best_t || (t == best_t && ei < best_e)) {
@@ -310,10 +431,16 @@ struct Tracer {
         for (int32_t k = 0; k < count; ++k) {
             const int32_t ti = first + k;
             const float4* tp = reinterpret_cast<const float4*>(S.tris) + size_t(ti) * 3;
-            const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
             if (COUNT) cnt->tris++;
             float t, u, v;
-            if (mt_test<EXACT, ANY>(r, p0, p1, p2, best_t, &t, &u, &v)) {
+            bool hit;
+            if (ISECT == ISECT_WATERTIGHT) {
+                const float4* bc = reinterpret_cast<const float4*>(S.tri_bc) + size_t(ti) * 2;
+                hit = wt_test<ANY>(r, w, __ldg(tp), __ldg(bc), __ldg(bc + 1), best_t, &t, &u, &v);
+            } else {
+                hit = mt_test<ISECT == ISECT_EXACT, ANY>(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), best_t, &t, &u, &v);
+            }
+            if (hit) {
                 if (ANY) { best_e = cur_entity; best_t = t; found = true; return kDone; }
                 if (t < best_t || (t == best_t && (cur_entity < best_e || (cur_entity == best_e && ti < best_tri)))) {
                     best_t = t; best_e = cur_entity; best_tri = ti; best_u = u; best_v = v;
@@ -377,6 +504,7 @@ struct Tracer {
             if (link == kSentinel) {
                 cur_entity = -1;
                 r.o = wo; r.d = wd; r.inv = winv;
+                if (ISECT == ISECT_WATERTIGHT) w = wt_setup(wd);
                 link = pop();
                 continue;
             }
@@ -406,11 +534,11 @@ struct Tracer {
 
 // Trace one ray to the end.  Returns true if something was hit (ANY:
 // occluded); `watchdog` is set when the traversal stack would overflow.
-template <bool EXACT, bool ANY, bool COUNT = false>
+template <int ISECT, bool ANY, bool COUNT = false>
 __device__ bool trace_ray(const Scene& S, Vec3 wo, Vec3 wd, float tmin, float tmax, Hit* hit, int* watchdog,
                           TraceCount* cnt = nullptr) {
     int32_t stack[kStackSize];
-    Tracer<EXACT, ANY, COUNT> t;
+    Tracer<ISECT, ANY, COUNT> t;
     t.init(S, stack, wo, wd, tmin, tmax);
     while (!t.step(S, watchdog, cnt)) {
     }
@@ -427,7 +555,7 @@ __device__ bool trace_entity(const Scene& S, int32_t ei, Vec3 wo, Vec3 wd, float
                              int* watchdog) {
     const Entity& e = S.entities[ei];
     Vec3 lo, ld;
-    to_entity_space<EXACT>(e, wo, wd, &lo, &ld);
+    to_entity_space(e, wo, wd, &lo, &ld);
     if (e.kind != LEAF_TRIANGLES) {
         RayState lr;
         lr.o = lo; lr.d = ld; lr.tmin = tmin; lr.tmax = tmax; lr.inv = Vec3();

@@ -976,6 +976,48 @@ int atrc_guide_train_records(AtrcGuide* g, const float* records, size_t n, int s
     });
 }
 
+// The loss gradients of one batch of host records (n x 24 floats, at most
+// the record capacity) at the current parameters: the training kernel
+// without the Adam step.  The gradient buffers are read back and cleared, so
+// the parameters and the optimiser state are untouched.
+int atrc_guide_gradients(AtrcGuide* g, const float* records, size_t n, float* grad_weights, float* grad_table,
+                         float* loss) {
+    if (!g || !records || n < kTile || !grad_weights || !grad_table)
+        return gfail(ATRC_ERR_INVALID_ARG, "atrc_guide_gradients: invalid argument");
+    return gguarded([&] {
+        GuideImpl& G = g->impl;
+        CK(cudaSetDevice(G.device));
+        if (n > size_t(G.desc.record_capacity)) throw std::runtime_error("more records than the guide's capacity");
+        cudaStream_t s = G.stream;
+        CK(cudaMemcpyAsync(G.records.p, records, n * sizeof(GuideRecord), cudaMemcpyHostToDevice, s));
+        float* sc = G.scratch.as<float>();
+        CK(cudaMemsetAsync(sc, 0, 2 * sizeof(float), s));
+        CK(cudaMemsetAsync(G.w_g.p, 0, kWeights * sizeof(float), s));
+        CK(cudaMemsetAsync(G.t_g.p, 0, G.table_n * sizeof(float), s));
+        const GuideRecord* rec = G.records.as<GuideRecord>();
+        k_target_sum<<<G.sm_count * 2, 256, 0, s>>>(rec, int(n), sc);
+        TrainArgs a;
+        a.rec = rec;
+        a.n = int(n);
+        a.weight_sum = sc;
+        a.grad_w = G.w_g.as<float>();
+        a.grad_table = G.t_g.as<float>();
+        a.loss = sc + 1;
+        const int tiles = int((n + kTile - 1) / kTile);
+        k_guide_train<<<std::min(tiles, G.sm_count), kTile, kTrSmem, s>>>(G.view(), a, G.err.as<int>());
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(grad_weights, G.w_g.p, kWeights * sizeof(float), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(grad_table, G.t_g.p, G.table_n * sizeof(float), cudaMemcpyDeviceToHost, s));
+        float l = 0;
+        CK(cudaMemcpyAsync(&l, sc + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemsetAsync(G.w_g.p, 0, kWeights * sizeof(float), s));
+        CK(cudaMemsetAsync(G.t_g.p, 0, G.table_n * sizeof(float), s));
+        check_err(G, "atrc_guide_gradients");
+        if (loss) *loss = l;
+        return int(ATRC_OK);
+    });
+}
+
 // Copy the records of the last recording render to the host.
 int atrc_guide_records(AtrcGuide* g, float* records, size_t cap, size_t* count) {
     if (!g || !count) return gfail(ATRC_ERR_INVALID_ARG, "atrc_guide_records: null argument");

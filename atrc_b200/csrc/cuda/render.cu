@@ -73,7 +73,7 @@ __device__ __forceinline__ int warp_append(int* counter, bool pred) {
 }
 
 // ------------------------------------------------------------ ray queries
-template <bool EXACT, bool ANY>
+template <int ISECT, bool ANY>
 __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_trace_rays(Scene S, const AtrcRay* __restrict__ rays, size_t n, AtrcHit* __restrict__ hits,
                              int* watchdog) {
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_trace_ra
         Hit h;
         h.entity = -1;
         int wd = 0;
-        const bool hit = trace_ray<EXACT, ANY>(S, Vec3(q.o[0], q.o[1], q.o[2]), Vec3(q.d[0], q.d[1], q.d[2]), q.t_min,
+        const bool hit = trace_ray<ISECT, ANY>(S, Vec3(q.o[0], q.o[1], q.o[2]), Vec3(q.d[0], q.d[1], q.d[2]), q.t_min,
                                                q.t_max, &h, &wd);
         if (wd) atomicMax(watchdog, wd);
         AtrcHit r;
@@ -514,7 +514,7 @@ __global__ void k_sort_scatter(Pool P, Counters* c, int nkeys) {
     }
 }
 
-template <bool EXACT, bool COUNT>
+template <int ISECT, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(Scene S, Pool P, Counters* c,
                                                                               int sort_mode, int nkeys) {
     const int n = c->n_ext, in = c->in;
@@ -526,7 +526,7 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(S
         h.entity = -1;
         h.tri = -1;
         int wd = 0;
-        const bool hit = trace_ray<EXACT, false, COUNT>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd, &tc);
+        const bool hit = trace_ray<ISECT, false, COUNT>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd, &tc);
         if (wd) atomicMax(&c->watchdog, wd);
         P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.entity : -1));
         P.hit_tri[slot] = h.tri;
@@ -544,14 +544,14 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend(S
 // Results, sort keys and counts are those of k_extend.
 constexpr int kRefillLanes = 16;
 
-template <bool EXACT, bool COUNT>
+template <int ISECT, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend_fetch(Scene S, Pool P, Counters* c,
                                                                                     int sort_mode, int nkeys) {
     const int n = c->n_ext, in = c->in;
     const int lane = threadIdx.x & 31;
     TraceCount tc{0, 0, 0};
     int32_t stack[kStackSize];
-    Tracer<EXACT, false, COUNT> tr;
+    Tracer<ISECT, false, COUNT> tr;
     int i = -1, slot = -1, wd = 0;
     bool drained = false;
     for (;;) {
@@ -1114,7 +1114,7 @@ __global__ void __launch_bounds__(128) k_subsurface(Scene S, Params p, Pool P, C
     }
 }
 
-template <bool EXACT, bool COUNT>
+template <int ISECT, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, ATRC_SHADOW_MIN_BLOCKS) k_shadow(Scene S, Pool P, Counters* c) {
     const int n = min(c->n_shadow, P.shadow_cap);
     TraceCount tc{0, 0, 0};
@@ -1122,7 +1122,7 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_SHADOW_MIN_BLOCKS) k_shadow(
         const float4 o = P.sh_o[i], d = P.sh_d[i];
         Hit h;
         int wd = 0;
-        const bool occluded = trace_ray<EXACT, true, COUNT>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd, &tc);
+        const bool occluded = trace_ray<ISECT, true, COUNT>(S, xyz(o), xyz(d), o.w, d.w, &h, &wd, &tc);
         if (wd) atomicMax(&c->watchdog, wd);
         if (!occluded) {
             const float4 cc = P.sh_c[i];
@@ -1140,13 +1140,13 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_SHADOW_MIN_BLOCKS) k_shadow(
 // step their any-hit traversals round by round and refill the lanes whose
 // rays are done (occluded at the first hit, or through the scene) from the
 // shadow queue.  Contributions and counts are those of k_shadow.
-template <bool EXACT, bool COUNT>
+template <int ISECT, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_shadow_fetch(Scene S, Pool P, Counters* c) {
     const int n = min(c->n_shadow, P.shadow_cap);
     const int lane = threadIdx.x & 31;
     TraceCount tc{0, 0, 0};
     int32_t stack[kStackSize];
-    Tracer<EXACT, true, COUNT> tr;
+    Tracer<ISECT, true, COUNT> tr;
     int i = -1, wd = 0;
     bool drained = false;
     for (;;) {
@@ -1311,7 +1311,7 @@ struct DeviceSceneImpl {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     Scene scene{};
-    DevBuf nodes, tris, tri_shade, tri_orig, entities, tlas_order, materials, tex2d, tex3d, texels, media, alias_prob,
+    DevBuf nodes, tris, tri_bc, tri_shade, tri_orig, entities, tlas_order, materials, tex2d, tex3d, texels, media, alias_prob,
         alias_idx, env_probs, env_alias_prob, env_alias_idx;
     DevBuf watchdog;
     DevBuf tiles;  // tile tables of the film's sample grid
@@ -1614,6 +1614,7 @@ int atrc_cuda_scene_create(const AtrcSceneDesc* desc, AtrcScene** out) {
         Scene S = hs->scene;
         S.nodes = upload(d.nodes, hs->nodes, s);
         S.tris = upload(d.tris, hs->tris, s);
+        S.tri_bc = upload(d.tri_bc, hs->tri_bc, s);
         S.tri_shade = upload(d.tri_shade, hs->tri_shade, s);
         S.tri_orig = upload(d.tri_orig, hs->tri_orig, s);
         S.entities = upload(d.entities, hs->entities, s);
@@ -1647,18 +1648,25 @@ int atrc_cuda_trace_rays_device(AtrcScene* scene, const AtrcRay* d_rays, size_t 
                                 int exact) {
     if (!scene || (n && (!d_rays || !d_hits))) return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_trace_rays: null argument");
     if (mode != ATRC_QUERY_CLOSEST && mode != ATRC_QUERY_ANY) return fail(ATRC_ERR_INVALID_ARG, "bad query mode");
+    if (exact < ATRC_ISECT_FAST || exact > ATRC_ISECT_WATERTIGHT)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_trace_rays: bad intersection mode");
     return guarded([&] {
         DeviceSceneImpl& d = scene->impl;
         if (n == 0) return int(ATRC_OK);
         CK(cudaMemsetAsync(d.watchdog.p, 0, sizeof(int), d.stream));
         const int grid = grid_for(d.sm_count, 8);
         int* wd = d.watchdog.as<int>();
+        cudaStream_t st = d.stream;
         if (mode == ATRC_QUERY_ANY) {
-            if (exact) k_trace_rays<true, true><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
-            else k_trace_rays<false, true><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
+            if (exact == ATRC_ISECT_WATERTIGHT)
+                k_trace_rays<ISECT_WATERTIGHT, true><<<grid, 128, 0, st>>>(d.scene, d_rays, n, d_hits, wd);
+            else if (exact == ATRC_ISECT_EXACT) k_trace_rays<ISECT_EXACT, true><<<grid, 128, 0, st>>>(d.scene, d_rays, n, d_hits, wd);
+            else k_trace_rays<ISECT_FAST, true><<<grid, 128, 0, st>>>(d.scene, d_rays, n, d_hits, wd);
         } else {
-            if (exact) k_trace_rays<true, false><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
-            else k_trace_rays<false, false><<<grid, 128, 0, d.stream>>>(d.scene, d_rays, n, d_hits, wd);
+            if (exact == ATRC_ISECT_WATERTIGHT)
+                k_trace_rays<ISECT_WATERTIGHT, false><<<grid, 128, 0, st>>>(d.scene, d_rays, n, d_hits, wd);
+            else if (exact == ATRC_ISECT_EXACT) k_trace_rays<ISECT_EXACT, false><<<grid, 128, 0, st>>>(d.scene, d_rays, n, d_hits, wd);
+            else k_trace_rays<ISECT_FAST, false><<<grid, 128, 0, st>>>(d.scene, d_rays, n, d_hits, wd);
         }
         CK(cudaGetLastError());
         int w = 0;
@@ -1695,7 +1703,7 @@ __global__ void k_subsurface_probe(Scene S, Vec3 o, Vec3 d, int n, uint64_t seed
     Vec3 wv, xp;
     Hit h;
     int wd = 0;
-    if (!trace_ray<false, false>(S, o, d, 0.0f, INFINITY, &h, &wd)) {
+    if (!trace_ray<ISECT_FAST, false>(S, o, d, 0.0f, INFINITY, &h, &wd)) {
         if (i == 0) *status = 1;
     } else {
         const Surface s = make_surface(S, h, o, d);
@@ -1731,6 +1739,9 @@ static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: invalid renderer");
     if (desc->renderer == ATRC_RENDERER_AO && (desc->ao_sample_count <= 0 || desc->ao_sample_count > 4096))
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render: ao_sample_count must be in [1, 4096]");
+    if (desc->isect_mode != ATRC_ISECT_FAST && desc->isect_mode != ATRC_ISECT_WATERTIGHT)
+        return fail(ATRC_ERR_INVALID_ARG,
+                    "atrc_cuda_render: isect_mode must be ATRC_ISECT_FAST (0) or ATRC_ISECT_WATERTIGHT (2)");
     return ATRC_OK;
 }
 
@@ -1884,7 +1895,10 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     static_assert(sizeof(Counters) <= 512, "pinned counter buffer too small");
     Counters* pinned = static_cast<Counters*>(d.pinned_counters);
     int status = ATRC_OK;
-    const bool count = desc->count_traversal != 0;
+    // the traversal counts (count_traversal) are taken with Moller-Trumbore
+    // only; a watertight render ignores them
+    const bool wt = desc->isect_mode == ATRC_ISECT_WATERTIGHT;
+    const bool count = desc->count_traversal != 0 && !wt;
     // The bounce loop runs in windows of `window` iterations.  One window
     // (6 kernels per iteration, the timing events and the counter
     // read-back) is captured once per call as a CUDA graph and relaunched
@@ -1900,12 +1914,15 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             CK(cudaEventRecordWithFlags(kev[k * 4 + 0], s, cudaEventRecordExternal));
             if (d.tuned_fetch) {
                 const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
-                if (count) k_extend_fetch<false, true><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
-                else k_extend_fetch<false, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                if (wt) k_extend_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                else if (count) k_extend_fetch<ISECT_FAST, true><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                else k_extend_fetch<ISECT_FAST, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+            } else if (wt) {
+                k_extend<ISECT_WATERTIGHT, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
             } else if (count) {
-                k_extend<false, true><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                k_extend<ISECT_FAST, true><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
             } else {
-                k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                k_extend<ISECT_FAST, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
             }
             if (p.sort_mode != ATRC_SORT_NONE) {
                 k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
@@ -1921,12 +1938,15 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
             if (d.tuned_shadow_fetch) {
                 const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
-                if (count) k_shadow_fetch<false, true><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
-                else k_shadow_fetch<false, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+                if (wt) k_shadow_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+                else if (count) k_shadow_fetch<ISECT_FAST, true><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+                else k_shadow_fetch<ISECT_FAST, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+            } else if (wt) {
+                k_shadow<ISECT_WATERTIGHT, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
             } else if (count) {
-                k_shadow<false, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+                k_shadow<ISECT_FAST, true><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
             } else {
-                k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+                k_shadow<ISECT_FAST, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
             }
             CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
             k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, c);
@@ -2315,6 +2335,8 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: invalid renderer");
     if (desc->renderer == ATRC_RENDERER_AO && (desc->ao_sample_count <= 0 || desc->ao_sample_count > 4096))
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: ao_sample_count must be in [1, 4096]");
+    if (desc->isect_mode != ATRC_ISECT_FAST && desc->isect_mode != ATRC_ISECT_WATERTIGHT)
+        return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: isect_mode must be 0 or 2");
     return guarded([&] {
         DeviceSceneImpl& d = scene->impl;
         CK(cudaSetDevice(d.device));
@@ -2334,6 +2356,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         if (size_t(view.TX) * view.TY >= (size_t(1) << kTileBits))
             return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: film too large: more than 2^22 filter tiles");
         const int nl = shadow_rays_per_path(d.scene, *desc);
+        const bool wt = desc->isect_mode == ATRC_ISECT_WATERTIGHT;
         // the array holds the counters, the view, the tile tables, then the path pool
         const size_t counters_bytes = 512;
         const size_t view_bytes = (sizeof(View) + 255) & ~size_t(255);
@@ -2382,11 +2405,15 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
             for (int k = 0; k < DeviceSceneImpl::kWindow; ++k) {
                 k_begin<<<1, 1, 0, s>>>(c);
                 k_generate<<<gsm, d.tuned_gen_threads, 0, s>>>(d.scene, p, P, c);
-                if (d.tuned_fetch)
-                    k_extend_fetch<false, false><<<d.sm_count * ATRC_TRACE_MIN_BLOCKS, kTraceBlock, 0, s>>>(
-                        d.scene, P, c, p.sort_mode, p.nkeys);
+                const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
+                if (d.tuned_fetch && wt)
+                    k_extend_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                else if (d.tuned_fetch)
+                    k_extend_fetch<ISECT_FAST, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                else if (wt)
+                    k_extend<ISECT_WATERTIGHT, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
                 else
-                    k_extend<false, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
+                    k_extend<ISECT_FAST, false><<<g_path, 128, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
                 if (p.sort_mode != ATRC_SORT_NONE) {
                     k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
                     k_sort_scatter<<<d.sm_count * 8, 128, 0, s>>>(P, c, p.nkeys);
@@ -2397,10 +2424,14 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
                     k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
                     launches += 1;
                 }
-                if (d.tuned_shadow_fetch)
-                    k_shadow_fetch<false, false><<<d.sm_count * ATRC_TRACE_MIN_BLOCKS, kTraceBlock, 0, s>>>(d.scene, P, c);
+                if (d.tuned_shadow_fetch && wt)
+                    k_shadow_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+                else if (d.tuned_shadow_fetch)
+                    k_shadow_fetch<ISECT_FAST, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
+                else if (wt)
+                    k_shadow<ISECT_WATERTIGHT, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 else
-                    k_shadow<false, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
+                    k_shadow<ISECT_FAST, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
                 k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, c);
                 launches += 6;
                 ext_launches += 1;

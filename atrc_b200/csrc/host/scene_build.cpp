@@ -54,9 +54,15 @@ Vec3 dpdu_as_ex(Vec3 ba, Vec3 ca, Vec2 tba, Vec2 tca, Vec3 nor) {
     return normalize(m11 * inv_det * ba - m01 * inv_det * ca);
 }
 
-void put_tri(HostScene* hs, Vec3 a, Vec3 ba, Vec3 ca, const dev::TriShade& sh, uint32_t orig) {
+// A triangle in leaf order: A, B - A, C - A for Moller-Trumbore (the edges
+// as the reference computes them) and the exact vertices B, C for the
+// watertight test, which needs every shared vertex bit-identical in the
+// triangles that share it (A + (B - A) does not round back to B).
+void put_tri(HostScene* hs, Vec3 a, Vec3 ba, Vec3 ca, Vec3 b, Vec3 c, const dev::TriShade& sh, uint32_t orig) {
     const float t[12] = {a.x, a.y, a.z, 0, ba.x, ba.y, ba.z, 0, ca.x, ca.y, ca.z, 0};
     hs->tris.insert(hs->tris.end(), t, t + 12);
+    const float v[8] = {b.x, b.y, b.z, 0, c.x, c.y, c.z, 0};
+    hs->tri_bc.insert(hs->tri_bc.end(), v, v + 8);
     hs->tri_shade.push_back(sh);
     hs->tri_orig.push_back(orig);
 }
@@ -161,17 +167,23 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
         LeafInfo& L = leaves[gi];
         const float* m = g.transform.m;
         std::vector<BuildPrim> prims;
-        std::vector<Vec3> ta, tba, tca;
+        std::vector<Vec3> ta, tba, tca, tb, tc;
         std::vector<dev::TriShade> tsh;
         std::vector<uint32_t> torig;
-        auto add_tri = [&](Vec3 a, Vec3 ba, Vec3 ca, const dev::TriShade& sh, uint32_t orig) {
+        // (a, b, c): the exact vertices; ba = b - a and ca = c - a as computed
+        // by the caller
+        auto add_tri = [&](Vec3 a, Vec3 ba, Vec3 ca, Vec3 b_exact, Vec3 c_exact, const dev::TriShade& sh,
+                           uint32_t orig) {
             BuildPrim bp;
             Vec3 b = a + ba, c = a + ca;
             Vec3 lo = vmin(a, vmin(b, c)), hi = vmax(a, vmax(b, c));
+            lo = vmin(lo, vmin(b_exact, c_exact));
+            hi = vmax(hi, vmax(b_exact, c_exact));
             bp.lo[0] = lo.x; bp.lo[1] = lo.y; bp.lo[2] = lo.z;
             bp.hi[0] = hi.x; bp.hi[1] = hi.y; bp.hi[2] = hi.z;
             prims.push_back(bp);
             ta.push_back(a); tba.push_back(ba); tca.push_back(ca);
+            tb.push_back(b_exact); tc.push_back(c_exact);
             tsh.push_back(sh);
             torig.push_back(orig);
         };
@@ -200,7 +212,7 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
                 set3(sh.x, x); set3(sh.z, z);
                 set3(sh.n_a, na); set3(sh.n_ba, nb - na); set3(sh.n_ca, nc - na);
                 set2(sh.t_a, uv[0]); set2(sh.t_ba, tba2); set2(sh.t_ca, tca2);
-                add_tri(a, ba, ca, sh, uint32_t(t));
+                add_tri(a, ba, ca, p[1], p[2], sh, uint32_t(t));
             }
         } else if (g.type == ATRC_GEOM_QUAD) {
             Vec3 A = apply_point_rn(m, V(g.p[0])), B = apply_point_rn(m, V(g.p[1]));
@@ -225,8 +237,8 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
             // geometric frame (quad.cpp:36,48 user_coord = geometry_coord)
             s1.pad[0] = 1.0f;  // marks "user frame = geometric frame"
             s2.pad[0] = 1.0f;
-            add_tri(A, ba, ca, s1, 0);
-            add_tri(A, ca, da, s2, 1);
+            add_tri(A, ba, ca, B, C, s1, 0);
+            add_tri(A, ca, da, C, D, s2, 1);
             L.bound = Bound();
             L.bound.add(A); L.bound.add(A + ba); L.bound.add(A + ca); L.bound.add(A + da);
             widen_degenerate(L.bound);
@@ -242,7 +254,7 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
             set3(s.x, x); set3(s.z, z); set3(s.n_a, z);
             set2(s.t_a, ta2); set2(s.t_ba, tba2); set2(s.t_ca, tca2);
             s.pad[0] = 1.0f;
-            add_tri(a, ba, ca, s, 0);
+            add_tri(a, ba, ca, V(g.p[1]), V(g.p[2]), s, 0);
             L.bound = Bound();
             L.bound.add(apply_point_rn(m, a)); L.bound.add(apply_point_rn(m, a + ba)); L.bound.add(apply_point_rn(m, a + ca));
             widen_degenerate(L.bound);
@@ -311,7 +323,7 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
         for (uint32_t k : bvh.order) {
             if (k >= prims.size() || placed[k]) throw std::runtime_error("BVH leaf order is not a permutation");
             placed[k] = 1;
-            put_tri(hs, ta[k], tba[k], tca[k], tsh[k], torig[k]);
+            put_tri(hs, ta[k], tba[k], tca[k], tb[k], tc[k], tsh[k], torig[k]);
             L.tri_areas.push_back(double(tri_area(tba[k], tca[k])));
         }
     }

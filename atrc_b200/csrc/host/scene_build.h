@@ -15,6 +15,7 @@ namespace atrc {
 struct HostScene {
     std::vector<Bvh4Node> nodes;  // every 4-wide node (each BLAS, then the TLAS)
     std::vector<float> tris;          // 12 per triangle
+    std::vector<float> tri_bc;        // 8 per triangle: exact B and C
     std::vector<dev::TriShade> tri_shade;
     std::vector<uint32_t> tri_orig;
     std::vector<dev::Entity> entities;

@@ -699,6 +699,7 @@ public:
         d.path_pool = rp.child_int_or("path_pool", 0);
         d.sort_mode = rp.child_int_or("sort_mode", ATRC_SORT_AUTO);
         d.disney_fixed = rp.child_int_or("disney_fixed", 0) != 0;
+        d.isect_mode = rp.child_int_or("watertight", 0) != 0 ? ATRC_ISECT_WATERTIGHT : ATRC_ISECT_FAST;
         if (d.sort_mode < ATRC_SORT_AUTO || d.sort_mode > ATRC_SORT_MATERIAL)
             throw ConfigError("invalid sort_mode value (-1 auto, 0 none, 1 material type, 2 material)");
         d.first_spp = 0;

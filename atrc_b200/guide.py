@@ -111,6 +111,17 @@ class Guide:
         _check(load_library().atrc_guide_train_records(self._h, _fp(r), len(r), steps, C.byref(loss)))
         return loss.value
 
+    def gradients(self, records: np.ndarray) -> tuple[np.ndarray, np.ndarray, float]:
+        """Loss gradients of the weights and the table over `records` at the
+        current parameters (atrc_guide_gradients: no Adam step)."""
+        r = np.ascontiguousarray(records, np.float32).reshape(-1, RECORD_FLOATS)
+        inf = self.info()
+        gw = np.empty(inf["weights"], np.float32)
+        gt = np.empty(inf["table_floats"], np.float32)
+        loss = C.c_float()
+        _check(load_library().atrc_guide_gradients(self._h, _fp(r), len(r), _fp(gw), _fp(gt), C.byref(loss)))
+        return gw, gt, loss.value
+
     def records(self) -> np.ndarray:
         n = C.c_size_t()
         lib = load_library()

@@ -108,15 +108,61 @@ def _normals_from_faces(v: np.ndarray, f: np.ndarray) -> np.ndarray:
     return vn / np.where(ln > 0, ln, 1)
 
 
-def icosphere(level: int, seed: int, amplitude: float = 0.05) -> tuple:
-    """Unit icosphere subdivided `level` times, radially displaced by 5-octave fBm."""
+def _icosahedron() -> tuple:
     t = (1 + 5 ** 0.5) / 2
     v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
                   [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
     f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
                   [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
                   [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
-    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v / np.linalg.norm(v, axis=1, keepdims=True), f
+
+
+def _displace(v: np.ndarray, f: np.ndarray, seed: int, amplitude: float) -> tuple:
+    disp = 1 + amplitude * fbm3(v * 2.0, seed, 5)
+    v = v * disp[:, None]
+    n = _normals_from_faces(v, f)
+    d = v / np.linalg.norm(v, axis=1, keepdims=True)
+    uv = np.stack([0.5 + np.arctan2(d[:, 1], d[:, 0]) / (2 * np.pi), np.arccos(np.clip(d[:, 2], -1, 1)) / np.pi], 1)
+    return v.astype(np.float32), n.astype(np.float32), uv.astype(np.float32), f
+
+
+def geodesic_sphere(freq: int, seed: int, amplitude: float = 0.05) -> tuple:
+    """Unit sphere from the icosahedron with every face cut into freq^2
+    triangles (class-I geodesic subdivision, 20 freq^2 triangles: 200,000 for
+    freq 100), radially displaced by 5-octave fBm."""
+    v0, f0 = _icosahedron()
+    n = int(freq)
+    # barycentric lattice of one face: point (i, j) = A + (B - A) i/n + (C - A) j/n
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    keep = ii + jj <= n
+    ii, jj = ii[keep], jj[keep]
+    lattice = -np.ones((n + 1, n + 1), np.int64)
+    lattice[ii, jj] = np.arange(len(ii))
+    up = [(i, j) for i in range(n) for j in range(n - i)]
+    down = [(i, j) for i in range(n - 1) for j in range(n - 1 - i)]
+    ui, uj = np.array(up).T
+    tri = [np.stack([lattice[ui, uj], lattice[ui + 1, uj], lattice[ui, uj + 1]], 1)]
+    if down:
+        di, dj = np.array(down).T
+        tri.append(np.stack([lattice[di + 1, dj], lattice[di + 1, dj + 1], lattice[di, dj + 1]], 1))
+    local = np.concatenate(tri)
+    pts, faces = [], []
+    for k, (a, b, c) in enumerate(f0):
+        A, B, C = v0[a], v0[b], v0[c]
+        P = A + np.outer(ii / n, B - A) + np.outer(jj / n, C - A)
+        pts.append(P / np.linalg.norm(P, axis=1, keepdims=True))
+        faces.append(local + k * len(ii))
+    pts = np.concatenate(pts)
+    faces = np.concatenate(faces)
+    # points on shared edges and corners are computed once per face: merge them
+    _, first, inv = np.unique(np.round(pts * 1e7).astype(np.int64), axis=0, return_index=True, return_inverse=True)
+    return _displace(pts[first], inv.reshape(-1)[faces], seed, amplitude)
+
+
+def icosphere(level: int, seed: int, amplitude: float = 0.05) -> tuple:
+    """Unit icosphere subdivided `level` times, radially displaced by 5-octave fBm."""
+    v, f = _icosahedron()
     for _ in range(level):
         e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
         e.sort(axis=1)
@@ -132,12 +178,7 @@ def icosphere(level: int, seed: int, amplitude: float = 0.05) -> tuple:
         m01, m12, m20 = inv[:nf] + base, inv[nf:2 * nf] + base, inv[2 * nf:] + base
         f = np.concatenate([np.stack([f[:, 0], m01, m20], 1), np.stack([f[:, 1], m12, m01], 1),
                             np.stack([f[:, 2], m20, m12], 1), np.stack([m01, m12, m20], 1)])
-    disp = 1 + amplitude * fbm3(v * 2.0, seed, 5)
-    v = v * disp[:, None]
-    n = _normals_from_faces(v, f)
-    d = v / np.linalg.norm(v, axis=1, keepdims=True)
-    uv = np.stack([0.5 + np.arctan2(d[:, 1], d[:, 0]) / (2 * np.pi), np.arccos(np.clip(d[:, 2], -1, 1)) / np.pi], 1)
-    return v.astype(np.float32), n.astype(np.float32), uv.astype(np.float32), f
+    return _displace(v, f, seed, amplitude)
 
 
 def heightfield(res: int, seed: int, amplitude: float = 0.15) -> tuple:
@@ -327,14 +368,18 @@ def instanced_disney(out_dir: Path | None = None, seed: int = 1001, width: int =
 
 # ----------------------------------------------------------- media (cfg 2)
 def media_scene(out_dir: Path | None = None, seed: int = 1002, width: int = 1024, height: int = 1024, spp: int = 512,
-                max_depth: int = 32, renderer: str = "pt_cuda", grid_res: int = 128, sphere_level: int = 6) -> Path:
+                max_depth: int = 32, renderer: str = "pt_cuda", grid_res: int = 128, sphere_level: int | None = None,
+                sphere_freq: int = 100) -> Path:
     """A homogeneous box medium (sigma_a 0.05, sigma_s 0.5, g 0.6) and a 128^3
     fBm density grid scaled to sigma_t in [0, 8] (albedo 0.9, delta tracking)
-    enclosing a displaced sphere, two quad lights and the procedural sky.
+    enclosing a displaced sphere (a frequency-100 geodesic sphere of 200,000
+    triangles by default; `sphere_level` selects a recursively subdivided
+    icosphere instead), two quad lights and the procedural sky.
     The medium boxes float 0.02 above the floor: coplanar boundaries would make
     the medium of the segments below them depend on how ties between equal
     hit distances are broken, which the reference leaves to traversal order."""
-    out = Path(out_dir) if out_dir else cache_dir() / f"media_{seed}_{grid_res}_{sphere_level}"
+    sphere_tag = f"l{sphere_level}" if sphere_level is not None else f"f{sphere_freq}"
+    out = Path(out_dir) if out_dir else cache_dir() / f"media_{seed}_{grid_res}_{sphere_tag}"
     out.mkdir(parents=True, exist_ok=True)
     rng = np.random.default_rng(seed)
     env = out / "sky.pfm"
@@ -347,9 +392,11 @@ def media_scene(out_dir: Path | None = None, seed: int = 1002, width: int = 1024
         d = fbm3(np.stack([X, Y, Z], -1) * 4, seed, 5)
         d = (d - d.min()) / (d.max() - d.min()) * 8.0
         write_grid(g, d.astype(np.float32))
-    sph = out / "sphere.bm"
+    sph = out / f"sphere_{sphere_tag}.bm"
     if not sph.exists():
-        _mesh_to_bm(sph, icosphere(sphere_level, seed + 5, 0.05))
+        mesh = icosphere(sphere_level, seed + 5, 0.05) if sphere_level is not None else \
+            geodesic_sphere(sphere_freq, seed + 5, 0.05)
+        _mesh_to_bm(sph, mesh)
     unit_box = lambda: {"type": "triangle_bvh", "filename": "${scene-directory}/unitbox.bm"}  # noqa: E731
     p, n, uv = _box_mesh((0.5, 0.5, 0.5))
     write_bm(out / "unitbox.bm", p + 0.5, n, uv)  # [0,1]^3, outward
@@ -369,7 +416,7 @@ def media_scene(out_dir: Path | None = None, seed: int = 1002, width: int = 1024
                     "density": {"type": "image3d", "format": "real", "binary_filename": "${scene-directory}/density.bin"},
                     "albedo": {"type": "constant", "texel": [0.9]},
                     "g": {"type": "constant", "texel": [0.0]}}},
-        {"type": "geometric", "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/sphere.bm",
+        {"type": "geometric", "geometry": {"type": "triangle_bvh", "filename": f"${{scene-directory}}/{sph.name}",
                                            "transform": [{"type": "translate", "offset": [1.6, 0, 0.2]},
                                                          {"type": "scale", "ratio": 0.6}]},
          "material": {"type": "disney", "base_color": _const([0.8, 0.3, 0.2]), "metallic": _const(0.0),

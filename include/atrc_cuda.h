@@ -303,7 +303,10 @@ typedef struct AtrcRenderDesc {
     float    ao_low[3];              /* low_color, default 0                 */
     float    ao_high[3];             /* high_color, default 1                */
     float    ao_background[3];       /* background_color, default 0          */
-    int32_t  pad_;
+    int32_t  isect_mode;             /* ray-triangle test of the render:     */
+                                     /* ATRC_ISECT_FAST (Moller-Trumbore,    */
+                                     /* the reference's test) or             */
+                                     /* ATRC_ISECT_WATERTIGHT                */
 } AtrcRenderDesc;
 
 /* Renderer of a render call. */
@@ -383,6 +386,18 @@ typedef struct AtrcHit {       /* 16 bytes */
 
 typedef enum AtrcQueryMode { ATRC_QUERY_CLOSEST = 0, ATRC_QUERY_ANY = 1 } AtrcQueryMode;
 
+/* Ray-primitive tests.  The reference uses Moller-Trumbore
+ * (src/tracer/include/agz/tracer/utility/triangle_aux.h:9-69), which can let
+ * a ray through an edge or vertex shared by two triangles miss both. */
+typedef enum AtrcIsectMode {
+    ATRC_ISECT_FAST       = 0,  /* Moller-Trumbore, compiler-scheduled (FMAs)   */
+    ATRC_ISECT_EXACT      = 1,  /* Moller-Trumbore in the reference's operation */
+                                /* order without FMAs: bit-identical hits       */
+    ATRC_ISECT_WATERTIGHT = 2   /* Woop, Benthin and Wald's watertight test     */
+                                /* (JCGT 2(1), 2013) on the exact vertices, and */
+                                /* sphere roots without cancellation            */
+} AtrcIsectMode;
+
 /* ------------------------------------------------------------- functions */
 
 typedef struct AtrcConfig AtrcConfig;   /* parsed JSON config (host)        */
@@ -449,8 +464,9 @@ void atrc_cuda_scene_destroy(AtrcScene* scene);
 
 /* Trace `n` rays from host memory into host `hits`.  mode: AtrcQueryMode.
  * ANY mode writes t = 1 / entity = 0 for an occluded ray and t = -1 otherwise.
- * `exact` = 1 selects the reference-exact Moller-Trumbore test (same
- * operation order, no fused multiply-add), 0 the fast test. */
+ * `exact` is an AtrcIsectMode: 1 selects the reference-exact Moller-Trumbore
+ * test (same operation order, no fused multiply-add), 0 the fast test, 2 the
+ * watertight test. */
 int atrc_cuda_trace_rays(AtrcScene* scene, const AtrcRay* rays, size_t n,
                          AtrcHit* hits, int mode, int exact);
 
@@ -508,6 +524,15 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc,
 /* Read or replace a scene's launch configuration (e.g. a cached tuning). */
 int atrc_cuda_get_tuning(AtrcScene* scene, AtrcTuning* out);
 int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in);
+
+/* Streaming-read bandwidth (GB/s) of `device`: a zero-filled buffer of
+ * `bytes` (a multiple of 16, at least 1 MiB) read `passes` (>= 2) times with
+ * 16-byte loads that bypass L1, after one untimed pass, timed with CUDA
+ * events.  A buffer of a few tens of MB stays in L2 and measures L2 read
+ * bandwidth; one of several GB measures HBM.  The roofline denominator of
+ * the traversal kernels, whose working set is served from L1 and L2.  No
+ * counterpart in the reference (it has no GPU code). */
+int atrc_cuda_stream_read_gbs(int device, uint64_t bytes, int passes, double* gbs);
 
 /* Size of the static device array behind atrc_cuda_render_noalloc. */
 #define ATRC_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
@@ -651,6 +676,15 @@ int  atrc_guide_train_records(AtrcGuide* guide, const float* records, size_t n,
                               int steps, float* last_loss);
 /* Copy out the records of the last recording render (24 floats each). */
 int  atrc_guide_records(AtrcGuide* guide, float* records, size_t cap, size_t* count);
+
+/* Gradients of the training loss over `n` host records (n x 24 floats, as
+ * atrc_guide_records returns them; 128 <= n <= record_capacity) at the
+ * current parameters, computed by the tensor-core training kernel without
+ * the Adam step: `grad_weights` (AtrcGuideInfo.weights floats), `grad_table`
+ * (table_floats) and the loss sum.  Parameters and optimiser state are left
+ * unchanged.  For checking the backward pass against a reference. */
+int  atrc_guide_gradients(AtrcGuide* guide, const float* records, size_t n,
+                          float* grad_weights, float* grad_table, float* loss);
 
 /* Batched multi-view render (no counterpart in the reference, which renders
  * one camera per `rendering` entry): n views (camera, size, spp, seed,

@@ -31,8 +31,9 @@ def load() -> C.CDLL:
         lib.oracle_scene_destroy.argtypes = [C.c_void_p]
         lib.oracle_scene_destroy.restype = None
         lib.oracle_trace_rays.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRay), C.c_size_t, C.POINTER(abi.AtrcHit),
-                                          C.c_int, C.c_int]
-        lib.oracle_prim_hit.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRay), C.c_int, C.c_int, C.POINTER(C.c_float)]
+                                          C.c_int, C.c_int, C.c_int]
+        lib.oracle_prim_hit.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRay), C.c_int, C.c_int, C.c_int,
+                                        C.POINTER(C.c_float)]
         lib.oracle_render.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRenderDesc), C.POINTER(abi.AtrcFilm), C.c_int]
         lib.oracle_render_sample.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRenderDesc), C.POINTER(abi.AtrcFilm),
                                              C.c_int, C.c_int]
@@ -69,18 +70,22 @@ class OracleScene:
             _lib.oracle_scene_destroy(self._h)
             self._h = None
 
-    def trace_rays(self, rays: np.ndarray, mode: str = "closest", threads: int = 0) -> np.ndarray:
+    def trace_rays(self, rays: np.ndarray, mode: str = "closest", threads: int = 0,
+                   watertight: bool = False) -> np.ndarray:
+        """Closest / any hits with the reference's Moller-Trumbore test, or the
+        watertight test with `watertight`."""
         r = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
         hits = np.empty(len(r), dtype=HIT_DTYPE)
         _check(load().oracle_trace_rays(self._h, r.ctypes.data_as(C.POINTER(abi.AtrcRay)), len(r),
                                         hits.ctypes.data_as(C.POINTER(abi.AtrcHit)), 0 if mode == "closest" else 1,
-                                        threads))
+                                        2 if watertight else 1, threads))
         return hits
 
-    def prim_hit(self, ray: np.ndarray, entity: int, prim: int) -> float:
+    def prim_hit(self, ray: np.ndarray, entity: int, prim: int, watertight: bool = False) -> float:
         r = np.ascontiguousarray(ray, dtype=RAY_DTYPE).reshape(1)
         t = C.c_float()
-        _check(load().oracle_prim_hit(self._h, r.ctypes.data_as(C.POINTER(abi.AtrcRay)), entity, prim, C.byref(t)))
+        _check(load().oracle_prim_hit(self._h, r.ctypes.data_as(C.POINTER(abi.AtrcRay)), entity, prim,
+                                      2 if watertight else 1, C.byref(t)))
         return t.value
 
     def render(self, desc: abi.AtrcRenderDesc, film, threads: int = 0) -> None:

@@ -34,16 +34,18 @@ int oracle_scene_create(const AtrcSceneDesc* desc, float eps, OracleScene** out)
 void oracle_scene_destroy(OracleScene* s);
 
 /* Closest / any hit for each ray (Scene::closest_intersection /
- * has_intersection).  `threads` <= 0 uses all hardware threads. */
+ * has_intersection).  `isect` is ATRC_ISECT_EXACT (the reference's
+ * Moller-Trumbore) or ATRC_ISECT_WATERTIGHT (the watertight triangle test and
+ * cancellation-free sphere roots, not in the reference).  `threads` <= 0 uses
+ * all hardware threads. */
 int oracle_trace_rays(OracleScene* s, const AtrcRay* rays, size_t n,
-                      AtrcHit* hits, int mode, int threads);
+                      AtrcHit* hits, int mode, int isect, int threads);
 
-/* Reference-exact Moller-Trumbore test of one primitive of one entity against
- * a world ray (ray moved to the entity's local space as transform_wrapper
- * does).  Writes t (or -1 when the primitive is not hit).  Used to adjudicate
- * hit mismatches. */
+/* The `isect` test of one primitive of one entity against a world ray (ray
+ * moved to the entity's local space as transform_wrapper does).  Writes t (or
+ * -1 when the primitive is not hit).  Used to adjudicate hit mismatches. */
 int oracle_prim_hit(OracleScene* s, const AtrcRay* ray, int entity, int prim,
-                    float* t_out);
+                    int isect, float* t_out);
 
 /* Render with the reference's `pt` algorithm (perpixel_renderer.cpp:13-53 +
  * path_tracing.cpp:15-225) and ADD into `film` (host pointers).  Samples

@@ -143,6 +143,18 @@ struct Ray {
     bool between(float t) const { return t_min <= t && t <= t_max; }  // common.h:320-323
 };
 
+// The ray-primitive test of the calling thread's current query batch:
+// ATRC_ISECT_EXACT (the reference's) or ATRC_ISECT_WATERTIGHT (not in the
+// reference).  In watertight mode the box tests also accept a box whose entry
+// distance exceeds its exit distance by a relative 5e-7 (the device's slack):
+// the reference's exact box test culls a leaf whose corner the ray passes
+// through, so its traversal misses hits that the watertight test finds.
+thread_local int g_isect = ATRC_ISECT_EXACT;
+
+inline bool box_overlap(float lo, float hi) {
+    return g_isect == ATRC_ISECT_WATERTIGHT ? lo <= hi * 1.0000005f + 1e-30f : lo <= hi;
+}
+
 struct AABB {
     V3 low{REAL_MAX}, high{-REAL_MAX};
     void add(V3 p) {
@@ -158,7 +170,7 @@ struct AABB {
             lo = std::max(lo, std::min(n[i], f[i]));
             hi = std::min(hi, std::max(n[i], f[i]));
         }
-        return lo <= hi;
+        return box_overlap(lo, hi);
     }
 };
 
@@ -426,6 +438,91 @@ bool closest_tri(const Ray& r, V3 A, V3 B_A, V3 C_A, float* t_out, V2* uv) {
     return true;
 }
 float triangle_area(V3 B_A, V3 C_A) { return len(cross(B_A, C_A)) / 2; }
+
+// Ray-primitive tests: ATRC_ISECT_EXACT runs the reference's
+// Moller-Trumbore above; ATRC_ISECT_WATERTIGHT (g_isect, set per query batch)
+// the watertight triangle test of Woop, Benthin and Wald (JCGT 2(1), 2013) on
+// the exact vertices and the cancellation-free sphere roots of Haines et al.
+// (Ray Tracing Gems, 2019), with the same float operations in the same order
+// as the device's watertight mode.
+
+float wt_comp(V3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Shear the ray onto +z: kz = axis of the largest |d| component, kx, ky
+// cyclic after it and swapped when d[kz] < 0 (keeps the winding); then the
+// signs of the 2D edge functions of the sheared vertices decide the hit.
+// Edge functions that round to 0 are evaluated again in double precision.
+bool wt_tri(const Ray& r, V3 pa, V3 pb, V3 pc, float* t_out, V2* uv) {
+    const float ax = std::fabs(r.d.x), ay = std::fabs(r.d.y), az = std::fabs(r.d.z);
+    const int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    const float dz = wt_comp(r.d, kz);
+    if (dz < 0) std::swap(kx, ky);
+    const float sx = wt_comp(r.d, kx) / dz, sy = wt_comp(r.d, ky) / dz, sz = 1.0f / dz;
+    const V3 A = pa - r.o, B = pb - r.o, C = pc - r.o;
+    const float Az = wt_comp(A, kz), Bz = wt_comp(B, kz), Cz = wt_comp(C, kz);
+    const float Ax = wt_comp(A, kx) - sx * Az, Ay = wt_comp(A, ky) - sy * Az;
+    const float Bx = wt_comp(B, kx) - sx * Bz, By = wt_comp(B, ky) - sy * Bz;
+    const float Cx = wt_comp(C, kx) - sx * Cz, Cy = wt_comp(C, ky) - sy * Cz;
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    if ((U < 0 || V < 0 || W < 0) && (U > 0 || V > 0 || W > 0)) return false;
+    const float det = (U + V) + W;
+    if (det == 0.0f) return false;
+    const float T = (U * (sz * Az) + V * (sz * Bz)) + W * (sz * Cz);
+    const float rcp = 1.0f / det;
+    const float t = T * rcp;
+    if (!r.between(t)) return false;
+    *t_out = t;
+    *uv = V2(V * rcp, W * rcp);
+    return true;
+}
+
+bool tri_has(const Ray& r, V3 A, V3 B_A, V3 C_A, V3 B, V3 C) {
+    if (g_isect == ATRC_ISECT_WATERTIGHT) {
+        float t;
+        V2 uv;
+        return wt_tri(r, A, B, C, &t, &uv);
+    }
+    return has_tri(r, A, B_A, C_A);
+}
+bool tri_closest(const Ray& r, V3 A, V3 B_A, V3 C_A, V3 B, V3 C, float* t, V2* uv) {
+    return g_isect == ATRC_ISECT_WATERTIGHT ? wt_tri(r, A, B, C, t, uv) : closest_tri(r, A, B_A, C_A, t, uv);
+}
+
+// Sphere roots: the reference's (sphere_aux.h:53-86), or without
+// cancellation in watertight mode.  Returns false when the quadratic has no
+// real root.
+bool sphere_roots(const Ray& lr, float radius, float* t0, float* t1) {
+    if (g_isect == ATRC_ISECT_WATERTIGHT) {
+        const float a = len2(lr.d);
+        if (!(a > 0)) return false;
+        const float b = dot(lr.o, lr.d);
+        const V3 l = lr.o - (b / a) * lr.d;
+        const float disc = a * (radius * radius - len2(l));
+        if (disc < 0) return false;
+        const float c = len2(lr.o) - radius * radius;
+        const float q = -(b + std::copysign(std::sqrt(disc), b));
+        float r0 = q / a, r1 = q != 0.0f ? c / q : r0;
+        if (r0 > r1) std::swap(r0, r1);
+        *t0 = r0;
+        *t1 = r1;
+        return true;
+    }
+    float A = len2(lr.d), B = 2 * dot(lr.d, lr.o), C = len2(lr.o) - radius * radius;
+    float delta = B * B - 4 * A * C;
+    if (delta < 0) return false;
+    delta = std::sqrt(delta);
+    float inv2A = 0.5f / A;
+    *t0 = (-B - delta) * inv2A;
+    *t1 = (-B + delta) * inv2A;
+    return true;
+}
 // triangle_aux.h:76-88
 V3 dpdu_as_ex(V3 B_A, V3 C_A, V2 b_a, V2 c_a, V3 nor) {
     float m00 = b_a.x, m01 = b_a.y, m10 = c_a.x, m11 = c_a.y;
@@ -453,10 +550,10 @@ struct TriBVH {
             t_max = std::min(t_max, std::max(ny, fy));
             t_max = std::min(t_max, std::max(nz, fz));
             *t = t_min;
-            return t_min <= t_max;
+            return box_overlap(t_min, t_max);
         }
     };
-    struct Prim { V3 a, b_a, c_a; };
+    struct Prim { V3 a, b_a, c_a, b, c; };  // b, c: exact vertices (watertight test)
     struct Info { V3 n_a, n_b_a, n_c_a; V2 t_a, t_b_a, t_c_a; V3 x, z; };
 
     std::vector<Node> nodes;
@@ -562,6 +659,8 @@ struct TriBVH {
                     p.a = tri.v[0].p;
                     p.b_a = tri.v[1].p - tri.v[0].p;
                     p.c_a = tri.v[2].p - tri.v[0].p;
+                    p.b = tri.v[1].p;
+                    p.c = tri.v[2].p;
                     V3 na = normalize(tri.v[0].n), nb = normalize(tri.v[1].n), nc = normalize(tri.v[2].n);
                     in.n_a = na; in.n_b_a = nb - na; in.n_c_a = nc - na;
                     in.t_a = tri.v[0].t; in.t_b_a = tri.v[1].t - tri.v[0].t; in.t_c_a = tri.v[2].t - tri.v[0].t;
@@ -595,7 +694,7 @@ struct TriBVH {
             const Node& n = nodes[idx];
             if (n.is_leaf()) {
                 for (uint32_t i = n.start; i < n.end_or_right; ++i)
-                    if (has_tri(r, prims[i].a, prims[i].b_a, prims[i].c_a)) return true;
+                    if (tri_has(r, prims[i].a, prims[i].b_a, prims[i].c_a, prims[i].b, prims[i].c)) return true;
             } else {
                 if (top + 2 > 128) return false;
                 if (nodes[idx + 1].hit(ori, inv, r.t_min, r.t_max, &t)) stack[top++] = idx + 1;
@@ -624,7 +723,7 @@ struct TriBVH {
                 for (uint32_t i = n.start; i < n.end_or_right; ++i) {
                     float t;
                     V2 uv;
-                    if (closest_tri(r, prims[i].a, prims[i].b_a, prims[i].c_a, &t, &uv)) {
+                    if (tri_closest(r, prims[i].a, prims[i].b_a, prims[i].c_a, prims[i].b, prims[i].c, &t, &uv)) {
                         best_t = t; best_uv = uv; r.t_max = t; best = i;
                     }
                 }
@@ -677,6 +776,7 @@ struct Leaf {
     std::shared_ptr<TriBVH> bvh;
     // quad / triangle (quad.cpp:134-157, triangle.cpp)
     V3 a, b_a, c_a, d_a;
+    V3 b, c, d;            // exact vertices (watertight test)
     V2 t_a, t_b_a, t_c_a, t_d_a;
     V3 x_abc, x_acd, z;
     float area = 1, abc_prob = 0;
@@ -712,6 +812,7 @@ struct Leaf {
             V3 A = xpoint(xf.m, V3(g.p[0])), B = xpoint(xf.m, V3(g.p[1]));
             V3 C = xpoint(xf.m, V3(g.p[2])), D = xpoint(xf.m, V3(g.p[3]));
             a = A; b_a = B - A; c_a = C - A; d_a = D - A;
+            b = B; c = C; d = D;
             t_a = V2(g.uv[0][0], g.uv[0][1]);
             t_b_a = V2(g.uv[1][0], g.uv[1][1]) - t_a;
             t_c_a = V2(g.uv[2][0], g.uv[2][1]) - t_a;
@@ -728,6 +829,7 @@ struct Leaf {
         } else if (type == ATRC_GEOM_TRIANGLE) {
             // Triangle (triangle.cpp): local vertices, ray moved to local space
             a = V3(g.p[0]); b_a = V3(g.p[1]) - a; c_a = V3(g.p[2]) - a;
+            b = V3(g.p[1]); c = V3(g.p[2]);
             t_a = V2(g.uv[0][0], g.uv[0][1]);
             t_b_a = V2(g.uv[1][0], g.uv[1][1]) - t_a;
             t_c_a = V2(g.uv[2][0], g.uv[2][1]) - t_a;
@@ -759,16 +861,12 @@ struct Leaf {
     bool has(const Ray& r) const {
         switch (type) {
         case ATRC_GEOM_TRIANGLE_BVH: return bvh->has(r);
-        case ATRC_GEOM_QUAD: return has_tri(r, a, b_a, c_a) || has_tri(r, a, c_a, d_a);
-        case ATRC_GEOM_TRIANGLE: return has_tri(to_local(r), a, b_a, c_a);
+        case ATRC_GEOM_QUAD: return tri_has(r, a, b_a, c_a, b, c) || tri_has(r, a, c_a, d_a, c, d);
+        case ATRC_GEOM_TRIANGLE: return tri_has(to_local(r), a, b_a, c_a, b, c);
         case ATRC_GEOM_SPHERE: {  // sphere_aux.h:53-66
             Ray lr = to_local(r);
-            float A = len2(lr.d), B = 2 * dot(lr.d, lr.o), C = len2(lr.o) - radius * radius;
-            float delta = B * B - 4 * A * C;
-            if (delta < 0) return false;
-            delta = std::sqrt(delta);
-            float inv2A = 0.5f / A;
-            float t0 = (-B - delta) * inv2A, t1 = (-B + delta) * inv2A;
+            float t0, t1;
+            if (!sphere_roots(lr, radius, &t0, &t1)) return false;
             return lr.between(t0) || lr.between(t1);
         }
         case ATRC_GEOM_DISK: {  // disk.cpp:43-55
@@ -813,7 +911,7 @@ struct Leaf {
         case ATRC_GEOM_QUAD: {  // quad.cpp:30-58
             float t;
             V2 uv;
-            if (closest_tri(r, a, b_a, c_a, &t, &uv)) {
+            if (tri_closest(r, a, b_a, c_a, b, c, &t, &uv)) {
                 inct->pos = r.at(t);
                 inct->geo = Coord(x_abc, cross(z, x_abc), z);
                 inct->uv = t_a + uv.x * t_b_a + uv.y * t_c_a;
@@ -823,7 +921,7 @@ struct Leaf {
                 inct->prim = 0;
                 return true;
             }
-            if (closest_tri(r, a, c_a, d_a, &t, &uv)) {
+            if (tri_closest(r, a, c_a, d_a, c, d, &t, &uv)) {
                 inct->pos = r.at(t);
                 inct->geo = Coord(x_acd, cross(z, x_acd), z);
                 inct->uv = t_a + uv.x * t_c_a + uv.y * t_d_a;
@@ -839,7 +937,7 @@ struct Leaf {
             Ray lr = to_local(r);
             float t;
             V2 uv;
-            if (!closest_tri(lr, a, b_a, c_a, &t, &uv)) return false;
+            if (!tri_closest(lr, a, b_a, c_a, b, c, &t, &uv)) return false;
             inct->pos = lr.at(t);
             inct->geo = Coord(x_abc, cross(z, x_abc), z);
             inct->uv = t_a + uv.x * t_b_a + uv.y * t_c_a;
@@ -852,12 +950,8 @@ struct Leaf {
         }
         case ATRC_GEOM_SPHERE: {  // sphere.cpp:35-60, sphere_aux.h:68-86
             Ray lr = to_local(r);
-            float A = len2(lr.d), B = 2 * dot(lr.d, lr.o), C = len2(lr.o) - radius * radius;
-            float delta = B * B - 4 * A * C;
-            if (delta < 0) return false;
-            delta = std::sqrt(delta);
-            float inv2A = 0.5f / A;
-            float t0 = (-B - delta) * inv2A, t1 = (-B + delta) * inv2A;
+            float t0, t1;
+            if (!sphere_roots(lr, radius, &t0, &t1)) return false;
             if (lr.t_max < t0 || t1 < lr.t_min) return false;
             bool not_t0 = t0 < lr.t_min;
             if (not_t0 && t1 > lr.t_max) return false;
@@ -2622,10 +2716,19 @@ static void parallel_for(size_t n, int threads, const std::function<void(size_t)
     for (auto& th : pool) th.join();
 }
 
-int oracle_trace_rays(OracleScene* s, const AtrcRay* rays, size_t n, AtrcHit* hits, int mode, int threads) {
+// Sets the calling thread's ray-primitive test for a scope.
+struct IsectScope {
+    int saved;
+    explicit IsectScope(int mode) : saved(g_isect) { g_isect = mode; }
+    ~IsectScope() { g_isect = saved; }
+};
+
+int oracle_trace_rays(OracleScene* s, const AtrcRay* rays, size_t n, AtrcHit* hits, int mode, int isect, int threads) {
     if (!s || (!rays && n) || (!hits && n)) { g_err = "null argument"; return ATRC_ERR_INVALID_ARG; }
+    if (isect != ATRC_ISECT_EXACT && isect != ATRC_ISECT_WATERTIGHT) { g_err = "bad isect mode"; return ATRC_ERR_INVALID_ARG; }
     const size_t chunk = 4096;
     parallel_for((n + chunk - 1) / chunk, threads, [&](size_t c) {
+        IsectScope scope(isect);
         for (size_t i = c * chunk; i < std::min(n, (c + 1) * chunk); ++i) {
             const AtrcRay& q = rays[i];
             Ray r(V3(q.o), V3(q.d), q.t_min, q.t_max);
@@ -2652,8 +2755,10 @@ int oracle_trace_rays(OracleScene* s, const AtrcRay* rays, size_t n, AtrcHit* hi
     return ATRC_OK;
 }
 
-int oracle_prim_hit(OracleScene* s, const AtrcRay* q, int entity, int prim, float* t_out) {
+int oracle_prim_hit(OracleScene* s, const AtrcRay* q, int entity, int prim, int isect, float* t_out) {
     if (!s || !q || !t_out || entity < 0 || size_t(entity) >= s->entities.size()) return ATRC_ERR_INVALID_ARG;
+    if (isect != ATRC_ISECT_EXACT && isect != ATRC_ISECT_WATERTIGHT) return ATRC_ERR_INVALID_ARG;
+    IsectScope scope(isect);
     const Entity& e = s->entities[entity];
     Ray r(V3(q->o), V3(q->d), q->t_min, q->t_max);
     if (e.has_wrap) r = Ray(xpoint(e.wrap.inv, r.o), xvec(e.wrap.inv, r.d), r.t_min, r.t_max);
@@ -2665,13 +2770,15 @@ int oracle_prim_hit(OracleScene* s, const AtrcRay* q, int entity, int prim, floa
         const TriBVH& b = *l.bvh;
         for (size_t i = 0; i < b.orig.size(); ++i) {
             if (int(b.orig[i]) != prim) continue;
-            if (closest_tri(r, b.prims[i].a, b.prims[i].b_a, b.prims[i].c_a, &t, &uv)) *t_out = t;
+            const TriBVH::Prim& pr = b.prims[i];
+            if (tri_closest(r, pr.a, pr.b_a, pr.c_a, pr.b, pr.c, &t, &uv)) *t_out = t;
             return ATRC_OK;
         }
         return ATRC_ERR_INVALID_ARG;
     }
     if (l.type == ATRC_GEOM_QUAD) {
-        bool ok = prim == 0 ? closest_tri(r, l.a, l.b_a, l.c_a, &t, &uv) : closest_tri(r, l.a, l.c_a, l.d_a, &t, &uv);
+        bool ok = prim == 0 ? tri_closest(r, l.a, l.b_a, l.c_a, l.b, l.c, &t, &uv)
+                            : tri_closest(r, l.a, l.c_a, l.d_a, l.c, l.d, &t, &uv);
         if (ok) *t_out = t;
         return ATRC_OK;
     }
@@ -2690,6 +2797,7 @@ int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film
     if (film->on_device) { g_err = "the oracle renders into host memory only"; return ATRC_ERR_INVALID_ARG; }
     g_eps = s->eps = d->eps;
     g_disney_fixed = d->disney_fixed;
+    const int isect = d->isect_mode == ATRC_ISECT_WATERTIGHT ? ATRC_ISECT_WATERTIGHT : ATRC_ISECT_EXACT;
     const int W = d->width, H = d->height;
     const int spp = d->spp_count > 0 ? d->spp_count : d->spp;
     // camera (thin_lens.cpp:34-94); look-at frame: z = forward, x = up x z
@@ -2708,6 +2816,7 @@ int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film
     std::mutex mtx;
     const size_t n_tiles = size_t(tx) * ty;
     parallel_for((n_tiles + tile_stride - 1) / tile_stride, threads, [&](size_t tile_k) {
+        IsectScope scope(isect);
         const size_t tile = tile_k * size_t(tile_stride);
         const int gx = int(tile % tx), gy = int(tile / tx);
         const int x0 = gx * grid, y0 = gy * grid;

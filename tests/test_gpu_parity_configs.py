@@ -1,0 +1,142 @@
+"""GPU parity against the CPU oracle on the benchmark scenes at their stated
+settings, through the C ABI.
+
+* the seeded Cornell box at its full size (256 x 256, 64 spp,
+  max depth 8, Russian roulette from depth 3, box filter), every pixel in the
+  3-sigma band.
+* the media scene with its 128^3 fBm density grid (delta and
+  ratio tracking) around the 200,000-triangle displaced sphere, two area
+  lights and the sky, at its full 512 spp and max depth 32 on a 48 x 48
+  film; plus closest hits against the oracle's BVH on that scene.
+* the indoor room (403,000 triangles, Disney, lit only through
+  the window), plain pt_cuda at 64 x 36 against the oracle.
+* Guided rendering with the fixed Disney sampler (the mode the guided
+  benchmark uses) against plain rendering, on the room and on the instanced
+  Disney + IBL scene: guiding changes the sampling, not the expectation.
+
+Reference: src/tracer/src/render/path_tracing.cpp:15-225 (trace_std),
+src/tracer/src/core/medium/heterogeneous.cpp:52-123,
+src/tracer/src/core/renderer/perpixel_renderer.cpp:13-207.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from atrc_b200 import Config, DeviceScene, Film
+from atrc_b200.guide import Guide
+from tests.parity import band_test, classify_closest, global_mean_z, seeded_rays
+
+pytestmark = pytest.mark.gpu
+
+BOX = 1 / (4 * (0.5 - 3e-4) ** 2)  # box filter weight of one sample
+
+
+def _render_pair(path, **overrides):
+    cfg = Config.from_file(path)
+    desc, _ = cfg.rendering(0)
+    for k, v in overrides.items():
+        setattr(desc, k, v)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    fg = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    fc = Film(desc.width, desc.height, value_sq=True, gbuffer=True)
+    st = dev.render(desc, fg)
+    ora.render(desc, fc)
+    return cfg, desc, dev, ora, fg, fc, st
+
+
+def test_cornell_config0_full_size_within_3_sigma(scene_dir):
+    from atrc_b200.scenes import cornell_box
+    cfg, desc, dev, ora, fg, fc, st = _render_pair(cornell_box(scene_dir / "cornell_cfg0"))
+    assert (desc.width, desc.height, desc.spp, desc.max_depth, desc.min_depth) == (256, 256, 64, 8, 2)
+    assert st["samples"] == 256 * 256 * 64 and st["watchdog_flags"] == 0
+    frac, allowed, info = band_test(fg, fc, BOX)
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fg, fc) < 4.0
+    ga = fg.albedo.reshape(-1, 3) / fg.weight.reshape(-1, 1)
+    ca = fc.albedo.reshape(-1, 3) / fc.weight.reshape(-1, 1)
+    assert np.abs(ga - ca).mean() < 0.01
+
+
+@pytest.fixture(scope="module")
+def media_cfg2(scene_dir):
+    from atrc_b200.scenes import media_scene
+    return media_scene(scene_dir / "media_cfg2", width=48, height=48, spp=512)
+
+
+def test_media_config2_grid_and_sphere_within_3_sigma(media_cfg2):
+    cfg, desc, dev, ora, fg, fc, st = _render_pair(media_cfg2)
+    assert (desc.spp, desc.max_depth) == (512, 32)
+    sd = cfg.scene_desc().contents
+    tex3 = [sd.textures3d[i] for i in range(sd.texture3d_count)]
+    assert any(t.width == t.height == t.depth == 128 for t in tex3)
+    assert any(sd.meshes[i].triangle_count == 200_000 for i in range(sd.mesh_count))
+    assert st["watchdog_flags"] == 0
+    frac, allowed, info = band_test(fg, fc, BOX)
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fg, fc) < 4.0
+
+
+def test_media_config2_closest_hits_bit_exact(media_cfg2):
+    cfg = Config.from_file(media_cfg2)
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    rays = seeded_rays(1_000_000, [-6.0, -6.0, -1.0], [6.0, 6.0, 4.0], list(desc.camera.pos), seed=17)
+    g = dev.trace_rays(rays, "closest", exact=True)
+    r = ora.trace_rays(rays, "closest")
+    c = classify_closest(rays, g, r, ora)
+    assert c["error"] == 0, c["errors"]
+    assert c["max_ulp_same_prim"] == 0
+    assert c["exact"] + c["tie"] + c["ref_fn"] == len(rays)
+    assert c["exact"] >= len(rays) * 0.999, c
+
+
+@pytest.fixture(scope="module")
+def room(scene_dir):
+    from atrc_b200.scenes import indoor_room
+    return indoor_room(scene_dir / "room_cfg3", width=64, height=36, spp=256)
+
+
+def test_room_config3_plain_within_3_sigma(room):
+    cfg, desc, dev, ora, fg, fc, st = _render_pair(room)
+    assert desc.max_depth == 16 and st["watchdog_flags"] == 0
+    frac, allowed, info = band_test(fg, fc, BOX)
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fg, fc) < 4.0
+
+
+def _train(dev, g, cfg, w, h, passes=6):
+    d, _ = cfg.rendering(0)
+    d.width, d.height, d.spp = w, h, 16
+    d.disney_fixed = 1
+    for k in range(passes):
+        d.seed = 500 + k
+        dev.render_guided(g, d, Film(w, h), record=True)
+        g.train(steps=16)
+
+
+@pytest.mark.parametrize("scene", ["room", "instanced"])
+def test_guided_disney_fixed_matches_plain(scene, room, scene_dir):
+    if scene == "room":
+        path, w, h, spp = room, 64, 36, 2048
+    else:
+        from atrc_b200.scenes import instanced_disney
+        path, w, h, spp = instanced_disney(scene_dir / "inst_guided", ico_level=4, hf_res=128, width=64, height=36,
+                                           spp=1024), 64, 36, 1024
+    cfg = Config.from_file(path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = w, h, spp
+    desc.disney_fixed = 1
+    dev = DeviceScene(cfg)
+    g = Guide.for_scene(dev, record_capacity=1 << 18, batch=1 << 16)
+    _train(dev, g, cfg, w, h)
+    plain = Film(w, h, value_sq=True)
+    guided = Film(w, h, value_sq=True)
+    dev.render(desc, plain)
+    desc.seed = 4321
+    st = dev.render_guided(g, desc, guided)
+    assert st["samples"] == w * h * spp and st["watchdog_flags"] == 0
+    frac, allowed, info = band_test(guided, plain, BOX)
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(guided, plain) < 4.0
