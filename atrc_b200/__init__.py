@@ -160,6 +160,14 @@ class Film:
         self.albedo = mk(3) if gbuffer else None
         self.normal = mk(3) if gbuffer else None
         self.denoise = mk(1) if gbuffer else None
+        self._sync()
+
+    def _sync(self) -> None:
+        # the library renders on its own stream, which does not wait for
+        # torch's: the zero fill must be complete before a render adds to it
+        if self.device:
+            import torch
+            torch.cuda.current_stream().synchronize()
 
     def _ptr(self, a):
         if a is None:
@@ -183,6 +191,7 @@ class Film:
         for a in (self.value, self.weight, self.value_sq, self.albedo, self.normal, self.denoise):
             if a is not None:
                 a.fill(0) if not self.device else a.zero_()
+        self._sync()
 
     def _host(self, a):
         return a.cpu().numpy() if self.device else a

@@ -127,8 +127,20 @@ struct Counters {
     unsigned long long gen_base, issued, total, completed;
     unsigned long long rays_closest, rays_shadow, iterations;
     unsigned long long cnt_closest[3], cnt_shadow[3];  // nodes, tris, entities
+    unsigned long long t_start;  // %globaltimer when the render's counters were reset
+    int windows;                 // bounce-loop windows run by the device-side loop
     int watchdog, done;
 };
+
+// Watchdog code of the device-side bounce loop (atrc_cuda_render_batch):
+// the loop ran more windows than any path length allows.
+constexpr int kWatchdogLoop = 8;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ void flush_count(unsigned long long* dst, const TraceCount& tc) {
     unsigned long long v[3] = {tc.nodes, tc.tris, tc.ents};
@@ -184,6 +196,7 @@ struct Params {
     int nviews;
     const View* views;                 // device array
     unsigned long long* view_done;     // per view: finished samples (batch renders; else null)
+    unsigned long long* view_time;     // per view: %globaltimer when its last sample was splatted
     int sort_mode, nkeys;   // shade-queue sort (AtrcSortMode, resolved) and key count
     int slot_queue;         // 1: extend queue in slot order (AtrcTuning::queue_order)
     int min_depth, max_depth, specular_depth;
@@ -232,7 +245,21 @@ __global__ void k_init(Pool P, int cap, int nkeys, Counters* c, unsigned long lo
         c->n_free = cap;
         c->total = total;
         c->out = 0;
+        c->t_start = global_ns();
     }
+}
+
+// End of one window of the device-side bounce loop: run another window
+// unless the work is done or a watchdog fired; after max_windows the loop
+// stops with kWatchdogLoop instead of running on (no path lives that long).
+__global__ void k_loop_cond(Counters* c, cudaGraphConditionalHandle h, int max_windows) {
+    const int w = ++c->windows;
+    bool more = c->done == 0 && c->watchdog == 0;
+    if (more && w >= max_windows) {
+        c->watchdog = kWatchdogLoop;
+        more = false;
+    }
+    cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 __global__ void k_begin(Counters* c) {
@@ -1201,7 +1228,12 @@ __global__ void k_finish(Params p, Pool P, Counters* c) {
         const Film& F = v.film;
         if (p.view_done) {  // one atomic per view present in the warp
             const unsigned same = __match_any_sync(__activemask(), vi);
-            if (int(threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(p.view_done + vi, (unsigned long long)__popc(same));
+            if (int(threadIdx.x & 31) == __ffs(same) - 1) {
+                const unsigned long long k = (unsigned long long)__popc(same);
+                const unsigned long long before = atomicAdd(p.view_done + vi, k);
+                // the one add that completes the view stamps its time
+                if (p.view_time && before < v.count && before + k >= v.count) p.view_time[vi] = global_ns();
+            }
         }
         if (p.gf.records) {
             // targets of the path's guide records: luminance of the radiance
@@ -1289,6 +1321,28 @@ struct CaptureGuard {
     }
 };
 
+// Capture of a stream's work into an existing graph (the body of a
+// conditional node); ends the capture on scope exit if end() was not reached.
+struct BodyCapture {
+    cudaStream_t s;
+    bool open = false;
+    BodyCapture(cudaStream_t st, cudaGraph_t body) : s(st) {
+        CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        open = true;
+    }
+    void end() {
+        open = false;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(s, &g));
+    }
+    ~BodyCapture() {
+        if (!open) return;
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        cudaGetLastError();
+    }
+};
+
 // Reuse an executable graph when the new graph has the same topology (only
 // kernel parameters differ); otherwise instantiate afresh.
 cudaGraphExec_t instantiate_or_update(cudaGraphExec_t exec, cudaGraph_t g) {
@@ -1317,8 +1371,6 @@ struct DeviceSceneImpl {
     DevBuf tiles;  // tile tables of the film's sample grid
     // render workspace (kept between calls)
     DevBuf pool_buf, counters, film_buf;
-    size_t pool_cap = 0;
-    int pool_lights = 0;
     // per-call resources kept between render calls
     static constexpr int kWindow = 4;  // wavefront iterations between host checks
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, kev[kWindow * 4] = {};
@@ -1337,6 +1389,7 @@ struct DeviceSceneImpl {
         view_stage_bytes = bytes;
     }
     cudaGraphExec_t window_exec = nullptr;  // the captured bounce-loop window
+    cudaGraphExec_t loop_exec = nullptr;    // the device-side bounce loop (batches)
     void* stage = nullptr;             // pinned host staging for host films
     size_t stage_bytes = 0;
     // launch configuration (atrc_cuda_autotune chooses it; these are the
@@ -1381,6 +1434,7 @@ struct DeviceSceneImpl {
         for (auto& e : kev) if (e) cudaEventDestroy(e);
         for (auto& e : copy_ev) if (e) cudaEventDestroy(e);
         if (window_exec) cudaGraphExecDestroy(window_exec);
+        if (loop_exec) cudaGraphExecDestroy(loop_exec);
         if (view_stage) cudaFreeHost(view_stage);
         if (pinned_counters) cudaFreeHost(pinned_counters);
         if (stage) cudaFreeHost(stage);
@@ -1784,7 +1838,8 @@ int atrc_cuda_subsurface_probe(AtrcScene* scene, const float o[3], const float d
 // sample was splatted, observed at window granularity.
 static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const AtrcFilm* films, int nviews,
                        AtrcCancelFn should_stop, AtrcProgressFn progress, void* user, AtrcRenderStats* stats,
-                       GuideImpl* guide = nullptr, bool record = false, double* view_seconds = nullptr) {
+                       GuideImpl* guide = nullptr, bool record = false, double* view_seconds = nullptr,
+                       bool device_loop = false) {
     const auto t_start = std::chrono::steady_clock::now();
     const AtrcRenderDesc* desc = descs;
     const AtrcFilm* film = films;
@@ -1825,11 +1880,10 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     cap = std::min<size_t>(cap, (size_t(1) << 28) / nl);
     const size_t shadow_cap = cap * nl;
     const PoolLayout L = pool_layout(cap, shadow_cap, p.nkeys);
-    if (d.pool_buf.bytes < L.total || d.pool_cap != cap || d.pool_lights != nl) {
-        d.pool_buf.alloc(L.total);
-        d.pool_cap = cap;
-        d.pool_lights = nl;
-    }
+    // the buffer only grows: a smaller pool is laid out inside it (k_init
+    // resets every word that must start from a known value), so renders of
+    // changing sizes do not pay a cudaFree + cudaMalloc each
+    if (d.pool_buf.bytes < L.total) d.pool_buf.alloc(L.total);
     if (!d.counters.p) d.counters.alloc(sizeof(Counters));
     if (guide) {
         if (guide_device(guide) != d.device) throw std::runtime_error("the guide lives on another device than the scene");
@@ -1864,16 +1918,20 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
         if (film->normal) { F.normal = b; b += npix * 3; host_targets.push_back({film->normal, npix * 3}); }
         if (film->denoise) { F.denoise = b; b += npix; host_targets.push_back({film->denoise, npix}); }
     }
-    // view table on the device (+ per-view completion counters of batches)
-    const size_t vbytes = nviews * sizeof(View), dbytes = nviews > 1 ? nviews * sizeof(unsigned long long) : 0;
-    if (d.views_buf.bytes < vbytes + dbytes) d.views_buf.alloc(vbytes + dbytes);
-    CK(cudaMemcpyAsync(d.views_buf.p, views.data(), vbytes, cudaMemcpyHostToDevice, s));
+    // view table on the device; the device-side loop (batches) also keeps
+    // per-view finished-sample counters and completion timestamps
+    const size_t vbytes = (nviews * sizeof(View) + 255) & ~size_t(255);
+    const size_t dbytes = device_loop ? nviews * sizeof(unsigned long long) : 0;
+    if (d.views_buf.bytes < vbytes + 2 * dbytes) d.views_buf.alloc(vbytes + 2 * dbytes);
+    CK(cudaMemcpyAsync(d.views_buf.p, views.data(), nviews * sizeof(View), cudaMemcpyHostToDevice, s));
     p.nviews = nviews;
     p.views = d.views_buf.as<View>();
     p.view_done = nullptr;
+    p.view_time = nullptr;
     if (dbytes) {
         p.view_done = reinterpret_cast<unsigned long long*>(d.views_buf.as<char>() + vbytes);
-        CK(cudaMemsetAsync(p.view_done, 0, dbytes, s));
+        p.view_time = p.view_done + nviews;
+        CK(cudaMemsetAsync(p.view_done, 0, 2 * dbytes, s));
         d.ensure_view_stage(dbytes);
     }
     k_tiles<<<nviews, 32, 0, s>>>(p);
@@ -1884,13 +1942,10 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
     CK(cudaGetLastError());
     uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
-    std::vector<char> view_finished(nviews, 0);
-    int views_left = nviews;
     cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
     cudaEvent_t* kev = d.kev;
     const int window = DeviceSceneImpl::kWindow;
     double t_ext = 0, t_shade = 0, t_shadow = 0;
-    CK(cudaEventRecord(ev0, s));
     Counters hc{};
     static_assert(sizeof(Counters) <= 512, "pinned counter buffer too small");
     Counters* pinned = static_cast<Counters*>(d.pinned_counters);
@@ -1899,19 +1954,17 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     // only; a watertight render ignores them
     const bool wt = desc->isect_mode == ATRC_ISECT_WATERTIGHT;
     const bool count = desc->count_traversal != 0 && !wt;
-    // The bounce loop runs in windows of `window` iterations.  One window
-    // (6 kernels per iteration, the timing events and the counter
-    // read-back) is captured once per call as a CUDA graph and relaunched
-    // until the device-side counters say the work is done: the kernels
-    // take their sizes from the counters, so every window is the same
-    // graph.  The executable graph is kept with the scene and updated in
-    // place when the next call's parameters differ.
-    {
-        CaptureGuard cap(s);
+    const int per_iter = 6 + (p.sort_mode != ATRC_SORT_NONE ? 2 : 0) + (guide ? 2 : 0) + (d.scene.has_subsurface ? 1 : 0);
+    // The kernels of one window of `window` wavefront iterations.  The
+    // kernels take their sizes from the device-side counters, so every window
+    // is the same sequence of launches.  `timed` records the events that
+    // split the window's device time into traversal, shading and shadow rays
+    // (event nodes are not allowed inside the device-side loop).
+    auto enqueue_window = [&](bool timed) {
         for (int k = 0; k < window; ++k) {
             k_begin<<<1, 1, 0, s>>>(c);
             k_generate<<<gsm, d.tuned_gen_threads, 0, s>>>(d.scene, p, P, c);
-            CK(cudaEventRecordWithFlags(kev[k * 4 + 0], s, cudaEventRecordExternal));
+            if (timed) CK(cudaEventRecordWithFlags(kev[k * 4 + 0], s, cudaEventRecordExternal));
             if (d.tuned_fetch) {
                 const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
                 if (wt) k_extend_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c, p.sort_mode, p.nkeys);
@@ -1928,14 +1981,14 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
                 k_sort_scan<<<1, 1024, 0, s>>>(P, p.nkeys);
                 k_sort_scatter<<<d.sm_count * 8, 128, 0, s>>>(P, c, p.nkeys);
             }
-            CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
+            if (timed) CK(cudaEventRecordWithFlags(kev[k * 4 + 1], s, cudaEventRecordExternal));
             if (guide) {
                 k_guide_features<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
                 guide_infer(guide, &c->n_guide, s);
             }
             k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             if (d.scene.has_subsurface) k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
-            CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
+            if (timed) CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
             if (d.tuned_shadow_fetch) {
                 const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
                 if (wt) k_shadow_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
@@ -1948,48 +2001,97 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             } else {
                 k_shadow<ISECT_FAST, false><<<g_shadow, 128, 0, s>>>(d.scene, P, c);
             }
-            CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
+            if (timed) CK(cudaEventRecordWithFlags(kev[k * 4 + 3], s, cudaEventRecordExternal));
             k_finish<<<gsm, d.tuned_fin_threads, 0, s>>>(p, P, c);
         }
         CK(cudaGetLastError());
+    };
+    CK(cudaEventRecord(ev0, s));
+    if (device_loop) {
+        // The whole bounce loop is one graph launch: a WHILE conditional node
+        // whose body is one window followed by k_loop_cond, which decides on
+        // the device whether another window runs.  The host waits once, at
+        // the end; per-view completion times are the device's timestamps.
+        // No path lives longer than max_depth + specular_depth iterations
+        // (plus a few for the MIS ray of its last vertex), and a slot starts
+        // a new path as soon as one ends, so the loop is bounded by
+        // (samples / pool + 1) path lengths; four times that stops it with a
+        // watchdog status should a bug keep it from finishing.
+        const unsigned long long per_path =
+            (unsigned long long)std::max(desc->max_depth, 1) + (unsigned long long)std::max(desc->specular_depth, 0) + 8;
+        const unsigned long long bound_iters = 4ULL * (total / cap + 2) * per_path + 256;
+        const int max_windows = int(std::min<unsigned long long>(bound_iters / window + 1, (1ULL << 30)));
+        cudaGraph_t outer = nullptr;
+        CK(cudaGraphCreate(&outer, 0));
+        struct GraphOwner {
+            cudaGraph_t g;
+            ~GraphOwner() { cudaGraphDestroy(g); }
+        } owner{outer};
+        cudaGraphConditionalHandle handle;
+        CK(cudaGraphConditionalHandleCreate(&handle, outer, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = handle;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        CK(cudaGraphAddNode(&node, outer, nullptr, 0, &np));
+        {
+            BodyCapture body(s, np.conditional.phGraph_out[0]);
+            enqueue_window(false);
+            k_loop_cond<<<1, 1, 0, s>>>(c, handle, max_windows);
+            CK(cudaGetLastError());
+            body.end();
+        }
+        d.loop_exec = instantiate_or_update(d.loop_exec, outer);
+        CK(cudaGraphLaunch(d.loop_exec, s));
         CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-        if (dbytes) CK(cudaMemcpyAsync(d.view_stage, p.view_done, dbytes, cudaMemcpyDeviceToHost, s));
-        cudaGraph_t g = cap.end();
-        d.window_exec = instantiate_or_update(d.window_exec, g);
-        cudaGraphDestroy(g);
-    }
-    for (int iter_block = 0;; ++iter_block) {
-        CK(cudaGraphLaunch(d.window_exec, s));
-        launches += (6 + (p.sort_mode != ATRC_SORT_NONE ? 2 : 0) + (guide ? 2 : 0) + (d.scene.has_subsurface ? 1 : 0)) *
-                    window;
-        ext_launches += window;
+        CK(cudaMemcpyAsync(d.view_stage, p.view_time, dbytes, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         hc = *pinned;
-        if (view_seconds && views_left) {
-            const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-            const unsigned long long* done = static_cast<const unsigned long long*>(d.view_stage);
-            for (int v = 0; v < nviews; ++v) {
-                const bool fin = nviews == 1 ? hc.done != 0 || hc.completed >= total : done[v] >= views[v].count;
-                if (!view_finished[v] && fin) {
-                    view_finished[v] = 1;
-                    view_seconds[v] = now;
-                    --views_left;
-                }
+        launches += uint64_t(hc.windows) * (uint64_t(window) * per_iter + 1);
+        ext_launches = uint64_t(hc.windows) * window;
+        if (view_seconds) {
+            const unsigned long long* vt = static_cast<const unsigned long long*>(d.view_stage);
+            for (int v = 0; v < nviews; ++v)
+                view_seconds[v] = vt[v] >= hc.t_start ? double(vt[v] - hc.t_start) * 1e-9 : 0.0;
+        }
+        if (hc.watchdog) status = ATRC_ERR_WATCHDOG;
+    } else {
+        // One window (its kernels, the timing events and the counter
+        // read-back) is captured once per call as a CUDA graph and relaunched
+        // until the device-side counters say the work is done; the host
+        // polls progress and the cancel callback between windows.  The
+        // executable graph is kept with the scene and updated in place when
+        // the next call's parameters differ.
+        {
+            CaptureGuard capg(s);
+            enqueue_window(true);
+            CK(cudaMemcpyAsync(pinned, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+            cudaGraph_t g = capg.end();
+            d.window_exec = instantiate_or_update(d.window_exec, g);
+            cudaGraphDestroy(g);
+        }
+        for (;;) {
+            CK(cudaGraphLaunch(d.window_exec, s));
+            launches += uint64_t(per_iter) * window;
+            ext_launches += window;
+            CK(cudaStreamSynchronize(s));
+            hc = *pinned;
+            for (int k = 0; k < window; ++k) {
+                float a = 0, b2 = 0, e3 = 0;
+                CK(cudaEventElapsedTime(&a, kev[k * 4 + 0], kev[k * 4 + 1]));
+                CK(cudaEventElapsedTime(&b2, kev[k * 4 + 1], kev[k * 4 + 2]));
+                CK(cudaEventElapsedTime(&e3, kev[k * 4 + 2], kev[k * 4 + 3]));
+                t_ext += a * 1e-3;
+                t_shade += b2 * 1e-3;
+                t_shadow += e3 * 1e-3;
             }
+            if (hc.watchdog) { status = ATRC_ERR_WATCHDOG; break; }
+            if (hc.done) break;
+            if (progress) progress(100.0 * double(hc.completed) / double(std::max(1ULL, total)), user);
+            if (should_stop && should_stop(user)) { status = ATRC_ERR_CANCELLED; break; }
         }
-        for (int k = 0; k < window; ++k) {
-            float a = 0, b2 = 0, e3 = 0;
-            CK(cudaEventElapsedTime(&a, kev[k * 4 + 0], kev[k * 4 + 1]));
-            CK(cudaEventElapsedTime(&b2, kev[k * 4 + 1], kev[k * 4 + 2]));
-            CK(cudaEventElapsedTime(&e3, kev[k * 4 + 2], kev[k * 4 + 3]));
-            t_ext += a * 1e-3;
-            t_shade += b2 * 1e-3;
-            t_shadow += e3 * 1e-3;
-        }
-        if (hc.watchdog) { status = ATRC_ERR_WATCHDOG; break; }
-        if (hc.done) break;
-        if (progress) progress(100.0 * double(hc.completed) / double(std::max(1ULL, total)), user);
-        if (should_stop && should_stop(user)) { status = ATRC_ERR_CANCELLED; break; }
     }
     CK(cudaEventRecord(ev1, s));
     CK(cudaEventSynchronize(ev1));
@@ -2111,6 +2213,7 @@ int atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide, const AtrcRenderD
         if (b.min_depth != a.min_depth || b.max_depth != a.max_depth || b.cont_prob != a.cont_prob ||
             b.specular_depth != a.specular_depth || b.eps != a.eps || b.sort_mode != a.sort_mode ||
             b.disney_fixed != a.disney_fixed || b.path_pool != a.path_pool || b.count_traversal != a.count_traversal ||
+            b.isect_mode != a.isect_mode ||
             b.renderer != a.renderer || b.ao_sample_count != a.ao_sample_count ||
             b.ao_max_distance != a.ao_max_distance ||
             std::memcmp(b.ao_low, a.ao_low, sizeof(a.ao_low)) || std::memcmp(b.ao_high, a.ao_high, sizeof(a.ao_high)) ||
@@ -2121,7 +2224,7 @@ int atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide, const AtrcRenderD
     }
     return guarded([&] {
         return render_impl(scene, views, films, n, nullptr, nullptr, nullptr, stats, guide ? guide_impl(guide) : nullptr,
-                           false, view_seconds);
+                           false, view_seconds, true);
     });
 }
 

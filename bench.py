@@ -56,9 +56,13 @@ def parse():
     p.add_argument("--guided-train-steps", type=int, default=4)
     p.add_argument("--no-batch", action="store_true", help="skip the batched multi-view comparison")
     p.add_argument("--no-ingest", action="store_true", help="skip the BVH builder comparison")
+    p.add_argument("--no-media", action="store_true", help="skip the participating-media workload")
+    p.add_argument("--media-spp", type=int, default=4)
+    p.add_argument("--media-steps", type=int, default=4)
     p.add_argument("--batch-views", type=int, default=64)
-    p.add_argument("--batch-spp-scale", type=float, default=1.0 / 64,
-                   help="scale of the [16, 1024] spp budgets (1/64 keeps the default run within minutes)")
+    p.add_argument("--batch-spp-scale", type=float, default=1.0 / 8,
+                   help="scale of the [16, 1024] spp budgets (1/8 keeps the default run within minutes; "
+                        "the full budgets are about 10 G samples)")
     return p.parse_args()
 
 
@@ -278,6 +282,75 @@ def guided_comparison(args) -> dict:
             "time_ratio_guided_over_plain": (mean_guided / mean_plain) if (mean_guided and mean_plain) else None}
 
 
+def media_comparison(args, l2_peak: float) -> dict:
+    """The participating-media workload at its stated size: a homogeneous box
+    medium and a 128^3 fBm density grid (delta tracking, ratio-tracked shadow
+    rays) around a 200,000-triangle displaced sphere, two area lights and the
+    sky, 1024 x 1024, max depth 32.  Steps of --media-spp samples per pixel,
+    timed with CUDA events on a device film (a rate: the stated 512 spp would
+    be 128 such steps); the closest-hit kernel's roofline as for the headline;
+    the oracle on a bounded sample of the same film as the CPU baseline."""
+    import torch
+
+    import oracle
+    from atrc_b200 import Config, DeviceScene, Film, scenes
+    cfg = Config.from_file(scenes.media_scene())
+    desc, _ = cfg.rendering(0)
+    dev = DeviceScene(cfg)
+    dev.autotune(desc, trial_spp=1)
+    spp = args.media_spp
+    desc.spp_count = spp
+    film = Film(desc.width, desc.height, device=True)
+    step = [0]
+
+    def run(count=False):
+        desc.first_spp = step[0] * spp
+        desc.count_traversal = 1 if count else 0
+        step[0] += 1
+        return dev.render(desc, film)
+    run()
+    cst = run(count=True)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record()
+    for _ in range(args.media_steps):
+        stats.append(run())
+    ev1.record()
+    torch.cuda.synchronize()
+    sec = ev0.elapsed_time(ev1) / 1e3
+    samples = desc.width * desc.height * spp * args.media_steps
+    crays = max(cst["rays_closest"], 1)
+    bpr = (cst["nodes_closest"] * 112 + cst["tris_closest"] * 48 + cst["ents_closest"] * 64) / crays + 56
+    ext = sum(st["extend_seconds"] for st in stats)
+    rays = sum(st["rays_closest"] for st in stats)
+    achieved = bpr * rays / max(ext, 1e-9) / 1e9
+    # CPU baseline: every 64th 32x32 tile of the film at 1 spp, on all host threads
+    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+    threads = oracle.hardware_threads()
+    hf = Film(desc.width, desc.height)
+    d1, _ = cfg.rendering(0)
+    d1.spp_count = 1
+    stride = 64
+    t0 = time.perf_counter()
+    ora.render_sample(d1, hf, threads, stride)
+    cpu_s = time.perf_counter() - t0
+    tiles = ((desc.width + 31) // 32) * ((desc.height + 31) // 32)
+    cpu_samples = len(range(0, tiles, stride)) * 32 * 32
+    return {"workload": "media_homogeneous_box_heterogeneous_128cube_200k_sphere_1024x1024_depth32",
+            "Msamples_per_s": samples / sec / 1e6, "steps": args.media_steps, "spp_per_step": spp,
+            "ms_per_step": sec / args.media_steps * 1e3,
+            "rays_closest_per_sample": rays / samples, "rays_shadow_per_sample":
+                sum(st["rays_shadow"] for st in stats) / samples,
+            "kernel_time_share": {"extend": ext / sec, "shade": sum(st["shade_seconds"] for st in stats) / sec,
+                                  "shadow": sum(st["shadow_seconds"] for st in stats) / sec},
+            "roofline": {"bound": "l2", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,
+                         "peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak, "bytes_per_ray": bpr},
+            "cpu_baseline": {"value": cpu_samples / cpu_s / 1e6, "unit": "Msamples/s", "cores": threads,
+                             "kind": "port", "sample": f"1 spp of every {stride}th 32x32 tile ({cpu_samples} "
+                                                       f"camera samples), {cpu_s:.1f} s"}}
+
+
 def batch_views(cfg, n: int, seed: int, spp_scale: float):
     """Seeded camera poses in the indoor room with resolutions drawn from
     {128^2, 256^2, 512^2, 1024^2, 1920x1080} and spp drawn log-uniformly from
@@ -324,7 +397,7 @@ def batch_comparison(args) -> dict:
         guide.train(steps=4)
     q = lambda a: {"median_s": float(np.median(a)), "p90_s": float(np.quantile(a, 0.9)), "max_s": float(np.max(a))}  # noqa: E731
 
-    def compare(views):
+    def compare(views, device_loop_one_by_one: bool):
         samples = sum(v.width * v.height * v.spp for v in views)
         films = [Film(v.width, v.height, device=True) for v in views]
         dev.render_batch(views[:2], films[:2], guide=guide)       # warm-up (graph, buffers)
@@ -340,18 +413,31 @@ def batch_comparison(args) -> dict:
             dev.render_guided(guide, v, f)
             one_secs.append(time.perf_counter() - t0)
         t_one = one_secs[-1]
-        return {"views": len(views), "samples": samples,
-                "resolutions": sorted({f"{v.width}x{v.height}" for v in views}),
-                "spp_range": [min(v.spp for v in views), max(v.spp for v in views)],
-                "batched": {"seconds": t_batch, "Msamples_per_s": samples / t_batch / 1e6, "completion": q(secs)},
-                "one_by_one": {"seconds": t_one, "Msamples_per_s": samples / t_one / 1e6, "completion": q(one_secs)},
-                "speedup": t_one / t_batch}
-    full = compare(batch_views(cfg, args.batch_views, 1004, args.batch_spp_scale))
+        out = {"views": len(views), "samples": samples,
+               "resolutions": sorted({f"{v.width}x{v.height}" for v in views}),
+               "spp_range": [min(v.spp for v in views), max(v.spp for v in views)],
+               "batched": {"seconds": t_batch, "Msamples_per_s": samples / t_batch / 1e6, "completion": q(secs),
+                           "loop": "one graph launch: device-side WHILE node, per-view device timestamps"},
+               "one_by_one": {"seconds": t_one, "Msamples_per_s": samples / t_one / 1e6, "completion": q(one_secs),
+                              "loop": "atrc_cuda_render_guided per view (windowed graph, host polls)"},
+               "speedup": t_one / t_batch}
+        if device_loop_one_by_one:
+            # the same views one by one through the device-side loop: what
+            # sharing one path pool gains, apart from the loop itself
+            t0 = time.perf_counter()
+            for v, f in zip(views, films):
+                f.clear()
+                dev.render_batch([v], [f], guide=guide)
+            t_one_loop = time.perf_counter() - t0
+            out["one_by_one_device_loop"] = {"seconds": t_one_loop, "Msamples_per_s": samples / t_one_loop / 1e6}
+            out["speedup_vs_device_loop"] = t_one_loop / t_batch
+        return out
+    full = compare(batch_views(cfg, args.batch_views, 1004, args.batch_spp_scale), True)
     # the regime batching is for: many small views that cannot fill the GPU alone
     small = batch_views(cfg, args.batch_views, 1005, 1.0 / 64)
     for v in small:
         v.width = v.height = 128 if v.width < 1024 else 256
-    small_r = compare(small)
+    small_r = compare(small, False)
     return {"workload": f"indoor_room_{args.batch_views}_views", "spp_scale": args.batch_spp_scale,
             "tuning": {k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
                                               "finish_threads", "extend_fetch", "queue_order", "shadow_fetch")},
@@ -505,6 +591,8 @@ def main():
         batch = batch_comparison(args) if world == 1 and not args.no_batch else None
         ingest = ingest_comparison(args, cfg, desc, tuning, build_s, value) if world == 1 and not args.no_ingest \
             else None
+        media = media_comparison(args, l2_peak) if world == 1 and not args.no_media and args.scene == "instanced" \
+            else None
         clocks = clk.summary()
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -550,6 +638,7 @@ def main():
             "guided": guided,
             "batch": batch,
             "ingest": ingest,
+            "media": media,
         }
         print(json.dumps(line), flush=True)
     if dist:

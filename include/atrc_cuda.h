@@ -688,12 +688,18 @@ int  atrc_guide_gradients(AtrcGuide* guide, const float* records, size_t n,
 
 /* Batched multi-view render (no counterpart in the reference, which renders
  * one camera per `rendering` entry): n views (camera, size, spp, seed,
- * filter may differ; depth, roulette, eps, sort, Disney and pool settings
- * must be equal) share one wavefront path pool, so small views fill the GPU
- * together.  Films must hold device pointers.  `guide` may be NULL (plain)
- * or a trained guide (sampling only).  view_seconds (may be NULL) receives
- * per view the time from the start of the call at which its last sample was
- * splatted.  At most 1024 views. */
+ * filter may differ; depth, roulette, eps, sort, Disney, pool and
+ * intersection settings must be equal) share one wavefront path pool, so
+ * small views fill the GPU together and one view's tail overlaps the next
+ * view's start.  The whole bounce loop is one graph launch: a device-side
+ * WHILE conditional node runs windows of wavefront iterations until the
+ * counters say every sample is splatted (bounded: a loop that ran longer than
+ * any path allows ends with ATRC_ERR_WATCHDOG); the host waits once.  Films
+ * must hold device pointers.  `guide` may be NULL (plain) or a trained guide
+ * (sampling only).  view_seconds (may be NULL) receives per view the time,
+ * on the device's global timer, from the start of the render to the splat of
+ * the view's last sample.  `stats` has counts but no per-kernel timings.
+ * At most 1024 views. */
 int  atrc_cuda_render_batch(AtrcScene* scene, AtrcGuide* guide,
                             const AtrcRenderDesc* views, int32_t n,
                             const AtrcFilm* films, double* view_seconds,

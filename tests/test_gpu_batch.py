@@ -67,3 +67,24 @@ def test_guided_batch(cornell_path):
     for d, f in zip(views, films):
         img = f.image()
         assert np.all(np.isfinite(img)) and img.mean() > 0
+
+
+def test_device_loop_long_paths_small_pool(scene_dir):
+    # depth-32 paths through media with a 1024-path pool: many refills of the
+    # pool inside one graph launch; the loop bound must not cut the render
+    # short, and the batch must equal the single-view render of the same view
+    from atrc_b200.scenes import media_scene
+    cfg = Config.from_file(media_scene(scene_dir / "media_loop", width=24, height=24, spp=64, grid_res=32,
+                                       sphere_level=3))
+    dev = DeviceScene(cfg)
+    d, _ = cfg.rendering(0)
+    d.sort_mode, d.path_pool = 0, 1024
+    fb = Film(d.width, d.height, device=True)
+    st, secs = dev.render_batch([d], [fb])
+    assert st["samples"] == 24 * 24 * 64 and st["watchdog_flags"] == 0
+    # 36,864 samples through 1,024 slots: the pool is refilled about 36 times
+    assert secs[0] > 0 and st["iterations"] > 40
+    one = Film(d.width, d.height, device=True)
+    dev.render(d, one)
+    np.testing.assert_allclose(fb.weight.cpu().numpy(), one.weight.cpu().numpy(), rtol=1e-12)
+    np.testing.assert_allclose(fb.value.cpu().numpy(), one.value.cpu().numpy(), rtol=1e-6, atol=1e-9)

@@ -172,3 +172,80 @@ def test_guided_render_is_unbiased(cornell_path):
     frac, allowed, info = band_test(guided, plain, 1 / (4 * r * r))
     assert frac <= allowed, (frac, allowed, info)
     assert global_mean_z(guided, plain) < 4.0
+
+
+def _train_records(rng, n):
+    rec = np.zeros((n, RECORD_FLOATS), np.float32)
+    rec[:, :3] = rng.uniform(-1, 1, (n, 3))
+    rec[:, 3:6] = _unit(rng, n)
+    rec[:, 6:9] = _unit(rng, n)
+    rec[:, 9] = rng.uniform(0, 1, n)
+    # half the sampled directions near one lobe, half uniform
+    lobe = np.array([0.3, -0.5, 0.81]) / np.linalg.norm([0.3, -0.5, 0.81])
+    near = lobe + 0.3 * rng.normal(size=(n, 3))
+    wi = np.where(rng.uniform(size=(n, 1)) < 0.5, near, rng.normal(size=(n, 3)))
+    rec[:, 10:13] = wi / np.linalg.norm(wi, axis=1, keepdims=True)
+    rec[:, 13] = rng.uniform(0.05, 1.0, n)
+    rec[:, 17] = rng.uniform(0, 2, n) * (rng.uniform(size=n) > 0.1)
+    rec[:, 21] = -1
+    return rec
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def test_training_gradients_match_fp64_backward():
+    # 300 tiles of 128 records on 148 SMs: CTAs accumulate dW^T in TMEM over
+    # two or three tiles before their atomic flush
+    g, w, t, info = _random_guide(seed=5)
+    g.close()
+    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=5, record_capacity=1 << 16)
+    info = g.info()
+    g.set_params(w, t)
+    rng = np.random.default_rng(17)
+    rec = _train_records(rng, 128 * 300)
+    gw, gt, loss = g.gradients(rec)
+    rw, rt, rloss = R.backward(rec, w, t, info, bf16_ops=True)
+    assert abs(loss - rloss) <= 1e-3 * abs(rloss)
+    # the kernel computes exactly the BF16-operand backward up to FP32 sums
+    assert _rel(gw, rw) < 5e-3, _rel(gw, rw)
+    assert _rel(gt, rt) < 5e-3, _rel(gt, rt)
+    cos = float(np.dot(gw, rw) / np.linalg.norm(gw) / np.linalg.norm(rw))
+    assert cos > 0.99999, cos
+    # per layer, so that a wrong layer cannot hide behind a large one
+    offs = np.cumsum([0, 64 * 112, 64 * 64, 64 * 64, 48 * 64])
+    for a, b in zip(offs[:-1], offs[1:]):
+        assert _rel(gw[a:b], rw[a:b]) < 1e-2, (a, _rel(gw[a:b], rw[a:b]))
+    # and against the all-FP64 network to BF16 precision
+    fw, ft, _ = R.backward(rec, w, t, info, bf16_ops=False)
+    assert _rel(gw, fw) < 0.05 and _rel(gt, ft) < 0.05
+
+
+def test_adam_steps_match_reference():
+    g, w, t, info = _random_guide(seed=6)
+    g.close()
+    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=6, record_capacity=1 << 16, batch=1 << 16)
+    info = g.info()
+    g.set_params(w, t)
+    lr = g.desc.learning_rate
+    rng = np.random.default_rng(23)
+    batches = [_train_records(rng, 128 * 64), _train_records(rng, 128 * 64)]
+    p = np.concatenate([w, t]).astype(np.float64)
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    for step, rec in enumerate(batches, 1):
+        gw, gt, _ = g.gradients(rec)          # at the current parameters
+        grad = np.concatenate([gw, gt]).astype(np.float64)
+        g.train_records(rec, steps=1)         # the same gradient, then one Adam step
+        want, m, v = R.adam_step(p, grad, m, v, step, lr)
+        pw, pt = g.params()
+        got = np.concatenate([pw, pt]).astype(np.float64)
+        # the step's gradient is summed again inside train_records, in another
+        # atomic order: a component whose sum is within rounding of zero may
+        # take the other sign; everything else moves as the formula says
+        err = np.abs(got - want)
+        assert np.mean(err <= 1e-6 + 1e-5 * lr) > 0.999, (step, np.quantile(err, [0.5, 0.999]))
+        moved = np.abs(want - p) > 0
+        assert moved.mean() > 0.01
+        p = got
