@@ -122,13 +122,14 @@ class AtrcTuning(C.Structure):
     _fields_ = [("path_pool", C.c_int32), ("sort_mode", C.c_int32), ("gen_blocks_per_sm", C.c_int32),
                 ("gen_threads", C.c_int32), ("finish_threads", C.c_int32), ("trials", C.c_int32),
                 ("ms_per_msample", C.c_double), ("default_ms_per_msample", C.c_double), ("extend_fetch", C.c_int32),
-                ("queue_order", C.c_int32), ("shadow_fetch", C.c_int32), ("pad_", C.c_int32)]
+                ("queue_order", C.c_int32), ("shadow_fetch", C.c_int32), ("shadow_sort", C.c_int32)]
 
 
 class AtrcGuideDesc(C.Structure):
     _fields_ = [("log2_table", C.c_int32), ("base_resolution", C.c_int32), ("max_resolution", C.c_int32),
                 ("batch", C.c_int32), ("record_capacity", C.c_int32), ("learning_rate", C.c_float),
-                ("max_depth", C.c_int32), ("pad_", C.c_int32), ("seed", C.c_uint64)]
+                ("max_depth", C.c_int32), ("max_select", C.c_float), ("seed", C.c_uint64),
+                ("target_clamp", C.c_float), ("pad_", C.c_int32)]
 
 
 class AtrcGuideInfo(C.Structure):

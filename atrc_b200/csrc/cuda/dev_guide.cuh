@@ -36,7 +36,7 @@ constexpr int kGuideOut = 48;
 constexpr int kGuideUsed = 5 * kGuideLobes + 1;
 constexpr int kHashLevels = 16;
 constexpr int kHashFeatures = 2;
-constexpr float kGuideMaxSelect = 0.9f;   // c = kGuideMaxSelect * sigmoid(o[40] + kSelectOffset)
+constexpr float kGuideMaxSelect = 0.9f;   // default cap: c = max_select * sigmoid(o[40] + kSelectOffset)
 constexpr float kSelectOffset = -2.0f;    // an untrained guide (o ~ 0) is picked with c ~ 0.11
 constexpr float kLogKappaMin = -6.9f;     // kappa in [1e-3, 1e4]
 constexpr float kLogKappaMax = 9.2f;
@@ -125,7 +125,8 @@ __device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + __ex
 // vMF lobe density: kappa / (2 pi (1 - e^{-2 kappa})) exp(kappa (cos - 1)).
 __device__ __forceinline__ float vmf_norm(float kappa) { return kappa / (2.0f * kPi * -expm1f(-2.0f * kappa)); }
 
-__device__ __forceinline__ void guide_decode(const float* o, GuideMix* m) {
+// max_select: the cap on the selection probability (AtrcGuideDesc.max_select).
+__device__ __forceinline__ void guide_decode(const float* o, GuideMix* m, float max_select = kGuideMaxSelect) {
     float mx = -1e30f;
     for (int k = 0; k < kGuideLobes; ++k) mx = fmaxf(mx, o[5 * k + 4]);
     float sum = 0;
@@ -141,7 +142,7 @@ __device__ __forceinline__ void guide_decode(const float* o, GuideMix* m) {
         sum += m->w[k];
     }
     for (int k = 0; k < kGuideLobes; ++k) m->w[k] /= sum;
-    m->c = kGuideMaxSelect * sigmoidf_(o[5 * kGuideLobes] + kSelectOffset);
+    m->c = max_select * sigmoidf_(o[5 * kGuideLobes] + kSelectOffset);
 }
 
 __device__ __forceinline__ float guide_pdf(const GuideMix& m, Vec3 d) {

@@ -61,6 +61,7 @@ struct NetView {
     const __half* table_h;    // FP16 table (inference)
     const float* table_f;     // FP32 table (training)
     HashGrid grid;
+    float max_select;         // cap on the selection probability
 };
 
 // Copy W (rows x cols, row-major, BF16 in global) into a K-major operand in
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(kTile, 2) k_guide_mlp(NetView net, const uint8
         float* o = reinterpret_cast<float*>(X) + t * kGuideOut;
         if (DECODE) {
             GuideMix m;
-            guide_decode(v, &m);
+            guide_decode(v, &m, net.max_select);
             for (int k = 0; k < kGuideLobes; ++k) {
                 o[5 * k] = m.mu[k][0];
                 o[5 * k + 1] = m.mu[k][1];
@@ -283,15 +284,16 @@ struct TrainArgs {
     float* grad_w;             // FP32 gradients of the packed weights
     float* grad_table;         // FP32 gradients of the table
     float* loss;               // sum of the batch's loss terms
+    float target_clamp;        // > 0: record targets capped at this multiple of the batch mean
 };
 
 // Gradient of loss = -w log(c g + (1 - c) b) with respect to the raw outputs.
-__device__ void loss_grad(const float* o, const GuideRecord& r, float w, float* d, float* loss) {
+__device__ void loss_grad(const float* o, const GuideRecord& r, float w, float max_select, float* d, float* loss) {
     for (int k = 0; k < kGuideOut; ++k) d[k] = 0.0f;
     *loss = 0.0f;
     if (!(w > 0.0f)) return;
     GuideMix m;
-    guide_decode(o, &m);
+    guide_decode(o, &m, max_select);
     const Vec3 wi(r.wi[0], r.wi[1], r.wi[2]);
     float v[kGuideLobes], dots[kGuideLobes];
     float g = 0.0f;
@@ -306,7 +308,7 @@ __device__ void loss_grad(const float* o, const GuideRecord& r, float w, float* 
     *loss = -w * logf(q);
     const float dq = -w / q;
     // selection: c = cmax sigmoid(s), dc/ds = c (1 - sigmoid(s))
-    const float sg = m.c / kGuideMaxSelect;
+    const float sg = m.c / max_select;
     d[5 * kGuideLobes] = dq * (g - b) * m.c * (1.0f - sg);
     const float dg = dq * m.c;
     for (int k = 0; k < kGuideLobes; ++k) {
@@ -377,6 +379,9 @@ __global__ void __launch_bounds__(kTile, 1) k_guide_train(NetView net, TrainArgs
     const uint32_t tm = *tslot;
     auto S = [&](int off) { return tc::smem_addr(smem + off); };
     const float inv_wsum = *a.weight_sum > 0 ? 1.0f / *a.weight_sum : 0.0f;
+    // a few records of a batch can carry most of its weight (a path that found
+    // the light): capping the targets keeps one step from following them alone
+    const float tcap = a.target_clamp > 0.0f ? a.target_clamp * *a.weight_sum / float(max(a.n, 1)) : INFINITY;
     uint32_t phase = 0;
     const int t = threadIdx.x;
     bool first = true, ok = true;
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(kTile, 1) k_guide_train(NetView net, TrainArgs
         for (int j = 0; j < 3; ++j) { q.pos[j] = r.pos[j]; q.nrm[j] = r.nrm[j]; q.wo[j] = r.wo[j]; }
         q.rough = r.rough;
         q.slot = 0;
-        const float w = i < a.n ? r.target * inv_wsum : 0.0f;
+        const float w = i < a.n ? fminf(r.target, tcap) * inv_wsum : 0.0f;
         // ---- forward
         write_inputs<float>(net.grid, net.table_f, q, t, smem + kTrP0, smem + kTrXT);
         float v[kGuideHidden];
@@ -408,7 +413,7 @@ __global__ void __launch_bounds__(kTile, 1) k_guide_train(NetView net, TrainArgs
         // ---- loss gradient of this thread's record
         float d[kGuideHidden];
         float lo;
-        loss_grad(v, r, w, d, &lo);
+        loss_grad(v, r, w, net.max_select, d, &lo);
         loss_acc += lo;
         dz_store(d, kGuideOut, smem + kTrDZ, smem + kTrDZT, t);
         // ---- backward: dA3 = dZ4 W4, dW4^T += H3^T dZ4
@@ -577,6 +582,7 @@ struct GuideImpl {
         v.table_h = t_h.as<__half>();
         v.table_f = t_f.as<float>();
         v.grid = grid;
+        v.max_select = desc.max_select;
         return v;
     }
     ~GuideImpl() {
@@ -686,6 +692,8 @@ int atrc_guide_default_desc(AtrcGuideDesc* d) {
     // depths 2, 3, 4 and all)
     d->max_depth = 3;
     d->learning_rate = 1e-2f;
+    d->max_select = kGuideMaxSelect;
+    d->target_clamp = 0.0f;
     d->batch = 1 << 18;
     d->record_capacity = 1 << 20;
     d->seed = 7;
@@ -698,7 +706,8 @@ int atrc_guide_create(int device, const float scene_lo[3], const float scene_hi[
     *out = nullptr;
     if (desc->log2_table < 8 || desc->log2_table > 22 || desc->base_resolution < 2 ||
         desc->max_resolution < desc->base_resolution || desc->batch < kTile || desc->record_capacity < kTile ||
-        !(desc->learning_rate > 0) || desc->max_depth < 0)
+        !(desc->learning_rate > 0) || desc->max_depth < 0 || !(desc->max_select > 0 && desc->max_select <= 0.99f) ||
+        !(desc->target_clamp >= 0))
         return gfail(ATRC_ERR_INVALID_ARG, "atrc_guide_create: parameter out of range");
     return gguarded([&] {
         auto g = std::make_unique<AtrcGuide>();
@@ -805,7 +814,7 @@ int atrc_guide_info(AtrcGuide* g, AtrcGuideInfo* info) {
     for (int a = 0; a < 3; ++a) { info->grid_lo[a] = G.grid.lo[a]; info->grid_inv_extent[a] = G.grid.inv_ext[a]; }
     for (int l = 0; l < kHashLevels; ++l) info->grid_res[l] = G.grid.res[l];
     info->log2_table = G.grid.log2_table;
-    info->max_select = kGuideMaxSelect;
+    info->max_select = G.desc.max_select;
     return ATRC_OK;
 }
 
@@ -907,6 +916,7 @@ static void train_step(GuideImpl& G, const GuideRecord* rec, int n, float* loss_
     a.grad_w = G.w_g.as<float>();
     a.grad_table = G.t_g.as<float>();
     a.loss = sc + 1;
+    a.target_clamp = G.desc.target_clamp;
     const int tiles = (n + kTile - 1) / kTile;
     k_guide_train<<<std::min(tiles, G.sm_count), kTile, kTrSmem, s>>>(G.view(), a, G.err.as<int>());
     ++G.steps;
@@ -1003,6 +1013,7 @@ int atrc_guide_gradients(AtrcGuide* g, const float* records, size_t n, float* gr
         a.grad_w = G.w_g.as<float>();
         a.grad_table = G.t_g.as<float>();
         a.loss = sc + 1;
+        a.target_clamp = G.desc.target_clamp;
         const int tiles = int((n + kTile - 1) / kTile);
         k_guide_train<<<std::min(tiles, G.sm_count), kTile, kTrSmem, s>>>(G.view(), a, G.err.as<int>());
         CK(cudaGetLastError());

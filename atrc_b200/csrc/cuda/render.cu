@@ -233,13 +233,24 @@ struct Pool {
     int* q_sss;                   // paths whose BSDF sample entered a subsurface material
     int* slot_state;              // per slot: kSlotFree / kSlotCont / kSlotBusy
     float4 *sh_o, *sh_d, *sh_c;   // shadow rays: o.tmin, d.tmax, contribution + path
+    // shadow-queue sort by origin cell (AtrcTuning.shadow_sort): a 16^3 grid
+    // over the scene bound in Morton order; k_shadow reads the queue through
+    // sh_sorted so that a warp's rays start near each other
+    int shadow_sort;
+    int* sh_key;                  // per shadow entry: its origin's cell
+    int* sh_sorted;               // shadow entries in cell order
+    int* sh_count;                // per cell: entries this iteration
+    int* sh_cursor;               // per cell: next write position in sh_sorted
+    float sk_lo[3], sk_scale[3];  // origin -> cell coordinates (16 / extent)
     int cap, shadow_cap;
 };
+constexpr int kShadowKeys = 4096;  // 16 x 16 x 16 origin cells
 
 __global__ void k_init(Pool P, int cap, int nkeys, Counters* c, unsigned long long total) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < cap) P.slot_state[i] = kSlotFree;
     if (i < nkeys) P.key_count[i] = 0;
+    if (i < kShadowKeys) P.sh_count[i] = 0;
     if (i == 0) {
         memset(c, 0, sizeof(Counters));
         c->n_free = cap;
@@ -466,14 +477,14 @@ __device__ __forceinline__ void count_key(const Scene& S, Pool& P, int sort_mode
     if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(P.key_count + key, __popc(same));
 }
 
-// Exclusive scan of the key counts into write cursors (one block of 1024);
+// Exclusive scan of key counts into write cursors (one block of 1024);
 // clears the counts for the next iteration.
-__global__ void __launch_bounds__(1024) k_sort_scan(Pool P, int nkeys) {
+__device__ __forceinline__ void scan_counts(int* count, int* cursor, int nkeys) {
     __shared__ int part[1024];
     const int t = threadIdx.x, per = (nkeys + 1023) / 1024;
     const int b0 = min(nkeys, t * per), b1 = min(nkeys, b0 + per);
     int sum = 0;
-    for (int k = b0; k < b1; ++k) sum += P.key_count[k];
+    for (int k = b0; k < b1; ++k) sum += count[k];
     part[t] = sum;
     __syncthreads();
     for (int o = 1; o < 1024; o <<= 1) {
@@ -484,12 +495,16 @@ __global__ void __launch_bounds__(1024) k_sort_scan(Pool P, int nkeys) {
     }
     int acc = part[t] - sum;
     for (int k = b0; k < b1; ++k) {
-        const int cnt = P.key_count[k];
-        P.key_cursor[k] = acc;
+        const int cnt = count[k];
+        cursor[k] = acc;
         acc += cnt;
-        P.key_count[k] = 0;
+        count[k] = 0;
     }
 }
+
+__global__ void __launch_bounds__(1024) k_sort_scan(Pool P, int nkeys) { scan_counts(P.key_count, P.key_cursor, nkeys); }
+
+__global__ void __launch_bounds__(1024) k_shsort_scan(Pool P) { scan_counts(P.sh_count, P.sh_cursor, kShadowKeys); }
 
 // Scatter the extend queue into key order (order within a key is arbitrary).
 // A block takes kScatterPer x blockDim entries per pass, counts them per key
@@ -537,6 +552,40 @@ __global__ void k_sort_scatter(Pool P, Counters* c, int nkeys) {
 #pragma unroll
         for (int e = 0; e < kScatterPer; ++e)
             if (key[e] >= 0) P.q_sorted[run[key[e]] + rank[e]] = slot[e];
+        __syncthreads();
+    }
+}
+
+// Scatter the shadow queue's entry indices into cell order, with the same
+// block-aggregated key runs as k_sort_scatter (4096 cells: 16 KB of shared
+// memory per block).
+__global__ void __launch_bounds__(128) k_shsort_scatter(Pool P, Counters* c) {
+    __shared__ int run[kShadowKeys];
+    const int n = min(c->n_shadow, P.shadow_cap), lane = threadIdx.x & 31;
+    const int span = kScatterPer * blockDim.x;
+    for (int i0 = blockIdx.x * span; i0 < n; i0 += gridDim.x * span) {  // block-uniform
+        for (int k = threadIdx.x; k < kShadowKeys; k += blockDim.x) run[k] = 0;
+        __syncthreads();
+        int key[kScatterPer], rank[kScatterPer];
+#pragma unroll
+        for (int e = 0; e < kScatterPer; ++e) {
+            const int i = i0 + e * int(blockDim.x) + int(threadIdx.x);
+            key[e] = i < n ? P.sh_key[i] : -1;
+            const unsigned same = __match_any_sync(0xffffffffu, key[e]);
+            const int leader = __ffs(same) - 1;
+            int r = 0;
+            if (lane == leader && key[e] >= 0) r = atomicAdd(run + key[e], __popc(same));
+            rank[e] = __shfl_sync(0xffffffffu, r, leader) + __popc(same & ((1u << lane) - 1u));
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kShadowKeys; k += blockDim.x)
+            if (run[k] > 0) run[k] = atomicAdd(P.sh_cursor + k, run[k]);
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < kScatterPer; ++e) {
+            const int i = i0 + e * int(blockDim.x) + int(threadIdx.x);
+            if (key[e] >= 0) P.sh_sorted[run[key[e]] + rank[e]] = i;
+        }
         __syncthreads();
     }
 }
@@ -615,6 +664,18 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_extend_f
     if (COUNT) flush_count(c->cnt_closest, tc);
 }
 
+// Morton code of the 16^3 cell holding p (coordinates clamped to the grid).
+__device__ __forceinline__ int shadow_cell(const Pool& P, Vec3 p) {
+    const float v[3] = {p.x, p.y, p.z};
+    int code = 0;
+    for (int a = 0; a < 3; ++a) {
+        const float x = (v[a] - P.sk_lo[a]) * P.sk_scale[a];
+        const int c = min(15, max(0, int(x)));  // NaN and out-of-range origins go to the edge cells
+        for (int b = 0; b < 4; ++b) code |= ((c >> b) & 1) << (3 * b + a);
+    }
+    return code;
+}
+
 __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d, float tmin, float tmax, Vec3 contrib,
                                             int slot) {
     const int k = warp_append(&c->n_shadow, true);
@@ -622,6 +683,12 @@ __device__ __forceinline__ void push_shadow(Pool& P, Counters* c, Vec3 o, Vec3 d
     P.sh_o[k] = make_float4(o.x, o.y, o.z, tmin);
     P.sh_d[k] = make_float4(d.x, d.y, d.z, tmax);
     P.sh_c[k] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(slot));
+    if (P.shadow_sort) {
+        const int key = shadow_cell(P, o);
+        P.sh_key[k] = key;
+        const unsigned same = __match_any_sync(__activemask(), key);
+        if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(P.sh_count + key, __popc(same));
+    }
 }
 
 // Materials the guide samples for: the non-delta BSDFs whose sampler
@@ -1145,7 +1212,8 @@ template <int ISECT, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, ATRC_SHADOW_MIN_BLOCKS) k_shadow(Scene S, Pool P, Counters* c) {
     const int n = min(c->n_shadow, P.shadow_cap);
     TraceCount tc{0, 0, 0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int i = P.shadow_sort ? P.sh_sorted[j] : j;
         const float4 o = P.sh_o[i], d = P.sh_d[i];
         Hit h;
         int wd = 0;
@@ -1186,7 +1254,7 @@ __global__ void __launch_bounds__(kTraceBlock, ATRC_TRACE_MIN_BLOCKS) k_shadow_f
             if (i < 0) {
                 const int k = base + __popc(idle & ((1u << lane) - 1u));
                 if (k < n) {
-                    i = k;
+                    i = P.shadow_sort ? P.sh_sorted[k] : k;
                     const float4 o = P.sh_o[i], d = P.sh_d[i];
                     tr.init(S, stack, xyz(o), xyz(d), o.w, d.w);
                 }
@@ -1403,6 +1471,7 @@ struct DeviceSceneImpl {
     int tuned_fetch = 0;          // k_extend_fetch instead of k_extend
     int tuned_queue = 0;          // extend queue in slot order (1) or shade order (0)
     int tuned_shadow_fetch = 0;   // k_shadow_fetch instead of k_shadow
+    int tuned_shadow_sort = 0;    // shadow queue in origin-cell order
     int tuned_trials = 0;
     double tuned_ms = 0, default_ms = 0;
     DevBuf tune_film;
@@ -1478,7 +1547,7 @@ void check_device_ready() {
 
 // Layout of the path pool inside one allocation.
 struct PoolLayout {
-    size_t off[24];
+    size_t off[28];
     size_t total;
 };
 
@@ -1497,6 +1566,7 @@ PoolLayout pool_layout(size_t cap, size_t shadow_cap, int nkeys) {
     take(15, shadow_cap * 16); take(16, shadow_cap * 16); take(17, shadow_cap * 16);
     take(18, cap * 4); take(19, cap * 4); take(20, size_t(nkeys) * 4); take(21, size_t(nkeys) * 4);
     take(22, cap * 4);
+    take(23, shadow_cap * 4); take(24, shadow_cap * 4); take(25, kShadowKeys * 4); take(26, kShadowKeys * 4);
     L.total = (o + 255) & ~size_t(255);
     return L;
 }
@@ -1527,9 +1597,26 @@ Pool pool_from(void* base, const PoolLayout& L, size_t cap, size_t shadow_cap) {
     P.key_count = reinterpret_cast<int*>(b + L.off[20]);
     P.key_cursor = reinterpret_cast<int*>(b + L.off[21]);
     P.q_sss = reinterpret_cast<int*>(b + L.off[22]);
+    P.sh_key = reinterpret_cast<int*>(b + L.off[23]);
+    P.sh_sorted = reinterpret_cast<int*>(b + L.off[24]);
+    P.sh_count = reinterpret_cast<int*>(b + L.off[25]);
+    P.sh_cursor = reinterpret_cast<int*>(b + L.off[26]);
+    P.shadow_sort = 0;
+    for (int a = 0; a < 3; ++a) P.sk_lo[a] = P.sk_scale[a] = 0.0f;
     P.cap = int(cap);
     P.shadow_cap = int(shadow_cap);
     return P;
+}
+
+// The shadow-queue sort of a render: on when the scene's tuning asks for
+// it, over the scene's bound.
+void set_shadow_sort(Pool* P, const Scene& S, int on) {
+    P->shadow_sort = on;
+    for (int a = 0; a < 3; ++a) {
+        const float ext = S.scene_hi[a] - S.scene_lo[a];
+        P->sk_lo[a] = S.scene_lo[a];
+        P->sk_scale[a] = ext > 0.0f ? 16.0f / ext : 0.0f;
+    }
 }
 
 // Settings shared by the views of a render (taken from the first view).
@@ -1891,6 +1978,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
         p.gf = guide_frame(guide, cap, record, s);
     }
     Pool P = pool_from(d.pool_buf.p, L, cap, shadow_cap);
+    set_shadow_sort(&P, d.scene, d.tuned_shadow_sort);
     Counters* c = d.counters.as<Counters>();
     // films
     const size_t npix = size_t(desc->width) * desc->height;
@@ -1939,7 +2027,8 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     // one path / ray per thread for the heavy kernels (grids cover the
     // pool; threads past the device-side count return at once)
     const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
-    k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
+    k_init<<<int((std::max<size_t>({cap, size_t(p.nkeys), size_t(kShadowKeys)}) + 255) / 256), 256, 0, s>>>(
+        P, int(cap), p.nkeys, c, total);
     CK(cudaGetLastError());
     uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
     cudaEvent_t ev0 = d.ev0, ev1 = d.ev1;
@@ -1954,7 +2043,8 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     // only; a watertight render ignores them
     const bool wt = desc->isect_mode == ATRC_ISECT_WATERTIGHT;
     const bool count = desc->count_traversal != 0 && !wt;
-    const int per_iter = 6 + (p.sort_mode != ATRC_SORT_NONE ? 2 : 0) + (guide ? 2 : 0) + (d.scene.has_subsurface ? 1 : 0);
+    const int per_iter = 6 + (p.sort_mode != ATRC_SORT_NONE ? 2 : 0) + (guide ? 2 : 0) + (d.scene.has_subsurface ? 1 : 0) +
+                         (P.shadow_sort ? 2 : 0);
     // The kernels of one window of `window` wavefront iterations.  The
     // kernels take their sizes from the device-side counters, so every window
     // is the same sequence of launches.  `timed` records the events that
@@ -1989,6 +2079,10 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
             k_shade<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             if (d.scene.has_subsurface) k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
             if (timed) CK(cudaEventRecordWithFlags(kev[k * 4 + 2], s, cudaEventRecordExternal));
+            if (P.shadow_sort) {
+                k_shsort_scan<<<1, 1024, 0, s>>>(P);
+                k_shsort_scatter<<<d.sm_count * 8, 128, 0, s>>>(P, c);
+            }
             if (d.tuned_shadow_fetch) {
                 const int g_fetch = d.sm_count * ATRC_TRACE_MIN_BLOCKS;
                 if (wt) k_shadow_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);
@@ -2240,7 +2334,7 @@ static void tuning_out(const DeviceSceneImpl& d, AtrcTuning* out) {
     out->extend_fetch = d.tuned_fetch;
     out->queue_order = d.tuned_queue;
     out->shadow_fetch = d.tuned_shadow_fetch;
-    out->pad_ = 0;
+    out->shadow_sort = d.tuned_shadow_sort;
 }
 
 int atrc_cuda_get_tuning(AtrcScene* scene, AtrcTuning* out) {
@@ -2255,7 +2349,7 @@ static bool tuning_valid(const AtrcTuning& t) {
            t.sort_mode <= ATRC_SORT_MATERIAL && t.gen_blocks_per_sm >= 1 && t.gen_blocks_per_sm <= 64 &&
            pow2_in(t.gen_threads, 32, 1024) && pow2_in(t.finish_threads, 32, 1024) &&
            (t.extend_fetch == 0 || t.extend_fetch == 1) && (t.queue_order == 0 || t.queue_order == 1) &&
-           (t.shadow_fetch == 0 || t.shadow_fetch == 1);
+           (t.shadow_fetch == 0 || t.shadow_fetch == 1) && (t.shadow_sort == 0 || t.shadow_sort == 1);
 }
 
 int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
@@ -2270,6 +2364,7 @@ int atrc_cuda_set_tuning(AtrcScene* scene, const AtrcTuning* in) {
     d.tuned_fetch = in->extend_fetch;
     d.tuned_queue = in->queue_order;
     d.tuned_shadow_fetch = in->shadow_fetch;
+    d.tuned_shadow_sort = in->shadow_sort;
     return ATRC_OK;
 }
 
@@ -2351,6 +2446,7 @@ int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc, int32_t tri
             c.gen_blocks_per_sm = sh[0]; c.gen_threads = sh[1]; c.finish_threads = sh[2];
             consider(c);
         }
+        { AtrcTuning c = best; c.shadow_sort = 1; consider(c); }
         atrc_cuda_set_tuning(scene, &best);
         d.tuned_trials = trials;
         d.tuned_ms = best_ms;
@@ -2495,11 +2591,13 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         p.view_done = nullptr;
         k_tiles<<<1, 32, 0, s>>>(p);
         Pool P = pool_from(base + counters_bytes + tiles_bytes, L, cap, shadow_cap);
+        set_shadow_sort(&P, d.scene, d.tuned_shadow_sort);
         const int gsm = grid_for(d.sm_count, d.tuned_gen_blocks);
         const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
         // k_init rewrites the counters and the slot states (all state that must
         // start from a known value)
-        k_init<<<int((std::max<size_t>(cap, p.nkeys) + 255) / 256), 256, 0, s>>>(P, int(cap), p.nkeys, c, total);
+        k_init<<<int((std::max<size_t>({cap, size_t(p.nkeys), size_t(kShadowKeys)}) + 255) / 256), 256, 0, s>>>(
+            P, int(cap), p.nkeys, c, total);
         CK(cudaGetLastError());
         uint64_t launches = 2, ext_launches = 0;  // k_tiles, k_init
         Counters hc{};
@@ -2526,6 +2624,11 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
                 if (d.scene.has_subsurface) {
                     k_subsurface<<<g_path, 128, 0, s>>>(d.scene, p, P, c);
                     launches += 1;
+                }
+                if (P.shadow_sort) {
+                    k_shsort_scan<<<1, 1024, 0, s>>>(P);
+                    k_shsort_scatter<<<d.sm_count * 8, 128, 0, s>>>(P, c);
+                    launches += 2;
                 }
                 if (d.tuned_shadow_fetch && wt)
                     k_shadow_fetch<ISECT_WATERTIGHT, false><<<g_fetch, kTraceBlock, 0, s>>>(d.scene, P, c);

@@ -506,7 +506,11 @@ typedef struct AtrcTuning {
     int32_t shadow_fetch;       /* any-hit traversal: 1 = persistent warps that  */
                                 /* refill finished lanes, 0 = one ray per thread */
                                 /* (set by the caller; the autotuner leaves 0)   */
-    int32_t pad_;
+    int32_t shadow_sort;        /* shadow queue: 1 = counting sort by the cell   */
+                                /* of the ray origin (16^3 over the scene bound, */
+                                /* Morton order) before any-hit traversal, so a  */
+                                /* warp's rays start near each other; 0 = order  */
+                                /* of shading                                    */
 } AtrcTuning;
 
 /* Project autotuner (the reference has no counterpart: it renders with a
@@ -517,8 +521,9 @@ typedef struct AtrcTuning {
  * reused).  It searches the closest-hit kernel (extend_fetch), sort
  * granularity with the extend-queue order
  * (queue_order), then path-pool size, then the generate / finish launch
- * shapes (coordinate descent, best of two timings each), and stores the
- * fastest configuration in the scene.  The caller's films are untouched. */
+ * shapes, then the shadow-queue sort (coordinate descent, best of two
+ * timings each), and stores the fastest configuration in the scene.  The
+ * caller's films are untouched. */
 int atrc_cuda_autotune(AtrcScene* scene, const AtrcRenderDesc* desc,
                        int32_t trial_spp, AtrcTuning* out);
 /* Read or replace a scene's launch configuration (e.g. a cached tuning). */
@@ -545,10 +550,10 @@ int atrc_cuda_stream_read_gbs(int device, uint64_t bytes, int passes, double* gb
  *  - The wavefront scratch (path pool, queues, shadow rays, counters) lives in
  *    a static device array of ATRC_NOALLOC_SCRATCH_BYTES that every GPU which
  *    loads this library keeps reserved until the process exits.  A path
- *    takes 192 bytes plus 48 per shadow ray it may emit in one iteration (one
+ *    takes 192 bytes plus 56 per shadow ray it may emit in one iteration (one
  *    per light for pt, ao_sample_count for ao), so the pool holds about 100k
  *    paths with one light.  Calls that leave room for fewer than 1024 paths
- *    (more than 508 lights, or ao_sample_count above 508) are rejected with
+ *    (more than 434 lights, or ao_sample_count above 434) are rejected with
  *    ATRC_ERR_UNSUPPORTED; a desc->path_pool above the maximum, and a film
  *    of 2^22 or more filter tiles, with ATRC_ERR_INVALID_ARG.  Nothing is
  *    launched before these checks.
@@ -636,8 +641,15 @@ typedef struct AtrcGuideDesc {
     float    learning_rate;    /* Adam step size (1e-2)                      */
     int32_t  max_depth;        /* guide vertices up to this path depth (3;   */
                                /* 0: every depth)                            */
-    int32_t  pad_;
+    float    max_select;       /* cap on the probability of sampling the     */
+                               /* guide instead of the BSDF (0.9; at most    */
+                               /* 0.99): the BSDF keeps 1 - max_select of    */
+                               /* every sample, which bounds the variance an */
+                               /* overconfident guide can add                */
     uint64_t seed;             /* parameter initialisation                   */
+    float    target_clamp;     /* > 0: training targets capped at this       */
+                               /* multiple of their batch mean (0: off)      */
+    int32_t  pad_;
 } AtrcGuideDesc;
 
 typedef struct AtrcGuideInfo {

@@ -306,3 +306,31 @@ def test_shadow_fetch_matches_one_ray_per_thread(scene, scene_dir):
         assert abs(sa[k] - sb[k]) <= 0.01 * sa[k], k
     np.testing.assert_allclose(fb.value, fa.value, rtol=2e-6, atol=1e-9)
     np.testing.assert_array_equal(fb.weight, fa.weight)
+
+
+@pytest.mark.parametrize("scene", ["cornell", "media", "instanced"])
+def test_shadow_queue_sort_changes_nothing(scene, cornell_path, scene_dir):
+    # the shadow-queue sort (AtrcTuning.shadow_sort) only changes the order in
+    # which any-hit rays are traced: the films agree up to the order in which
+    # the FP32 shadow-ray results of several lights add into one path
+    from atrc_b200 import scenes
+    if scene == "cornell":
+        cfg = Config.from_file(cornell_path)
+    elif scene == "media":
+        cfg = Config.from_file(scenes.media_scene(scene_dir / "media_shsort", grid_res=32, sphere_level=3))
+    else:
+        cfg = Config.from_file(scenes.instanced_disney(scene_dir / "inst_shsort", ico_level=4, hf_res=128))
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 64, 48, 8
+    desc.path_pool = 1 << 14  # slots are reused: the queue is sorted in every iteration
+    dev = DeviceScene(cfg)
+    films = []
+    for on in (0, 1):
+        dev.set_tuning(shadow_sort=on)
+        assert dev.tuning()["shadow_sort"] == on
+        f = Film(desc.width, desc.height, value_sq=True)
+        st = dev.render(desc, f)
+        assert st["watchdog_flags"] == 0 and st["rays_shadow"] > 0
+        films.append(f)
+    np.testing.assert_allclose(films[1].value, films[0].value, rtol=2e-6, atol=1e-9)
+    np.testing.assert_allclose(films[1].weight, films[0].weight, rtol=1e-12)
