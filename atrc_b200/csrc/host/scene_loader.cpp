@@ -492,8 +492,13 @@ public:
         } else if (type == "metal") {  // MetalCreator (material_creators.cpp:235-268)
             m.type = ATRC_MAT_METAL;
             m.tex[0] = create_texture2d(p.child_group("color"));
-            m.tex[1] = create_texture2d(p.child_group("eta"));
-            m.tex[2] = create_texture2d(p.child_group("k"));
+            // the reference's create_metal(color, eta, k, ...) forwards its
+            // arguments in that order to Metal(color, k, eta, ...)
+            // (metal.cpp:23-27, 65-78), so the conductor Fresnel it renders
+            // with takes the "k" map as the index of refraction and the "eta"
+            // map as the absorption: the same swap here keeps parity
+            m.tex[2] = create_texture2d(p.child_group("eta"));
+            m.tex[1] = create_texture2d(p.child_group("k"));
             m.tex[3] = create_texture2d(p.child_group("roughness"));
             m.tex[4] = create_texture2d(p.child_group("anisotropic"));
             if (auto n = p.find_child_group("normal_map")) m.normal_map = create_texture2d(*n);

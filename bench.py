@@ -10,8 +10,10 @@ Metric: Msamples/s (camera samples rendered per second; one step renders
 `value` is measured with CUDA events with the scene and the FP64 film resident
 on the device; `e2e` times the C-ABI call a user makes (atrc_cuda_render into a
 host film, i.e. including the device-to-host copy of the step's film).  With
---impl reference the CPU oracle (the restatement of the reference's `pt`
-renderer) is timed on the host cores on a bounded sample of the same workload.
+--impl reference the reference's own CPU `pt` (its tracer and factory sources
+built into oracle/_ref/libatrc_ref.so; the oracle's restatement where that
+library is absent) is timed on all host cores, one whole-film 1 spp pass of
+the same workload per step.
 Multi-GPU: one process per GPU; every rank renders its own disjoint range of
 sample indices of the same frame and the films are summed to rank 0 with one
 NCCL reduce per step (weak scaling).
@@ -119,49 +121,79 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+class CpuRenderer:
+    """The CPU `pt` timed beside the GPU: the reference's own renderer built
+    from its sources (oracle/_ref/libatrc_ref.so, kind "reference") when that
+    library is present, else the oracle's restatement (kind "port").  Both
+    render 1 spp of every `stride`-th 32x32 task tile of the film per call,
+    on all host threads."""
+
+    def __init__(self, path, cfg, desc):
+        import oracle
+        self.threads = oracle.hardware_threads()
+        self.desc = desc
+        if oracle.ref_available():
+            self.kind = "reference"
+            self._ref = oracle.RefScene(path)
+        else:
+            self.kind = "port"
+            self._ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
+
+    def render(self, film, first_spp: int, stride: int) -> None:
+        if self.kind == "reference":
+            self._ref.render(film, spp=1, first_spp=first_spp, threads=self.threads, tile_stride=stride)
+        else:
+            self.desc.spp_count = 1
+            self.desc.first_spp = first_spp
+            self._ora.render_sample(self.desc, film, self.threads, stride)
+
+    def samples(self, stride: int, grid: int = 32) -> int:
+        """Camera samples one call renders: the pixels of the sampled tiles."""
+        w, h = self.desc.width, self.desc.height
+        tx = (w + grid - 1) // grid
+        tiles = tx * ((h + grid - 1) // grid)
+        px = 0
+        for k in range(0, tiles, stride):
+            gx, gy = k % tx, k // tx
+            px += (min(w, gx * grid + grid) - gx * grid) * (min(h, gy * grid + grid) - gy * grid)
+        return px
+
+    def describe(self) -> str:
+        return ("the reference's own pt (tracer and factory sources built by oracle/ref/build_ref.py)"
+                if self.kind == "reference" else "the oracle's restatement of the reference's pt")
+
+
 def reference_arm(args, rank: int, world: int) -> None:
-    """The reference's CPU `pt` algorithm (oracle restatement) on the host cores."""
+    """The reference's CPU `pt` on the host cores: its own code built from
+    its sources when available (else the oracle restatement); each step one
+    whole-film 1 spp pass of the same workload."""
     if rank != 0:
         return
-    import oracle
     from atrc_b200 import Config, Film
-    cfg = Config.from_file(scene_path(args.scene))
+    path = scene_path(args.scene)
+    cfg = Config.from_file(path)
     desc, _ = cfg.rendering(0)
-    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
-    threads = oracle.hardware_threads()
-    tiles = ((desc.width + 31) // 32) * ((desc.height + 31) // 32)
-    stride = 1  # each step: one whole-film 1 spp pass
-    desc.spp_count = 1
-    samples_per_step = 0
+    cpu = CpuRenderer(path, cfg, desc)
     film = Film(desc.width, desc.height)
     times = []
     for i in range(args.warmup + args.steps):
-        desc.first_spp = i
         t = time.perf_counter()
-        ora.render_sample(desc, film, threads, stride)
+        cpu.render(film, i, 1)
         dt = time.perf_counter() - t
         if i >= args.warmup:
             times.append(dt)
-    n_tiles = (tiles + stride - 1) // stride
-    # samples rendered per step = pixels of the sampled tiles x 1 spp
-    tx = (desc.width + 31) // 32
-    px = 0
-    for k in range(0, tiles, stride):
-        gx, gy = k % tx, k // tx
-        px += (min(desc.width, gx * 32 + 32) - gx * 32) * (min(desc.height, gy * 32 + 32) - gy * 32)
-    samples_per_step = px
-    total = samples_per_step * args.steps
+    samples_per_step = cpu.samples(1)
     sec = float(np.sum(times))
-    value = total / sec / 1e6
+    value = samples_per_step * args.steps / sec / 1e6
     line = {"metric": METRIC, "value": value, "unit": "Msamples/s", "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD if args.scene == "instanced" else args.scene,
-                       "sample": f"1 spp of every pixel per step ({n_tiles} tiles of 32x32)",
+                       "sample": f"1 spp of every pixel per step ({desc.width}x{desc.height})",
                        "global_batch": samples_per_step},
-            "cpu_baseline": {"value": value, "unit": "Msamples/s", "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": "Msamples/s", "cores": cpu.threads, "kind": cpu.kind,
                              "sample": f"{samples_per_step} camera samples per step (one whole-film 1 spp "
-                                       f"pass of the {desc.width}x{desc.height} film)"},
+                                       f"pass of the {desc.width}x{desc.height} film) by {cpu.describe()}"},
             "e2e": {"value": value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -191,30 +223,28 @@ def stream_read_peaks(device: int) -> dict:
 
 
 def cpu_baseline(args) -> dict:
-    """Timed run of the oracle on all host cores: whole-film 1 spp passes of the
-    same workload, repeated until at least 10 s of CPU work (at most 30 s)."""
-    import oracle
+    """The CPU `pt` (CpuRenderer) on all host cores: whole-film 1 spp passes
+    of the same workload, repeated until at least 10 s of CPU work (at most
+    30 s)."""
     from atrc_b200 import Config, Film
-    cfg = Config.from_file(scene_path(args.scene))
+    path = scene_path(args.scene)
+    cfg = Config.from_file(path)
     desc, _ = cfg.rendering(0)
-    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
-    threads = oracle.hardware_threads()
-    desc.spp_count = 1
+    cpu = CpuRenderer(path, cfg, desc)
     film = Film(desc.width, desc.height)
-    desc.first_spp = 0
-    ora.render_sample(desc, film, threads, 8)  # warm-up (page-in)
+    cpu.render(film, 0, 8)  # warm-up (page-in)
     total, passes, t0 = 0.0, 0, time.perf_counter()
     while total < 10.0 and passes < 64:
-        desc.first_spp = 1 + passes
         t = time.perf_counter()
-        ora.render(desc, film, threads)
+        cpu.render(film, 1 + passes, 1)
         total += time.perf_counter() - t
         passes += 1
         if time.perf_counter() - t0 > 30:
             break
-    samples = desc.width * desc.height * passes
-    return {"value": samples / total / 1e6, "unit": "Msamples/s", "cores": threads, "kind": "port",
-            "sample": f"{passes} whole-film 1 spp passes ({samples} camera samples), {total:.1f} s"}
+    samples = cpu.samples(1) * passes
+    return {"value": samples / total / 1e6, "unit": "Msamples/s", "cores": cpu.threads, "kind": cpu.kind,
+            "sample": f"{passes} whole-film 1 spp passes ({samples} camera samples), {total:.1f} s, by "
+                      f"{cpu.describe()}"}
 
 
 def guided_comparison(args) -> dict:
@@ -289,12 +319,13 @@ def media_comparison(args, l2_peak: float) -> dict:
     sky, 1024 x 1024, max depth 32.  Steps of --media-spp samples per pixel,
     timed with CUDA events on a device film (a rate: the stated 512 spp would
     be 128 such steps); the closest-hit kernel's roofline as for the headline;
-    the oracle on a bounded sample of the same film as the CPU baseline."""
+    the CPU `pt` (CpuRenderer) on a bounded sample of the same film as the CPU
+    baseline."""
     import torch
 
-    import oracle
     from atrc_b200 import Config, DeviceScene, Film, scenes
-    cfg = Config.from_file(scenes.media_scene())
+    path = scenes.media_scene()
+    cfg = Config.from_file(path)
     desc, _ = cfg.rendering(0)
     dev = DeviceScene(cfg)
     dev.autotune(desc, trial_spp=1)
@@ -326,17 +357,14 @@ def media_comparison(args, l2_peak: float) -> dict:
     rays = sum(st["rays_closest"] for st in stats)
     achieved = bpr * rays / max(ext, 1e-9) / 1e9
     # CPU baseline: every 64th 32x32 tile of the film at 1 spp, on all host threads
-    ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
-    threads = oracle.hardware_threads()
-    hf = Film(desc.width, desc.height)
     d1, _ = cfg.rendering(0)
-    d1.spp_count = 1
+    cpu = CpuRenderer(path, cfg, d1)
+    hf = Film(desc.width, desc.height)
     stride = 64
     t0 = time.perf_counter()
-    ora.render_sample(d1, hf, threads, stride)
+    cpu.render(hf, 0, stride)
     cpu_s = time.perf_counter() - t0
-    tiles = ((desc.width + 31) // 32) * ((desc.height + 31) // 32)
-    cpu_samples = len(range(0, tiles, stride)) * 32 * 32
+    cpu_samples = cpu.samples(stride)
     return {"workload": "media_homogeneous_box_heterogeneous_128cube_200k_sphere_1024x1024_depth32",
             "Msamples_per_s": samples / sec / 1e6, "steps": args.media_steps, "spp_per_step": spp,
             "ms_per_step": sec / args.media_steps * 1e3,
@@ -346,9 +374,9 @@ def media_comparison(args, l2_peak: float) -> dict:
                                   "shadow": sum(st["shadow_seconds"] for st in stats) / sec},
             "roofline": {"bound": "l2", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,
                          "peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak, "bytes_per_ray": bpr},
-            "cpu_baseline": {"value": cpu_samples / cpu_s / 1e6, "unit": "Msamples/s", "cores": threads,
-                             "kind": "port", "sample": f"1 spp of every {stride}th 32x32 tile ({cpu_samples} "
-                                                       f"camera samples), {cpu_s:.1f} s"}}
+            "cpu_baseline": {"value": cpu_samples / cpu_s / 1e6, "unit": "Msamples/s", "cores": cpu.threads,
+                             "kind": cpu.kind, "sample": f"1 spp of every {stride}th 32x32 tile ({cpu_samples} "
+                                                         f"camera samples), {cpu_s:.1f} s, by {cpu.describe()}"}}
 
 
 def batch_views(cfg, n: int, seed: int, spp_scale: float):
@@ -440,7 +468,7 @@ def batch_comparison(args) -> dict:
     small_r = compare(small, False)
     return {"workload": f"indoor_room_{args.batch_views}_views", "spp_scale": args.batch_spp_scale,
             "tuning": {k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
-                                              "finish_threads", "extend_fetch", "queue_order", "shadow_fetch")},
+                                              "finish_threads", "extend_fetch", "queue_order", "shadow_fetch", "shadow_sort")},
             **full, "small_views": small_r}
 
 
@@ -459,7 +487,7 @@ def ingest_comparison(args, cfg, desc, tuning, sah_build_s: float, sah_value: fl
     scene = DeviceScene(pcfg)
     ploc_s = time.perf_counter() - t0
     scene.set_tuning(**{k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
-                                               "finish_threads", "extend_fetch", "queue_order", "shadow_fetch")})
+                                               "finish_threads", "extend_fetch", "queue_order", "shadow_fetch", "shadow_sort")})
     film = Film(desc.width, desc.height, device=True)
     for k in range(args.warmup):
         desc.first_spp = k * desc.spp_count
@@ -605,7 +633,7 @@ def main():
                        "l2": "inputs larger than L2 (BVH + triangles + shading data > 126 MB)",
                        "scene_build_s": round(build_s, 3), "autotune_s": round(tune_s, 3),
                        "tuning": {k: tuning[k] for k in ("path_pool", "sort_mode", "gen_blocks_per_sm", "gen_threads",
-                                                         "finish_threads", "extend_fetch", "queue_order", "shadow_fetch", "trials")}},
+                                                         "finish_threads", "extend_fetch", "queue_order", "shadow_fetch", "shadow_sort", "trials")}},
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
             # k_extend reads its nodes and triangles mostly from L1 / L2 (ncu:
             # 235 of ~1,800 algorithmic bytes per ray come from DRAM), so its

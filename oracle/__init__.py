@@ -2,8 +2,10 @@
 
 TEST INFRASTRUCTURE ONLY: tests/, ``__graft_entry__.smoke()`` and the CPU
 baseline of ``bench.py`` use it as the checker / the timed CPU baseline.  The
-product package ``atrc_b200`` never imports it.  Parity status: unpinned (the
-reference has no golden vectors and cannot be built here; see oracle.h).
+product package ``atrc_b200`` never imports it.  Parity status: pinned to the
+reference's own tracer and factory code, built from its sources against an
+agz-utils compatibility shim into ``oracle/_ref/libatrc_ref.so`` (``RefScene``
+below; see oracle.h for what the shim leaves unpinned).
 """
 from __future__ import annotations
 
@@ -142,3 +144,80 @@ class OracleScene:
 
 def hardware_threads() -> int:
     return int(load().oracle_hardware_threads())
+
+
+# ----------------------------------------------------------------------------
+# The reference's own renderer: Atrc's tracer and factory sources compiled
+# against the agz-utils compatibility shim (oracle/ref/build_ref.py ->
+# oracle/_ref/libatrc_ref.so).  Same role as the restatement above -- a
+# checker, never the product -- but its scene parsing, BVHs, intersection
+# tests, materials, lights, media and trace_std are the reference's code.
+
+REF_SO = Path(__file__).resolve().parent / "_ref" / "libatrc_ref.so"
+_ref_lib = None
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def load_ref() -> C.CDLL:
+    global _ref_lib
+    if _ref_lib is None:
+        if not REF_SO.exists():
+            raise RuntimeError(f"{REF_SO} is missing: build it with `python oracle/ref/build_ref.py` "
+                               "where the reference checkout is present")
+        lib = C.CDLL(str(REF_SO))
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_scene_create.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]
+        lib.ref_scene_destroy.argtypes = [C.c_void_p]
+        lib.ref_scene_destroy.restype = None
+        lib.ref_entity_count.argtypes = [C.c_void_p]
+        lib.ref_trace_rays.argtypes = [C.c_void_p, C.POINTER(abi.AtrcRay), C.c_size_t, C.POINTER(abi.AtrcHit),
+                                       C.c_int, C.c_int]
+        dp = C.POINTER(C.c_double)
+        lib.ref_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int,
+                                   C.c_int, dp, dp, dp]
+        _ref_lib = lib
+    return _ref_lib
+
+
+def _ref_check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(f"reference renderer: {load_ref().ref_last_error().decode()}")
+
+
+class RefScene:
+    """A scene built by the reference's own factory from its JSON file."""
+
+    def __init__(self, json_path):
+        p = Path(json_path)
+        h = C.c_void_p()
+        _ref_check(load_ref().ref_scene_create(p.read_text().encode(), str(p.parent).encode(), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _ref_lib is not None:
+            _ref_lib.ref_scene_destroy(self._h)
+            self._h = None
+
+    def entity_count(self) -> int:
+        return int(load_ref().ref_entity_count(self._h))
+
+    def trace_rays(self, rays: np.ndarray, mode: str = "closest", threads: int = 0) -> np.ndarray:
+        r = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        hits = np.empty(len(r), dtype=HIT_DTYPE)
+        _ref_check(load_ref().ref_trace_rays(self._h, r.ctypes.data_as(C.POINTER(abi.AtrcRay)), len(r),
+                                             hits.ctypes.data_as(C.POINTER(abi.AtrcHit)),
+                                             0 if mode == "closest" else 1, threads))
+        return hits
+
+    def render(self, film, index: int = 0, spp: int = 1, first_spp: int = 0, seed: int = 1, threads: int = 0,
+               width: int = 0, height: int = 0, tile_stride: int = 1) -> None:
+        """Add `spp` samples per pixel of rendering entry `index` into a host
+        Film (value, weight and, if present, value_sq); tile_stride > 1
+        renders only every tile_stride-th task tile."""
+        dp = C.POINTER(C.c_double)
+        ptr = lambda a: None if a is None else a.ctypes.data_as(dp)  # noqa: E731
+        _ref_check(load_ref().ref_render(self._h, index, width, height, first_spp, spp, seed, threads, tile_stride,
+                                         ptr(film.value), ptr(film.weight), ptr(film.value_sq)))

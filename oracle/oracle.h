@@ -7,11 +7,20 @@
  * load it, and only as the checker / the timed CPU baseline.  The product
  * (libatrc_cuda.so) never links, loads or calls it.
  *
- * Parity status: unpinned.  The reference ships no tests, golden images or
- * known-answer vectors for this path, and it cannot be compiled here (its
- * agz-utils submodule is absent), so no reference output exists to pin the
- * oracle to.  The analytic known-answer tests in tests/ (furnace, slab
- * transmittance, MT edge cases, pdf normalisation) check it instead.
+ * Parity status: pinned to the reference's own code.  The reference ships no
+ * tests, golden images or known-answer vectors for this path, and its
+ * agz-utils submodule is absent, so oracle/ref/ builds the reference's tracer
+ * and factory sources, unchanged, against a compatibility shim for the
+ * agz-utils parts they use (vector/matrix/colour types, texture containers,
+ * sampling helpers, threads, file loaders) into oracle/_ref/libatrc_ref.so.
+ * tests/test_ref_oracle.py checks this restatement against that library
+ * (closest hits bit-identical in t where no rotation or nested wrapper is
+ * involved; images within the 3-sigma band), and the analytic known-answer
+ * tests in tests/ (furnace, slab transmittance, MT edge cases, pdf
+ * normalisation) check both.  What remains unpinned is what the shim itself
+ * restates: agz-utils' matrix inverse / rotation rounding and its sampling
+ * helpers' exact sequences (they are distribution-level equal, not
+ * bit-equal).
  */
 #ifndef ATRC_ORACLE_H
 #define ATRC_ORACLE_H

@@ -2,7 +2,8 @@
 //
 // TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
 // CPU-baseline leg of bench.py as the checker / the timed CPU baseline.  The
-// product never calls it.  Parity status: unpinned (see oracle.h).
+// product never calls it.  Parity status: pinned to the reference's own
+// code built from its sources (see oracle.h).
 //
 // Every function restates the reference algorithm it names (file:line inside
 // the reference checkout, src/tracer/... unless noted).  The small vector

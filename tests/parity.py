@@ -69,9 +69,13 @@ def classify_closest(rays, gpu, ref, oracle_scene, watertight: bool = False):
     return out
 
 
-def band_test(gpu_film, ref_film, filter_value: float, sigmas: float = 3.0):
+def band_test(gpu_film, ref_film, filter_value: float, sigmas: float = 3.0, cluster: int = 1):
     """Per-pixel, per-channel |mu_g - mu_c| <= k sqrt(s_g^2/N_g + s_c^2/N_c).
     Returns (failing fraction, allowed fraction, details).
+
+    `cluster` = 3 treats the three channels of a pixel as one draw (they
+    share every path, so they tend to fail together), which widens the
+    binomial margin by sqrt(3).
 
     With the variances estimated from the samples, the statistic of a pixel
     follows Student's t with the Welch-Satterthwaite degrees of freedom, not
@@ -100,7 +104,7 @@ def band_test(gpu_film, ref_film, filter_value: float, sigmas: float = 3.0):
     dof = np.where(den > 0, (a + b) ** 2 / np.where(den > 0, den, 1), np.inf)
     p_each = np.where(se > 0, 2 * student_t.sf(sigmas, np.broadcast_to(dof, se.shape)), 0.0)
     p = float(p_each.mean())
-    allowed = p + 3.1 * math.sqrt(p * (1 - p) / tests)  # binomial upper 99.9 % bound
+    allowed = p + 3.1 * math.sqrt(p * (1 - p) * cluster / tests)  # binomial upper 99.9 % bound
     return float(fail.mean()), allowed, {"max_z": float(np.max(diff / np.maximum(se, 1e-12))),
                                          "mean_rel": float(np.mean(np.abs(mg - mc)) / max(np.mean(np.abs(mc)), 1e-12))}
 
