@@ -532,6 +532,23 @@ __global__ void k_target_sum(const GuideRecord* rec, int n, float* sum) {
     if ((threadIdx.x & 31) == 0) atomicAdd(sum, s);
 }
 
+// The records of a pass whose target is positive, compacted into `out`: a
+// zero-target record adds nothing to the loss or to its gradient, so the
+// training batches carry only records that do (order not kept).
+__global__ void k_live_records(const GuideRecord* __restrict__ rec, int n, GuideRecord* __restrict__ out,
+                               int* count) {
+    const int lane = threadIdx.x & 31;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const bool live = i < n && rec[i].target > 0.0f;
+        const unsigned m = __ballot_sync(0xffffffffu, live);
+        int base = 0;
+        if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (live) out[base + __popc(m & ((1u << lane) - 1u))] = rec[i];
+    }
+}
+
 struct AdamArgs {
     float lr, b1, b2, eps, c1, c2;  // c1 = 1 / (1 - b1^t), c2 = 1 / (1 - b2^t)
 };
@@ -574,8 +591,10 @@ struct GuideImpl {
     DevBuf w_f, w_g, w_m, w_v, w_bf;          // weights: master, grad, Adam m / v, BF16 copy
     DevBuf t_f, t_g, t_m, t_v, t_h;           // table: master, grad, m, v, FP16 copy
     DevBuf records, rec_count, rec_last, queries, mixes, gidx, xtiles, scratch, err;
+    DevBuf live;          // the records of a pass with a non-zero target, compacted for training
     size_t slots = 0;
     int steps = 0;
+    float record_keep = 1.0f;  // recording probability of the next pass (from the last one's vertex count)
     NetView view() const {
         NetView v;
         v.w = w_bf.as<__nv_bfloat16>();
@@ -608,11 +627,12 @@ GuideFrame guide_frame(GuideImpl* g, size_t cap, bool record, cudaStream_t s) {
     f.table_h = g->t_h.as<__half>();
     f.grid = g->grid;
     if (record) {
-        CK(cudaMemsetAsync(g->rec_count.p, 0, sizeof(int), s));
+        CK(cudaMemsetAsync(g->rec_count.p, 0, 2 * sizeof(int), s));
         CK(cudaMemsetAsync(g->rec_last.p, 0xff, cap * sizeof(int), s));
         f.records = g->records.as<GuideRecord>();
         f.record_count = g->rec_count.as<int>();
         f.record_cap = int(g->desc.record_capacity);
+        f.record_keep = g->record_keep;
         f.record_last = g->rec_last.as<int>();
     }
     return f;
@@ -753,7 +773,7 @@ int atrc_guide_create(int device, const float scene_lo[3], const float scene_hi[
         G.t_f.alloc(G.table_n * 4); G.t_g.alloc(G.table_n * 4); G.t_m.alloc(G.table_n * 4); G.t_v.alloc(G.table_n * 4);
         G.t_h.alloc(G.table_n * 2);
         G.records.alloc(size_t(desc->record_capacity) * sizeof(GuideRecord));
-        G.rec_count.alloc(sizeof(int));
+        G.rec_count.alloc(2 * sizeof(int));
         G.scratch.alloc(64);
         G.err.alloc(sizeof(int));
         cudaStream_t s = G.stream;
@@ -940,21 +960,35 @@ int atrc_guide_train(AtrcGuide* g, int steps, float* last_loss) {
     return gguarded([&] {
         GuideImpl& G = g->impl;
         CK(cudaSetDevice(G.device));
+        cudaStream_t s = G.stream;
+        int counts[2] = {0, 0};  // records stored, guided vertices seen
+        CK(cudaMemcpyAsync(counts, G.rec_count.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const int cap = int(G.desc.record_capacity);
+        const int stored = std::min(counts[0], cap);
+        // the next recording pass keeps about 0.95 cap of its guided vertices
+        // (this pass's count stands in for the next one's)
+        if (counts[1] > 0)
+            G.record_keep = std::min(1.0f, std::max(1.0f / 4096.0f, 0.95f * float(cap) / float(counts[1])));
+        if (last_loss) *last_loss = 0;
+        if (stored < kTile) return int(ATRC_OK);
+        if (G.live.bytes < size_t(cap) * sizeof(GuideRecord)) G.live.alloc(size_t(cap) * sizeof(GuideRecord));
+        int* live_n = reinterpret_cast<int*>(G.scratch.as<float>() + 4);
+        CK(cudaMemsetAsync(live_n, 0, sizeof(int), s));
+        k_live_records<<<G.sm_count * 4, 256, 0, s>>>(G.records.as<GuideRecord>(), stored,
+                                                     G.live.as<GuideRecord>(), live_n);
+        CK(cudaGetLastError());
         int n = 0;
-        CK(cudaMemcpyAsync(&n, G.rec_count.p, sizeof(int), cudaMemcpyDeviceToHost, G.stream));
-        CK(cudaStreamSynchronize(G.stream));
-        n = std::min(n, int(G.desc.record_capacity));
-        if (n < kTile) {
-            if (last_loss) *last_loss = 0;
-            return int(ATRC_OK);
-        }
+        CK(cudaMemcpyAsync(&n, live_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (n < kTile) return int(ATRC_OK);
         const int batch = std::min(n, int(G.desc.batch));
         float loss = 0;
         for (int k = 0; k < steps; ++k) {
-            // consecutive batches through the records (wrapping)
+            // consecutive batches through the live records (wrapping)
             const int start = int((size_t(k) * batch) % size_t(n));
             const int cnt = std::min(batch, n - start);
-            train_step(G, G.records.as<GuideRecord>() + start, cnt, &loss);
+            train_step(G, G.live.as<GuideRecord>() + start, cnt, &loss);
         }
         check_err(G, "atrc_guide_train");
         if (last_loss) *last_loss = loss;

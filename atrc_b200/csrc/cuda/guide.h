@@ -34,8 +34,9 @@ struct GuideFrame {
     const __half* table_h;    // FP16 hash table
     // recording (null when the call does not record)
     GuideRecord* records;
-    int* record_count;
+    int* record_count;        // records stored ([0]) and guided vertices seen ([1])
     int record_cap;
+    float record_keep;        // probability that a guided vertex is recorded
     int* record_last;         // per path slot: last record of the path
     dev::HashGrid grid;
 };

@@ -1071,8 +1071,17 @@ __global__ void __launch_bounds__(128, ATRC_SHADE_MIN_BLOCKS) k_shade(Scene S, P
                 if (black(bs.f) || (guided && !(bs.pdf > 0.0f))) {
                     finish = true;
                 } else {
+                    // training record of this vertex, kept with probability
+                    // record_keep so that a pass's records sample all its
+                    // guided vertices (every depth, every pixel) rather than
+                    // the first record_cap of them; targets are set when the
+                    // path ends
+                    bool keep = false;
                     if (guided && p.gf.records) {
-                        // training record of this vertex; its targets are set when the path ends
+                        atomicAdd(p.gf.record_count + 1, 1);
+                        keep = p.gf.record_keep >= 1.0f || rng.u() < p.gf.record_keep;
+                    }
+                    if (keep) {
                         const int r = atomicAdd(p.gf.record_count, 1);
                         if (r < p.gf.record_cap) {
                             const GuideQuery& gq = p.gf.queries[gq_i];

@@ -228,12 +228,15 @@ def _const(v) -> dict:
 
 # ----------------------------------------------------------- Cornell (cfg 0)
 def cornell_box(out_dir: Path | None = None, seed: int = 1000, width: int = 256, height: int = 256, spp: int = 64,
-                renderer: str = "pt", max_depth: int = 8, min_depth: int = 2) -> Path:
+                renderer: str = "pt", max_depth: int = 8, min_depth: int = 2, subsurface: bool = False) -> Path:
     """Plain pt on a seeded Cornell box: 5 quad walls of [-1,1]^3, two 12-triangle
     boxes rotated by U[0, 30] degrees about y, a 0.5x0.5 quad light at the
     ceiling with radiance (17, 12, 4), Lambertian albedos U[0.1, 0.8]^3 with a
-    red and a green wall, pinhole camera with 40 degree FOV, box filter."""
-    out = Path(out_dir) if out_dir else cache_dir() / f"cornell_{seed}"
+    red and a green wall, pinhole camera with 40 degree FOV, box filter.
+    With `subsurface` the two boxes are Disney materials with subsurface
+    scattering instead (base colour and bssrdf_A = the box's drawn albedo,
+    transmission 0.8, mean free paths of a few hundredths of the box)."""
+    out = Path(out_dir) if out_dir else cache_dir() / f"cornell_{seed}{'_sss' if subsurface else ''}"
     out.mkdir(parents=True, exist_ok=True)
     rng = np.random.default_rng(seed)
     alb = lambda: v3(rng.uniform(0.1, 0.8, 3))  # noqa: E731
@@ -255,11 +258,18 @@ def cornell_box(out_dir: Path | None = None, seed: int = 1000, width: int = 256,
         fn = out / f"box{k}.bm"
         write_bm(fn, p, n, uv)
         deg = r6(rng.uniform(0, 30))
+        albedo = rng.uniform(0.1, 0.8, 3)
+        if subsurface:
+            mat = {"type": "disney", "base_color": _const(albedo), "metallic": _const(0.0),
+                   "roughness": _const(0.4), "transmission": _const(0.8), "ior": _const(1.4),
+                   "bssrdf_dmfp": _const([0.06, 0.03, 0.02]), "bssrdf_A": _const(albedo)}
+        else:
+            mat = {"type": "ideal_diffuse", "albedo": _const(albedo)}
         ents.append({"type": "geometric",
                      "geometry": {"type": "triangle_bvh", "filename": "${scene-directory}/" + fn.name,
                                   "transform": [{"type": "translate", "offset": v3(pos)},
                                                 {"type": "rotate_y", "deg": deg}]},
-                     "material": {"type": "ideal_diffuse", "albedo": _const(rng.uniform(0.1, 0.8, 3))}})
+                     "material": mat})
     ents.append({"type": "geometric",
                  "geometry": {"type": "quad", "A": [-0.25, 0.999, -0.25], "B": [0.25, 0.999, -0.25],
                               "C": [0.25, 0.999, 0.25], "D": [-0.25, 0.999, 0.25], "transform": []},

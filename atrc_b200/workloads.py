@@ -7,8 +7,11 @@ times).
         warm-up steps, then `steps` steps of `spp` samples per pixel; each
         timed step is wrapped in an NVTX range named "step"
     python -m atrc_b200.workloads guided-room [--train-passes 3] [--passes 3]
-        the 1280x720 indoor room: plain passes, guided passes that record and
-        train, then guided passes that only sample (1 spp each)
+        the 1280x720 indoor room: autotune, plain passes, guided passes that
+        record and train, then guided passes that only sample (1 spp each)
+    python -m atrc_b200.workloads subsurface [--spp 4] [--warmup 2] [--steps 1]
+        the Cornell box at 1024x1024 with its two boxes made of Disney
+        materials with subsurface scattering (the k_subsurface walk)
 """
 from __future__ import annotations
 
@@ -36,12 +39,30 @@ def instanced(spp: int, warmup: int, steps: int) -> None:
             print(f"step {k - warmup}: closest rays {stats['rays_closest']}, shadow rays {stats['rays_shadow']}")
 
 
+def subsurface(spp: int, warmup: int, steps: int) -> None:
+    import torch
+
+    from . import Config, DeviceScene, Film, scenes
+    cfg = Config.from_file(scenes.cornell_box(width=1024, height=1024, renderer="pt_cuda", subsurface=True))
+    desc, _ = cfg.rendering(0)
+    scene = DeviceScene(cfg)
+    film = Film(desc.width, desc.height, device=True)
+    desc.spp_count = spp
+    for k in range(warmup + steps):
+        desc.first_spp = k * spp
+        stats = scene.render(desc, film)
+        torch.cuda.synchronize()
+        if k >= warmup:
+            print(f"step {k - warmup}: closest rays {stats['rays_closest']}, shadow rays {stats['rays_shadow']}")
+
+
 def guided_room(train_passes: int, passes: int) -> None:
     from . import Config, DeviceScene, Film, scenes
     from .guide import Guide
     cfg = Config.from_file(scenes.indoor_room())
     desc, _ = cfg.rendering(0)
     scene = DeviceScene(cfg)
+    scene.autotune(desc, trial_spp=1)
     film = Film(desc.width, desc.height, device=True)
     desc.spp_count = 1
     for k in range(3):
@@ -68,9 +89,15 @@ def main() -> None:
     b = sub.add_parser("guided-room")
     b.add_argument("--train-passes", type=int, default=3)
     b.add_argument("--passes", type=int, default=3)
+    c = sub.add_parser("subsurface")
+    c.add_argument("--spp", type=int, default=4)
+    c.add_argument("--warmup", type=int, default=2)
+    c.add_argument("--steps", type=int, default=1)
     args = p.parse_args()
     if args.workload == "instanced":
         instanced(args.spp, args.warmup, args.steps)
+    elif args.workload == "subsurface":
+        subsurface(args.spp, args.warmup, args.steps)
     else:
         guided_room(args.train_passes, args.passes)
 

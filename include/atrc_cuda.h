@@ -678,8 +678,12 @@ int  atrc_guide_eval(AtrcGuide* guide, const float* queries, size_t n, float* ra
  * selection probability c, as the renderer computes them on the GPU. */
 int  atrc_guide_pdf(AtrcGuide* guide, const float* queries, const float* dirs,
                     size_t n, float* pdf, float* select);
-/* `steps` Adam steps over the records of the last recording render
- * (batches of desc.batch, in order); last_loss may be NULL. */
+/* `steps` Adam steps over the records of the last recording render whose
+ * target is positive (zero-target records add nothing to the loss or its
+ * gradient and are dropped first), in batches of desc.batch; last_loss may be
+ * NULL.  It also sets the recording probability of the next recording render
+ * to about 0.95 record_capacity / (guided vertices of the last one), so that
+ * a pass's records sample all of its guided vertices, not its first ones. */
 int  atrc_guide_train(AtrcGuide* guide, int steps, float* last_loss);
 /* The same on host records (n x 24 floats: position, normal, outgoing
  * direction, roughness, sampled direction, its BSDF pdf, throughput (3),

@@ -71,6 +71,12 @@ def test_device_pdf_matches_fp64_evaluation():
     ref = R.pdf(ref_raw, d)
     rel = np.abs(pdf - ref) / ref
     assert np.median(rel) < 0.02 and np.quantile(rel, 0.95) < 0.15, (np.median(rel), np.quantile(rel, 0.95))
+    # against the same network with BF16 operands (FP64 sums), the device pdf
+    # differs only by FP32 summation and the FP32 decode: an order of
+    # magnitude tighter
+    emu = R.pdf(R.forward(q, w, t, info, bf16_ops=True), d)
+    rel16 = np.abs(pdf - emu) / emu
+    assert np.median(rel16) < 2e-3 and np.quantile(rel16, 0.95) < 2e-2, (np.median(rel16), np.quantile(rel16, 0.95))
     np.testing.assert_allclose(c, c_ref, atol=0.01)
     assert np.all(c >= 0) and np.all(c <= 0.9 + 1e-6)
 
@@ -147,6 +153,30 @@ def test_recording_render_keeps_targets(cornell_path):
     assert np.all(rec[:, 13] >= 0)
     loss = g.train(steps=4)
     assert np.isfinite(loss)
+
+
+def test_recording_subsamples_after_a_full_pass(cornell_path):
+    # a pass with more guided vertices than record_capacity fills the
+    # capacity with its first vertices; training then sets the next pass's
+    # recording probability so that it keeps about 0.95 of the capacity,
+    # drawn from all of its vertices
+    cfg = Config.from_file(cornell_path)
+    desc, _ = cfg.rendering(0)
+    desc.width, desc.height, desc.spp = 64, 64, 4
+    dev = DeviceScene(cfg)
+    cap = 1 << 12
+    g = Guide.for_scene(dev, log2_table=14, record_capacity=cap, batch=1 << 12)
+    dev.render_guided(g, desc, Film(64, 64), record=True)
+    assert len(g.records()) == cap                  # saturated: 64 x 64 x 4 samples, several vertices each
+    g.train(steps=1)
+    desc.first_spp = 4
+    dev.render_guided(g, desc, Film(64, 64), record=True)
+    rec = g.records()
+    assert 0.75 * cap < len(rec) < cap, len(rec)    # about 0.95 cap, not saturated
+    # the kept records come from the whole box, not one corner of the film
+    pos = rec[:, 0:3]
+    assert np.all(pos.max(0) - pos.min(0) > 1.5)
+    assert np.mean(rec[:, 17] > 0) > 0.2
 
 
 def test_guided_render_is_unbiased(cornell_path):
@@ -234,18 +264,27 @@ def test_adam_steps_match_reference():
     p = np.concatenate([w, t]).astype(np.float64)
     m = np.zeros_like(p)
     v = np.zeros_like(p)
+    ambiguous = np.zeros(p.shape, bool)
     for step, rec in enumerate(batches, 1):
         gw, gt, _ = g.gradients(rec)          # at the current parameters
         grad = np.concatenate([gw, gt]).astype(np.float64)
+        # the gradient is an atomic sum: a second evaluation, in another
+        # order, measures each component's rounding
+        gw2, gt2, _ = g.gradients(rec)
+        noise = np.abs(grad - np.concatenate([gw2, gt2]).astype(np.float64))
         g.train_records(rec, steps=1)         # the same gradient, then one Adam step
         want, m, v = R.adam_step(p, grad, m, v, step, lr)
         pw, pt = g.params()
         got = np.concatenate([pw, pt]).astype(np.float64)
-        # the step's gradient is summed again inside train_records, in another
-        # atomic order: a component whose sum is within rounding of zero may
-        # take the other sign; everything else moves as the formula says
+        # train_records sums the gradient once more: a component whose sum is
+        # within rounding of zero may take the other sign, and Adam (eps
+        # 1e-15) turns that into a full step the other way, now and in every
+        # later step through m; everything else moves as the formula says
+        ambiguous |= np.abs(grad) <= 8 * noise + 1e-7 * np.sqrt(np.mean(grad ** 2))
         err = np.abs(got - want)
-        assert np.mean(err <= 1e-6 + 1e-5 * lr) > 0.999, (step, np.quantile(err, [0.5, 0.999]))
+        ok = err <= 1e-6 + 1e-5 * lr
+        assert np.mean(ok[~ambiguous]) > 0.9999, (step, np.quantile(err[~ambiguous], [0.5, 0.9999]))
+        assert np.mean(ok) > 0.995 and ambiguous.mean() < 0.01, (step, np.mean(ok), ambiguous.mean())
         moved = np.abs(want - p) > 0
         assert moved.mean() > 0.01
         p = got
