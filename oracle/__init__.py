@@ -177,7 +177,7 @@ def load_ref() -> C.CDLL:
                                        C.c_int, C.c_int]
         dp = C.POINTER(C.c_double)
         lib.ref_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int,
-                                   C.c_int, dp, dp, dp]
+                                   C.c_int, dp, dp, dp, dp, dp, dp]
         _ref_lib = lib
     return _ref_lib
 
@@ -214,10 +214,12 @@ class RefScene:
 
     def render(self, film, index: int = 0, spp: int = 1, first_spp: int = 0, seed: int = 1, threads: int = 0,
                width: int = 0, height: int = 0, tile_stride: int = 1) -> None:
-        """Add `spp` samples per pixel of rendering entry `index` into a host
-        Film (value, weight and, if present, value_sq); tile_stride > 1
-        renders only every tile_stride-th task tile."""
+        """Add `spp` samples per pixel of rendering entry `index` (renderer
+        pt or ao) into a host Film (value, weight and, where the film has
+        them, value_sq and the G-buffer); tile_stride > 1 renders only every
+        tile_stride-th task tile."""
         dp = C.POINTER(C.c_double)
         ptr = lambda a: None if a is None else a.ctypes.data_as(dp)  # noqa: E731
         _ref_check(load_ref().ref_render(self._h, index, width, height, first_spp, spp, seed, threads, tile_stride,
-                                         ptr(film.value), ptr(film.weight), ptr(film.value_sq)))
+                                         ptr(film.value), ptr(film.weight), ptr(film.value_sq),
+                                         ptr(film.albedo), ptr(film.normal), ptr(film.denoise)))

@@ -185,14 +185,18 @@ int ref_trace_rays(RefScene* s, const AtrcRay* rays, size_t n, AtrcHit* hits, in
 
 // Render samples [first_spp, first_spp + spp_count) of every pixel of
 // rendering entry `index` with the reference's pt (its renderer keys and
-// defaults, renderer_creators.cpp:115-151) and ADD into the caller's FP64
-// films (width x height pixels, rows as the reference's film): value (3 per
-// pixel, sum w L), weight (sum w), value_sq (3 per pixel, sum w L^2, may be
-// null).  `width` / `height` override the entry's film size when positive.
-// tile_stride > 1 renders only every tile_stride-th task tile (row-major tile
-// index), a bounded sample of the image for timing the reference.
+// defaults, renderer_creators.cpp:115-151) or ao (renderer_creators.cpp:8-44,
+// render::trace_ao) and ADD into the caller's FP64 films (width x height
+// pixels, rows as the reference's film): value (3 per pixel, sum w L),
+// weight (sum w), value_sq (3 per pixel, sum w L^2), and the G-buffer the
+// reference's PerPixelRenderer keeps (perpixel_renderer.cpp:38-44): albedo
+// and normal (3 per pixel) and denoise (1 per pixel), each sum w x; the last
+// four may be null.  `width` / `height` override the entry's film size when
+// positive.  tile_stride > 1 renders only every tile_stride-th task tile
+// (row-major tile index), a bounded sample of the image for timing.
 int ref_render(RefScene* s, int index, int width, int height, int first_spp, int spp_count, uint64_t seed,
-               int threads, int tile_stride, double* value, double* weight, double* value_sq) {
+               int threads, int tile_stride, double* value, double* weight, double* value_sq, double* albedo,
+               double* normal, double* denoise) {
     if (!s || !value || !weight || spp_count < 1 || first_spp < 0 || tile_stride < 1)
         return fail("invalid argument");
     if (index < 0 || size_t(index) >= s->renderings.size()) return fail("rendering index out of range");
@@ -211,7 +215,17 @@ int ref_render(RefScene* s, int index, int width, int height, int first_spp, int
         // the pt creator's keys (renderer_creators.cpp:127-146)
         const ConfigGroup& rp = r.child_group("renderer");
         const std::string type = rp.child_str("type");
-        if (type != "pt" && type != "pt_cuda") return fail("renderer must be pt or pt_cuda, not " + type);
+        const bool is_ao = type == "ao";
+        if (type != "pt" && type != "pt_cuda" && !is_ao) return fail("renderer must be pt, pt_cuda or ao, not " + type);
+        // the ao creator's keys (renderer_creators.cpp:21-40)
+        render::AOParams ao;
+        if (is_ao) {
+            ao.ao_sample_count = rp.child_int_or("ao_sample_count", 5);
+            ao.low_color = rp.child_spectrum_or("low_color", Spectrum(0));
+            ao.high_color = rp.child_spectrum_or("high_color", Spectrum(1));
+            ao.max_occlusion_distance = rp.child_real_or("max_occlusion_distance", 1);
+            ao.background_color = rp.child_spectrum_or("background_color", Spectrum(0));
+        }
         render::TraceParams params;
         params.min_depth = rp.child_int_or("min_depth", 5);
         params.max_depth = rp.child_int_or("max_depth", 10);
@@ -223,8 +237,8 @@ int ref_render(RefScene* s, int index, int width, int height, int first_spp, int
         s->scene->set_camera(camera);
         s->scene->start_rendering();
         FilmFilterApplier filter(W, H, film_filter);
-        Image2D<DSpec> img_value(H, W), img_value_sq(H, W);
-        Image2D<double> img_weight(H, W);
+        Image2D<DSpec> img_value(H, W), img_value_sq(H, W), img_albedo(H, W), img_normal(H, W);
+        Image2D<double> img_weight(H, W), img_denoise(H, W);
         std::mutex merge_mutex;
         const int tiles_x = (W + grid_size - 1) / grid_size;
         const int nt = thread::actual_worker_count(threads);
@@ -235,7 +249,8 @@ int ref_render(RefScene* s, int index, int width, int height, int first_spp, int
             const uint64_t h = misc::hash(seed, uint64_t(tile), uint64_t(first_spp));
             NativeSampler sampler(int(h & 0x7fffffff), false);
             Arena arena;
-            auto grid = filter.create_subgrid<DSpec, double, DSpec>({rect.low, rect.high - Vec2i(1)});
+            auto grid = filter.create_subgrid<DSpec, double, DSpec, DSpec, DSpec, double>(
+                {rect.low, rect.high - Vec2i(1)});
             const auto bound = grid.sample_pixels();
             for (int py = bound.low.y; py <= bound.high.y; ++py)
                 for (int px = bound.low.x; px <= bound.high.x; ++px)
@@ -245,17 +260,21 @@ int ref_render(RefScene* s, int index, int width, int height, int first_spp, int
                         const real pixel_x = px + film_sam.u, pixel_y = py + film_sam.v;
                         auto cam_ray = camera->sample_we({pixel_x / W, pixel_y / H}, sampler.sample2());
                         const Ray ray(cam_ray.pos_on_cam, cam_ray.pos_to_out);
-                        const render::Pixel pixel = use_mis ? render::trace_std(params, *s->scene, ray, sampler, arena)
-                                                            : render::trace_nomis(params, *s->scene, ray, sampler, arena);
+                        const render::Pixel pixel =
+                            is_ao     ? render::trace_ao(ao, *s->scene, ray, sampler)
+                            : use_mis ? render::trace_std(params, *s->scene, ray, sampler, arena)
+                                      : render::trace_nomis(params, *s->scene, ray, sampler, arena);
                         if (pixel.value.is_finite()) {
                             const Spectrum v = cam_ray.throughput * pixel.value;
                             const DSpec dv(v.r, v.g, v.b);
-                            grid.apply(pixel_x, pixel_y, dv, 1.0, DSpec(dv.r * dv.r, dv.g * dv.g, dv.b * dv.b));
+                            grid.apply(pixel_x, pixel_y, dv, 1.0, DSpec(dv.r * dv.r, dv.g * dv.g, dv.b * dv.b),
+                                       DSpec(pixel.albedo.r, pixel.albedo.g, pixel.albedo.b),
+                                       DSpec(pixel.normal.x, pixel.normal.y, pixel.normal.z), double(pixel.denoise));
                         }
                         arena.release();
                     }
             std::lock_guard<std::mutex> lk(merge_mutex);
-            grid.merge_into(img_value, img_weight, img_value_sq);
+            grid.merge_into(img_value, img_weight, img_value_sq, img_albedo, img_normal, img_denoise);
             return true;
         });
         for (int y = 0; y < H; ++y)
@@ -266,12 +285,16 @@ int ref_render(RefScene* s, int index, int width, int height, int first_spp, int
                 value[3 * i + 1] += v.g;
                 value[3 * i + 2] += v.b;
                 weight[i] += img_weight(y, x);
-                if (value_sq) {
-                    const DSpec& q = img_value_sq(y, x);
-                    value_sq[3 * i] += q.r;
-                    value_sq[3 * i + 1] += q.g;
-                    value_sq[3 * i + 2] += q.b;
-                }
+                auto add3 = [&](double* dst, const DSpec& q) {
+                    if (!dst) return;
+                    dst[3 * i] += q.r;
+                    dst[3 * i + 1] += q.g;
+                    dst[3 * i + 2] += q.b;
+                };
+                add3(value_sq, img_value_sq(y, x));
+                add3(albedo, img_albedo(y, x));
+                add3(normal, img_normal(y, x));
+                if (denoise) denoise[i] += img_denoise(y, x);
             }
         return 0;
     } catch (const std::exception& e) {

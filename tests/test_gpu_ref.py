@@ -126,3 +126,39 @@ def test_images_match_reference(tmp_path, name, spp):
     frac, allowed, info = band_test(fg, fr, 1 / (4 * r * r), cluster=3)
     assert frac <= allowed, (frac, allowed, info)
     assert global_mean_z(fg, fr) < 4.0
+
+
+def test_ao_matches_reference(tmp_path):
+    cfgd = K.ao_slab(spp=512)
+    cfgd["rendering"]["width"] = cfgd["rendering"]["height"] = 32
+    p = tmp_path / "ao.json"
+    p.write_text(K.dumps(cfgd))
+    cfg = Config.from_file(p)
+    desc, _ = cfg.rendering(0)
+    fg = Film(desc.width, desc.height, value_sq=True)
+    DeviceScene(cfg).render(desc, fg)
+    fr = Film(desc.width, desc.height, value_sq=True)
+    oracle.RefScene(p).render(fr, spp=desc.spp, seed=31)
+    r = 0.5 - desc.eps
+    frac, allowed, info = band_test(fg, fr, 1 / (4 * r * r), cluster=3)
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fg, fr) < 4.0
+
+
+def test_gbuffer_matches_reference(tmp_path):
+    sub = tmp_path / "feature"
+    sub.mkdir()
+    p = sub / "scene.json"
+    p.write_text(K.dumps(K.feature_scene(sub, spp=64)))
+    cfg = Config.from_file(p)
+    desc, _ = cfg.rendering(0)
+    fg = Film(desc.width, desc.height, gbuffer=True)
+    DeviceScene(cfg).render(desc, fg)
+    fr = Film(desc.width, desc.height, gbuffer=True)
+    oracle.RefScene(p).render(fr, spp=desc.spp, seed=3)
+    wg, wr = fg.weight.reshape(-1, 1), fr.weight.reshape(-1, 1)
+    for k in ("albedo", "normal"):
+        a = getattr(fg, k).reshape(-1, 3) / wg
+        b = getattr(fr, k).reshape(-1, 3) / wr
+        assert np.all(np.abs(a.mean(0) - b.mean(0)) < 1e-3), (k, a.mean(0), b.mean(0))
+    np.testing.assert_array_equal(fg.denoise / fg.weight, fr.denoise / fr.weight)

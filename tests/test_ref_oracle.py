@@ -161,3 +161,45 @@ def test_images_match_reference(tmp_path, name, spp):
     frac, allowed, info = band_test(fr, fo, 1 / (4 * r * r), cluster=3)
     assert frac <= allowed, (frac, allowed, info)
     assert global_mean_z(fr, fo) < 4.0
+
+
+def test_ao_matches_reference(tmp_path):
+    # the reference's ao renderer (render::trace_ao): the parallel-plane known
+    # answer and the 3-sigma band against the restated oracle
+    cfgd = K.ao_slab(spp=256)
+    cfgd["rendering"]["width"] = cfgd["rendering"]["height"] = 32
+    p = _write(tmp_path, "ao", cfgd)
+    desc, fr, fo = _render_both(p)
+    e = desc.eps
+    frac = ((0.5 - e) / (1.0 - e)) ** 2
+    low, high = np.array([0.1, 0.2, 0.3]), np.array([0.9, 0.8, 0.7])
+    want = low + (high - low) * frac
+    n = desc.width * desc.height * desc.spp
+    sigma = np.abs(high - low) * np.sqrt(frac * (1 - frac) / (n * 5))
+    assert np.all(np.abs(fr.image().reshape(-1, 3).mean(0) - want) < 4 * sigma)
+    r = 0.5 - desc.eps
+    f, allowed, info = band_test(fr, fo, 1 / (4 * r * r), cluster=3)
+    assert f <= allowed, (f, allowed, info)
+
+
+def test_gbuffer_matches_reference(tmp_path):
+    # the G-buffer PerPixelRenderer keeps beside the image
+    # (perpixel_renderer.cpp:38-44): first-hit albedo and normal and the
+    # denoise flag.  Per pixel they are Monte Carlo averages over the pixel's
+    # footprint, so the image-wide means are compared
+    sub = tmp_path / "feature"
+    sub.mkdir()
+    p = _write(sub, "scene", K.feature_scene(sub, spp=64))
+    cfg = Config.from_file(p)
+    desc, _ = cfg.rendering(0)
+    fr = Film(desc.width, desc.height, gbuffer=True)
+    oracle.RefScene(p).render(fr, spp=desc.spp, seed=3)
+    fo = Film(desc.width, desc.height, gbuffer=True)
+    oracle.OracleScene(cfg.scene_desc(), desc.eps).render(desc, fo)
+    wr, wo = fr.weight.reshape(-1, 1), fo.weight.reshape(-1, 1)
+    for k in ("albedo", "normal"):
+        a = getattr(fr, k).reshape(-1, 3) / wr
+        b = getattr(fo, k).reshape(-1, 3) / wo
+        assert np.all(np.abs(a.mean(0) - b.mean(0)) < 1e-3), (k, a.mean(0), b.mean(0))
+        assert np.mean(np.abs(a - b).max(1) < 1e-4) > 0.4     # pixels inside one flat surface agree exactly
+    np.testing.assert_array_equal(fr.denoise / fr.weight, fo.denoise / fo.weight)
