@@ -773,6 +773,7 @@ int atrc_guide_create(int device, const float scene_lo[3], const float scene_hi[
         G.t_f.alloc(G.table_n * 4); G.t_g.alloc(G.table_n * 4); G.t_m.alloc(G.table_n * 4); G.t_v.alloc(G.table_n * 4);
         G.t_h.alloc(G.table_n * 2);
         G.records.alloc(size_t(desc->record_capacity) * sizeof(GuideRecord));
+        G.live.alloc(size_t(desc->record_capacity) * sizeof(GuideRecord));
         G.rec_count.alloc(2 * sizeof(int));
         G.scratch.alloc(64);
         G.err.alloc(sizeof(int));
@@ -972,7 +973,6 @@ int atrc_guide_train(AtrcGuide* g, int steps, float* last_loss) {
             G.record_keep = std::min(1.0f, std::max(1.0f / 4096.0f, 0.95f * float(cap) / float(counts[1])));
         if (last_loss) *last_loss = 0;
         if (stored < kTile) return int(ATRC_OK);
-        if (G.live.bytes < size_t(cap) * sizeof(GuideRecord)) G.live.alloc(size_t(cap) * sizeof(GuideRecord));
         int* live_n = reinterpret_cast<int*>(G.scratch.as<float>() + 4);
         CK(cudaMemsetAsync(live_n, 0, sizeof(int), s));
         k_live_records<<<G.sm_count * 4, 256, 0, s>>>(G.records.as<GuideRecord>(), stored,

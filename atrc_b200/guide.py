@@ -162,15 +162,19 @@ def time_to(curve, target: float) -> Optional[float]:
 
 def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, train_fraction: float = 0.25,
                   train_steps: int = 4, spp_per_pass: int = 1, reference=None, checkpoints=(), first_spp: int = 0,
-                  ref_var=None, stop_at: Optional[float] = None):
+                  ref_var=None, stop_at: Optional[float] = None, warmup: bool = True):
     """Render passes of `spp_per_pass` samples per pixel into one device film
     until `seconds` of render time have passed.  With a guide, the passes of
     the first `train_fraction` of the budget record training data and run
     `train_steps` Adam steps after each pass; later passes only sample with
     the guide.  The clock runs only inside the render / training calls (the
     calls are synchronous), so the relMSE checkpoints against `reference`
-    (a torch CUDA tensor H x W x 3) cost nothing.  Returns the film, the
-    (time, spp, relMSE) checkpoints and per-phase times."""
+    (a torch CUDA tensor H x W x 3) cost nothing.  With `warmup`, untimed
+    passes into a scratch film first do the one-time set-up of the render
+    calls the loop makes (graph capture, the guide's per-path buffers); they
+    neither record training data that is used nor train, and their samples
+    are dropped.  Returns the film, the (time, spp, relMSE) checkpoints and
+    per-phase times."""
     import time
 
     import torch
@@ -178,6 +182,18 @@ def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, tr
     from . import Film
     film = Film(desc.width, desc.height, device=True)
     desc.spp_count = spp_per_pass
+    if warmup:
+        scratch = Film(desc.width, desc.height, device=True)
+        desc.first_spp = first_spp + (1 << 24)
+        if guide is None:
+            scene.render(desc, scratch)
+        else:
+            # a recording render's records are replaced by the next one's
+            if train_fraction > 0:
+                scene.render_guided(guide, desc, scratch, record=True)
+            scene.render_guided(guide, desc, scratch, record=False)
+        torch.cuda.synchronize()
+        del scratch
     elapsed = t_render = t_train = 0.0
     passes = 0
     curve = []

@@ -280,11 +280,14 @@ def test_adam_steps_match_reference():
         # within rounding of zero may take the other sign, and Adam (eps
         # 1e-15) turns that into a full step the other way, now and in every
         # later step through m; everything else moves as the formula says
-        ambiguous |= np.abs(grad) <= 8 * noise + 1e-7 * np.sqrt(np.mean(grad ** 2))
+        # (parameters no record touches have a gradient of exactly zero in
+        # every sum, and Adam leaves them where m and v put them)
+        touched = (grad != 0) | (noise != 0)
+        ambiguous |= touched & (np.abs(grad) <= 8 * noise + 1e-7 * np.sqrt(np.mean(grad ** 2)))
         err = np.abs(got - want)
         ok = err <= 1e-6 + 1e-5 * lr
         assert np.mean(ok[~ambiguous]) > 0.9999, (step, np.quantile(err[~ambiguous], [0.5, 0.9999]))
-        assert np.mean(ok) > 0.995 and ambiguous.mean() < 0.01, (step, np.mean(ok), ambiguous.mean())
+        assert np.mean(ok) > 0.995, (step, np.mean(ok), ambiguous.mean())
         moved = np.abs(want - p) > 0
         assert moved.mean() > 0.01
         p = got

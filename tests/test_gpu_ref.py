@@ -8,9 +8,10 @@ tests against the restated oracle:
 * closest hits of 10^7 seeded rays on the Cornell scene at its benchmark
   geometry: the same entity and t within 2 ulp (the reference's intersection
   records carry no primitive index, so a primitive is identified by its
-  entity and t), with the remaining rays classified as ties (two entities at
-  the same t) or genuine hits the reference's BVH skipped (confirmed by the
-  restated Moller-Trumbore test of the device's primitive);
+  entity and t), with the remaining rays classified as ties (coplanar
+  surfaces at the same t up to a few ulp) or genuine hits the reference's
+  BVH skipped (confirmed by the restated Moller-Trumbore test of the
+  device's primitive);
 * instanced geometry: same entity, t within the matrix-rounding tolerance;
 * images: the per-pixel 3-sigma band and the image-mean z-score.
 """
@@ -30,14 +31,21 @@ pytestmark = [pytest.mark.gpu,
 
 def classify_vs_reference(rays, dev, ref, ora):
     """exact: same entity and t within 2 ulp, or both miss; tie: both hit at
-    t within 2 ulp on different entities; ref_fn: the device hit is closer (or
-    the reference missed) and the restated test of the device's primitive
+    t within 2 ulp on different entities, or within 4 ulp where the restated
+    test of the device's primitive confirms the device's hit (coplanar
+    surfaces -- the Cornell boxes stand on the floor -- meet the ray at one t
+    in exact arithmetic, and their float t differ by a few ulp; which one a
+    BVH reaches first decides); ref_fn: the device hit is closer (or the
+    reference missed) and the restated test of the device's primitive
     confirms it; error: anything else."""
     both_miss = (dev["entity"] < 0) & (ref["entity"] < 0)
     both_hit = (dev["entity"] >= 0) & (ref["entity"] >= 0)
-    close = ulp_diff(dev["t"], ref["t"]) <= 2
-    exact = both_miss | (both_hit & (dev["entity"] == ref["entity"]) & close)
-    tie = both_hit & (dev["entity"] != ref["entity"]) & close
+    u = ulp_diff(dev["t"], ref["t"])
+    exact = both_miss | (both_hit & (dev["entity"] == ref["entity"]) & (u <= 2))
+    tie = both_hit & (dev["entity"] != ref["entity"]) & (u <= 2)
+    for i in np.nonzero(both_hit & ~exact & ~tie & (u <= 4))[0]:
+        t = ora.prim_hit(rays[i], int(dev["entity"][i]), int(dev["prim"][i]))
+        tie[i] = t >= 0 and ulp_diff(t, dev["t"][i]) <= 2
     out = {"n": len(rays), "exact": int(exact.sum()), "tie": int(tie.sum()), "ref_fn": 0, "error": 0, "errors": []}
     for i in np.nonzero(~exact & ~tie)[0]:
         g, r = dev[i], ref[i]
