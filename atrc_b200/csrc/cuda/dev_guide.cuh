@@ -19,7 +19,7 @@
 //   [96]       roughness (0 for non-Disney materials).
 // Output (kGuideOut = 48 raw values, 41 used): per lobe k the unnormalised
 // mean direction o[5k..5k+2], log kappa o[5k+3] and mixture logit o[5k+4];
-// o[40] is the selection logit (c = 0.9 sigmoid(o[40] - 2)).
+// o[40] is the selection logit (c = max_select sigmoid(o[40] - 2)).
 #pragma once
 
 #include <cstdint>
@@ -36,8 +36,13 @@ constexpr int kGuideOut = 48;
 constexpr int kGuideUsed = 5 * kGuideLobes + 1;
 constexpr int kHashLevels = 16;
 constexpr int kHashFeatures = 2;
-constexpr float kGuideMaxSelect = 0.9f;   // default cap: c = max_select * sigmoid(o[40] + kSelectOffset)
-constexpr float kSelectOffset = -2.0f;    // an untrained guide (o ~ 0) is picked with c ~ 0.11
+// Default cap: c = max_select * sigmoid(o[40] + kSelectOffset).  The weight
+// of a vertex is at most 1 / (1 - c) times the BSDF sampler's, so the cap
+// bounds the variance a guide that is still learning can add: on the indoor
+// room's equal-time protocol (5 seeds) caps of 0.9 / 0.5 / 0.3 / 0.25 / 0.15
+// gave time ratios of 1.13 / 0.74 / 0.63-0.73 / 0.56 / 0.61.
+constexpr float kGuideMaxSelect = 0.25f;
+constexpr float kSelectOffset = -2.0f;    // an untrained guide (o ~ 0) is picked with c ~ 0.12 max_select
 constexpr float kLogKappaMin = -6.9f;     // kappa in [1e-3, 1e4]
 constexpr float kLogKappaMax = 9.2f;
 

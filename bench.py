@@ -249,7 +249,7 @@ def cpu_baseline(args) -> dict:
 
 def guided_comparison(args) -> dict:
     """Time to relMSE 1e-3 of guided and of plain pt_cuda on the indoor room
-    (1280x720, depth 16, fixed Disney sampling), three seeds per arm (relMSE
+    (1280x720, depth 16, fixed Disney sampling), five seeds per arm (relMSE
     at this level swings by tens of percent between seeds): plain renders
     until it reaches the target; each guided render gets 1.6 x the mean plain
     time (stopping at the target), trains during the first quarter of the
@@ -276,7 +276,7 @@ def guided_comparison(args) -> dict:
     n = (w / fv).clamp_min(2.0)
     ref_var = ((ref.value_sq.view(H, W, 3) / w - R * R).clamp_min(0) / (n - 1)).float()
     R = R.float()
-    seeds = [42, 43, 44]
+    seeds = [42, 43, 44, 45, 46]
     plains = []
     for sd in seeds:
         desc.seed = sd

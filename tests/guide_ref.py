@@ -9,7 +9,7 @@ import numpy as np
 
 LEVELS = 16
 IN, HID, OUT, LOBES = 112, 64, 48, 8
-MAX_SELECT = 0.9
+MAX_SELECT = 0.9      # the selection cap the tests give their guides (AtrcGuideDesc.max_select)
 SELECT_OFFSET = -2.0
 LOG_KAPPA = (-6.9, 9.2)
 

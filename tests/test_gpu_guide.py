@@ -20,7 +20,7 @@ def _unit(rng, n):
 
 
 def _random_guide(seed=3):
-    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=seed)
+    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=seed, max_select=R.MAX_SELECT)
     info = g.info()
     rng = np.random.default_rng(seed)
     w = np.concatenate([rng.normal(0, 1.5 / math.sqrt(fi), fo * fi)
@@ -78,7 +78,7 @@ def test_device_pdf_matches_fp64_evaluation():
     rel16 = np.abs(pdf - emu) / emu
     assert np.median(rel16) < 2e-3 and np.quantile(rel16, 0.95) < 2e-2, (np.median(rel16), np.quantile(rel16, 0.95))
     np.testing.assert_allclose(c, c_ref, atol=0.01)
-    assert np.all(c >= 0) and np.all(c <= 0.9 + 1e-6)
+    assert np.all(c >= 0) and np.all(c <= R.MAX_SELECT + 1e-6)
 
 
 def test_mixture_is_a_density():
@@ -107,7 +107,8 @@ def _vmf_sample(rng, mu, kappa, n):
 def test_training_learns_a_lobe():
     # every record's direction follows one vMF lobe (kappa 30): the optimum
     # of the loss is that lobe chosen with the largest selection probability
-    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, base_resolution=2, max_resolution=16, batch=1 << 14, seed=9)
+    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, base_resolution=2, max_resolution=16, batch=1 << 14, seed=9,
+              max_select=0.9)
     rng = np.random.default_rng(21)
     n = 1 << 17
     mu = np.array([0.3, -0.5, 0.81])
@@ -230,7 +231,7 @@ def test_training_gradients_match_fp64_backward():
     # two or three tiles before their atomic flush
     g, w, t, info = _random_guide(seed=5)
     g.close()
-    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=5, record_capacity=1 << 16)
+    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=5, record_capacity=1 << 16, max_select=R.MAX_SELECT)
     info = g.info()
     g.set_params(w, t)
     rng = np.random.default_rng(17)
@@ -255,7 +256,8 @@ def test_training_gradients_match_fp64_backward():
 def test_adam_steps_match_reference():
     g, w, t, info = _random_guide(seed=6)
     g.close()
-    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=6, record_capacity=1 << 16, batch=1 << 16)
+    g = Guide([-1, -1, -1], [1, 1, 1], log2_table=12, seed=6, record_capacity=1 << 16, batch=1 << 16,
+              max_select=R.MAX_SELECT)
     info = g.info()
     g.set_params(w, t)
     lr = g.desc.learning_rate
