@@ -189,6 +189,7 @@ PROTOTYPES = {
     "atrc_guide_create": (C.c_int, [C.c_int, c_float_p, c_float_p, C.POINTER(AtrcGuideDesc), C.POINTER(C.c_void_p)]),
     "atrc_guide_destroy": (None, [C.c_void_p]),
     "atrc_guide_info": (C.c_int, [C.c_void_p, C.POINTER(AtrcGuideInfo)]),
+    "atrc_guide_set_max_select": (C.c_int, [C.c_void_p, C.c_float]),
     "atrc_guide_params": (C.c_int, [C.c_void_p, c_float_p, c_float_p, C.c_int]),
     "atrc_guide_eval": (C.c_int, [C.c_void_p, c_float_p, C.c_size_t, c_float_p]),
     "atrc_guide_train": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),

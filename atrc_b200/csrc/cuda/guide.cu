@@ -820,6 +820,13 @@ int atrc_guide_params(AtrcGuide* g, float* weights, float* table, int set) {
     });
 }
 
+int atrc_guide_set_max_select(AtrcGuide* g, float max_select) {
+    if (!g || !(max_select > 0 && max_select <= 0.99f))
+        return gfail(ATRC_ERR_INVALID_ARG, "atrc_guide_set_max_select: max_select must be in (0, 0.99]");
+    g->impl.desc.max_select = max_select;
+    return int(ATRC_OK);
+}
+
 int atrc_guide_info(AtrcGuide* g, AtrcGuideInfo* info) {
     if (!g || !info) return gfail(ATRC_ERR_INVALID_ARG, "atrc_guide_info: null argument");
     const GuideImpl& G = g->impl;

@@ -62,6 +62,10 @@ class Guide:
     def handle(self) -> C.c_void_p:
         return self._h
 
+    def set_max_select(self, max_select: float) -> None:
+        """Cap on the selection probability for the renders that follow."""
+        _check(load_library().atrc_guide_set_max_select(self._h, max_select))
+
     def info(self) -> dict:
         i = abi.AtrcGuideInfo()
         _check(load_library().atrc_guide_info(self._h, C.byref(i)))
@@ -162,7 +166,8 @@ def time_to(curve, target: float) -> Optional[float]:
 
 def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, train_fraction: float = 0.25,
                   train_steps: int = 4, spp_per_pass: int = 1, reference=None, checkpoints=(), first_spp: int = 0,
-                  ref_var=None, stop_at: Optional[float] = None, warmup: bool = True):
+                  ref_var=None, stop_at: Optional[float] = None, warmup: bool = True,
+                  select_after: Optional[float] = None):
     """Render passes of `spp_per_pass` samples per pixel into one device film
     until `seconds` of render time have passed.  With a guide, the passes of
     the first `train_fraction` of the budget record training data and run
@@ -173,8 +178,9 @@ def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, tr
     passes into a scratch film first do the one-time set-up of the render
     calls the loop makes (graph capture, the guide's per-path buffers); they
     neither record training data that is used nor train, and their samples
-    are dropped.  Returns the film, the (time, spp, relMSE) checkpoints and
-    per-phase times."""
+    are dropped.  `select_after`, if given, becomes the guide's selection
+    cap once training ends.  Returns the film, the (time, spp, relMSE)
+    checkpoints and per-phase times."""
     import time
 
     import torch
@@ -199,9 +205,13 @@ def render_budget(scene, desc, seconds: float, guide: Optional[Guide] = None, tr
     curve = []
     pending = sorted(checkpoints)
     stopped = False
+    raised = False
     while elapsed < seconds and not stopped:
         desc.first_spp = first_spp + passes * spp_per_pass
         training = guide is not None and elapsed < train_fraction * seconds
+        if guide is not None and not training and select_after is not None and not raised:
+            guide.set_max_select(select_after)
+            raised = True
         t0 = time.perf_counter()
         if guide is None:
             scene.render(desc, film)

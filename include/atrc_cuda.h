@@ -668,6 +668,11 @@ int  atrc_guide_create(int device, const float lo[3], const float hi[3],
                        const AtrcGuideDesc* desc, AtrcGuide** out);
 void atrc_guide_destroy(AtrcGuide* guide);
 int  atrc_guide_info(AtrcGuide* guide, AtrcGuideInfo* info);
+/* Change the cap on the selection probability (0 < max_select <= 0.99) for
+ * the renders and training steps that follow, e.g. a low cap while the guide
+ * learns and a higher one once it has: every render uses one cap for both
+ * its sampling and its pdfs, so the estimator stays unbiased. */
+int  atrc_guide_set_max_select(AtrcGuide* guide, float max_select);
 /* Read (set = 0) or replace (set = 1) the FP32 master parameters; either
  * pointer may be NULL.  Sizes as in AtrcGuideInfo. */
 int  atrc_guide_params(AtrcGuide* guide, float* weights, float* table, int set);
