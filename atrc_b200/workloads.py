@@ -12,6 +12,12 @@ times).
     python -m atrc_b200.workloads subsurface [--spp 4] [--warmup 2] [--steps 1]
         the Cornell box at 1024x1024 with its two boxes made of Disney
         materials with subsurface scattering (the k_subsurface walk)
+    python -m atrc_b200.workloads ploc
+        the instanced scene with every mesh tree built by the device PLOC
+        builder (bvh_gpu.cu), then one 1-spp render
+    python -m atrc_b200.workloads rays [--count 10000000]
+        closest-hit queries of seeded rays against the instanced scene
+        through atrc_cuda_trace_rays (k_trace_rays)
 """
 from __future__ import annotations
 
@@ -56,6 +62,41 @@ def subsurface(spp: int, warmup: int, steps: int) -> None:
             print(f"step {k - warmup}: closest rays {stats['rays_closest']}, shadow rays {stats['rays_shadow']}")
 
 
+def ploc() -> None:
+    import json
+    from pathlib import Path
+
+    from . import Config, DeviceScene, Film, scenes
+    path = Path(scenes.instanced_disney())
+    d = json.loads(path.read_text())
+    d["scene"]["bvh_builder"] = "ploc"
+    cfg = Config.from_string(json.dumps(d), str(path.parent))
+    desc, _ = cfg.rendering(0)
+    scene = DeviceScene(cfg)
+    desc.spp_count = 1
+    stats = scene.render(desc, Film(desc.width, desc.height, device=True))
+    print(f"closest rays {stats['rays_closest']}")
+
+
+def rays(count: int) -> None:
+    import numpy as np
+
+    from . import RAY_DTYPE, Config, DeviceScene, scenes
+    cfg = Config.from_file(scenes.instanced_disney())
+    desc, _ = cfg.rendering(0)
+    scene = DeviceScene(cfg)
+    rng = np.random.default_rng(7)
+    r = np.zeros(count, RAY_DTYPE)
+    r["o"] = np.broadcast_to(np.asarray(desc.camera.pos, np.float32), (count, 3))
+    tgt = rng.uniform(-20, 20, (count, 3))
+    dd = tgt - r["o"]
+    r["d"] = dd / np.linalg.norm(dd, axis=1, keepdims=True)
+    r["t_max"] = np.inf
+    for _ in range(2):
+        h = scene.trace_rays(r, "closest")
+    print(f"hits {(h['entity'] >= 0).mean():.3f}")
+
+
 def guided_room(train_passes: int, passes: int) -> None:
     from . import Config, DeviceScene, Film, scenes
     from .guide import Guide
@@ -89,6 +130,9 @@ def main() -> None:
     b = sub.add_parser("guided-room")
     b.add_argument("--train-passes", type=int, default=3)
     b.add_argument("--passes", type=int, default=3)
+    sub.add_parser("ploc")
+    e = sub.add_parser("rays")
+    e.add_argument("--count", type=int, default=10_000_000)
     c = sub.add_parser("subsurface")
     c.add_argument("--spp", type=int, default=4)
     c.add_argument("--warmup", type=int, default=2)
@@ -98,6 +142,10 @@ def main() -> None:
         instanced(args.spp, args.warmup, args.steps)
     elif args.workload == "subsurface":
         subsurface(args.spp, args.warmup, args.steps)
+    elif args.workload == "ploc":
+        ploc()
+    elif args.workload == "rays":
+        rays(args.count)
     else:
         guided_room(args.train_passes, args.passes)
 
