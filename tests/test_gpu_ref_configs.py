@@ -5,11 +5,12 @@ benchmark scenes at their stated geometry and settings, through the C ABI.
   max depth 8), every pixel in the 3-sigma band.
 * the instanced Disney + IBL scene, 3.08M unique triangles in 64
   instances, at its full 1920 x 1080 film and depth 16 with 16 spp (the
-  reference's CPU time at 256 spp would be minutes); closest hits of 10^6
-  seeded rays.
+  reference's CPU time at 256 spp would be minutes), the band over 8 x 8
+  pixel blocks; closest hits of 10^6 seeded rays.
 * the media scene (128^3 fBm grid, 200,000-triangle sphere, two
   area lights and the sky) at its 512 spp and depth 32 on a 48 x 48 film.
-* the indoor room at its full 1280 x 720 film with 16 spp.
+* the indoor room at its full 1280 x 720 film with 16 spp, the
+  band over 8 x 8 pixel blocks.
 
 The reference renders through its own factory, BVHs, materials, lights,
 media and trace_std (`tests/test_ref_oracle.py` pins the restated oracle to
@@ -44,7 +45,23 @@ def _device_and_reference(path, spp=None, seed=41):
     return desc, fg, fr
 
 
-def _assert_band(fg, fr):
+class _Blocks:
+    """A film's sums over b x b pixel blocks (value, weight and value_sq are
+    sums over samples, so block sums estimate block means): at 16 spp a
+    pixel's few samples from a heavy-tailed distribution (sun and sky hits)
+    do not follow the t law the band test assumes; 8 x 8 blocks of 1,024
+    samples do."""
+
+    def __init__(self, f, w, h, b):
+        H, W = h // b, w // b
+        def agg(a, c):
+            return a.reshape(h, w, c)[:H * b, :W * b].reshape(H, b, W, b, c).sum((1, 3)).reshape(-1)
+        self.value, self.weight, self.value_sq = agg(f.value, 3), agg(f.weight, 1), agg(f.value_sq, 3)
+
+
+def _assert_band(fg, fr, desc=None, block=1):
+    if block > 1:
+        fg, fr = _Blocks(fg, desc.width, desc.height, block), _Blocks(fr, desc.width, desc.height, block)
     frac, allowed, info = band_test(fg, fr, BOX, cluster=3)
     assert frac <= allowed, (frac, allowed, info)
     assert global_mean_z(fg, fr) < 4.0
@@ -64,7 +81,7 @@ def instanced_cfg1(scene_dir):
 def test_instanced_config1_full_film_matches_reference(instanced_cfg1):
     desc, fg, fr = _device_and_reference(instanced_cfg1, spp=16)
     assert (desc.width, desc.height, desc.max_depth) == (1920, 1080, 16)
-    _assert_band(fg, fr)
+    _assert_band(fg, fr, desc, block=8)
 
 
 def test_instanced_config1_closest_hits_match_reference(instanced_cfg1):
@@ -94,4 +111,4 @@ def test_media_config2_matches_reference(scene_dir):
 def test_room_config3_full_film_matches_reference(scene_dir):
     desc, fg, fr = _device_and_reference(scenes.indoor_room(scene_dir / "ref_room_cfg3"), spp=16)
     assert (desc.width, desc.height, desc.max_depth) == (1280, 720, 16)
-    _assert_band(fg, fr)
+    _assert_band(fg, fr, desc, block=8)
