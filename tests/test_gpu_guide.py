@@ -6,7 +6,7 @@ import math
 import numpy as np
 import pytest
 
-from atrc_b200 import Config, DeviceScene, Film
+from atrc_b200 import AtrcError, Config, DeviceScene, Film
 from atrc_b200.guide import RECORD_FLOATS, Guide
 from tests import guide_ref as R
 from tests.parity import band_test, global_mean_z
@@ -79,6 +79,22 @@ def test_device_pdf_matches_fp64_evaluation():
     assert np.median(rel16) < 2e-3 and np.quantile(rel16, 0.95) < 2e-2, (np.median(rel16), np.quantile(rel16, 0.95))
     np.testing.assert_allclose(c, c_ref, atol=0.01)
     assert np.all(c >= 0) and np.all(c <= R.MAX_SELECT + 1e-6)
+
+
+def test_selection_cap_can_change_between_renders():
+    g, _, _, _ = _random_guide(8)
+    rng = np.random.default_rng(14)
+    q = _queries(rng, 512)
+    d = _unit(rng, 512).astype(np.float32)
+    _, c9 = g.pdf(q, d)
+    g.set_max_select(0.3)
+    assert g.info()["max_select"] == pytest.approx(0.3)
+    _, c3 = g.pdf(q, d)
+    # c = cap * sigmoid(o - 2): the same network, the cap rescales c
+    np.testing.assert_allclose(c3, c9 * (0.3 / R.MAX_SELECT), rtol=1e-5, atol=1e-7)
+    for bad in (0.0, -0.1, 1.0):
+        with pytest.raises(AtrcError):
+            g.set_max_select(bad)
 
 
 def test_mixture_is_a_density():
