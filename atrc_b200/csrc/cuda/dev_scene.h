@@ -102,10 +102,6 @@ struct Medium {
     int32_t density, albedo, g_tex;
     int32_t white_for_indirect;
     float max_density, inv_max_density;
-    // majorant grid (heterogeneous media whose density texture is clamped
-    // and gamma-free): maj_res^3 cell maxima of the density over texture
-    // space at Scene::majorants[maj_offset]; maj_res 0: the global maximum
-    int32_t maj_res, maj_offset;
 };
 
 struct Env {
@@ -135,7 +131,6 @@ struct Scene {
     const Texture2D* tex2d;
     const Texture3D* tex3d;
     const float* texels;
-    const float* majorants;         // majorant grids of the heterogeneous media
     const Medium* media;
     int32_t medium_count;
     int32_t has_media;              // any non-void medium referenced

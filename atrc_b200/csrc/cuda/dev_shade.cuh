@@ -1202,76 +1202,6 @@ __device__ BSDFSample hg_sample(const Phase& ph, Vec3 wo, float u0, float u1) {
     return r;
 }
 
-// The segment a -> b (world length t_max) cut into spans, each with a
-// majorant of the medium's density: the cells of its majorant grid that the
-// segment crosses, in the density texture's coordinates (an affine image of
-// the segment), by a 3D DDA (Amanatides and Woo 1987); the parts outside the
-// texture's unit cube, and the whole segment of a medium without a grid,
-// get the global maximum.  f(t0, t1, majorant) returns false to stop.
-// Delta tracking with these majorants samples the same free-flight
-// distribution as with the global one, and ratio tracking estimates the
-// same transmittance, with fewer null collisions where the density is low
-// (the majorant-grid scheme of PBRT-v4's grid medium).
-template <class F>
-__device__ __forceinline__ void majorant_spans(const Scene& S, const Medium& m, Vec3 a, Vec3 b, float t_max, F&& f) {
-    if (m.maj_res <= 0 || !(t_max > 0.0f)) {
-        f(0.0f, t_max, m.max_density);
-        return;
-    }
-    const Texture3D& tx = S.tex3d[m.density];
-    const Vec3 ua = apply_point_rn(tx.uvw, apply_point_rn(m.inv, a));
-    const Vec3 du = apply_point_rn(tx.uvw, apply_point_rn(m.inv, b)) - ua;
-    // the segment parameter range inside [0, 1]^3
-    float s0 = 0.0f, s1 = 1.0f;
-    for (int k = 0; k < 3; ++k) {
-        if (du[k] != 0.0f) {
-            const float ta = -ua[k] / du[k], tb = (1.0f - ua[k]) / du[k];
-            s0 = fmaxf(s0, fminf(ta, tb));
-            s1 = fminf(s1, fmaxf(ta, tb));
-        } else if (ua[k] < 0.0f || ua[k] > 1.0f) {
-            s1 = -1.0f;
-        }
-    }
-    if (!(s0 < s1)) {
-        f(0.0f, t_max, m.max_density);
-        return;
-    }
-    if (s0 > 0.0f && !f(0.0f, s0 * t_max, m.max_density)) return;
-    const int R = m.maj_res;
-    const float* maj = S.majorants + m.maj_offset;
-    int c[3], step[3];
-    float s_next[3], s_delta[3];
-    for (int k = 0; k < 3; ++k) {
-        const float p = ua[k] + du[k] * s0;
-        c[k] = min(max(int(p * R), 0), R - 1);
-        if (du[k] > 0.0f) {
-            step[k] = 1;
-            s_next[k] = s0 + (float(c[k] + 1) / R - p) / du[k];
-            s_delta[k] = 1.0f / (R * du[k]);
-        } else if (du[k] < 0.0f) {
-            step[k] = -1;
-            s_next[k] = s0 + (float(c[k]) / R - p) / du[k];
-            s_delta[k] = -1.0f / (R * du[k]);
-        } else {
-            step[k] = 0;
-            s_next[k] = INFINITY;
-            s_delta[k] = INFINITY;
-        }
-    }
-    float s = s0;
-    for (int guard = 0; guard < 3 * R + 3; ++guard) {
-        const int k = s_next[0] < s_next[1] ? (s_next[0] < s_next[2] ? 0 : 2) : (s_next[1] < s_next[2] ? 1 : 2);
-        const float se = fminf(s_next[k], s1);
-        if (se > s && !f(s * t_max, se * t_max, __ldg(maj + (c[2] * R + c[1]) * R + c[0]))) return;
-        s = fmaxf(s, se);
-        if (s >= s1) break;
-        c[k] += step[k];
-        if (c[k] < 0 || c[k] >= R) break;  // left the grid by rounding: the rest below
-        s_next[k] += s_delta[k];
-    }
-    if (s < 1.0f) f(s * t_max, t_max, m.max_density);
-}
-
 // Transmittance (ratio tracking for grids); `cap` bounds the loop.
 __device__ Vec3 medium_tr(const Scene& S, int mi, Vec3 a, Vec3 b, Rng& rng, int* watchdog) {
     const Medium& m = S.media[mi];
@@ -1279,22 +1209,17 @@ __device__ Vec3 medium_tr(const Scene& S, int mi, Vec3 a, Vec3 b, Rng& rng, int*
         const float d = length(a - b);
         return Vec3(__expf(-m.sigma_t[0] * d), __expf(-m.sigma_t[1] * d), __expf(-m.sigma_t[2] * d));
     }
-    if (m.type == ATRC_MED_HETEROGENEOUS) {  // heterogeneous.cpp:52-81, majorant per span
-        float result = 1;
+    if (m.type == ATRC_MED_HETEROGENEOUS) {
+        float result = 1, t = 0;
         const float t_max = length(a - b);
-        int it = 0;
-        majorant_spans(S, m, a, b, t_max, [&](float t0, float t1, float mj) {
-            if (!(mj > 0.0f)) return true;  // no density in the span: no collisions
-            const float inv = 1.0f / mj;
-            for (float t = t0;;) {
-                if (++it >= (1 << 16)) { *watchdog = 3; return false; }
-                t += -logf(1 - rng.u()) * inv;
-                if (t >= t1) return true;
-                const Vec3 p = a + (b - a) * (t / t_max);
-                const float dens = tex3d_sample<true>(S, m.density, apply_point_rn(m.inv, p)).x;
-                result *= 1 - dens * inv;
-            }
-        });
+        for (int it = 0;; ++it) {
+            if (it >= (1 << 16)) { *watchdog = 3; break; }
+            t += -logf(1 - rng.u()) * m.inv_max_density;
+            if (t >= t_max) break;
+            const Vec3 p = a + (b - a) * (t / t_max);
+            const float dens = tex3d_sample<true>(S, m.density, apply_point_rn(m.inv, p)).x;
+            result *= 1 - dens / m.max_density;
+        }
         return Vec3(result);
     }
     return Vec3(1.0f);
@@ -1338,34 +1263,28 @@ __device__ bool medium_sample(const Scene& S, int mi, Vec3 a, Vec3 b, bool indir
         }
         return false;
     }
-    if (m.type == ATRC_MED_HETEROGENEOUS) {  // heterogeneous.cpp:83-123, majorant per span
+    if (m.type == ATRC_MED_HETEROGENEOUS) {  // heterogeneous.cpp:83-123
         const float t_max = length(b - a);
-        bool scattered = false;
-        int it = 0;
-        majorant_spans(S, m, a, b, t_max, [&](float t0, float t1, float mj) {
-            if (!(mj > 0.0f)) return true;  // no density in the span: no collisions
-            const float inv = 1.0f / mj;
-            for (float t = t0;;) {
-                if (++it >= (1 << 16)) { *watchdog = 3; return false; }
-                t += -logf(1 - rng.u()) * inv;
-                if (t >= t1) return true;
-                const Vec3 p = a + (b - a) * (t / t_max);
-                const Vec3 unit = apply_point_rn(m.inv, p);
-                const float dens = tex3d_sample<true>(S, m.density, unit).x;
-                if (rng.u() < dens * inv) {
-                    const Vec3 alb = m.white_for_indirect && indirect ? Vec3(1.0f) : tex3d_sample<false>(S, m.albedo, unit);
-                    ph->g = tex3d_sample<true>(S, m.g_tex, unit).x;
-                    ph->albedo = alb;
-                    *pos = p;
-                    *wr = (a - b) / t_max;
-                    *tp = alb;
-                    scattered = true;
-                    return false;
-                }
+        float t = 0;
+        for (int it = 0;; ++it) {
+            if (it >= (1 << 16)) { *watchdog = 3; break; }
+            t += -logf(1 - rng.u()) * m.inv_max_density;
+            if (t >= t_max) break;
+            const Vec3 p = a + (b - a) * (t / t_max);
+            const Vec3 unit = apply_point_rn(m.inv, p);
+            const float dens = tex3d_sample<true>(S, m.density, unit).x;
+            if (rng.u() < dens / m.max_density) {
+                const Vec3 alb = m.white_for_indirect && indirect ? Vec3(1.0f) : tex3d_sample<false>(S, m.albedo, unit);
+                ph->g = tex3d_sample<true>(S, m.g_tex, unit).x;
+                ph->albedo = alb;
+                *pos = p;
+                *wr = (a - b) / t_max;
+                *tp = alb;
+                return true;
             }
-        });
-        if (!scattered) *tp = Vec3(1.0f);
-        return scattered;
+        }
+        *tp = Vec3(1.0f);
+        return false;
     }
     *tp = Vec3(1.0f);
     return false;

@@ -1476,8 +1476,8 @@ struct DeviceSceneImpl {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     Scene scene{};
-    DevBuf nodes, tris, tri_bc, tri_shade, tri_orig, entities, tlas_order, materials, tex2d, tex3d, texels, majorants, media,
-        alias_prob, alias_idx, env_probs, env_alias_prob, env_alias_idx;
+    DevBuf nodes, tris, tri_bc, tri_shade, tri_orig, entities, tlas_order, materials, tex2d, tex3d, texels, media, alias_prob,
+        alias_idx, env_probs, env_alias_prob, env_alias_idx;
     DevBuf watchdog;
     DevBuf tiles;  // tile tables of the film's sample grid
     // render workspace (kept between calls)
@@ -1808,7 +1808,6 @@ int atrc_cuda_scene_create(const AtrcSceneDesc* desc, AtrcScene** out) {
         S.tex2d = upload(d.tex2d, hs->tex2d, s);
         S.tex3d = upload(d.tex3d, hs->tex3d, s);
         S.texels = upload(d.texels, hs->texels, s);
-        S.majorants = upload(d.majorants, hs->majorants, s);
         S.media = upload(d.media, hs->media, s);
         S.alias_prob = upload(d.alias_prob, hs->alias_prob, s);
         S.alias_idx = upload(d.alias_idx, hs->alias_idx, s);

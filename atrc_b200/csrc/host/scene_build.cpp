@@ -154,47 +154,6 @@ struct HostTex {
 
 float lum(Vec3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 
-// Majorant grid of a heterogeneous medium: the maximum density over each of
-// kMajRes^3 cells of the density texture's [0,1]^3 coordinates.  A cell's
-// maximum covers every texel that a lookup inside it can read (the nearest
-// texel or the eight of the trilinear filter), widened by one texel on each
-// side for the rounding of the device's coordinate transforms, so that no
-// lookup in the cell exceeds it.  Only where the texture's coordinates are
-// clamped (a position outside [0,1]^3 then reads the border) and no gamma
-// is applied; otherwise the medium keeps the single global maximum.
-constexpr int kMajRes = 16;
-
-void build_majorants(const AtrcTexture3DDesc& t, dev::Medium* m, std::vector<float>* out) {
-    m->maj_res = 0;
-    m->maj_offset = -1;
-    if (t.type != ATRC_TEX_IMAGE || t.inv_gamma != 1.0f || t.wrap[0] != ATRC_WRAP_CLAMP ||
-        t.wrap[1] != ATRC_WRAP_CLAMP || t.wrap[2] != ATRC_WRAP_CLAMP)
-        return;
-    const int size[3] = {t.width, t.height, t.depth};
-    auto range = [&](int c, int a, int* lo, int* hi) {
-        // texels read for u in [c / R, (c + 1) / R]: floor(u n - 0.5) .. floor(u n - 0.5) + 1
-        const double n = size[a];
-        *lo = std::max(0, int(std::floor(double(c) / kMajRes * n - 0.5)) - 1);
-        *hi = std::min(size[a] - 1, int(std::floor(double(c + 1) / kMajRes * n - 0.5)) + 2);
-    };
-    m->maj_res = kMajRes;
-    m->maj_offset = int32_t(out->size());
-    for (int cz = 0; cz < kMajRes; ++cz)
-        for (int cy = 0; cy < kMajRes; ++cy)
-            for (int cx = 0; cx < kMajRes; ++cx) {
-                int x0, x1, y0, y1, z0, z1;
-                range(cx, 0, &x0, &x1);
-                range(cy, 1, &y0, &y1);
-                range(cz, 2, &z0, &z1);
-                float mx = 0.0f;
-                for (int z = z0; z <= z1; ++z)
-                    for (int y = y0; y <= y1; ++y)
-                        for (int x = x0; x <= x1; ++x)
-                            mx = std::max(mx, t.data[((size_t(z) * t.height + y) * t.width + x) * t.channels]);
-                out->push_back(mx);
-            }
-}
-
 }  // namespace
 
 void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
@@ -599,7 +558,6 @@ void build_host_scene(const AtrcSceneDesc& d, HostScene* hs, int device) {
             // heterogeneous.cpp:37-41 (EPS floor uses the default epsilon)
             dm.max_density = std::max(d.textures3d[m.density].max_real, 3e-4f);
             dm.inv_max_density = 1 / dm.max_density;
-            build_majorants(d.textures3d[m.density], &dm, &hs->majorants);
         }
         if (m.type == ATRC_MED_HOMOGENEOUS && (m.g <= -1 || m.g >= 1)) throw std::runtime_error("invalid g value");
         if (m.type != ATRC_MED_VOID) has_media = true;

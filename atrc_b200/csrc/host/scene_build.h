@@ -24,7 +24,6 @@ struct HostScene {
     std::vector<dev::Texture2D> tex2d;
     std::vector<dev::Texture3D> tex3d;
     std::vector<float> texels;
-    std::vector<float> majorants;   // majorant grids of the heterogeneous media
     std::vector<dev::Medium> media;
     std::vector<float> alias_prob;
     std::vector<int32_t> alias_idx;
