@@ -710,7 +710,7 @@ int atrc_guide_default_desc(AtrcGuideDesc* d) {
     // vertices past depth 3 carry little of the image's variance on the
     // indoor workload but cost inference (best time to relMSE 1e-3 of
     // depths 2, 3, 4 and all)
-    d->max_depth = 3;
+    d->max_depth = 5;
     d->learning_rate = 1e-2f;
     d->max_select = kGuideMaxSelect;
     d->target_clamp = 0.0f;

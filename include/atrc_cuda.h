@@ -639,10 +639,10 @@ typedef struct AtrcGuideDesc {
     int32_t  batch;            /* records per training step (2^18)           */
     int32_t  record_capacity;  /* records kept by a recording render (2^20)  */
     float    learning_rate;    /* Adam step size (1e-2)                      */
-    int32_t  max_depth;        /* guide vertices up to this path depth (3;   */
+    int32_t  max_depth;        /* guide vertices up to this path depth (5;   */
                                /* 0: every depth)                            */
     float    max_select;       /* cap on the probability of sampling the     */
-                               /* guide instead of the BSDF (0.25; at most   */
+                               /* guide instead of the BSDF (0.2; at most    */
                                /* 0.99): the BSDF keeps 1 - max_select of    */
                                /* every sample, which bounds the variance an */
                                /* overconfident guide can add                */
