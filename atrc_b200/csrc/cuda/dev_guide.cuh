@@ -41,8 +41,10 @@ constexpr int kHashFeatures = 2;
 // bounds the variance a guide that is still learning can add: on the indoor
 // room's equal-time protocol (5 seeds) caps of 0.9 / 0.5 / 0.3 / 0.25 / 0.15
 // gave time ratios of 1.13 / 0.74 / 0.63-0.73 / 0.56 / 0.61 with guided
-// depth 3, and a cap of 0.2 with depth 5 gave 0.49 and 0.45 on two seed sets.
-constexpr float kGuideMaxSelect = 0.2f;
+// depth 3; with depth 5, caps of 0.2 / 0.15 / 0.125 / 0.1 averaged 0.50 /
+// 0.48 / 0.47 / 0.49 over runs on two seed sets (run-to-run spread about
+// +-0.05).
+constexpr float kGuideMaxSelect = 0.15f;
 constexpr float kSelectOffset = -2.0f;    // an untrained guide (o ~ 0) is picked with c ~ 0.12 max_select
 constexpr float kLogKappaMin = -6.9f;     // kappa in [1e-3, 1e4]
 constexpr float kLogKappaMax = 9.2f;

@@ -642,7 +642,7 @@ typedef struct AtrcGuideDesc {
     int32_t  max_depth;        /* guide vertices up to this path depth (5;   */
                                /* 0: every depth)                            */
     float    max_select;       /* cap on the probability of sampling the     */
-                               /* guide instead of the BSDF (0.2; at most    */
+                               /* guide instead of the BSDF (0.15; at most   */
                                /* 0.99): the BSDF keeps 1 - max_select of    */
                                /* every sample, which bounds the variance an */
                                /* overconfident guide can add                */
