@@ -20,8 +20,23 @@ def first_spp(step: int, rank: int, world: int, spp_per_rank: int) -> int:
 
 
 def reduce_film(film, dist, dst: int = 0) -> None:
-    """Sum every accumulator of `film` (torch tensors) onto rank `dst`."""
+    """Sum every accumulator of `film` (torch tensors) onto rank `dst`.
+
+    The other ranks' accumulators restart from zero afterwards (a reduce
+    leaves a non-root buffer unspecified), so a reduce after every step adds
+    each rank's new samples to `dst` once: `dst` then holds every sample
+    rendered so far and the others only what they rendered since."""
+    rank = dist.get_rank()
+    on_device = False
     for name in FILM_FIELDS:
         t = getattr(film, name, None)
         if t is not None:
             dist.reduce(t, dst)
+            if rank != dst:
+                t.zero_()
+            on_device = on_device or t.is_cuda
+    if on_device:
+        # the library renders on its own stream, which does not wait for
+        # torch's: the reduce and the zero fill end before the next render
+        import torch
+        torch.cuda.current_stream().synchronize()

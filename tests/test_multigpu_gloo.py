@@ -1,6 +1,8 @@
 """The sample-split multi-GPU path on CPU: two gloo ranks render disjoint
 sample ranges (with the oracle standing in for the GPU kernels) and reduce
-their films to rank 0; the result equals rendering both ranges in one process."""
+their films to rank 0 after every step, as the benchmark's timed loop does;
+the result equals rendering every range in one process, each sample counted
+once."""
 import os
 import socket
 
@@ -9,6 +11,8 @@ import pytest
 import torch.multiprocessing as mp
 
 from atrc_b200.multigpu import first_spp
+
+STEPS = 2
 
 
 def test_sample_ranges_are_disjoint():
@@ -45,14 +49,21 @@ def _worker(rank, world, port, scene_path, out_dir):
     cfg = Config.from_file(scene_path)
     desc, _ = cfg.rendering(0)
     ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
-    film = Film(desc.width, desc.height)
-    desc.spp_count = 2
-    desc.first_spp = first_spp(0, rank, world, 2)
-    ora.render(desc, film, threads=1)
     tf = type("F", (), {})()
-    tf.value = torch.from_numpy(film.value.copy())
-    tf.weight = torch.from_numpy(film.weight.copy())
-    reduce_film(tf, dist, 0)
+    tf.value = torch.zeros(desc.width * desc.height * 3, dtype=torch.float64)
+    tf.weight = torch.zeros(desc.width * desc.height, dtype=torch.float64)
+    desc.spp_count = 2
+    for step in range(STEPS):
+        film = Film(desc.width, desc.height)
+        film.value[:] = tf.value.numpy().reshape(film.value.shape)
+        film.weight[:] = tf.weight.numpy().reshape(film.weight.shape)
+        desc.first_spp = first_spp(step, rank, world, 2)
+        ora.render(desc, film, threads=1)
+        tf.value.copy_(torch.from_numpy(film.value.reshape(-1)))
+        tf.weight.copy_(torch.from_numpy(film.weight.reshape(-1)))
+        reduce_film(tf, dist, 0)
+        if rank != 0:
+            assert not tf.value.any() and not tf.weight.any()
     if rank == 0:
         np.save(os.path.join(out_dir, "value.npy"), tf.value.numpy())
         np.save(os.path.join(out_dir, "weight.npy"), tf.weight.numpy())
@@ -73,9 +84,10 @@ def test_two_rank_gloo_film_reduce(tmp_path):
     ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
     ref = Film(desc.width, desc.height)
     desc.spp_count = 2
-    for rank in range(2):
-        desc.first_spp = first_spp(0, rank, 2, 2)
-        ora.render(desc, ref, threads=1)
-    np.testing.assert_allclose(value, ref.value, rtol=1e-12, atol=1e-12)
-    np.testing.assert_allclose(weight, ref.weight, rtol=1e-12)
+    for step in range(STEPS):
+        for rank in range(2):
+            desc.first_spp = first_spp(step, rank, 2, 2)
+            ora.render(desc, ref, threads=1)
+    np.testing.assert_allclose(value.reshape(ref.value.shape), ref.value, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(weight.reshape(ref.weight.shape), ref.weight, rtol=1e-12)
     assert weight.sum() > 0
