@@ -23,6 +23,8 @@
 #include <agz/tracer/core/scene.h>
 #include <agz/tracer/render/path_tracing.h>
 #include <agz/tracer/utility/parallel_grid.h>
+#include <spdlog/spdlog.h>
+#include <spdlog/sinks/stdout_color_sinks.h>
 
 #include <filesystem>
 #include <fstream>
@@ -107,6 +109,11 @@ int ref_scene_create(const char* json, const char* scene_dir, RefScene** out) {
     if (!json || !scene_dir || !out) return fail("null argument");
     *out = nullptr;
     try {
+        // the reference logs through spdlog's default logger (AGZ_INFO,
+        // logger.h:14), which writes to stdout: send it to stderr, so that a
+        // caller's stdout holds only what the caller prints
+        static std::once_flag log_once;
+        std::call_once(log_once, [] { spdlog::set_default_logger(spdlog::stderr_color_mt("atrc_ref")); });
         auto rs = std::make_unique<RefScene>();
         rs->mapper.add_replacer(AGZ_FACTORY_SCENE_DESC_PATH_NAME, scene_dir);
         rs->mapper.add_replacer(AGZ_FACTORY_WORKING_DIR_PATH_NAME, std::filesystem::current_path().string());
