@@ -1,14 +1,14 @@
 """GPU parity against the CPU oracle on the benchmark scenes at their stated
 settings, through the C ABI.
 
-* configs[0]: the seeded Cornell box at its full size (256 x 256, 64 spp,
+* the seeded Cornell box at its full size (256 x 256, 64 spp,
   max depth 8, Russian roulette from depth 3, box filter), every pixel in the
   3-sigma band.
-* configs[2]: the media scene with its 128^3 fBm density grid (delta and
+* the media scene with its 128^3 fBm density grid (delta and
   ratio tracking) around the 200,000-triangle displaced sphere, two area
   lights and the sky, at its full 512 spp and max depth 32 on a 48 x 48
   film; plus closest hits against the oracle's BVH on that scene.
-* configs[3]: the indoor room (403,000 triangles, Disney, lit only through
+* the indoor room (403,000 triangles, Disney, lit only through
   the window), plain pt_cuda at 64 x 36 against the oracle.
 * Guided rendering with the fixed Disney sampler (the mode the guided
   benchmark uses) against plain rendering, on the room and on the instanced
@@ -45,9 +45,9 @@ def _render_pair(path, **overrides):
     return cfg, desc, dev, ora, fg, fc, st
 
 
-def test_cornell_config0_full_size_within_3_sigma(scene_dir):
+def test_cornell_full_size_within_3_sigma(scene_dir):
     from atrc_b200.scenes import cornell_box
-    cfg, desc, dev, ora, fg, fc, st = _render_pair(cornell_box(scene_dir / "cornell_cfg0"))
+    cfg, desc, dev, ora, fg, fc, st = _render_pair(cornell_box(scene_dir / "cornell_256"))
     assert (desc.width, desc.height, desc.spp, desc.max_depth, desc.min_depth) == (256, 256, 64, 8, 2)
     assert st["samples"] == 256 * 256 * 64 and st["watchdog_flags"] == 0
     frac, allowed, info = band_test(fg, fc, BOX)
@@ -59,13 +59,13 @@ def test_cornell_config0_full_size_within_3_sigma(scene_dir):
 
 
 @pytest.fixture(scope="module")
-def media_cfg2(scene_dir):
+def media_128(scene_dir):
     from atrc_b200.scenes import media_scene
-    return media_scene(scene_dir / "media_cfg2", width=48, height=48, spp=512)
+    return media_scene(scene_dir / "media_128", width=48, height=48, spp=512)
 
 
-def test_media_config2_grid_and_sphere_within_3_sigma(media_cfg2):
-    cfg, desc, dev, ora, fg, fc, st = _render_pair(media_cfg2)
+def test_media_grid_and_sphere_within_3_sigma(media_128):
+    cfg, desc, dev, ora, fg, fc, st = _render_pair(media_128)
     assert (desc.spp, desc.max_depth) == (512, 32)
     sd = cfg.scene_desc().contents
     tex3 = [sd.textures3d[i] for i in range(sd.texture3d_count)]
@@ -77,8 +77,8 @@ def test_media_config2_grid_and_sphere_within_3_sigma(media_cfg2):
     assert global_mean_z(fg, fc) < 4.0
 
 
-def test_media_config2_closest_hits_bit_exact(media_cfg2):
-    cfg = Config.from_file(media_cfg2)
+def test_media_closest_hits_bit_exact(media_128):
+    cfg = Config.from_file(media_128)
     desc, _ = cfg.rendering(0)
     dev = DeviceScene(cfg)
     ora = oracle.OracleScene(cfg.scene_desc(), desc.eps)
@@ -95,10 +95,10 @@ def test_media_config2_closest_hits_bit_exact(media_cfg2):
 @pytest.fixture(scope="module")
 def room(scene_dir):
     from atrc_b200.scenes import indoor_room
-    return indoor_room(scene_dir / "room_cfg3", width=64, height=36, spp=256)
+    return indoor_room(scene_dir / "room_64x36", width=64, height=36, spp=256)
 
 
-def test_room_config3_plain_within_3_sigma(room):
+def test_room_plain_within_3_sigma(room):
     cfg, desc, dev, ora, fg, fc, st = _render_pair(room)
     assert desc.max_depth == 16 and st["watchdog_flags"] == 0
     frac, allowed, info = band_test(fg, fc, BOX)

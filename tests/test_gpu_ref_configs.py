@@ -1,15 +1,15 @@
 """The device path against the reference's own renderer (oracle/_ref) on the
 benchmark scenes at their stated geometry and settings, through the C ABI.
 
-* configs[0]: the seeded Cornell box at its full size (256 x 256, 64 spp,
+* the seeded Cornell box at its full size (256 x 256, 64 spp,
   max depth 8), every pixel in the 3-sigma band.
-* configs[1]: the instanced Disney + IBL scene, 3.08M unique triangles in 64
+* the instanced Disney + IBL scene, 3.08M unique triangles in 64
   instances, at its full 1920 x 1080 film and depth 16 with 16 spp (the
   reference's CPU time at 256 spp would be minutes), the band over 8 x 8
   pixel blocks; closest hits of 10^6 seeded rays.
-* configs[2]: the media scene (128^3 fBm grid, 200,000-triangle sphere, two
+* the media scene (128^3 fBm grid, 200,000-triangle sphere, two
   area lights and the sky) at its 512 spp and depth 32 on a 48 x 48 film.
-* configs[3]: the indoor room at its full 1280 x 720 film with 16 spp, the
+* the indoor room at its full 1280 x 720 film with 16 spp, the
   band over 8 x 8 pixel blocks.
 
 The reference renders through its own factory, BVHs, materials, lights,
@@ -67,31 +67,31 @@ def _assert_band(fg, fr, desc=None, block=1):
     assert global_mean_z(fg, fr) < 4.0
 
 
-def test_cornell_config0_full_size_matches_reference(scene_dir):
-    desc, fg, fr = _device_and_reference(scenes.cornell_box(scene_dir / "ref_cornell_cfg0"))
+def test_cornell_full_size_matches_reference(scene_dir):
+    desc, fg, fr = _device_and_reference(scenes.cornell_box(scene_dir / "ref_cornell_256"))
     assert (desc.width, desc.height, desc.spp, desc.max_depth) == (256, 256, 64, 8)
     _assert_band(fg, fr)
 
 
 @pytest.fixture(scope="module")
-def instanced_cfg1(scene_dir):
-    return scenes.instanced_disney(scene_dir / "ref_inst_cfg1")
+def instanced_full(scene_dir):
+    return scenes.instanced_disney(scene_dir / "ref_inst_full")
 
 
-def test_instanced_config1_full_film_matches_reference(instanced_cfg1):
-    desc, fg, fr = _device_and_reference(instanced_cfg1, spp=16)
+def test_instanced_full_film_matches_reference(instanced_full):
+    desc, fg, fr = _device_and_reference(instanced_full, spp=16)
     assert (desc.width, desc.height, desc.max_depth) == (1920, 1080, 16)
     _assert_band(fg, fr, desc, block=8)
 
 
-def test_instanced_config1_closest_hits_match_reference(instanced_cfg1):
-    cfg = Config.from_file(instanced_cfg1)
+def test_instanced_closest_hits_match_reference(instanced_full):
+    cfg = Config.from_file(instanced_full)
     desc, _ = cfg.rendering(0)
     sd = cfg.scene_desc().contents
     assert sum(int(sd.meshes[i].triangle_count) for i in range(sd.mesh_count)) == 3_076_098
     rays = seeded_rays(1_000_000, [-22.0] * 3, [22.0] * 3, list(desc.camera.pos), seed=23)
     g = DeviceScene(cfg).trace_rays(rays, "closest", exact=True)
-    r = oracle.RefScene(instanced_cfg1).trace_rays(rays, "closest")
+    r = oracle.RefScene(instanced_full).trace_rays(rays, "closest")
     assert (g["entity"] == r["entity"]).mean() >= 0.9999
     hit = (g["entity"] == r["entity"]) & (g["entity"] >= 0)
     assert hit.sum() > 100_000
@@ -101,14 +101,14 @@ def test_instanced_config1_closest_hits_match_reference(instanced_cfg1):
     assert np.median(u) <= 1 and np.quantile(u, 0.99) <= 128, np.quantile(u, [0.5, 0.99])
 
 
-def test_media_config2_matches_reference(scene_dir):
-    path = scenes.media_scene(scene_dir / "ref_media_cfg2", width=48, height=48, spp=512)
+def test_media_matches_reference(scene_dir):
+    path = scenes.media_scene(scene_dir / "ref_media_128", width=48, height=48, spp=512)
     desc, fg, fr = _device_and_reference(path)
     assert (desc.spp, desc.max_depth) == (512, 32)
     _assert_band(fg, fr)
 
 
-def test_room_config3_full_film_matches_reference(scene_dir):
-    desc, fg, fr = _device_and_reference(scenes.indoor_room(scene_dir / "ref_room_cfg3"), spp=16)
+def test_room_full_film_matches_reference(scene_dir):
+    desc, fg, fr = _device_and_reference(scenes.indoor_room(scene_dir / "ref_room_720p"), spp=16)
     assert (desc.width, desc.height, desc.max_depth) == (1280, 720, 16)
     _assert_band(fg, fr, desc, block=8)
