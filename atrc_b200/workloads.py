@@ -98,6 +98,8 @@ def rays(count: int) -> None:
 
 
 def guided_room(train_passes: int, passes: int) -> None:
+    import torch
+
     from . import Config, DeviceScene, Film, scenes
     from .guide import Guide
     cfg = Config.from_file(scenes.indoor_room())
@@ -110,13 +112,27 @@ def guided_room(train_passes: int, passes: int) -> None:
         desc.first_spp = k
         scene.render(desc, film)
     guide = Guide.for_scene(scene)
+    # the last recording pass (with its Adam steps) and the last guided pass
+    # run inside NVTX ranges "train_pass" and "guided_pass" for profilers
     for k in range(train_passes):
         desc.first_spp = 3 + k
+        last = k == train_passes - 1
+        if last:
+            torch.cuda.nvtx.range_push("train_pass")
         scene.render_guided(guide, desc, film, record=True)
         guide.train(steps=4)
+        if last:
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
     for k in range(passes):
         desc.first_spp = 3 + train_passes + k
+        last = k == passes - 1
+        if last:
+            torch.cuda.nvtx.range_push("guided_pass")
         scene.render_guided(guide, desc, film, record=False)
+        if last:
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
     guide.close()
 
 
