@@ -1594,6 +1594,20 @@ struct PoolLayout {
     size_t total;
 };
 
+// k_shadow's grid.  The queue's length is known only on the device, so the
+// grid is fixed when the window is captured; k_shadow strides over the queue
+// and a thread traces one ray as long as the queue holds at most
+// kShadowGridWaves resident waves (148 SMs x 10 blocks x 128 threads each).
+// A grid covering the whole capacity (the pool times the rays one path can
+// emit) would launch tens of thousands of blocks that find no ray: an
+// iteration of the instanced workload queues about 260,000 occlusion rays
+// against a capacity of 4M.
+constexpr int kShadowGridWaves = 8;
+int shadow_grid(size_t shadow_cap, int sm_count) {
+    const size_t full = (shadow_cap + 127) / 128;
+    return int(std::min<size_t>(full, size_t(sm_count) * ATRC_SHADOW_MIN_BLOCKS * kShadowGridWaves));
+}
+
 PoolLayout pool_layout(size_t cap, size_t shadow_cap, int nkeys) {
     PoolLayout L{};
     size_t o = 0;
@@ -2081,7 +2095,7 @@ static int render_impl(AtrcScene* scene, const AtrcRenderDesc* descs, const Atrc
     const int gsm = grid_for(d.sm_count, d.tuned_gen_blocks);
     // one path / ray per thread for the heavy kernels (grids cover the
     // pool; threads past the device-side count return at once)
-    const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
+    const int g_path = int((cap + 127) / 128), g_shadow = shadow_grid(shadow_cap, d.sm_count);
     k_init<<<int((std::max<size_t>({cap, size_t(p.nkeys), size_t(kShadowKeys)}) + 255) / 256), 256, 0, s>>>(
         P, int(cap), p.nkeys, c, total);
     CK(cudaGetLastError());
@@ -2648,7 +2662,7 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         Pool P = pool_from(base + counters_bytes + tiles_bytes, L, cap, shadow_cap);
         set_shadow_sort(&P, d.scene, d.tuned_shadow_sort);
         const int gsm = grid_for(d.sm_count, d.tuned_gen_blocks);
-        const int g_path = int((cap + 127) / 128), g_shadow = int((shadow_cap + 127) / 128);
+        const int g_path = int((cap + 127) / 128), g_shadow = shadow_grid(shadow_cap, d.sm_count);
         // k_init rewrites the counters and the slot states (all state that must
         // start from a known value)
         k_init<<<int((std::max<size_t>({cap, size_t(p.nkeys), size_t(kShadowKeys)}) + 255) / 256), 256, 0, s>>>(
