@@ -1,8 +1,12 @@
 """The C-ABI library loads, exports every declared entry point and agrees
-with its bindings on struct layouts (no GPU calls)."""
+with its bindings on struct layouts (no GPU calls), and on a machine without
+a GPU its device path fails with an error instead of falling back."""
 import ctypes as C
 import re
 from pathlib import Path
+
+import pytest
+import torch
 
 import atrc_b200
 from atrc_b200 import _abi as abi
@@ -56,3 +60,12 @@ def test_errors_are_reported_without_a_gpu():
     rc = lib.atrc_cuda_scene_create(None, C.byref(h))
     assert rc == -1
     assert b"null" in lib.atrc_last_error()
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the behaviour on a machine without a GPU")
+def test_device_path_fails_loudly_without_a_gpu(tmp_path):
+    """No CPU fallback: creating a device scene without a GPU is an error."""
+    from atrc_b200 import Config, DeviceScene, scenes
+    cfg = Config.from_file(scenes.cornell_box(tmp_path / "c", width=16, height=16, spp=1))
+    with pytest.raises(atrc_b200.AtrcError, match="ATRC_ERR_CUDA"):
+        DeviceScene(cfg)
