@@ -83,6 +83,7 @@ std::vector<float> load_rgbe(const std::string& fn, int* w, int* h) {
     char ya[4], xa[4];
     if (std::sscanf(line.c_str(), "%3s %d %3s %d", ya, h, xa, w) != 4 || std::string(ya) != "-Y" || std::string(xa) != "+X")
         throw ConfigError("unsupported HDR orientation: " + line);
+    if (*w <= 0 || *h <= 0 || *w > 65536 || *h > 65536) throw ConfigError("bad HDR size: " + line);
     std::vector<float> out(size_t(*w) * *h * 3);
     std::vector<uint8_t> scan(size_t(*w) * 4);
     for (int y = 0; y < *h; ++y) {
@@ -95,18 +96,26 @@ std::vector<float> load_rgbe(const std::string& fn, int* w, int* h) {
                 while (x < *w) {
                     int cnt = f.get();
                     if (cnt == EOF) throw ConfigError("truncated HDR: " + fn);
+                    if (cnt == 0 || x + (cnt > 128 ? cnt - 128 : cnt) > *w)
+                        throw ConfigError("bad HDR run length: " + fn);
                     if (cnt > 128) {
                         cnt -= 128;
-                        int v = f.get();
-                        for (int k = 0; k < cnt && x < *w; ++k) scan[size_t(x++) * 4 + c] = uint8_t(v);
+                        const int v = f.get();
+                        if (v == EOF) throw ConfigError("truncated HDR: " + fn);
+                        for (int k = 0; k < cnt; ++k) scan[size_t(x++) * 4 + c] = uint8_t(v);
                     } else {
-                        for (int k = 0; k < cnt && x < *w; ++k) scan[size_t(x++) * 4 + c] = uint8_t(f.get());
+                        for (int k = 0; k < cnt; ++k) {
+                            const int v = f.get();
+                            if (v == EOF) throw ConfigError("truncated HDR: " + fn);
+                            scan[size_t(x++) * 4 + c] = uint8_t(v);
+                        }
                     }
                 }
             }
         } else {
             std::memcpy(scan.data(), hdr, 4);
             f.read(reinterpret_cast<char*>(scan.data() + 4), (size_t(*w) - 1) * 4);
+            if (!f) throw ConfigError("truncated HDR: " + fn);
         }
         for (int x = 0; x < *w; ++x) {
             const uint8_t* p = &scan[size_t(x) * 4];

@@ -343,3 +343,51 @@ def test_solid_image_texture():
     assert len(t) == 1 and 0 <= t[0].tex3d < s.texture3d_count
     assert list(t[0].uv_transform) == [1, 0, 0, 0, 1, 0] and t[0].wrap_u == 0 and t[0].inv_gamma == 1
     assert list(s.textures3d[t[0].tex3d].texel) == pytest.approx([0.2, 0.4, 0.6])
+
+
+def _rgbe_decode(px):
+    m, e = px[..., :3].astype(np.float64), px[..., 3].astype(np.int64)
+    return np.where(e[..., None] > 0, m * np.ldexp(1.0, e - 136)[..., None], 0.0).astype(np.float32)
+
+
+def _rgbe_rle_scanline(row):
+    """New-style RLE scanline: per channel a run of the first five values
+    (all equal) then the rest as one literal."""
+    w = len(row)
+    out = bytes([2, 2, w >> 8, w & 255])
+    for c in range(4):
+        ch = row[:, c]
+        out += bytes([128 + 5, ch[0]]) + bytes([w - 5]) + bytes(ch[5:])
+    return out
+
+
+def test_radiance_hdr_flat_and_rle(tmp_path):
+    # .hdr textures: RGBE texels decode to m * 2^(e - 136), e = 0 is black;
+    # "-Y h +X w" puts the first scanline on top
+    rng = np.random.default_rng(11)
+    h, w = 3, 12
+    px = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+    px[:, :5] = px[:, :1]            # the run the encoder below writes
+    px[0, 7, 3] = 0                  # one black texel
+    head = b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y %d +X %d\n"
+    (tmp_path / "rle.hdr").write_bytes(head % (h, w) + b"".join(_rgbe_rle_scanline(px[y]) for y in range(h)))
+    flat = rng.integers(0, 256, (2, 4, 4), dtype=np.uint8)
+    (tmp_path / "flat.hdr").write_bytes(head % (2, 4) + flat.tobytes())
+    for fn, want in (("rle.hdr", _rgbe_decode(px)), ("flat.hdr", _rgbe_decode(flat))):
+        c = base([QUAD], env={"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/" + fn}})
+        cfg = Config.from_string(c, tmp_path)  # owns the texel arrays
+        s = cfg.scene_desc().contents
+        t = s.textures2d[s.env.tex]
+        assert (t.height, t.width) == want.shape[:2]
+        got = np.ctypeslib.as_array(t.data, shape=(want.size,)).reshape(want.shape)
+        np.testing.assert_array_equal(got, want)
+    # malformed files are configuration errors, not garbage texels
+    good = (tmp_path / "rle.hdr").read_bytes()
+    bad = {"trunc.hdr": (good[:-3], "truncated HDR"),
+           "run.hdr": (good.replace(bytes([128 + 5]), bytes([128 + 40]), 1), "bad HDR run length"),
+           "size.hdr": (head % (0, 4), "bad HDR size")}
+    for fn, (data, msg) in bad.items():
+        (tmp_path / fn).write_bytes(data)
+        c = base([QUAD], env={"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/" + fn}})
+        with pytest.raises(AtrcError, match=msg):
+            Config.from_string(c, tmp_path).scene_desc()
