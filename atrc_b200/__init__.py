@@ -116,6 +116,7 @@ class Config:
     def scene_desc(self) -> C.POINTER(abi.AtrcSceneDesc):
         p = C.POINTER(abi.AtrcSceneDesc)()
         _check(load_library().atrc_config_scene(self._h, C.byref(p)))
+        p._owner = self  # the description lives in this config's memory
         return p
 
     def rendering_count(self) -> int:

@@ -391,3 +391,18 @@ def test_radiance_hdr_flat_and_rle(tmp_path):
         c = base([QUAD], env={"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/" + fn}})
         with pytest.raises(AtrcError, match=msg):
             Config.from_string(c, tmp_path).scene_desc()
+
+
+def test_scene_description_keeps_its_config_alive(tmp_path):
+    # the description points into the config's memory: holding only the
+    # description (or its contents) must keep the config alive
+    import gc
+    from atrc_b200.scenes import write_pfm
+    img = np.arange(8 * 16 * 3, dtype=np.float32).reshape(8, 16, 3)
+    write_pfm(tmp_path / "e.pfm", img)
+    c = base([QUAD], env={"type": "ibl", "tex": {"type": "hdr", "filename": "${scene-directory}/e.pfm"}})
+    s = Config.from_string(c, tmp_path).scene_desc().contents
+    gc.collect()
+    t = s.textures2d[s.env.tex]
+    got = np.ctypeslib.as_array(t.data, shape=(img.size,)).reshape(img.shape)
+    np.testing.assert_array_equal(got, img)  # row 0 on top, as written
