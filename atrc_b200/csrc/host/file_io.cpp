@@ -432,23 +432,74 @@ void write_png_bytes(const std::string& fn, const uint8_t* rgb8, int w, int h) {
     png_chunk(f, "IEND", {});
 }
 
+// One component of a scanline in the new-style run-length encoding: runs of
+// 4 or more equal bytes as (128 + length, byte), up to 127 long; everything
+// else as literals (length, bytes...), up to 128 long.
+static void rle_component(std::ofstream& f, const uint8_t* v, int n) {
+    int x = 0;
+    while (x < n) {
+        int run = 1;
+        while (x + run < n && run < 127 && v[x + run] == v[x]) ++run;
+        if (run >= 4) {
+            const uint8_t rec[2] = {uint8_t(128 + run), v[x]};
+            f.write(reinterpret_cast<const char*>(rec), 2);
+            x += run;
+            continue;
+        }
+        // literals up to the next run of 4 (or 128 bytes)
+        int lit = 0;
+        while (x + lit < n && lit < 128) {
+            int r = 1;
+            while (x + lit + r < n && r < 4 && v[x + lit + r] == v[x + lit]) ++r;
+            if (r >= 4) break;
+            ++lit;
+        }
+        const uint8_t cnt = uint8_t(lit);
+        f.write(reinterpret_cast<const char*>(&cnt), 1);
+        f.write(reinterpret_cast<const char*>(v + x), lit);
+        x += lit;
+    }
+}
+
 void save_hdr_rgbe(const std::string& fn, const float* rgb, int w, int h) {
     std::ofstream f(fn, std::ios::binary);
     if (!f) throw ConfigError("failed to open output: " + fn);
     f << "#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y " << h << " +X " << w << "\n";
-    for (size_t k = 0; k < size_t(w) * h; ++k) {
-        const size_t i = size_t(h - 1 - k / w) * w + k % w;  // top row first
-        float r = rgb[3 * i], g = rgb[3 * i + 1], b = rgb[3 * i + 2];
-        float m = std::fmax(r, std::fmax(g, b));
-        uint8_t e[4] = {0, 0, 0, 0};
-        if (m > 1e-32f) {
-            int ex;
-            float s = std::frexp(m, &ex) * 256.0f / m;
-            e[0] = uint8_t(std::fmax(r, 0.f) * s); e[1] = uint8_t(std::fmax(g, 0.f) * s);
-            e[2] = uint8_t(std::fmax(b, 0.f) * s); e[3] = uint8_t(ex + 128);
+    // scanlines of 8 to 32767 pixels are run-length encoded, as Radiance
+    // writes them: a flat scanline whose first pixel reads (2, 2, w >> 8,
+    // w & 255) would otherwise be taken for an encoded one
+    const bool rle = w >= 8 && w < 32768;
+    std::vector<uint8_t> line(static_cast<size_t>(w) * 4), comp(static_cast<size_t>(w));
+    for (int y = 0; y < h; ++y) {
+        const size_t row = size_t(h - 1 - y) * w;  // top row first
+        for (int x = 0; x < w; ++x) {
+            const float* c = rgb + 3 * (row + x);
+            const float r = std::fmax(c[0], 0.f), g = std::fmax(c[1], 0.f), b = std::fmax(c[2], 0.f);
+            const float m = std::fmax(r, std::fmax(g, b));
+            uint8_t* e = &line[size_t(x) * 4];
+            e[0] = e[1] = e[2] = e[3] = 0;
+            if (m > 1e-32f) {
+                int ex;
+                const float s = std::frexp(m, &ex) * 256.0f / m;
+                if (ex > 127) {  // beyond RGBE's range: the largest value
+                    e[0] = e[1] = e[2] = e[3] = 255;
+                } else {
+                    e[0] = uint8_t(r * s); e[1] = uint8_t(g * s); e[2] = uint8_t(b * s); e[3] = uint8_t(ex + 128);
+                }
+            }
         }
-        f.write(reinterpret_cast<const char*>(e), 4);
+        if (!rle) {
+            f.write(reinterpret_cast<const char*>(line.data()), std::streamsize(line.size()));
+            continue;
+        }
+        const uint8_t head[4] = {2, 2, uint8_t(w >> 8), uint8_t(w & 255)};
+        f.write(reinterpret_cast<const char*>(head), 4);
+        for (int c = 0; c < 4; ++c) {
+            for (int x = 0; x < w; ++x) comp[size_t(x)] = line[size_t(x) * 4 + c];
+            rle_component(f, comp.data(), w);
+        }
     }
+    if (!f) throw ConfigError("failed to write: " + fn);
 }
 
 }  // namespace atrc
