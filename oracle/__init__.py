@@ -178,6 +178,8 @@ def load_ref() -> C.CDLL:
         dp = C.POINTER(C.c_double)
         lib.ref_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int,
                                    C.c_int, dp, dp, dp, dp, dp, dp]
+        fp = C.POINTER(C.c_float)
+        lib.ref_filter_eval.argtypes = [C.c_void_p, C.c_int, fp, fp, C.c_size_t, fp]
         _ref_lib = lib
     return _ref_lib
 
@@ -211,6 +213,17 @@ class RefScene:
                                              hits.ctypes.data_as(C.POINTER(abi.AtrcHit)),
                                              0 if mode == "closest" else 1, threads))
         return hits
+
+    def filter_eval(self, x, y, index: int = 0) -> np.ndarray:
+        """The reference's film filter of rendering entry `index` at the
+        offsets (x, y) from a pixel centre."""
+        fp = C.POINTER(C.c_float)
+        xa = np.ascontiguousarray(x, np.float32).ravel()
+        ya = np.ascontiguousarray(y, np.float32).ravel()
+        out = np.empty(len(xa), np.float32)
+        _ref_check(load_ref().ref_filter_eval(self._h, index, xa.ctypes.data_as(fp), ya.ctypes.data_as(fp), len(xa),
+                                              out.ctypes.data_as(fp)))
+        return out
 
     def render(self, film, index: int = 0, spp: int = 1, first_spp: int = 0, seed: int = 1, threads: int = 0,
                width: int = 0, height: int = 0, tile_stride: int = 1) -> None:

@@ -309,4 +309,22 @@ int ref_render(RefScene* s, int index, int width, int height, int first_spp, int
     }
 }
 
+// The film filter of rendering entry `index` evaluated at the offsets
+// (x[i], y[i]) from a pixel centre, as the reference splats with it
+// (FilmFilterApplier::FilmGrid::apply, render_target.h:384-395).
+int ref_filter_eval(RefScene* s, int index, const float* x, const float* y, size_t n, float* out) {
+    if (!s || (n && (!x || !y || !out))) return fail("invalid argument");
+    if (index < 0 || size_t(index) >= s->renderings.size()) return fail("rendering index out of range");
+    try {
+        const ConfigGroup& r = *s->renderings[size_t(index)];
+        RC<FilmFilter> film_filter;
+        if (auto group = r.find_child_group("film_filter")) film_filter = s->context.create<FilmFilter>(*group);
+        else film_filter = create_box_filter(real(0.5));
+        for (size_t i = 0; i < n; ++i) out[i] = float(film_filter->eval(real(x[i]), real(y[i])));
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(describe(e));
+    }
+}
+
 }  // extern "C"

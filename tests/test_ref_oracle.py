@@ -203,3 +203,40 @@ def test_gbuffer_matches_reference(tmp_path):
         assert np.all(np.abs(a.mean(0) - b.mean(0)) < 1e-3), (k, a.mean(0), b.mean(0))
         assert np.mean(np.abs(a - b).max(1) < 1e-4) > 0.4     # pixels inside one flat surface agree exactly
     np.testing.assert_array_equal(fr.denoise / fr.weight, fo.denoise / fo.weight)
+
+
+def test_gaussian_filter_matches_reference(tmp_path):
+    # the reference's FilmFilterApplier (render_target.h:80) with the Gaussian
+    # filter.  The reference scales the filter by a Monte Carlo estimate of
+    # 1 / (its integral) (gaussian_filter.cpp:16-38, 64-71); pt_cuda and the oracle
+    # leave it unscaled.  The constant cancels in value / weight, so the
+    # images agree; the reference's weights, divided by it, follow the same
+    # analytic expectation as the oracle's.
+    from math import erf, exp, pi, sqrt
+
+    from tests.parity import filter_weight_z
+    sub = tmp_path / "gauss"
+    sub.mkdir()
+    path = _write(sub, "scene", K.feature_scene(sub, spp=128, gaussian=True))
+    desc, fr, fo = _render_both(path)
+    r, a = desc.filter_radius, desc.filter_alpha
+    assert desc.filter_type != 0
+    g0 = 1 - exp(-a * r * r)
+    norm = float(oracle.RefScene(path).filter_eval([0.0], [0.0])[0]) / (g0 * g0)
+    integral = sqrt(pi / a) * erf(r * sqrt(a)) - 2 * r * exp(-a * r * r)
+    assert abs(norm * integral ** 2 - 1) < 0.01, norm
+    for w in (fr.weight / norm, fo.weight):
+        z = filter_weight_z(w, desc.width, desc.height, desc.spp, r, a)
+        assert np.mean(np.abs(z)) < 0.9 and np.mean(np.abs(z) > 4) < 0.002, (np.mean(np.abs(z)), np.abs(z).max())
+    wmax = g0 * g0
+
+    def st(f, scale):
+        w = f.weight.reshape(-1, 1)
+        mu = f.value.reshape(-1, 3) / w
+        var = np.maximum(f.value_sq.reshape(-1, 3) / w - mu * mu, 0)
+        return mu, var, w / (scale * wmax)
+    mr, vr, nr = st(fr, norm)
+    mo, vo, no = st(fo, 1.0)
+    z = np.abs(mr - mo) / np.sqrt(vr / nr + vo / no + 1e-12)
+    assert np.mean(z > 4) < 0.01, np.mean(z > 4)
+    assert global_mean_z(fr, fo) < 4.0
