@@ -1952,6 +1952,10 @@ static int check_render_args(AtrcScene* scene, const AtrcRenderDesc* desc, const
     if (desc->isect_mode != ATRC_ISECT_FAST && desc->isect_mode != ATRC_ISECT_WATERTIGHT)
         return fail(ATRC_ERR_INVALID_ARG,
                     "atrc_cuda_render: isect_mode must be ATRC_ISECT_FAST (0) or ATRC_ISECT_WATERTIGHT (2)");
+    // the reference's pt runs trace_nomis for use_mis = 0 (pt.cpp:8-42), an
+    // estimator whose image differs from trace_std's; it is not built here
+    if (desc->renderer == ATRC_RENDERER_PT && !desc->use_mis)
+        return fail(ATRC_ERR_UNSUPPORTED, "atrc_cuda_render: use_mis = 0 (trace_nomis) is not supported by pt_cuda");
     return ATRC_OK;
 }
 
@@ -2605,6 +2609,9 @@ int atrc_cuda_render_noalloc(AtrcScene* scene, const AtrcRenderDesc* desc, const
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: ao_sample_count must be in [1, 4096]");
     if (desc->isect_mode != ATRC_ISECT_FAST && desc->isect_mode != ATRC_ISECT_WATERTIGHT)
         return fail(ATRC_ERR_INVALID_ARG, "atrc_cuda_render_noalloc: isect_mode must be 0 or 2");
+    if (desc->renderer == ATRC_RENDERER_PT && !desc->use_mis)
+        return fail(ATRC_ERR_UNSUPPORTED,
+                    "atrc_cuda_render_noalloc: use_mis = 0 (trace_nomis) is not supported by pt_cuda");
     return guarded([&] {
         DeviceSceneImpl& d = scene->impl;
         CK(cudaSetDevice(d.device));

@@ -267,10 +267,11 @@ typedef struct AtrcRenderDesc {
     int32_t  min_depth, max_depth;   /* pt keys (renderer_creators.cpp:127-146) */
     float    cont_prob;
     int32_t  specular_depth;
-    int32_t  use_mis;                /* read from the pt key; the device
-                                        always renders trace_std (MIS): 0,
-                                        the reference's trace_nomis, is not
-                                        built                                */
+    int32_t  use_mis;                /* 1: trace_std (MIS).  0 selects the
+                                        reference's trace_nomis, which is not
+                                        built: renders of a pt entry with
+                                        use_mis = 0 return
+                                        ATRC_ERR_UNSUPPORTED                 */
     int32_t  filter_type;            /* AtrcFilterType                       */
     float    filter_radius;          /* user radius (box: 0.5 by default)    */
     float    filter_alpha;           /* gaussian                             */

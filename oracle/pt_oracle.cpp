@@ -2526,6 +2526,76 @@ Pixel trace_std(const OracleScene& sc, const AtrcRenderDesc& p, Ray r, Sampler& 
     return px;
 }
 
+// render::trace_nomis (path_tracing.cpp:227-381), the pt renderer's path
+// with use_mis = 0: BSDF sampling only, the emission of every light hit and
+// the environment on every miss added unweighted, no light sampling.
+Pixel trace_nomis(const OracleScene& sc, const AtrcRenderDesc& p, Ray r, Sampler& s) {
+    V3 coef(1);
+    Pixel px;
+    int scattering_count = 0;
+    for (int depth = 1, s_depth = 1; depth <= p.max_depth; ++depth) {
+        if (depth > p.min_depth) {
+            if (s.u() > p.cont_prob) return px;
+            coef /= p.cont_prob;
+        }
+        EntInct in;
+        if (!sc.closest(r, &in)) {
+            if (sc.env.type != ATRC_ENV_NONE) px.value += coef * sc.env.radiance(r.d);
+            return px;
+        }
+        V3 shading_normal;
+        BSDF b = sc.shade(in, &shading_normal);
+        if (depth == 1) {
+            px.normal = shading_normal;
+            px.albedo = b.albedo();
+            if (in.ent->no_denoise) px.denoise = 0;
+        }
+        const Medium& medium = sc.media[in.wr_medium()];
+        if (scattering_count < medium.max_scat) {
+            V3 tp, spos, swr;
+            Phase ph;
+            bool scattered = medium.sample_scattering(r.o, in.pos, s, scattering_count > 0, &tp, &spos, &swr, &ph);
+            coef *= tp;
+            if (scattered) {
+                ++scattering_count;
+                float sam[3] = {s.u(), s.u(), s.u()};
+                BSDFSample bs = ph.sample(in.wr, sam);
+                if (bs.f.black() || !(bs.pdf > 0)) return px;
+                coef *= bs.f / bs.pdf;
+                r = Ray(spos, normalize(bs.dir));
+                continue;
+            }
+        } else {
+            coef *= medium.ab(r.o, in.pos, s);
+        }
+        scattering_count = 0;
+        if (in.ent->is_light) px.value += coef * in.ent->light_radiance(in.geo.z, in.wr);
+        float sam[3] = {s.u(), s.u(), s.u()};
+        BSDFSample bs = b.sample(in.wr, sam);
+        if (bs.f.black() || !(bs.pdf > 0)) return px;
+        bool delta = bs.delta;
+        coef *= bs.f * std::abs(cosv(in.geo.z, bs.dir)) / bs.pdf;
+        r = Ray(in.eps_offset(bs.dir), normalize(bs.dir));
+        const AtrcMaterialDesc& mat = sc.materials[in.ent->material];
+        if (mat.type == ATRC_MAT_DISNEY && mat.bssrdf[1] >= 0 && !in.geo.in_positive_z_hemisphere(bs.dir) &&
+            in.geo.in_positive_z_hemisphere(in.wr)) {
+            EntInct x;
+            BSDF bx;
+            V3 w;
+            if (!subsurface_sample(sc, mat, in, s, &x, &bx, &w)) return px;
+            coef *= w;
+            float sam2[3] = {s.u(), s.u(), s.u()};
+            BSDFSample bs2 = bx.sample(x.wr, sam2);
+            if (bs2.f.black() || !(bs2.pdf > 0)) return px;
+            coef *= bs2.f * std::abs(cosv(x.geo.z, bs2.dir)) / bs2.pdf;
+            r = Ray(x.eps_offset(bs2.dir), normalize(bs2.dir));
+            delta = bs2.delta;
+        }
+        if (delta && depth >= 2 && s_depth <= p.specular_depth) { --depth; ++s_depth; }
+    }
+    return px;
+}
+
 // render::trace_ao (path_tracing.cpp:383-415)
 Pixel trace_ao(const OracleScene& sc, const AtrcRenderDesc& p, Ray r, Sampler& s) {
     Pixel px;
@@ -2846,7 +2916,8 @@ int oracle_render_sample(OracleScene* s, const AtrcRenderDesc* d, AtrcFilm* film
                     V3 ld = focal - lens;
                     V3 dir = normalize(fx * ld.x + fy * ld.y + fz * ld.z);
                     Pixel pv = d->renderer == ATRC_RENDERER_AO ? trace_ao(*s, *d, Ray(o, dir), smp)
-                                                               : trace_std(*s, *d, Ray(o, dir), smp);
+                               : d->use_mis                     ? trace_std(*s, *d, Ray(o, dir), smp)
+                                                                : trace_nomis(*s, *d, Ray(o, dir), smp);
                     if (!finite3(pv.value)) continue;
                     // apply_image_filter (framebuffer.h:49-80)
                     const int xmin = std::max(x0, int(std::ceil(pixel_x - filter.radius - 0.5f)));

@@ -240,3 +240,23 @@ def test_gaussian_filter_matches_reference(tmp_path):
     z = np.abs(mr - mo) / np.sqrt(vr / nr + vo / no + 1e-12)
     assert np.mean(z > 4) < 0.01, np.mean(z > 4)
     assert global_mean_z(fr, fo) < 4.0
+
+
+@pytest.mark.parametrize("name,spp", [("cornell", 256), ("feature", 256), ("subsurface", 256), ("media", 1024)])
+def test_nomis_images_match_reference(tmp_path, name, spp):
+    # use_mis = 0: the reference's trace_nomis (path_tracing.cpp:227-381),
+    # BSDF sampling only, against the oracle's restatement of it
+    import json
+    from pathlib import Path
+    p = Path(_scene(tmp_path, name, spp=spp))
+    cfgd = json.loads(p.read_text())
+    for entry in cfgd["rendering"] if isinstance(cfgd["rendering"], list) else [cfgd["rendering"]]:
+        entry["renderer"]["use_mis"] = 0
+    q = p.with_name(p.stem + "_nomis.json")
+    q.write_text(json.dumps(cfgd))
+    desc, fr, fo = _render_both(str(q))
+    assert desc.use_mis == 0
+    r = 0.5 - desc.eps
+    frac, allowed, info = band_test(fr, fo, 1 / (4 * r * r), cluster=3)
+    assert frac <= allowed, (frac, allowed, info)
+    assert global_mean_z(fr, fo) < 4.0
