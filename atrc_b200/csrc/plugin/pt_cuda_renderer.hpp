@@ -170,6 +170,12 @@ public:
         AtrcRenderDesc desc{};
         char type[32] = {};
         check(atrc_config_rendering(cfg, 0, &desc, type, sizeof(type)));
+        // use_mis = 0 selects trace_nomis in the reference's pt (pt.cpp:21-24),
+        // which pt_cuda does not implement: refuse before building anything
+        if (desc.renderer == ATRC_RENDERER_PT && !desc.use_mis)
+            throw factory::CreatingObjectException(
+                "pt_cuda: use_mis = 0 selects the reference's trace_nomis, which pt_cuda does not implement; "
+                "render this entry with pt");
         if (!scene_) {
             const AtrcSceneDesc* sd = nullptr;
             check(atrc_config_scene(cfg, &sd));

@@ -189,6 +189,18 @@ int main(int argc, char** argv) {
                               double(d.camera.lens_radius), double(d.camera.focal_distance), double(d.camera.pos[0]),
                               double(d.camera.pos[1]), double(d.camera.pos[2]));
                 out += buf;
+            } else if (mode == "refuse") {
+                // render each entry; report what it threw, if anything
+                CountingReporter rep(renderer.get());
+                std::string err;
+                try {
+                    renderer->render(applier, scene, rep);
+                } catch (const std::exception& ex) {
+                    err = ex.what();
+                }
+                for (char& ch : err)
+                    if (ch == '"' || ch == '\\' || ch == '\n') ch = ' ';
+                out += "{\"entry\": " + std::to_string(i) + ", \"error\": \"" + err + "\"}\n";
             } else if (mode == "async" && i == 0) {
                 // 1. run to the end: doing_rendering_ is raised throughout
                 CountingReporter full(renderer.get());

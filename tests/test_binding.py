@@ -116,6 +116,21 @@ def test_binding_compose_matches_whole_config(tmp_path):
     assert got[0]["spp"] != got[1]["spp"] and got[0]["filter_type"] != got[1]["filter_type"]
 
 
+def test_binding_refuses_use_mis_zero(tmp_path):
+    # the second entry asks for use_mis = 0 (the reference's trace_nomis):
+    # render() throws before building a device scene, with a message that
+    # names the key; the first entry does not fail for that reason
+    exe = _build(tmp_path)
+    scene = _two_entry_scene(tmp_path)
+    plan = _write_plan(tmp_path, scene)
+    r = subprocess.run([str(exe), "refuse", str(plan)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    got = [json.loads(line) for line in r.stdout.splitlines()]
+    assert [g["entry"] for g in got] == [0, 1]
+    assert "use_mis = 0" in got[1]["error"] and "trace_nomis" in got[1]["error"]
+    assert "use_mis" not in got[0]["error"]
+
+
 @pytest.mark.gpu
 def test_binding_async_cancel_uses_stop_rendering_only(tmp_path):
     from atrc_b200.scenes import cornell_box
